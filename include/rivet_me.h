@@ -1,0 +1,317 @@
+/*
+ * rivet_me.h — C ABI of the B200 motion-estimation library (librivet_me.so).
+ *
+ * The library replaces the motion-search stage of the rivet-h26x encoders:
+ *   H.264  Search::int_search / Search::refine        src/encode/h264_hpel.rs:789-1021
+ *          (driven per macroblock by p_mb)            src/encode/h264_analyse.rs:1884-1975
+ *   HEVC   InterPicture::search_full / refine_subpel  src/encode/h265_me.rs:3749-3922
+ *          (driven per prediction unit by pick_pu)    src/encode/h265_me.rs:1327-1380
+ * together with the per-reference plane builds they read
+ *   H.264  build_hpel / hpel_planes                   src/encode/h264_hpel.rs:95-189
+ *   HEVC   HalfPlanes::new                            src/encode/h265_search.rs:79-170
+ * and the DSP kernels underneath (dsp/distortion.rs sad/satd, dsp/hevc.rs
+ * qpel_h/v/v2, epel_h/v/v2, uni, dsp/h264.rs qpel/chroma).
+ *
+ * The reference calls one scalar/SIMD kernel per candidate through plain
+ * function pointers (DistortionDsp, HevcDsp, H264EncDsp). A GPU launch per
+ * candidate would cost more than the candidate, so this boundary is
+ * batched: a caller uploads pictures once, then submits whole frames (or
+ * lists of prediction-unit jobs), and reads back one result per job.
+ *
+ * Conventions
+ *  - Every function returns 0 on success or a negative RME_E* code; the
+ *    text of the last error of a context is rme_last_error(). No function
+ *    aborts or throws across the ABI.
+ *  - Motion vectors are quarter-sample int16 pairs, as rivet's Mv.
+ *  - Pictures are passed unpadded, row-major, `stride` samples per row;
+ *    8-bit pictures are uint8_t, deeper ones uint16_t (Sample = u8 | u16,
+ *    src/sample.rs:7-56). The library pads them on the device by edge
+ *    replication, which is what the reference's padded planes hold
+ *    (hevc/frame.rs:317-340 extend_rows, h264/frame.rs extend_edges).
+ *  - A context is bound to one CUDA device; calls on one context must not
+ *    overlap from several host threads. Separate contexts are independent.
+ *  - `stream` arguments are cudaStream_t passed as void* (0 = the legacy
+ *    default stream), so this header needs no CUDA include.
+ */
+#ifndef RIVET_ME_H
+#define RIVET_ME_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- error codes ------------------------------------------------------- */
+#define RME_OK             0
+#define RME_EINVAL        -1   /* bad argument (size, depth, id, pointer)   */
+#define RME_ENOMEM        -2   /* device or host allocation failed           */
+#define RME_ECUDA         -3   /* a CUDA call failed (text in last_error)    */
+#define RME_ENOTFOUND     -4   /* picture id not uploaded                    */
+#define RME_EDEVICE       -5   /* device status word set: a bounded wait ran
+                                  out or a bounds check fired in a kernel    */
+#define RME_EBUSY         -6   /* admission refused (budget / queue full)    */
+#define RME_ENOSYS        -7   /* not built for this configuration          */
+
+/* ---- enums -------------------------------------------------------------- */
+#define RME_CODEC_H264     0
+#define RME_CODEC_HEVC     1
+
+/* How prediction-unit seeds and predictors are supplied.
+ * GIVEN:      the caller passes one rme_job per (block, reference) with its
+ *             predictor(s) and candidate seeds — one encoder call exactly.
+ * STANDALONE: the library derives them from the frame's own results in a
+ *             fixed order (a wavefront), the rule restated in DESIGN.md
+ *             and in the oracle; used for whole-frame throughput runs.   */
+#define RME_PRED_GIVEN       0
+#define RME_PRED_STANDALONE  1
+
+/* H.264 GIVEN-mode job flags */
+#define RME_JOB_SCORE_ONLY   1  /* refine with MeCfg::SCORE (score the whole-
+                                   sample winner, no sub-sample rounds):
+                                   p_mb's refine_ratio branch             */
+
+#define RME_MAX_SEEDS        10 /* 3 + MAX_MERGE_CAND + 1 (h265_me.rs:1327) */
+#define RME_MAX_REFS         4
+
+typedef struct { int16_t x, y; } rme_mv;
+
+/* A picture as the caller holds it. */
+typedef struct {
+  int32_t codec;      /* RME_CODEC_*                                        */
+  int32_t bit_depth;  /* 8 (uint8_t samples) or 9..12 (uint16_t samples)   */
+  int32_t width;      /* luma width and height in samples                  */
+  int32_t height;
+  int32_t stride;     /* luma row stride of the host buffer, in samples     */
+} rme_picture_desc;
+
+/* Search settings: the reference's MeCfg / AnalysisCfg (H.264) and the
+ * h265_me constants / Tune knobs (HEVC). rme_params_default() fills the
+ * reference's medium tier. */
+typedef struct {
+  int32_t codec;
+  int32_t qp;
+  int32_t predictor_mode;     /* RME_PRED_*                                 */
+  /* H.264: MeCfg (h264_hpel.rs:492-519) of AnalysisCfg::me              */
+  int32_t h264_range;
+  int32_t h264_hpel_iters;
+  int32_t h264_qpel_iters;
+  int32_t h264_umh;
+  int32_t h264_qpel_diamond;
+  int32_t h264_dia;
+  float   h264_refine_ratio;  /* AnalysisCfg::refine_ratio (0: always)      */
+  int32_t h264_vertical_range;/* MotionLimits::vertical_search, full samples */
+  int32_t h264_pad;           /* search plane border, h264/frame.rs LUMA_PAD */
+  /* HEVC: h265_me.rs SEARCH_RANGE, Tune::search_rings / quarter_cross,
+   * Tune::lambda (P pictures), hevc/frame.rs LUMA_PAD                    */
+  int32_t hevc_search_range;
+  int32_t hevc_search_rings;
+  int32_t hevc_quarter_cross;
+  float   hevc_lambda_scale;
+  int32_t hevc_pad;
+  int32_t hevc_pu_mask;       /* STANDALONE: bit k -> 2Nx2N PUs of 8<<k     */
+  int32_t hevc_amp;           /* STANDALONE: also the AMP shapes 2NxnU,
+                                 2NxnD, nLx2N, nRx2N of every size >= 16   */
+} rme_params;
+
+/* One search job (GIVEN mode): a block, the reference it searches, its
+ * predictor(s) and seeds, in the order the encoder assembles them.
+ *  HEVC : mvp = the two AMVP predictors of this reference; seeds as pick_pu
+ *         builds them (zero, mvp0, mvp1, merge vectors of this ref,
+ *         parent seed).
+ *  H.264: mvp[0] = the rate predictor (Search::pred); seeds = int_search's
+ *         candidate list (p_mb: skip_mv, zero, neighbour vectors...).   */
+typedef struct {
+  int32_t x, y;        /* block position in luma samples                   */
+  int32_t w, h;        /* block size                                        */
+  int32_t ref;         /* index into the frame's reference list             */
+  int32_t nseeds;      /* 0..RME_MAX_SEEDS                                  */
+  int32_t flags;       /* RME_JOB_*                                         */
+  rme_mv  mvp[2];
+  rme_mv  seeds[RME_MAX_SEEDS];
+} rme_job;
+
+/* One search result. */
+typedef struct {
+  rme_mv   mv;         /* chosen quarter-sample vector                      */
+  int32_t  ref;        /* its reference index                               */
+  uint32_t cost;       /* SATD + rate of mv (H.264 STANDALONE: + ref bits)  */
+  uint32_t satd;       /* SATD of mv, no rate                               */
+  rme_mv   int_mv;     /* whole-sample stage winner                         */
+  uint32_t int_cost;   /* its SAD + rate                                    */
+  uint32_t n_sad;      /* SAD candidates scored (the reference's count)     */
+  uint32_t n_satd;     /* SATD candidates scored                            */
+} rme_result;
+
+/* A frame of work: the source picture, its references (most recent first,
+ * the order of refs_l0), the settings, and — in GIVEN mode — the jobs.   */
+typedef struct {
+  int32_t src_id;
+  int32_t nref;
+  int32_t ref_ids[RME_MAX_REFS];
+  const rme_job* jobs;       /* GIVEN mode; host memory; NULL otherwise     */
+  int32_t njobs;
+} rme_frame;
+
+/* Device-resident performance counters of the last completed call. */
+typedef struct {
+  uint64_t tasks;            /* (block, reference) searches run             */
+  uint64_t sad_candidates;   /* sum of n_sad                                */
+  uint64_t satd_candidates;  /* sum of n_satd                               */
+  uint64_t sad_samples;      /* sum over SAD candidates of w*h              */
+  uint64_t satd_samples;     /* sum over SATD candidates of w*h             */
+  float    kernel_ms;        /* device time of the search launch(es)        */
+  float    planes_ms;        /* device time of the plane builds             */
+} rme_stats;
+
+/* ---- lifecycle ---------------------------------------------------------- */
+
+/* Medium-tier settings of `codec` at `qp`: MeCfg MEDIUM with refine_ratio
+ * 1.5 (h264_analyse.rs:193-240), SEARCH_RANGE 48, no rings, the square
+ * quarter ring, Tune::lambda 0.85 (h265_tune.rs:411), 2Nx2N PUs 8..64. */
+void rme_params_default(rme_params* p, int32_t codec, int32_t qp);
+
+int  rme_ctx_create(void** ctx, int32_t device);
+void rme_ctx_destroy(void* ctx);
+const char* rme_last_error(void* ctx);
+
+/* ---- pictures ------------------------------------------------------------ */
+
+/* Upload a luma picture under `pic_id` (any non-negative id; re-uploading an
+ * id replaces it). `as_ref` != 0 also builds its search planes on the
+ * device: the padded integer plane plus H.264's three half-sample planes
+ * (b, h, j) or HEVC's fifteen fractional phases — what build_hpel and
+ * HalfPlanes::new compute on the CPU. Asynchronous on `stream`; `luma` may
+ * be reused once the stream has passed the call. */
+int rme_picture_upload(void* ctx, int32_t pic_id, const rme_picture_desc* d,
+                       const void* luma, int32_t as_ref, void* stream);
+
+/* Upload the two chroma planes of a 4:2:0 picture (width/2 x height/2,
+ * `cstride` samples per row) for rme_chroma_predict. */
+int rme_picture_upload_chroma(void* ctx, int32_t pic_id, const void* cb,
+                              const void* cr, int32_t cstride, void* stream);
+
+int rme_picture_release(void* ctx, int32_t pic_id);
+
+/* Copy one search plane of an uploaded reference to the host: plane 0 is
+ * the padded integer plane, H.264 planes 1..3 are b, h, j (Hpel::plane
+ * 0..2), HEVC planes 1..15 the fractional phase fy*4+fx (HalfPlanes'
+ * planes[phase-1]). `rows` and `cols` receive the padded geometry
+ * (height + 2*pad, width + 2*pad; H.264 at the coded size); `out` (may be
+ * NULL) receives rows*cols samples. Synchronous. */
+int rme_picture_download_plane(void* ctx, int32_t pic_id, int32_t plane, void* out,
+                               int32_t* rows, int32_t* cols);
+
+/* Bytes of device memory held by the context's pictures. */
+int rme_memory_used(void* ctx, uint64_t* bytes);
+
+/* ---- search --------------------------------------------------------------- */
+
+/* Number of results rme_frame_search writes for `f` under `p`: njobs in
+ * GIVEN mode; in STANDALONE mode one per (block, reference) for HEVC in
+ * the order of rme_standalone_blocks, one per macroblock for H.264. */
+int rme_frame_result_count(void* ctx, const rme_frame* f, const rme_params* p,
+                           int32_t* count);
+
+/* The STANDALONE blocks of a frame, in result order (HEVC: size levels from
+ * the largest, raster order within a level; H.264: macroblock raster).
+ * `blocks` receives 4 int32 per block (x, y, w, h); pass NULL to get the
+ * count only. */
+int rme_standalone_blocks(const rme_picture_desc* d, const rme_params* p,
+                          int32_t* blocks, int32_t* count);
+
+/* Search one frame. Results go to `out` (host memory, count from
+ * rme_frame_result_count). Synchronous: returns when `out` is written. */
+int rme_frame_search(void* ctx, const rme_frame* f, const rme_params* p,
+                     rme_result* out, void* stream);
+
+/* Search many frames in one persistent launch: frames[i] with params[i];
+ * results of frame i at out + offsets[i] (offsets from prefix sums of
+ * rme_frame_result_count). The launch pulls (block, reference) tasks from
+ * one device work queue that interleaves all frames, and is replayed as a
+ * CUDA graph when the same batch shape comes again. */
+int rme_batch_search(void* ctx, const rme_frame* frames, const rme_params* params,
+                     int32_t nframes, rme_result* out, const int64_t* offsets,
+                     void* stream);
+
+/* The STANDALONE decision over a frame's HEVC results (host side, cheap):
+ * per block the reference with the least cost + lambda * ref_idx bits, and
+ * the quadtree of 2Nx2N sizes whose summed costs are least. `best` gets one
+ * int32 per block (chosen reference, -1 where no reference was searched);
+ * `part` gets, per 8x8 cell of the picture, log2 of the chosen PU size. */
+int rme_hevc_decide(const rme_picture_desc* d, const rme_params* p, int32_t nref,
+                    const rme_result* res, int32_t* best, uint8_t* part);
+
+/* Statistics of the last search call on this context. */
+int rme_last_stats(void* ctx, rme_stats* s);
+
+/* ---- chroma of chosen vectors -------------------------------------------- */
+
+/* Chroma prediction of chosen luma vectors (4:2:0): HEVC predict_block's
+ * chroma arm (hevc/inter.rs:555-660, 4-tap EPEL_FILTERS, eighth samples,
+ * uni rounding) or H.264 chroma_pred_into (h264_me.rs:812-837, bilinear).
+ * blocks: 4 int32 per block (luma x, y, w, h); mvs: one per block.
+ * out: per block (w/2)*(h/2) Cb samples then as many Cr, blocks packed in
+ * order, sample type of the picture. */
+int rme_chroma_predict(void* ctx, int32_t ref_id, int32_t nblocks,
+                       const int32_t* blocks, const rme_mv* mvs, void* out,
+                       void* stream);
+
+/* ---- DSP kernels, batched (dsp/distortion.rs SadFn / SatdFn) -------------- */
+
+/* Device-pointer batch of the reference's size-generic distortion kernels:
+ * for i < n, out[i] = sad|satd(a + a_off[i], a_stride, b + b_off[i],
+ * b_stride, w, h) over samples of `bit_depth` (uint8_t at 8, else uint16_t).
+ * All pointers are device pointers; asynchronous on `stream`. */
+int rme_sad_batch(const void* a, int64_t a_stride, const int64_t* a_off,
+                  const void* b, int64_t b_stride, const int64_t* b_off,
+                  int32_t w, int32_t h, int32_t bit_depth, int32_t n,
+                  uint32_t* out, void* stream);
+int rme_satd_batch(const void* a, int64_t a_stride, const int64_t* a_off,
+                   const void* b, int64_t b_stride, const int64_t* b_off,
+                   int32_t w, int32_t h, int32_t bit_depth, int32_t n,
+                   uint32_t* out, void* stream);
+
+/* ---- serving loop --------------------------------------------------------- */
+
+/* A continuous-batching request loop on one context (C++ host thread plus
+ * the persistent search kernel). Streams are admitted against an HBM
+ * budget; each stream keeps its reference pictures resident. Requests are
+ * per-frame ME calls; they are admitted into free slots of the next launch
+ * as they arrive, overlapping with work already on the device. */
+typedef struct {
+  uint64_t hbm_budget_bytes;  /* admission limit for resident pictures      */
+  int32_t  max_frames_per_launch;
+  int32_t  max_streams;
+} rme_serve_opts;
+
+typedef struct {
+  int64_t  request_id;
+  int32_t  stream_id;
+  int32_t  status;            /* 0 ok, else RME_E*                           */
+  double   submit_s;          /* host clock (s) at submit                    */
+  double   done_s;            /* host clock (s) when results were complete  */
+  int32_t  nresults;
+} rme_completion;
+
+int rme_serve_start(void* ctx, const rme_serve_opts* o, void** server);
+/* Admit a stream of one format and settings; refused with RME_EBUSY when
+ * its resident pictures would pass the budget. */
+int rme_serve_open_stream(void* server, int32_t stream_id, const rme_picture_desc* d,
+                          const rme_params* p, int32_t nref);
+/* Submit one frame of a stream: its luma (host memory, copied before
+ * return). The frame is searched against the stream's resident references
+ * and then becomes its newest reference. Results land in `out` (host
+ * memory the caller keeps until the completion is seen). */
+int rme_serve_submit(void* server, int32_t stream_id, const void* luma,
+                     rme_result* out, int64_t* request_id);
+/* Completed requests since the last call (non-blocking). */
+int rme_serve_poll(void* server, rme_completion* done, int32_t max, int32_t* n);
+int rme_serve_close_stream(void* server, int32_t stream_id);
+int rme_serve_stop(void* server);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RIVET_ME_H */

@@ -1,0 +1,726 @@
+// ORACLE — test infrastructure, not product code.
+//
+// Frame-level drivers of the oracle and its C entry points (orc_*), loaded
+// by tests/ and bench.py through ctypes. The search arithmetic lives in
+// me_oracle.hpp; this file restates how the encoders drive it
+// (h264_analyse.rs p_mb's search section, h265_me.rs pick_pu's seed
+// assembly) in the two modes of include/rivet_me.h:
+//   GIVEN       one search per caller job, exactly as the encoder calls it;
+//   STANDALONE  the frame's own results feed the predictors, in the
+//               wavefront rule below (the same rule the CUDA library runs).
+#include <atomic>
+#include <functional>
+#include <chrono>
+#include <cstdio>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+
+#include "me_oracle.hpp"
+
+using namespace orc;
+
+namespace {
+
+int level_sizes(const rme_params* p, int* sizes) {  // largest first
+  int n = 0;
+  for (int k = 3; k >= 0; --k)
+    if (p->hevc_pu_mask & (1 << k)) sizes[n++] = 8 << k;
+  return n;
+}
+
+// HEVC STANDALONE blocks: per size level (largest first), the 2Nx2N PUs
+// that lie wholly inside the picture, raster order.
+int hevc_blocks(int W, int H, const rme_params* p, int32_t* blocks) {
+  int sizes[4], nl = level_sizes(p, sizes), n = 0;
+  for (int l = 0; l < nl; ++l) {
+    int N = sizes[l];
+    for (int by = 0; by + N <= H; by += N)
+      for (int bx = 0; bx + N <= W; bx += N) {
+        if (blocks) {
+          blocks[4 * n] = bx;
+          blocks[4 * n + 1] = by;
+          blocks[4 * n + 2] = N;
+          blocks[4 * n + 3] = N;
+        }
+        ++n;
+      }
+  }
+  return n;
+}
+
+int h264_blocks(int W, int H, int32_t* blocks) {
+  int mbw = (W + 15) / 16, mbh = (H + 15) / 16, n = 0;
+  for (int my = 0; my < mbh; ++my)
+    for (int mx = 0; mx < mbw; ++mx) {
+      if (blocks) {
+        blocks[4 * n] = mx * 16;
+        blocks[4 * n + 1] = my * 16;
+        blocks[4 * n + 2] = 16;
+        blocks[4 * n + 3] = 16;
+      }
+      ++n;
+    }
+  return n;
+}
+
+// An H.264 picture is searched at its coded size (whole macroblocks,
+// h264_syntax.rs:349-358), the picture extended to it by edge replication.
+template <class S>
+std::vector<S> coded_h264(const S* src, int W, int H, ptrdiff_t ss, int CW, int CH) {
+  std::vector<S> out((size_t)CW * CH);
+  for (int y = 0; y < CH; ++y)
+    for (int x = 0; x < CW; ++x) out[(size_t)y * CW + x] = src[(ptrdiff_t)std::min(y, H - 1) * ss + std::min(x, W - 1)];
+  return out;
+}
+
+struct NbMotion {  // h264/mb.rs:913-929
+  bool avail = false;
+  int ref = -1;
+  Mv mv;
+};
+
+// median_mvp (h264/mb.rs:1170-1189).
+Mv median_mvp(NbMotion a, NbMotion b, NbMotion c, int ref) {
+  if (!b.avail && !c.avail && a.avail) {
+    b = a;
+    c = a;
+  }
+  bool ma = a.ref == ref, mb = b.ref == ref, mc = c.ref == ref;
+  if (ma && !mb && !mc) return a.mv;
+  if (!ma && mb && !mc) return b.mv;
+  if (!ma && !mb && mc) return c.mv;
+  auto med = [](int x, int y, int z) { return std::min(std::max(x, y), std::max(std::min(x, y), z)); };
+  return Mv(med(a.mv.x, b.mv.x, c.mv.x), med(a.mv.y, b.mv.y, c.mv.y));
+}
+
+uint32_t h264_ref_bits_cost(float lam1, int r, int nref) {  // h264_analyse.rs:1934-1942
+  float bits;
+  if (nref == 1) bits = 0.0f;
+  else if (nref == 2) bits = 1.0f;
+  else bits = (float)(2 * (32 - __builtin_clz((unsigned)(r + 1))) - 1);
+  return (uint32_t)(lam1 * bits);
+}
+
+MeCfg h264_cfg(const rme_params* p) {
+  MeCfg c;
+  c.range = p->h264_range;
+  c.hpel_iters = p->h264_hpel_iters;
+  c.qpel_iters = p->h264_qpel_iters;
+  c.umh = p->h264_umh != 0;
+  c.qpel_diamond = p->h264_qpel_diamond != 0;
+  c.dia = p->h264_dia != 0;
+  return c;
+}
+
+template <class S>
+struct H264Ref {
+  Plane<S> g;
+  Hpel<S> hp;
+  MeRef<S> me;
+};
+
+template <class S>
+void h264_prepare_ref(H264Ref<S>& r, const S* luma, int W, int H, ptrdiff_t ss, int pad, int bd) {
+  int CW = (W + 15) / 16 * 16, CH = (H + 15) / 16 * 16;
+  auto coded = coded_h264(luma, W, H, ss, CW, CH);
+  r.g = Plane<S>(CW, CH, pad);
+  r.g.load(coded.data(), CW);
+  r.hp.build(r.g, (1 << bd) - 1);
+  r.me = MeRef<S>(&r.g, &r.hp);
+}
+
+template <class S>
+void h264_frame(const Dist<S>& dist, const S* src_luma, int W, int H, ptrdiff_t ss, int nref,
+                H264Ref<S>* const* refs, const rme_params* p, const rme_job* jobs, int njobs, rme_result* out) {
+  int CW = (W + 15) / 16 * 16, CH = (H + 15) / 16 * 16;
+  auto src = coded_h264(src_luma, W, H, ss, CW, CH);
+  float lam1 = h264_lambda_satd(p->qp);
+  std::vector<uint16_t> tab(MV_TAB);
+  h264_cost_table(lam1, tab.data());
+  MeCfg me = h264_cfg(p);
+  int pad = p->h264_pad, vr = p->h264_vertical_range;
+  if (p->predictor_mode == RME_PRED_GIVEN) {
+    for (int j = 0; j < njobs; ++j) {
+      const rme_job& jb = jobs[j];
+      H264Search<S> s{&dist, &refs[jb.ref]->me, src.data() + (size_t)jb.y * CW + jb.x, CW, jb.x, jb.y, jb.w, jb.h,
+                      Mv(jb.mvp[0].x, jb.mvp[0].y), tab.data(), {0, 0, 0, 0}};
+      h264_search_bounds(CW, CH, pad, jb.x, jb.y, jb.w, jb.h, vr, s.bounds);
+      Mv cands[RME_MAX_SEEDS];
+      for (int k = 0; k < jb.nseeds; ++k) cands[k] = Mv(jb.seeds[k].x, jb.seeds[k].y);
+      uint32_t ci, sat, c;
+      Mv mi = s.int_search(cands, jb.nseeds, me, &ci);
+      Mv m = s.refine(mi, (jb.flags & RME_JOB_SCORE_ONLY) ? MeCfg::score() : me, &sat, &c);
+      rme_result& o = out[j];
+      o.mv = {m.x, m.y};
+      o.ref = jb.ref;
+      o.cost = c;
+      o.satd = sat;
+      o.int_mv = {mi.x, mi.y};
+      o.int_cost = ci;
+      o.n_sad = s.n_sad;
+      o.n_satd = s.n_satd;
+    }
+    return;
+  }
+  // STANDALONE: p_mb's search section (h264_analyse.rs:1884-1975) per
+  // macroblock in raster order, its predictors derived from the frame's own
+  // results: every coded macroblock is a 16x16 inter one at its best
+  // reference, so A, B, C (or D) are available exactly where they exist.
+  int mbw = CW / 16, mbh = CH / 16;
+  std::vector<uint32_t> rb(nref);
+  for (int r = 0; r < nref; ++r) rb[r] = h264_ref_bits_cost(lam1, r, nref);
+  for (int my = 0; my < mbh; ++my)
+    for (int mx = 0; mx < mbw; ++mx) {
+      auto nb = [&](int x, int y) {
+        NbMotion m;
+        if (x < 0 || y < 0 || x >= mbw) return m;
+        const rme_result& q = out[y * mbw + x];
+        m.avail = true;
+        m.ref = q.ref;
+        m.mv = Mv(q.mv.x, q.mv.y);
+        return m;
+      };
+      NbMotion A = nb(mx - 1, my), B = nb(mx, my - 1), C = nb(mx + 1, my - 1), D = nb(mx - 1, my - 1);
+      NbMotion Cc = C.avail ? C : D;  // prediction_neighbours: C, else D
+      auto pmv = [&](int r) { return median_mvp(A, B, Cc, r); };
+      // p_skip_mv (h264/mb.rs:1235-1246)
+      Mv skip;
+      if (!(!A.avail || !B.avail || (A.ref == 0 && A.mv == Mv()) || (B.ref == 0 && B.mv == Mv()))) skip = pmv(0);
+      // cands = [skip_mv, 0, neighbour vectors] (h264_pic.rs:713-751, p_mb 1889-1899)
+      Mv cands[8];
+      int nc = 0;
+      cands[nc++] = skip;
+      cands[nc++] = Mv();
+      Mv nbv[4];
+      int nn = 0;
+      for (const NbMotion* q : {&A, &B, &C}) {
+        if (!q->avail || q->ref < 0 || nn >= 4) continue;
+        bool dup = false;
+        for (int k = 0; k < nn; ++k) dup = dup || nbv[k] == q->mv;
+        if (!dup) nbv[nn++] = q->mv;
+      }
+      for (int k = 0; k < nn && nc < 8; ++k) cands[nc++] = nbv[k];
+      int x = mx * 16, y = my * 16;
+      Mv mv16;
+      uint32_t c16 = UINT32_MAX, s16 = 0, int16 = UINT32_MAX, ci16 = 0, nsad = 0, nsatd = 0;
+      Mv mi16;
+      int r16 = 0;
+      for (int r = 0; r < nref; ++r) {
+        Mv pr = pmv(r);
+        if (r > 0 && nc < 8) cands[nc] = pr;
+        int k = r > 0 ? std::min(nc + 1, 8) : nc;
+        H264Search<S> s{&dist, &refs[r]->me, src.data() + (size_t)y * CW + x, CW, x, y, 16, 16, pr,
+                        tab.data(), {0, 0, 0, 0}};
+        h264_search_bounds(CW, CH, pad, x, y, 16, 16, vr, s.bounds);
+        uint32_t ci, sat, c;
+        Mv mi = s.int_search(cands, k, me, &ci);
+        ci += rb[r];
+        bool gate = r > 0 && p->h264_refine_ratio > 0.0f && (float)ci >= p->h264_refine_ratio * (float)int16;
+        Mv m = s.refine(mi, gate ? MeCfg::score() : me, &sat, &c);
+        int16 = std::min(int16, ci);
+        c += rb[r];
+        nsad += s.n_sad;
+        nsatd += s.n_satd;
+        if (c < c16) {
+          mv16 = m;
+          c16 = c;
+          s16 = sat;
+          r16 = r;
+          mi16 = mi;
+          ci16 = ci;
+        }
+      }
+      rme_result& o = out[my * mbw + mx];
+      o.mv = {mv16.x, mv16.y};
+      o.ref = r16;
+      o.cost = c16;
+      o.satd = s16;
+      o.int_mv = {mi16.x, mi16.y};
+      o.int_cost = ci16;
+      o.n_sad = nsad;
+      o.n_satd = nsatd;
+    }
+}
+
+template <class S>
+struct HevcRef {
+  Plane<S> g;
+  HalfPlanes<S> hp;
+};
+
+template <class S>
+void hevc_prepare_ref(HevcRef<S>& r, const S* luma, int W, int H, ptrdiff_t ss, int pad, int bd) {
+  r.g = Plane<S>(W, H, pad);
+  r.g.load(luma, ss);
+  r.hp.build(r.g, bd);
+}
+
+template <class S>
+void hevc_one(const Dist<S>& dist, const HevcRef<S>& ref, int bd, const S* src, ptrdiff_t ss, int x, int y,
+              int w, int h, float lam, const rme_params* p, const Mv mvp[2], const Mv* seeds, int ns, int r,
+              rme_result& o) {
+  HevcSearch<S> s{&dist, &ref.g, &ref.hp, bd, src + (ptrdiff_t)y * ss + x, ss, x, y, w, h, lam, {{0, 0}, {0, 0}}};
+  s.pq[0][0] = mvp[0].x;
+  s.pq[0][1] = mvp[0].y;
+  s.pq[1][0] = mvp[1].x;
+  s.pq[1][1] = mvp[1].y;
+  s.search_range = p->hevc_search_range;
+  s.search_rings = p->hevc_search_rings;
+  s.quarter_cross = p->hevc_quarter_cross != 0;
+  uint32_t fc, sat, c;
+  Mv full = s.search_full(seeds, ns, &fc);
+  Mv m = s.refine_subpel(full, &sat, &c);
+  o.mv = {m.x, m.y};
+  o.ref = r;
+  o.cost = c;
+  o.satd = sat;
+  o.int_mv = {full.x, full.y};
+  o.int_cost = fc;
+  o.n_sad = s.n_sad;
+  o.n_satd = s.n_satd;
+}
+
+template <class S>
+void hevc_frame(const Dist<S>& dist, const S* src, int W, int H, ptrdiff_t ss, int bd, int nref,
+                HevcRef<S>* const* refs, const rme_params* p, const rme_job* jobs, int njobs, rme_result* out) {
+  float lam = hevc_lambda(p->qp, bd, p->hevc_lambda_scale);
+  if (p->predictor_mode == RME_PRED_GIVEN) {
+    for (int j = 0; j < njobs; ++j) {
+      const rme_job& jb = jobs[j];
+      Mv mvp[2] = {Mv(jb.mvp[0].x, jb.mvp[0].y), Mv(jb.mvp[1].x, jb.mvp[1].y)};
+      Mv seeds[RME_MAX_SEEDS];
+      for (int k = 0; k < jb.nseeds; ++k) seeds[k] = Mv(jb.seeds[k].x, jb.seeds[k].y);
+      hevc_one(dist, *refs[jb.ref], bd, src, ss, jb.x, jb.y, jb.w, jb.h, lam, p, mvp, seeds, jb.nseeds, jb.ref,
+               out[j]);
+    }
+    return;
+  }
+  // STANDALONE: per size level (largest first), raster order, every
+  // reference: seeds = [zero, mvp0, mvp1, parent] as pick_pu orders them
+  // (h265_me.rs:1327-1348), where the AMVP pair is the spatial part of
+  // 8.5.3.2.7 over this level's results (left A, above B; a duplicate B
+  // dropped; zero-filled) and the parent seed is the result of the
+  // enclosing PU one evaluated size up (parent_seed, h265_me.rs:3709).
+  int sizes[4], nl = level_sizes(p, sizes);
+  int base[5] = {0}, nbx[4], nby[4];
+  for (int l = 0; l < nl; ++l) {
+    nbx[l] = W / sizes[l];
+    nby[l] = H / sizes[l];
+    base[l + 1] = base[l] + nbx[l] * nby[l];
+  }
+  auto at = [&](int l, int bx, int by, int r) -> rme_result& {
+    return out[(size_t)(base[l] + by * nbx[l] + bx) * nref + r];
+  };
+  for (int l = 0; l < nl; ++l) {
+    int N = sizes[l];
+    for (int by = 0; by < nby[l]; ++by)
+      for (int bx = 0; bx < nbx[l]; ++bx)
+        for (int r = 0; r < nref; ++r) {
+          Mv cand[2];
+          int na = 0;
+          if (bx > 0) cand[na++] = Mv(at(l, bx - 1, by, r).mv.x, at(l, bx - 1, by, r).mv.y);
+          if (by > 0) {
+            Mv b(at(l, bx, by - 1, r).mv.x, at(l, bx, by - 1, r).mv.y);
+            if (na == 0 || cand[0] != b) cand[na++] = b;
+          }
+          Mv mvp[2] = {na > 0 ? cand[0] : Mv(), na > 1 ? cand[1] : Mv()};
+          Mv seeds[4] = {Mv(), mvp[0], mvp[1], Mv()};
+          int ns = 3;
+          if (l > 0) {
+            int Np = sizes[l - 1], px = bx * N / Np, py = by * N / Np;
+            if (px < nbx[l - 1] && py < nby[l - 1]) {
+              const rme_result& q = at(l - 1, px, py, r);
+              seeds[ns++] = Mv(q.mv.x, q.mv.y);
+            }
+          }
+          hevc_one(dist, *refs[r], bd, src, ss, bx * N, by * N, N, N, lam, p, mvp, seeds, ns, r, at(l, bx, by, r));
+        }
+  }
+}
+
+template <class S>
+Dist<S> pick_dist(int simd);
+bool have_avx2() { return __builtin_cpu_supports("avx2"); }
+template <>
+Dist<uint8_t> pick_dist<uint8_t>(int simd) { return simd && have_avx2() ? dist_avx2_u8() : dist_scalar<uint8_t>(); }
+template <>
+Dist<uint16_t> pick_dist<uint16_t>(int simd) {
+  return simd && have_avx2() ? dist_avx2_u16() : dist_scalar<uint16_t>();
+}
+
+bool valid_desc(const rme_picture_desc* d) {
+  return d && (d->codec == RME_CODEC_H264 || d->codec == RME_CODEC_HEVC) && d->bit_depth >= 8 &&
+         d->bit_depth <= 12 && d->width >= 16 && d->height >= 16 && d->stride >= d->width;
+}
+
+// Run frames[i] (src pointer + nref reference pointers); references that
+// appear in several frames (a sequence: frame t searches t-1 and t-2) are
+// prepared once, as the encoders cache them (hpel_for, retain_reference).
+template <class S>
+int run_frames(const rme_picture_desc* d, int nframes, const void* const* srcs, int nref, const void* const* refs,
+               const rme_params* p, int simd, int threads, rme_result* out, const int64_t* offsets,
+               double* seconds, double* plane_seconds) {
+  Dist<S> dist = pick_dist<S>(simd);
+  int W = d->width, H = d->height, bd = d->bit_depth;
+  ptrdiff_t ss = d->stride;
+  auto t0 = std::chrono::steady_clock::now();
+  std::vector<const void*> uniq;
+  std::unordered_map<const void*, int> index;
+  for (int i = 0; i < nframes * nref; ++i)
+    if (!index.count(refs[i])) {
+      index[refs[i]] = (int)uniq.size();
+      uniq.push_back(refs[i]);
+    }
+  bool h264 = d->codec == RME_CODEC_H264;
+  std::vector<H264Ref<S>> r264(h264 ? uniq.size() : 0);
+  std::vector<HevcRef<S>> r265(h264 ? 0 : uniq.size());
+  threads = std::max(1, threads);
+  auto parallel = [&](int n, auto&& fn) {
+    std::atomic<int> next{0};
+    std::vector<std::thread> pool;
+    for (int t = 0; t < std::min(threads, std::max(n, 1)); ++t)
+      pool.emplace_back([&] {
+        for (int i; (i = next.fetch_add(1)) < n;) fn(i);
+      });
+    for (auto& th : pool) th.join();
+  };
+  parallel((int)uniq.size(), [&](int i) {
+    if (h264) h264_prepare_ref(r264[i], (const S*)uniq[i], W, H, ss, p->h264_pad, bd);
+    else hevc_prepare_ref(r265[i], (const S*)uniq[i], W, H, ss, p->hevc_pad, bd);
+  });
+  auto t1 = std::chrono::steady_clock::now();
+  parallel(nframes, [&](int f) {
+    rme_result* o = out + (offsets ? offsets[f] : 0);
+    if (h264) {
+      std::vector<H264Ref<S>*> rr(nref);
+      for (int r = 0; r < nref; ++r) rr[r] = &r264[index[refs[f * nref + r]]];
+      h264_frame<S>(dist, (const S*)srcs[f], W, H, ss, nref, rr.data(), p, nullptr, 0, o);
+    } else {
+      std::vector<HevcRef<S>*> rr(nref);
+      for (int r = 0; r < nref; ++r) rr[r] = &r265[index[refs[f * nref + r]]];
+      hevc_frame<S>(dist, (const S*)srcs[f], W, H, ss, bd, nref, rr.data(), p, nullptr, 0, o);
+    }
+  });
+  auto t2 = std::chrono::steady_clock::now();
+  if (seconds) *seconds = std::chrono::duration<double>(t2 - t0).count();
+  if (plane_seconds) *plane_seconds = std::chrono::duration<double>(t1 - t0).count();
+  return 0;
+}
+
+template <class S>
+int given_frame(const rme_picture_desc* d, const void* src, int nref, const void* const* refs, const rme_params* p,
+                const rme_job* jobs, int njobs, int simd, rme_result* out) {
+  Dist<S> dist = pick_dist<S>(simd);
+  int W = d->width, H = d->height, bd = d->bit_depth;
+  for (int j = 0; j < njobs; ++j)
+    if (jobs[j].ref < 0 || jobs[j].ref >= nref || jobs[j].nseeds < 0 || jobs[j].nseeds > RME_MAX_SEEDS)
+      return RME_EINVAL;
+  if (d->codec == RME_CODEC_H264) {
+    std::vector<H264Ref<S>> rr(nref);
+    std::vector<H264Ref<S>*> rp(nref);
+    for (int r = 0; r < nref; ++r) {
+      h264_prepare_ref(rr[r], (const S*)refs[r], W, H, d->stride, p->h264_pad, bd);
+      rp[r] = &rr[r];
+    }
+    h264_frame<S>(dist, (const S*)src, W, H, d->stride, nref, rp.data(), p, jobs, njobs, out);
+  } else {
+    std::vector<HevcRef<S>> rr(nref);
+    std::vector<HevcRef<S>*> rp(nref);
+    for (int r = 0; r < nref; ++r) {
+      hevc_prepare_ref(rr[r], (const S*)refs[r], W, H, d->stride, p->hevc_pad, bd);
+      rp[r] = &rr[r];
+    }
+    hevc_frame<S>(dist, (const S*)src, W, H, d->stride, bd, nref, rp.data(), p, jobs, njobs, out);
+  }
+  return 0;
+}
+
+uint32_t hevc_ref_idx_bits(int r, int nref) {  // ref_idx_lX, truncated unary, cMax nref-1
+  if (nref <= 1) return 0;
+  return r < nref - 1 ? (uint32_t)(r + 1) : (uint32_t)r;
+}
+
+}  // namespace
+
+extern "C" {
+
+void orc_params_default(rme_params* p, int32_t codec, int32_t qp) {
+  std::memset(p, 0, sizeof(*p));
+  p->codec = codec;
+  p->qp = qp;
+  p->predictor_mode = RME_PRED_STANDALONE;
+  p->h264_range = 16;  // AnalysisCfg::MEDIUM.me (h264_analyse.rs:193-240)
+  p->h264_hpel_iters = 2;
+  p->h264_qpel_iters = 2;
+  p->h264_refine_ratio = 1.5f;
+  p->h264_vertical_range = 0x7ffffffe;  // MotionLimits::NONE.vertical_search
+  p->h264_pad = 32;                     // h264/frame.rs LUMA_PAD
+  p->hevc_search_range = 48;            // h265_me.rs SEARCH_RANGE
+  p->hevc_search_rings = 0;             // Tune medium
+  p->hevc_quarter_cross = 0;
+  p->hevc_lambda_scale = 0.85f;  // h265_tune.rs:411
+  p->hevc_pad = 80;              // hevc/frame.rs LUMA_PAD
+  p->hevc_pu_mask = 0xF;
+  p->hevc_amp = 0;
+}
+
+int orc_standalone_blocks(const rme_picture_desc* d, const rme_params* p, int32_t* blocks, int32_t* count) {
+  if (!valid_desc(d) || !p || !count) return RME_EINVAL;
+  *count = d->codec == RME_CODEC_H264 ? h264_blocks(d->width, d->height, blocks)
+                                      : hevc_blocks(d->width, d->height, p, blocks);
+  return 0;
+}
+
+int orc_frame_result_count(const rme_picture_desc* d, const rme_params* p, int32_t nref, int32_t njobs,
+                           int32_t* count) {
+  if (!valid_desc(d) || !p || !count) return RME_EINVAL;
+  if (p->predictor_mode == RME_PRED_GIVEN) *count = njobs;
+  else if (d->codec == RME_CODEC_H264) *count = h264_blocks(d->width, d->height, nullptr);
+  else *count = hevc_blocks(d->width, d->height, p, nullptr) * nref;
+  return 0;
+}
+
+// One frame: src and the nref references are unpadded pictures of `d`.
+int orc_frame_search(const rme_picture_desc* d, const void* src, int32_t nref, const void* const* refs,
+                     const rme_params* p, const rme_job* jobs, int32_t njobs, int32_t simd, rme_result* out) {
+  if (!valid_desc(d) || !p || !src || !out || nref < 1 || nref > RME_MAX_REFS) return RME_EINVAL;
+  if (p->predictor_mode == RME_PRED_GIVEN) {
+    if (!jobs && njobs > 0) return RME_EINVAL;
+    return d->bit_depth == 8 ? given_frame<uint8_t>(d, src, nref, refs, p, jobs, njobs, simd, out)
+                             : given_frame<uint16_t>(d, src, nref, refs, p, jobs, njobs, simd, out);
+  }
+  return d->bit_depth == 8
+             ? run_frames<uint8_t>(d, 1, &src, nref, refs, p, simd, 1, out, nullptr, nullptr, nullptr)
+             : run_frames<uint16_t>(d, 1, &src, nref, refs, p, simd, 1, out, nullptr, nullptr, nullptr);
+}
+
+// Many STANDALONE frames on `threads` host threads (the timed CPU
+// baseline): frame f reads srcs[f] and refs[f*nref .. f*nref+nref), writes
+// out + offsets[f]. `seconds` = wall time including the plane builds.
+int orc_frames_search_mt(const rme_picture_desc* d, int32_t nframes, const void* const* srcs, int32_t nref,
+                         const void* const* refs, const rme_params* p, int32_t simd, int32_t threads,
+                         rme_result* out, const int64_t* offsets, double* seconds, double* plane_seconds) {
+  if (!valid_desc(d) || !p || nframes < 0 || nref < 1 || nref > RME_MAX_REFS) return RME_EINVAL;
+  if (p->predictor_mode != RME_PRED_STANDALONE) return RME_EINVAL;
+  return d->bit_depth == 8 ? run_frames<uint8_t>(d, nframes, srcs, nref, refs, p, simd, threads, out, offsets,
+                                                 seconds, plane_seconds)
+                           : run_frames<uint16_t>(d, nframes, srcs, nref, refs, p, simd, threads, out, offsets,
+                                                  seconds, plane_seconds);
+}
+
+// The STANDALONE decision (chosen reference per block and the 2Nx2N
+// quadtree), the rule rme_hevc_decide documents.
+int orc_hevc_decide(const rme_picture_desc* d, const rme_params* p, int32_t nref, const rme_result* res,
+                    int32_t* best, uint8_t* part) {
+  if (!valid_desc(d) || !p || !res || nref < 1) return RME_EINVAL;
+  int W = d->width, H = d->height;
+  float lam = hevc_lambda(p->qp, d->bit_depth, p->hevc_lambda_scale);
+  int sizes[4], nl = level_sizes(p, sizes);
+  int base[5] = {0}, nbx[4], nby[4];
+  for (int l = 0; l < nl; ++l) {
+    nbx[l] = W / sizes[l];
+    nby[l] = H / sizes[l];
+    base[l + 1] = base[l] + nbx[l] * nby[l];
+  }
+  std::vector<uint64_t> cost(base[nl]);
+  for (int b = 0; b < base[nl]; ++b) {
+    int br = 0;
+    uint64_t bc = UINT64_MAX;
+    for (int r = 0; r < nref; ++r) {
+      uint64_t c = (uint64_t)res[(size_t)b * nref + r].cost + hevc_rate(lam, hevc_ref_idx_bits(r, nref));
+      if (c < bc) {
+        bc = c;
+        br = r;
+      }
+    }
+    cost[b] = bc;
+    if (best) best[b] = br;
+  }
+  if (!part) return 0;
+  int cw = W / 8, ch = H / 8;
+  std::memset(part, 0, (size_t)cw * ch);
+  // decide(l, x, y): least summed cost over the area of a level-l block at
+  // (x, y): its own PU (when it exists) against its children's decisions;
+  // a tie keeps the larger PU. Returns UINT64_MAX where nothing covers it.
+  auto log2i = [](int v) { return 31 - __builtin_clz((unsigned)v); };
+  std::function<uint64_t(int, int, int, bool)> decide = [&](int l, int x, int y, bool mark) -> uint64_t {
+    int N = sizes[l];
+    if (x >= W || y >= H) return 0;
+    bool exists = x + N <= W && y + N <= H;
+    uint64_t own = exists ? cost[base[l] + (y / N) * nbx[l] + x / N] : UINT64_MAX;
+    uint64_t split = UINT64_MAX;
+    if (l + 1 < nl) {
+      int M = sizes[l + 1];
+      split = 0;
+      for (int yy = y; yy < y + N; yy += M)
+        for (int xx = x; xx < x + N; xx += M) {
+          uint64_t c = decide(l + 1, xx, yy, false);
+          if (c == UINT64_MAX) {
+            split = UINT64_MAX;
+            yy = y + N;
+            break;
+          }
+          split += c;
+        }
+    }
+    bool take_split = split < own;
+    if (mark) {
+      if (take_split) {
+        int M = sizes[l + 1];
+        for (int yy = y; yy < y + N; yy += M)
+          for (int xx = x; xx < x + N; xx += M) decide(l + 1, xx, yy, true);
+      } else if (exists) {
+        for (int yy = y / 8; yy < (y + N) / 8 && yy < ch; ++yy)
+          for (int xx = x / 8; xx < (x + N) / 8 && xx < cw; ++xx) part[yy * cw + xx] = (uint8_t)log2i(N);
+      }
+    }
+    return take_split ? split : own;
+  };
+  int N0 = sizes[0];
+  for (int y = 0; y < H; y += N0)
+    for (int x = 0; x < W; x += N0) decide(0, x, y, true);
+  return 0;
+}
+
+// ---- kernels and planes, for the property tests ----------------------------
+
+uint32_t orc_sad(int32_t bd, const void* a, int64_t as, const void* b, int64_t bs, int32_t w, int32_t h,
+                 int32_t simd) {
+  if (bd == 8) return pick_dist<uint8_t>(simd).sad((const uint8_t*)a, as, (const uint8_t*)b, bs, w, h);
+  return pick_dist<uint16_t>(simd).sad((const uint16_t*)a, as, (const uint16_t*)b, bs, w, h);
+}
+uint32_t orc_satd(int32_t bd, const void* a, int64_t as, const void* b, int64_t bs, int32_t w, int32_t h,
+                  int32_t simd) {
+  if (bd == 8) return pick_dist<uint8_t>(simd).satd((const uint8_t*)a, as, (const uint8_t*)b, bs, w, h);
+  return pick_dist<uint16_t>(simd).satd((const uint16_t*)a, as, (const uint16_t*)b, bs, w, h);
+}
+
+float orc_h264_lambda(int32_t qp) { return h264_lambda_satd(qp); }
+float orc_hevc_lambda(int32_t qp, int32_t bd, float scale) { return hevc_lambda(qp, bd, scale); }
+void orc_h264_cost_table(float lambda, uint16_t* tab) { h264_cost_table(lambda, tab); }
+uint32_t orc_hevc_mv_bits(int32_t mvx, int32_t mvy, const int32_t* pq4) {
+  int pq[2][2] = {{pq4[0], pq4[1]}, {pq4[2], pq4[3]}};
+  return hevc_mv_bits(mvx, mvy, pq);
+}
+
+// H.264: the padded plane (pad `pad`, coded size) and its b, h, j planes,
+// 4 planes of (CW+2pad)*(CH+2pad) samples into out.
+int orc_h264_planes(const rme_picture_desc* d, const void* luma, int32_t pad, void* out) {
+  if (!valid_desc(d)) return RME_EINVAL;
+  auto run = [&](auto tag) {
+    using S = decltype(tag);
+    H264Ref<S> r;
+    h264_prepare_ref(r, (const S*)luma, d->width, d->height, d->stride, pad, d->bit_depth);
+    size_t n = r.g.data.size();
+    std::memcpy((S*)out, r.g.data.data(), n * sizeof(S));
+    for (int k = 0; k < 3; ++k) std::memcpy((S*)out + (k + 1) * n, r.hp.p[k].data(), n * sizeof(S));
+  };
+  if (d->bit_depth == 8) run(uint8_t{});
+  else run(uint16_t{});
+  return 0;
+}
+
+// HEVC: the padded plane and its fifteen fractional phases (16 planes;
+// phases HalfPlanes left unbuilt are zero), and HalfPlanes::ext.
+int orc_hevc_planes(const rme_picture_desc* d, const void* luma, int32_t pad, int32_t force_quarter, void* out,
+                    int32_t* ext) {
+  if (!valid_desc(d)) return RME_EINVAL;
+  auto run = [&](auto tag) {
+    using S = decltype(tag);
+    HevcRef<S> r;
+    r.g = Plane<S>(d->width, d->height, pad);
+    r.g.load((const S*)luma, d->stride);
+    r.hp.build(r.g, d->bit_depth, force_quarter != 0);
+    size_t n = r.g.data.size();
+    std::memcpy((S*)out, r.g.data.data(), n * sizeof(S));
+    for (int k = 0; k < 15; ++k) {
+      if (r.hp.planes[k].empty()) std::memset((S*)out + (k + 1) * n, 0, n * sizeof(S));
+      else std::memcpy((S*)out + (k + 1) * n, r.hp.planes[k].data(), n * sizeof(S));
+    }
+    if (ext) *ext = r.hp.ext;
+  };
+  if (d->bit_depth == 8) run(uint8_t{});
+  else run(uint16_t{});
+  return 0;
+}
+
+// The decoders' direct predictions, for plane-equality tests: H.264 qpel[]
+// (dsp/h264.rs:436-495) of a w x h block at integer (xi, yi) and fraction
+// (xf, yf); HEVC predict14 + uni (8.5.3.3.3.1). `luma` unpadded.
+int orc_h264_qpel_direct(const rme_picture_desc* d, const void* luma, int32_t pad, int32_t xi, int32_t yi,
+                         int32_t xf, int32_t yf, int32_t w, int32_t h, void* out) {
+  if (!valid_desc(d)) return RME_EINVAL;
+  auto run = [&](auto tag) {
+    using S = decltype(tag);
+    H264Ref<S> r;
+    h264_prepare_ref(r, (const S*)luma, d->width, d->height, d->stride, pad, d->bit_depth);
+    h264_qpel_direct<S>((S*)out, w, r.g.data.data() + r.g.offset(xi - 2, yi - 2), r.g.stride, w, h, xf, yf,
+                        (1 << d->bit_depth) - 1);
+  };
+  if (d->bit_depth == 8) run(uint8_t{});
+  else run(uint16_t{});
+  return 0;
+}
+
+int orc_hevc_predict(const rme_picture_desc* d, const void* luma, int32_t pad, int32_t x, int32_t y, int32_t mvx,
+                     int32_t mvy, int32_t w, int32_t h, void* out) {
+  if (!valid_desc(d)) return RME_EINVAL;
+  auto run = [&](auto tag) {
+    using S = decltype(tag);
+    Plane<S> g(d->width, d->height, pad);
+    g.load((const S*)luma, d->stride);
+    std::vector<int16_t> p14((size_t)w * h);
+    hevc_interp(g, x + (mvx >> 2), y + (mvy >> 2), mvx & 3, mvy & 3, w, h, true, d->bit_depth, p14.data());
+    hevc_uni((S*)out, w, p14.data(), w, h, 14 - d->bit_depth, (1 << d->bit_depth) - 1);
+  };
+  if (d->bit_depth == 8) run(uint8_t{});
+  else run(uint16_t{});
+  return 0;
+}
+
+// Chroma of chosen vectors (4:2:0). cb/cr unpadded (W/2 x H/2, cstride).
+// HEVC: predict_block's chroma arm (hevc/inter.rs:555-660), CHROMA_PAD 40.
+// H.264: chroma_pred_into (h264_me.rs:812-837) + chroma_scalar
+// (dsp/h264.rs:499-520), CHROMA_PAD 16 (the window clamped outside it).
+int orc_chroma_predict(const rme_picture_desc* d, const void* cb, const void* cr, int32_t cstride, int32_t nblocks,
+                       const int32_t* blocks, const rme_mv* mvs, void* out) {
+  if (!valid_desc(d)) return RME_EINVAL;
+  int cw0 = d->width / 2, ch0 = d->height / 2;
+  auto run = [&](auto tag) {
+    using S = decltype(tag);
+    int pad = d->codec == RME_CODEC_HEVC ? 40 : 16;
+    Plane<S> pl[2] = {Plane<S>(cw0, ch0, pad), Plane<S>(cw0, ch0, pad)};
+    pl[0].load((const S*)cb, cstride);
+    pl[1].load((const S*)cr, cstride);
+    S* o = (S*)out;
+    int bd = d->bit_depth, maxv = (1 << bd) - 1;
+    for (int i = 0; i < nblocks; ++i) {
+      int x = blocks[4 * i], y = blocks[4 * i + 1], w = blocks[4 * i + 2] / 2, h = blocks[4 * i + 3] / 2;
+      int mx = mvs[i].x, my = mvs[i].y;
+      for (int c = 0; c < 2; ++c) {
+        if (d->codec == RME_CODEC_HEVC) {
+          std::vector<int16_t> p14((size_t)w * h);
+          hevc_interp(pl[c], x / 2 + (mx >> 3), y / 2 + (my >> 3), mx & 7, my & 7, w, h, false, bd, p14.data());
+          hevc_uni(o, w, p14.data(), w, h, 14 - bd, maxv);
+        } else {
+          int xci = x / 2 + (mx >> 3), yci = y / 2 + (my >> 3), xf = mx & 7, yf = my & 7;
+          int A = (8 - xf) * (8 - yf), B = xf * (8 - yf), C = (8 - xf) * yf, D = xf * yf;
+          for (int yy = 0; yy < h; ++yy)
+            for (int xx = 0; xx < w; ++xx) {
+              int v = A * pl[c].at_clamped(xci + xx, yci + yy) + B * pl[c].at_clamped(xci + xx + 1, yci + yy) +
+                      C * pl[c].at_clamped(xci + xx, yci + yy + 1) + D * pl[c].at_clamped(xci + xx + 1, yci + yy + 1);
+              o[yy * w + xx] = (S)((v + 32) >> 6);
+            }
+        }
+        o += (size_t)w * h;
+      }
+    }
+    (void)maxv;
+  };
+  if (d->bit_depth == 8) run(uint8_t{});
+  else run(uint16_t{});
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,201 @@
+"""ORACLE — test infrastructure, not product code.
+
+ctypes wrapper of liboracle_me.so (the C++ restatement of the reference's
+motion search in this directory). Imported only by tests/, by
+__graft_entry__.smoke() as the checker, and by bench.py's CPU legs.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+import rivet_h26x_codecs_b200.capi as capi
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle_me.so"
+
+_PD, _PP, _PR, _PJ = (C.POINTER(capi.PictureDesc), C.POINTER(capi.Params), C.POINTER(capi.Result),
+                      C.POINTER(capi.Job))
+_SIGS = {
+    "orc_params_default": (None, [_PP, C.c_int32, C.c_int32]),
+    "orc_standalone_blocks": (C.c_int, [_PD, _PP, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "orc_frame_result_count": (C.c_int, [_PD, _PP, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
+    "orc_frame_search": (C.c_int, [_PD, C.c_void_p, C.c_int32, C.POINTER(C.c_void_p), _PP, _PJ, C.c_int32,
+                                   C.c_int32, _PR]),
+    "orc_frames_search_mt": (C.c_int, [_PD, C.c_int32, C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p),
+                                       _PP, C.c_int32, C.c_int32, _PR, C.POINTER(C.c_int64),
+                                       C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "orc_hevc_decide": (C.c_int, [_PD, _PP, C.c_int32, _PR, C.POINTER(C.c_int32), C.POINTER(C.c_uint8)]),
+    "orc_sad": (C.c_uint32, [C.c_int32, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int32, C.c_int32,
+                             C.c_int32]),
+    "orc_satd": (C.c_uint32, [C.c_int32, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int32, C.c_int32,
+                              C.c_int32]),
+    "orc_h264_lambda": (C.c_float, [C.c_int32]),
+    "orc_hevc_lambda": (C.c_float, [C.c_int32, C.c_int32, C.c_float]),
+    "orc_h264_cost_table": (None, [C.c_float, C.POINTER(C.c_uint16)]),
+    "orc_hevc_mv_bits": (C.c_uint32, [C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
+    "orc_h264_planes": (C.c_int, [_PD, C.c_void_p, C.c_int32, C.c_void_p]),
+    "orc_hevc_planes": (C.c_int, [_PD, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.POINTER(C.c_int32)]),
+    "orc_h264_qpel_direct": (C.c_int, [_PD, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                       C.c_int32, C.c_int32, C.c_void_p]),
+    "orc_hevc_predict": (C.c_int, [_PD, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                   C.c_int32, C.c_int32, C.c_void_p]),
+    "orc_chroma_predict": (C.c_int, [_PD, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_int32),
+                                     C.POINTER(capi.Mv), C.c_void_p]),
+}
+
+_lib = None
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        h = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(h, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = h
+    return _lib
+
+
+def desc(codec: int, pic: np.ndarray, bit_depth: int) -> capi.PictureDesc:
+    if pic.strides[1] != pic.itemsize:
+        raise ValueError("pictures must be row-major with unit sample stride")
+    h, w = pic.shape
+    return capi.PictureDesc(codec, bit_depth, w, h, pic.strides[0] // pic.itemsize)
+
+
+def params(codec: int, qp: int, **kw) -> capi.Params:
+    p = capi.Params()
+    lib().orc_params_default(C.byref(p), codec, qp)
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def result_count(d, p, nref: int, njobs: int = 0) -> int:
+    n = C.c_int32()
+    rc = lib().orc_frame_result_count(C.byref(d), C.byref(p), nref, njobs, C.byref(n))
+    assert rc == 0, rc
+    return n.value
+
+
+def standalone_blocks(d, p) -> np.ndarray:
+    n = C.c_int32()
+    assert lib().orc_standalone_blocks(C.byref(d), C.byref(p), None, C.byref(n)) == 0
+    out = np.zeros((n.value, 4), np.int32)
+    assert lib().orc_standalone_blocks(C.byref(d), C.byref(p), out.ctypes.data_as(C.POINTER(C.c_int32)),
+                                       C.byref(n)) == 0
+    return out
+
+
+def frame_search(codec: int, bit_depth: int, src: np.ndarray, refs, p, jobs: np.ndarray | None = None,
+                 simd: int = 0) -> np.ndarray:
+    src = np.ascontiguousarray(src)
+    d = desc(codec, src, bit_depth)
+    njobs = 0 if jobs is None else len(jobs)
+    n = result_count(d, p, len(refs), njobs)
+    out = np.zeros(n, capi.RESULT_DTYPE)
+    refs = [np.ascontiguousarray(r) for r in refs]
+    rp = (C.c_void_p * len(refs))(*[r.ctypes.data for r in refs])
+    jp = None if jobs is None else C.cast(jobs.ctypes.data, _PJ)
+    rc = lib().orc_frame_search(C.byref(d), src.ctypes.data, len(refs), rp, C.byref(p), jp, njobs, simd,
+                                C.cast(out.ctypes.data, _PR))
+    if rc != 0:
+        raise RuntimeError(f"oracle frame_search rc={rc}")
+    return out
+
+
+def frames_search_mt(codec: int, bit_depth: int, srcs, refs_per_frame, p, simd: int = 1, threads: int = 1):
+    """STANDALONE frames on host threads. Returns (results, seconds, plane_seconds)."""
+    d = desc(codec, srcs[0], bit_depth)
+    nref = len(refs_per_frame[0])
+    per = result_count(d, p, nref)
+    out = np.zeros(per * len(srcs), capi.RESULT_DTYPE)
+    sp = (C.c_void_p * len(srcs))(*[s.ctypes.data for s in srcs])
+    flat = [r for rr in refs_per_frame for r in rr]
+    rp = (C.c_void_p * len(flat))(*[r.ctypes.data for r in flat])
+    offs = np.arange(len(srcs), dtype=np.int64) * per
+    secs, psecs = C.c_double(), C.c_double()
+    rc = lib().orc_frames_search_mt(C.byref(d), len(srcs), sp, nref, rp, C.byref(p), simd, threads,
+                                    C.cast(out.ctypes.data, _PR), offs.ctypes.data_as(C.POINTER(C.c_int64)),
+                                    C.byref(secs), C.byref(psecs))
+    if rc != 0:
+        raise RuntimeError(f"oracle frames_search_mt rc={rc}")
+    return out, secs.value, psecs.value
+
+
+def hevc_decide(d, p, nref: int, res: np.ndarray):
+    nb = len(res) // nref
+    best = np.zeros(nb, np.int32)
+    part = np.zeros((d.height // 8, d.width // 8), np.uint8)
+    rc = lib().orc_hevc_decide(C.byref(d), C.byref(p), nref, C.cast(res.ctypes.data, _PR),
+                               best.ctypes.data_as(C.POINTER(C.c_int32)), part.ctypes.data_as(C.POINTER(C.c_uint8)))
+    assert rc == 0
+    return best, part
+
+
+def sad(bd, a, b, simd=0) -> int:
+    h, w = a.shape
+    return lib().orc_sad(bd, a.ctypes.data, a.strides[0] // a.itemsize, b.ctypes.data, b.strides[0] // b.itemsize,
+                         w, h, simd)
+
+
+def satd(bd, a, b, simd=0) -> int:
+    h, w = a.shape
+    return lib().orc_satd(bd, a.ctypes.data, a.strides[0] // a.itemsize, b.ctypes.data, b.strides[0] // b.itemsize,
+                          w, h, simd)
+
+
+def h264_planes(pic: np.ndarray, bit_depth: int, pad: int = 32) -> np.ndarray:
+    d = desc(capi.RME_CODEC_H264, pic, bit_depth)
+    cw, ch = -(-d.width // 16) * 16, -(-d.height // 16) * 16
+    out = np.zeros((4, ch + 2 * pad, cw + 2 * pad), pic.dtype)
+    assert lib().orc_h264_planes(C.byref(d), pic.ctypes.data, pad, out.ctypes.data) == 0
+    return out
+
+
+def hevc_planes(pic: np.ndarray, bit_depth: int, pad: int = 80, force_quarter: bool = False):
+    d = desc(capi.RME_CODEC_HEVC, pic, bit_depth)
+    out = np.zeros((16, d.height + 2 * pad, d.width + 2 * pad), pic.dtype)
+    ext = C.c_int32()
+    assert lib().orc_hevc_planes(C.byref(d), pic.ctypes.data, pad, int(force_quarter), out.ctypes.data,
+                                 C.byref(ext)) == 0
+    return out, ext.value
+
+
+def h264_qpel_direct(pic, bit_depth, xi, yi, xf, yf, w, h, pad=32):
+    d = desc(capi.RME_CODEC_H264, pic, bit_depth)
+    out = np.zeros((h, w), pic.dtype)
+    assert lib().orc_h264_qpel_direct(C.byref(d), pic.ctypes.data, pad, xi, yi, xf, yf, w, h, out.ctypes.data) == 0
+    return out
+
+
+def hevc_predict(pic, bit_depth, x, y, mvx, mvy, w, h, pad=80):
+    d = desc(capi.RME_CODEC_HEVC, pic, bit_depth)
+    out = np.zeros((h, w), pic.dtype)
+    assert lib().orc_hevc_predict(C.byref(d), pic.ctypes.data, pad, x, y, mvx, mvy, w, h, out.ctypes.data) == 0
+    return out
+
+
+def chroma_predict(codec, bit_depth, luma_w, luma_h, cb, cr, blocks: np.ndarray, mvs: np.ndarray) -> np.ndarray:
+    d = capi.PictureDesc(codec, bit_depth, luma_w, luma_h, luma_w)
+    n = int(sum((b[2] // 2) * (b[3] // 2) * 2 for b in blocks))
+    out = np.zeros(n, cb.dtype)
+    blocks = np.ascontiguousarray(blocks, np.int32)
+    mvs = np.ascontiguousarray(mvs, np.int16)
+    rc = lib().orc_chroma_predict(C.byref(d), cb.ctypes.data, cr.ctypes.data, cb.strides[0] // cb.itemsize,
+                                  len(blocks), blocks.ctypes.data_as(C.POINTER(C.c_int32)),
+                                  C.cast(mvs.ctypes.data, C.POINTER(capi.Mv)), out.ctypes.data)
+    assert rc == 0
+    return out

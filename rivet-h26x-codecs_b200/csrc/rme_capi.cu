@@ -1,0 +1,856 @@
+// Host side of librivet_me.so: the C ABI of include/rivet_me.h.
+//
+// A context owns device pictures (padded planes built on upload), the cost
+// tables per (codec, QP, depth, multiplier), the task orders per frame
+// shape, and the launch buffers. A frame search (or a batch of frames) is:
+// frame descriptors + the work queue to the device, one persistent search
+// launch, results back. Host code here only prepares and moves data; every
+// candidate is scored on the device.
+//
+// The Lagrangian tables are computed in f32 exactly as the reference does
+// (this file is compiled with -ffp-contract=off): H.264 MvCostTable::new
+// (h264_hpel.rs:453-459) at lambda_satd (h264_analyse.rs:402-404); HEVC
+// (lam * bits as f32) as u32 (h265_me.rs:3776, 3890) at lambda * 2^(bd-8)
+// (h265_intra.rs:1141-2013).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "rme_internal.h"
+
+using namespace rme;
+
+namespace {
+
+// ---- Lagrangian tables -------------------------------------------------------
+float h264_mvd_bits(int d) {  // h264_hpel.rs:407-429
+  uint32_t a = (uint32_t)std::abs(d);
+  if (a == 0) return 1.0f;
+  float prefix = (float)std::min(a, 9u);
+  float bits = 1.0f + 0.85f * prefix;
+  if (a < 9) {
+    bits += 0.85f;
+  } else {
+    uint32_t v = a - 9, k = 3;
+    while (v >= (1u << k)) {
+      v -= 1u << k;
+      k += 1;
+    }
+    bits += (float)(k - 3 + 1 + k);
+  }
+  return bits + 1.0f;
+}
+float h264_lambda_satd(int qp) { return std::sqrt(0.85f * std::exp2((float)(qp - 12) / 3.0f)); }
+float hevc_lambda(int qp, int bd, float scale) {
+  float base = 0.85f * std::exp2((float)(qp - 12) / 3.0f) * scale;
+  return std::sqrt(base) * (float)(1u << (bd - 8));
+}
+uint32_t h264_ref_bits_cost(float lam1, int r, int nref) {  // h264_analyse.rs:1934-1942
+  float bits = nref == 1 ? 0.0f : nref == 2 ? 1.0f : (float)(2 * (32 - __builtin_clz((unsigned)(r + 1))) - 1);
+  return (uint32_t)(lam1 * bits);
+}
+uint32_t hevc_ref_idx_bits(int r, int nref) {
+  if (nref <= 1) return 0;
+  return r < nref - 1 ? (uint32_t)(r + 1) : (uint32_t)r;
+}
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  cudaError_t ensure(size_t want) {
+    if (want <= n) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    size_t grow = std::max(want, n * 3 / 2);
+    cudaError_t e = cudaMalloc(&p, grow * sizeof(T) + 64);
+    if (e == cudaSuccess) n = grow;
+    return e;
+  }
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+};
+template <class T>
+struct PinBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  cudaError_t ensure(size_t want) {
+    if (want <= n) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    n = 0;
+    size_t grow = std::max(want, n * 3 / 2);
+    cudaError_t e = cudaMallocHost(&p, grow * sizeof(T) + 64);
+    if (e == cudaSuccess) n = grow;
+    return e;
+  }
+  ~PinBuf() {
+    if (p) cudaFreeHost(p);
+  }
+};
+
+struct Picture {
+  rme_picture_desc d{};
+  int cw = 0, ch = 0, pad = 0, nplanes = 0;
+  void* buf = nullptr;
+  size_t bytes = 0;
+  DevPlanes planes{};
+  bool is_ref = false;
+  void* chroma = nullptr;  // cb then cr, unpadded (cw/2 x ch/2), packed
+  size_t chroma_bytes = 0;
+  ~Picture() {
+    if (buf) cudaFree(buf);
+    if (chroma) cudaFree(chroma);
+  }
+};
+
+struct Tables {
+  uint16_t* tab = nullptr;       // H.264
+  uint32_t* lam_bits = nullptr;  // HEVC
+  float lam = 0.0f;
+};
+
+struct Order {  // task order of one frame shape, and the keys it sorts by
+  std::vector<uint32_t> tasks;
+  std::vector<uint32_t> keys;
+};
+
+struct Graph {
+  cudaGraphExec_t exec = nullptr;
+  size_t nframes = 0, total = 0;
+};
+
+struct Ctx {
+  int device = 0, nsm = 0, bps = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp0 = nullptr, evp1 = nullptr;
+  std::map<int, std::unique_ptr<Picture>> pics;
+  std::map<std::tuple<int, int, int, uint32_t>, Tables> tables;
+  std::map<std::vector<int64_t>, Order> orders;
+  std::string err;
+  int32_t epoch = 0;
+  rme_stats last{};
+  // launch buffers
+  DevBuf<FrameDesc> d_frames;
+  DevBuf<uint32_t> d_queue;
+  DevBuf<rme_result> d_out;
+  DevBuf<int32_t> d_flags;
+  DevBuf<rme_job> d_jobs;
+  DevBuf<unsigned long long> d_misc;  // head, counters[5], status
+  DevBuf<uint8_t> d_stage;            // upload staging
+  PinBuf<FrameDesc> h_frames;
+  PinBuf<rme_result> h_out;
+  PinBuf<unsigned long long> h_misc;
+  std::vector<uint32_t> queue_key;  // identity of what d_queue holds
+  std::vector<int64_t> queue_sig;
+  std::map<std::vector<int64_t>, Graph> graphs;
+  float planes_ms_acc = 0.0f;
+  ~Ctx() {
+    for (auto& g : graphs)
+      if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
+    for (auto& t : tables) {
+      if (t.second.tab) cudaFree(t.second.tab);
+      if (t.second.lam_bits) cudaFree(t.second.lam_bits);
+    }
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (evp0) cudaEventDestroy(evp0);
+    if (evp1) cudaEventDestroy(evp1);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+int fail(Ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+int cuda_fail(Ctx* c, cudaError_t e, const char* what) {
+  return fail(c, RME_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define CK(call)                                         \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return cuda_fail(c, e_, #call); \
+  } while (0)
+
+bool valid_desc(const rme_picture_desc* d) {
+  return d && (d->codec == RME_CODEC_H264 || d->codec == RME_CODEC_HEVC) && d->bit_depth >= 8 &&
+         d->bit_depth <= 12 && d->width >= 16 && d->height >= 16 && d->stride >= d->width &&
+         d->width <= 8192 && d->height <= 4352;
+}
+
+int level_sizes(const rme_params* p, int* sizes) {
+  int n = 0;
+  for (int k = 3; k >= 0; --k)
+    if (p->hevc_pu_mask & (1 << k)) sizes[n++] = 8 << k;
+  return n;
+}
+
+int count_blocks(const rme_picture_desc* d, const rme_params* p, int32_t* blocks) {
+  int n = 0;
+  if (d->codec == RME_CODEC_H264) {
+    int mbw = (d->width + 15) / 16, mbh = (d->height + 15) / 16;
+    for (int my = 0; my < mbh; ++my)
+      for (int mx = 0; mx < mbw; ++mx, ++n)
+        if (blocks) {
+          blocks[4 * n] = mx * 16;
+          blocks[4 * n + 1] = my * 16;
+          blocks[4 * n + 2] = blocks[4 * n + 3] = 16;
+        }
+    return n;
+  }
+  int sizes[4], nl = level_sizes(p, sizes);
+  for (int l = 0; l < nl; ++l) {
+    int N = sizes[l];
+    for (int by = 0; by + N <= d->height; by += N)
+      for (int bx = 0; bx + N <= d->width; bx += N, ++n)
+        if (blocks) {
+          blocks[4 * n] = bx;
+          blocks[4 * n + 1] = by;
+          blocks[4 * n + 2] = blocks[4 * n + 3] = N;
+        }
+  }
+  return n;
+}
+
+int check_params(Ctx* c, const rme_params* p, const rme_picture_desc& d) {
+  if (!p) return fail(c, RME_EINVAL, "null params");
+  if (p->codec != d.codec) return fail(c, RME_EINVAL, "params codec differs from the picture's");
+  if (p->predictor_mode != RME_PRED_GIVEN && p->predictor_mode != RME_PRED_STANDALONE)
+    return fail(c, RME_EINVAL, "bad predictor_mode");
+  if (p->qp < -12 || p->qp > 63) return fail(c, RME_EINVAL, "qp out of range");
+  if (d.codec == RME_CODEC_H264) {
+    if (p->h264_pad < 8 || p->h264_pad > kH264Pad) return fail(c, RME_EINVAL, "h264_pad must be 8..32");
+    if (p->h264_range < 0 || p->h264_range > 512 || p->h264_hpel_iters < 0 || p->h264_qpel_iters < 0 ||
+        p->h264_hpel_iters > 64 || p->h264_qpel_iters > 64)
+      return fail(c, RME_EINVAL, "bad H.264 MeCfg");
+  } else {
+    if (p->hevc_pad < 8 || p->hevc_pad > kHevcPad) return fail(c, RME_EINVAL, "hevc_pad must be 8..80");
+    if (p->hevc_search_range < 0 || p->hevc_search_range > 1024 || p->hevc_search_rings < 0 ||
+        p->hevc_search_rings > 64)
+      return fail(c, RME_EINVAL, "bad HEVC search settings");
+    if (p->predictor_mode == RME_PRED_STANDALONE && ((p->hevc_pu_mask & 0xF) == 0 || (p->hevc_pu_mask & ~0xF)))
+      return fail(c, RME_EINVAL, "hevc_pu_mask must select sizes among 8..64");
+    if (p->hevc_amp) return fail(c, RME_ENOSYS, "AMP shapes in STANDALONE mode are not built");
+  }
+  return 0;
+}
+
+const Tables* get_tables(Ctx* c, const rme_params* p, int bd, int* rc) {
+  uint32_t scale_bits;
+  float scale = p->codec == RME_CODEC_HEVC ? p->hevc_lambda_scale : 1.0f;
+  std::memcpy(&scale_bits, &scale, 4);
+  auto key = std::make_tuple(p->codec, p->qp, p->codec == RME_CODEC_HEVC ? bd : 8, scale_bits);
+  auto it = c->tables.find(key);
+  if (it != c->tables.end()) return &it->second;
+  Tables t;
+  if (p->codec == RME_CODEC_H264) {
+    std::vector<uint16_t> tab(kMvTab);
+    float lam = h264_lambda_satd(p->qp);
+    for (int d = -kMvSpan; d <= kMvSpan; ++d) tab[d + kMvSpan] = (uint16_t)std::min(lam * h264_mvd_bits(d) + 0.5f, 65535.0f);
+    t.lam = lam;
+    cudaError_t e = cudaMalloc(&t.tab, kMvTab * sizeof(uint16_t));
+    if (e == cudaSuccess) e = cudaMemcpy(t.tab, tab.data(), kMvTab * sizeof(uint16_t), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      *rc = cuda_fail(c, e, "table upload");
+      return nullptr;
+    }
+  } else {
+    std::vector<uint32_t> lb(kLamBits);
+    float lam = hevc_lambda(p->qp, bd, scale);
+    for (int b = 0; b < kLamBits; ++b) lb[b] = (uint32_t)(lam * (float)b);
+    t.lam = lam;
+    cudaError_t e = cudaMalloc(&t.lam_bits, kLamBits * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemcpy(t.lam_bits, lb.data(), kLamBits * sizeof(uint32_t), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      *rc = cuda_fail(c, e, "table upload");
+      return nullptr;
+    }
+  }
+  return &(c->tables[key] = t);
+}
+
+// The STANDALONE task order of a frame shape: tasks sorted by a wavefront
+// key under which every task comes after the tasks it reads (HEVC: the
+// 8x8-unit anti-diagonal of the block's corner, larger blocks first at a
+// tie, so left, upper and enclosing blocks precede; H.264: mx + 2 my, so
+// A, B, C and D precede).
+const Order& get_order(Ctx* c, const rme_picture_desc& d, const rme_params* p, int nref) {
+  std::vector<int64_t> sig = {d.codec, d.width, d.height, nref, d.codec == RME_CODEC_HEVC ? p->hevc_pu_mask : 0};
+  auto it = c->orders.find(sig);
+  if (it != c->orders.end()) return it->second;
+  Order o;
+  std::vector<int32_t> blocks(4 * (size_t)count_blocks(&d, p, nullptr));
+  int nb = count_blocks(&d, p, blocks.data());
+  int per = d.codec == RME_CODEC_H264 ? 1 : nref;
+  std::vector<std::pair<uint32_t, uint32_t>> kt;
+  kt.reserve((size_t)nb * per);
+  for (int b = 0; b < nb; ++b) {
+    int x = blocks[4 * b], y = blocks[4 * b + 1];
+    uint32_t key = d.codec == RME_CODEC_H264 ? (uint32_t)(x / 16 + 2 * (y / 16)) : (uint32_t)(x / 8 + y / 8);
+    for (int r = 0; r < per; ++r) kt.push_back({key, (uint32_t)(b * per + r)});
+  }
+  std::stable_sort(kt.begin(), kt.end(), [](auto& a, auto& b) { return a.first < b.first; });
+  o.tasks.resize(kt.size());
+  o.keys.resize(kt.size());
+  for (size_t i = 0; i < kt.size(); ++i) {
+    o.tasks[i] = kt[i].second;
+    o.keys[i] = kt[i].first;
+  }
+  return c->orders[sig] = std::move(o);
+}
+
+int picture_of(Ctx* c, int id, Picture** out) {
+  auto it = c->pics.find(id);
+  if (it == c->pics.end()) return fail(c, RME_ENOTFOUND, "picture " + std::to_string(id) + " not uploaded");
+  *out = it->second.get();
+  return 0;
+}
+
+// Fill one FrameDesc. `slot_out`/`slot_flags` index the launch buffers.
+int make_frame(Ctx* c, const rme_frame* f, const rme_params* p, FrameDesc* fd, rme_result* dout, int32_t* dflags,
+               const rme_job* djobs, int* ntasks) {
+  Picture* src;
+  int rc = picture_of(c, f->src_id, &src);
+  if (rc) return rc;
+  if (f->nref < 1 || f->nref > RME_MAX_REFS) return fail(c, RME_EINVAL, "nref must be 1..4");
+  if ((rc = check_params(c, p, src->d))) return rc;
+  std::memset(fd, 0, sizeof(*fd));
+  fd->codec = src->d.codec;
+  fd->bd = src->d.bit_depth;
+  fd->mode = p->predictor_mode;
+  fd->nref = f->nref;
+  fd->width = src->cw;
+  fd->height = src->ch;
+  fd->src = src->planes;
+  for (int r = 0; r < f->nref; ++r) {
+    Picture* rp;
+    if ((rc = picture_of(c, f->ref_ids[r], &rp))) return rc;
+    if (!rp->is_ref) return fail(c, RME_EINVAL, "reference picture was uploaded without as_ref");
+    if (rp->d.codec != src->d.codec || rp->d.bit_depth != src->d.bit_depth || rp->d.width != src->d.width ||
+        rp->d.height != src->d.height)
+      return fail(c, RME_EINVAL, "reference format differs from the source's");
+    fd->ref[r] = rp->planes;
+  }
+  const Tables* t = get_tables(c, p, src->d.bit_depth, &rc);
+  if (!t) return rc;
+  if (fd->codec == RME_CODEC_HEVC) {
+    fd->pad = p->hevc_pad;
+    fd->search_range = p->hevc_search_range;
+    fd->search_rings = p->hevc_search_rings;
+    fd->quarter_cross = p->hevc_quarter_cross;
+    fd->lam_bits = t->lam_bits;
+    int sizes[4];
+    fd->nlevels = level_sizes(p, sizes);
+    for (int l = 0; l < fd->nlevels; ++l) {
+      fd->size[l] = sizes[l];
+      fd->nbx[l] = src->d.width / sizes[l];
+      fd->nby[l] = src->d.height / sizes[l];
+      fd->base[l + 1] = fd->base[l] + fd->nbx[l] * fd->nby[l];
+    }
+  } else {
+    fd->pad = p->h264_pad;
+    fd->tab = t->tab;
+    fd->range = p->h264_range;
+    fd->hpel_iters = p->h264_hpel_iters;
+    fd->qpel_iters = p->h264_qpel_iters;
+    fd->umh = p->h264_umh;
+    fd->qpel_diamond = p->h264_qpel_diamond;
+    fd->dia = p->h264_dia;
+    fd->vr = p->h264_vertical_range;
+    fd->refine_ratio = p->h264_refine_ratio;
+    for (int r = 0; r < f->nref; ++r) fd->ref_cost[r] = h264_ref_bits_cost(t->lam, r, f->nref);
+  }
+  if (p->predictor_mode == RME_PRED_GIVEN) {
+    if (f->njobs < 0 || (f->njobs > 0 && !f->jobs)) return fail(c, RME_EINVAL, "jobs missing");
+    for (int j = 0; j < f->njobs; ++j) {
+      const rme_job& jb = f->jobs[j];
+      if (jb.ref < 0 || jb.ref >= f->nref || jb.nseeds < 0 || jb.nseeds > RME_MAX_SEEDS || jb.w < 4 || jb.h < 4 ||
+          jb.w > 64 || jb.h > 64 || (jb.w & 3) || (jb.h & 3) || jb.x < 0 || jb.y < 0 || jb.x + jb.w > src->cw ||
+          jb.y + jb.h > src->ch)
+        return fail(c, RME_EINVAL, "job " + std::to_string(j) + " out of range");
+      if (fd->codec == RME_CODEC_H264 && jb.nseeds > 8)
+        return fail(c, RME_EINVAL, "H.264 jobs take at most 8 candidates (p_mb's cands)");
+    }
+    fd->jobs = djobs;
+    *ntasks = f->njobs;
+  } else {
+    int nb = count_blocks(&src->d, p, nullptr);
+    *ntasks = fd->codec == RME_CODEC_H264 ? nb : nb * f->nref;
+  }
+  fd->out = dout;
+  fd->flags = dflags;
+  fd->ntasks = *ntasks;
+  return 0;
+}
+
+// Launch frames[0..n) as one persistent search; results to host `out` at
+// offsets (count-prefix order).
+int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n, rme_result* out,
+               const int64_t* offsets, cudaStream_t s, bool use_graph) {
+  if (n < 1 || n > 255) return fail(c, RME_EINVAL, "1..255 frames per launch");
+  std::vector<int> ntask(n);
+  std::vector<int64_t> toff(n + 1, 0), jobs_off(n + 1, 0);
+  for (int i = 0; i < n; ++i) jobs_off[i + 1] = jobs_off[i] + (params[i].predictor_mode == RME_PRED_GIVEN ? frames[i].njobs : 0);
+  // Pass 1: sizes (make_frame with null device pointers validates too).
+  CK(c->h_frames.ensure(n));
+  for (int i = 0; i < n; ++i) {
+    int rc = make_frame(c, &frames[i], &params[i], &c->h_frames.p[i], nullptr, nullptr, nullptr, &ntask[i]);
+    if (rc) return rc;
+    toff[i + 1] = toff[i] + ntask[i];
+  }
+  const int64_t total = toff[n];
+  if (total >= (1 << 24) * (int64_t)1 && n > 1) return fail(c, RME_EINVAL, "too many tasks in one launch");
+  CK(c->d_frames.ensure(n));
+  CK(c->d_out.ensure(std::max<int64_t>(total, 1)));
+  CK(c->d_flags.ensure(std::max<int64_t>(total, 1)));
+  CK(c->d_queue.ensure(std::max<int64_t>(total, 1)));
+  CK(c->d_jobs.ensure(std::max<int64_t>(jobs_off[n], 1)));
+  CK(c->d_misc.ensure(8));
+  CK(c->h_out.ensure(std::max<int64_t>(total, 1)));
+  CK(c->h_misc.ensure(8));
+  if (c->epoch == 0) CK(cudaMemsetAsync(c->d_flags.p, 0, c->d_flags.n * sizeof(int32_t), s));
+  ++c->epoch;
+  if (c->epoch == INT32_MAX) {
+    c->epoch = 1;
+    CK(cudaMemsetAsync(c->d_flags.p, 0, c->d_flags.n * sizeof(int32_t), s));
+  }
+  // Pass 2: device pointers, queue.
+  std::vector<int64_t> sig;
+  sig.push_back(n);
+  for (int i = 0; i < n; ++i) {
+    FrameDesc& fd = c->h_frames.p[i];
+    fd.out = c->d_out.p + toff[i];
+    fd.flags = c->d_flags.p + toff[i];
+    fd.epoch = c->epoch;
+    if (params[i].predictor_mode == RME_PRED_GIVEN) {
+      fd.jobs = c->d_jobs.p + jobs_off[i];
+      if (frames[i].njobs > 0)
+        CK(cudaMemcpyAsync(c->d_jobs.p + jobs_off[i], frames[i].jobs, sizeof(rme_job) * frames[i].njobs,
+                           cudaMemcpyHostToDevice, s));
+      sig.push_back(-1);
+      sig.push_back(frames[i].njobs);
+    } else {
+      sig.push_back(fd.codec);
+      sig.push_back(fd.width);
+      sig.push_back(fd.height);
+      sig.push_back(fd.nref);
+      sig.push_back(params[i].hevc_pu_mask);
+    }
+  }
+  if (sig != c->queue_sig) {
+    // The merged queue: every frame's tasks in its own order, frames
+    // interleaved by their progress through that order (key / max key),
+    // so the launch advances all frames' wavefronts together.
+    std::vector<std::tuple<double, int, uint32_t>> all;
+    all.reserve(total);
+    for (int i = 0; i < n; ++i) {
+      if (params[i].predictor_mode == RME_PRED_GIVEN) {
+        for (int t = 0; t < ntask[i]; ++t) all.emplace_back((double)t / std::max(ntask[i], 1), i, (uint32_t)t);
+        continue;
+      }
+      Picture* src;
+      picture_of(c, frames[i].src_id, &src);
+      const Order& o = get_order(c, src->d, &params[i], frames[i].nref);
+      double mk = o.keys.empty() ? 1.0 : (double)o.keys.back() + 1.0;
+      for (size_t k = 0; k < o.tasks.size(); ++k) all.emplace_back((double)o.keys[k] / mk, i, o.tasks[k]);
+    }
+    if (n > 1) std::stable_sort(all.begin(), all.end(), [](auto& a, auto& b) {
+      return std::get<0>(a) < std::get<0>(b) || (std::get<0>(a) == std::get<0>(b) && std::get<1>(a) < std::get<1>(b));
+    });
+    std::vector<uint32_t> q(total);
+    for (int64_t k = 0; k < total; ++k) q[k] = ((uint32_t)std::get<1>(all[k]) << 24) | std::get<2>(all[k]);
+    CK(cudaMemcpyAsync(c->d_queue.p, q.data(), sizeof(uint32_t) * total, cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    c->queue_sig = sig;
+  }
+  LaunchDesc L;
+  L.frames = c->d_frames.p;
+  L.queue = c->d_queue.p;
+  L.total = total;
+  L.head = c->d_misc.p;
+  L.counters = c->d_misc.p + 1;
+  L.status = reinterpret_cast<uint32_t*>(c->d_misc.p + 6);
+  if (!c->bps) c->bps = std::max(1, search_blocks_per_sm(2));
+  int64_t want = (total + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)c->nsm * c->bps, want));
+  auto enqueue = [&]() -> cudaError_t {
+    cudaError_t e = cudaMemcpyAsync(c->d_frames.p, c->h_frames.p, sizeof(FrameDesc) * n, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->d_misc.p, 0, 8 * sizeof(unsigned long long), s);
+    if (e == cudaSuccess) e = cudaEventRecord(c->ev0, s);
+    if (e == cudaSuccess) e = launch_search(L, 2, grid, s);
+    if (e == cudaSuccess) e = cudaEventRecord(c->ev1, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(c->h_out.p, c->d_out.p, sizeof(rme_result) * total, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(c->h_misc.p, c->d_misc.p, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
+    return e;
+  };
+  bool has_given = false;
+  for (int i = 0; i < n; ++i) has_given |= params[i].predictor_mode == RME_PRED_GIVEN;
+  if (use_graph && !has_given) {
+    std::vector<int64_t> gsig = sig;
+    gsig.push_back(total);
+    gsig.push_back((int64_t)(uintptr_t)s);
+    Graph& g = c->graphs[gsig];
+    if (!g.exec) {
+      cudaGraph_t graph;
+      CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      cudaError_t e = enqueue();
+      cudaError_t e2 = cudaStreamEndCapture(s, &graph);
+      if (e != cudaSuccess) return cuda_fail(c, e, "graph capture");
+      if (e2 != cudaSuccess) return cuda_fail(c, e2, "graph capture end");
+      e = cudaGraphInstantiate(&g.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) {
+        g.exec = nullptr;
+        return cuda_fail(c, e, "graph instantiate");
+      }
+    }
+    CK(cudaGraphLaunch(g.exec, s));
+  } else {
+    CK(enqueue());
+  }
+  CK(cudaStreamSynchronize(s));
+  uint32_t status = (uint32_t)(c->h_misc.p[6] & 0xffffffffu);
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  c->last.tasks = c->h_misc.p[1];
+  c->last.sad_candidates = c->h_misc.p[2];
+  c->last.satd_candidates = c->h_misc.p[3];
+  c->last.sad_samples = c->h_misc.p[4];
+  c->last.satd_samples = c->h_misc.p[5];
+  c->last.kernel_ms = ms;
+  c->last.planes_ms = c->planes_ms_acc;
+  c->planes_ms_acc = 0.0f;
+  if (status) return fail(c, RME_EDEVICE, "device status " + std::to_string(status));
+  for (int i = 0; i < n; ++i) {
+    int64_t off = offsets ? offsets[i] : toff[i];
+    std::memcpy(out + off, c->h_out.p + toff[i], sizeof(rme_result) * ntask[i]);
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+void rme_params_default(rme_params* p, int32_t codec, int32_t qp) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->codec = codec;
+  p->qp = qp;
+  p->predictor_mode = RME_PRED_STANDALONE;
+  p->h264_range = 16;
+  p->h264_hpel_iters = 2;
+  p->h264_qpel_iters = 2;
+  p->h264_refine_ratio = 1.5f;
+  p->h264_vertical_range = 0x7ffffffe;
+  p->h264_pad = kH264Pad;
+  p->hevc_search_range = 48;
+  p->hevc_search_rings = 0;
+  p->hevc_quarter_cross = 0;
+  p->hevc_lambda_scale = 0.85f;
+  p->hevc_pad = kHevcPad;
+  p->hevc_pu_mask = 0xF;
+  p->hevc_amp = 0;
+}
+
+int rme_ctx_create(void** out, int32_t device) {
+  if (!out) return RME_EINVAL;
+  *out = nullptr;
+  auto c = std::make_unique<Ctx>();
+  c->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return RME_ECUDA;
+  int nsm = 0;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return RME_ECUDA;
+  c->nsm = nsm;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return RME_ECUDA;
+  if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+      cudaEventCreate(&c->evp0) != cudaSuccess || cudaEventCreate(&c->evp1) != cudaSuccess)
+    return RME_ECUDA;
+  *out = c.release();
+  return 0;
+}
+
+void rme_ctx_destroy(void* ctx) {
+  if (!ctx) return;
+  Ctx* c = (Ctx*)ctx;
+  cudaSetDevice(c->device);
+  cudaDeviceSynchronize();
+  delete c;
+}
+
+const char* rme_last_error(void* ctx) { return ctx ? ((Ctx*)ctx)->err.c_str() : "null context"; }
+
+int rme_picture_upload(void* ctx, int32_t pic_id, const rme_picture_desc* d, const void* luma, int32_t as_ref,
+                       void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return RME_EINVAL;
+  if (!valid_desc(d) || !luma || pic_id < 0) return fail(c, RME_EINVAL, "bad picture description");
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  CK(cudaSetDevice(c->device));
+  auto pic = std::make_unique<Picture>();
+  pic->d = *d;
+  bool h264 = d->codec == RME_CODEC_H264;
+  pic->cw = h264 ? (d->width + 15) / 16 * 16 : d->width;
+  pic->ch = h264 ? (d->height + 15) / 16 * 16 : d->height;
+  pic->pad = h264 ? kH264Pad : kHevcPad;
+  pic->is_ref = as_ref != 0;
+  pic->nplanes = as_ref ? (h264 ? 4 : 16) : 1;
+  int bps = d->bit_depth == 8 ? 1 : 2;
+  // Rows padded to 128 bytes; the visible origin 16-byte aligned
+  // (pad * bytes is a multiple of 16 for both pads).
+  int stride_bytes = ((pic->cw + 2 * pic->pad) * bps + 127) / 128 * 128;
+  int stride = stride_bytes / bps, rows = pic->ch + 2 * pic->pad;
+  pic->planes.stride = stride;
+  pic->planes.plane_elems = (int64_t)stride * rows;
+  pic->planes.origin = pic->pad * stride + pic->pad;
+  pic->bytes = (size_t)pic->planes.plane_elems * bps * pic->nplanes + 256;
+  CK(cudaMalloc(&pic->buf, pic->bytes));
+  pic->planes.base = pic->buf;
+  size_t src_bytes = (size_t)d->width * d->height * bps;
+  CK(c->d_stage.ensure(src_bytes));
+  CK(cudaMemcpy2DAsync(c->d_stage.p, (size_t)d->width * bps, luma, (size_t)d->stride * bps, (size_t)d->width * bps,
+                       d->height, cudaMemcpyHostToDevice, s));
+  CK(cudaEventRecord(c->evp0, s));
+  CK(launch_pad_plane(c->d_stage.p, d->bit_depth, d->width, d->height, d->width, pic->planes, pic->cw, pic->ch,
+                      pic->pad, s));
+  if (as_ref) {
+    if (h264) CK(launch_h264_hpel(pic->planes, d->bit_depth, pic->cw, pic->ch, pic->pad, s));
+    else CK(launch_hevc_phases(pic->planes, d->bit_depth, pic->cw, pic->ch, pic->pad, s));
+  }
+  CK(cudaEventRecord(c->evp1, s));
+  // The staging buffer is reused by the next upload: finish this one.
+  CK(cudaStreamSynchronize(s));
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, c->evp0, c->evp1);
+  c->planes_ms_acc += ms;
+  c->pics[pic_id] = std::move(pic);
+  return 0;
+}
+
+int rme_picture_upload_chroma(void* ctx, int32_t pic_id, const void* cb, const void* cr, int32_t cstride,
+                              void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return RME_EINVAL;
+  Picture* p;
+  int rc = picture_of(c, pic_id, &p);
+  if (rc) return rc;
+  if (!cb || !cr || cstride < p->d.width / 2) return fail(c, RME_EINVAL, "bad chroma planes");
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  int bps = p->d.bit_depth == 8 ? 1 : 2, w = p->d.width / 2, h = p->d.height / 2;
+  if (p->chroma) cudaFree(p->chroma);
+  p->chroma = nullptr;
+  p->chroma_bytes = (size_t)w * h * bps * 2;
+  CK(cudaMalloc(&p->chroma, p->chroma_bytes + 64));
+  CK(cudaMemcpy2DAsync(p->chroma, (size_t)w * bps, cb, (size_t)cstride * bps, (size_t)w * bps, h,
+                       cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpy2DAsync((uint8_t*)p->chroma + (size_t)w * h * bps, (size_t)w * bps, cr, (size_t)cstride * bps,
+                       (size_t)w * bps, h, cudaMemcpyHostToDevice, s));
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+int rme_picture_release(void* ctx, int32_t pic_id) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return RME_EINVAL;
+  auto it = c->pics.find(pic_id);
+  if (it == c->pics.end()) return fail(c, RME_ENOTFOUND, "picture not uploaded");
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  c->pics.erase(it);
+  return 0;
+}
+
+int rme_picture_download_plane(void* ctx, int32_t pic_id, int32_t plane, void* out, int32_t* rows, int32_t* cols) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return RME_EINVAL;
+  Picture* p;
+  int rc = picture_of(c, pic_id, &p);
+  if (rc) return rc;
+  if (plane < 0 || plane >= p->nplanes) return fail(c, RME_EINVAL, "plane index out of range");
+  int R = p->ch + 2 * p->pad, C = p->cw + 2 * p->pad, bps = p->d.bit_depth == 8 ? 1 : 2;
+  if (rows) *rows = R;
+  if (cols) *cols = C;
+  if (!out) return 0;
+  const uint8_t* src = (const uint8_t*)p->buf + (size_t)plane * p->planes.plane_elems * bps;
+  CK(cudaMemcpy2D(out, (size_t)C * bps, src, (size_t)p->planes.stride * bps, (size_t)C * bps, R,
+                  cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int rme_memory_used(void* ctx, uint64_t* bytes) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !bytes) return RME_EINVAL;
+  uint64_t b = 0;
+  for (auto& kv : c->pics) b += kv.second->bytes + kv.second->chroma_bytes;
+  *bytes = b;
+  return 0;
+}
+
+int rme_standalone_blocks(const rme_picture_desc* d, const rme_params* p, int32_t* blocks, int32_t* count) {
+  if (!valid_desc(d) || !p || !count) return RME_EINVAL;
+  *count = count_blocks(d, p, blocks);
+  return 0;
+}
+
+int rme_frame_result_count(void* ctx, const rme_frame* f, const rme_params* p, int32_t* count) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !f || !p || !count) return RME_EINVAL;
+  if (p->predictor_mode == RME_PRED_GIVEN) {
+    *count = f->njobs;
+    return 0;
+  }
+  Picture* src;
+  int rc = picture_of(c, f->src_id, &src);
+  if (rc) return rc;
+  int nb = count_blocks(&src->d, p, nullptr);
+  *count = src->d.codec == RME_CODEC_H264 ? nb : nb * f->nref;
+  return 0;
+}
+
+int rme_frame_search(void* ctx, const rme_frame* f, const rme_params* p, rme_result* out, void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !f || !p || !out) return c ? fail(c, RME_EINVAL, "null argument") : RME_EINVAL;
+  CK(cudaSetDevice(c->device));
+  return run_launch(c, f, p, 1, out, nullptr, stream ? (cudaStream_t)stream : c->stream, false);
+}
+
+int rme_batch_search(void* ctx, const rme_frame* frames, const rme_params* params, int32_t nframes, rme_result* out,
+                     const int64_t* offsets, void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !frames || !params || !out || nframes < 1) return c ? fail(c, RME_EINVAL, "null argument") : RME_EINVAL;
+  CK(cudaSetDevice(c->device));
+  return run_launch(c, frames, params, nframes, out, offsets, stream ? (cudaStream_t)stream : c->stream, true);
+}
+
+int rme_hevc_decide(const rme_picture_desc* d, const rme_params* p, int32_t nref, const rme_result* res,
+                    int32_t* best, uint8_t* part) {
+  if (!valid_desc(d) || !p || !res || nref < 1 || nref > RME_MAX_REFS || d->codec != RME_CODEC_HEVC)
+    return RME_EINVAL;
+  int W = d->width, H = d->height;
+  float lam = hevc_lambda(p->qp, d->bit_depth, p->hevc_lambda_scale);
+  int sizes[4], nl = level_sizes(p, sizes);
+  int base[5] = {0}, nbx[4], nby[4];
+  for (int l = 0; l < nl; ++l) {
+    nbx[l] = W / sizes[l];
+    nby[l] = H / sizes[l];
+    base[l + 1] = base[l] + nbx[l] * nby[l];
+  }
+  std::vector<uint64_t> cost(base[nl]);
+  for (int b = 0; b < base[nl]; ++b) {
+    int br = 0;
+    uint64_t bc = UINT64_MAX;
+    for (int r = 0; r < nref; ++r) {
+      uint64_t cc = (uint64_t)res[(size_t)b * nref + r].cost + (uint32_t)(lam * (float)hevc_ref_idx_bits(r, nref));
+      if (cc < bc) {
+        bc = cc;
+        br = r;
+      }
+    }
+    cost[b] = bc;
+    if (best) best[b] = br;
+  }
+  if (!part) return 0;
+  int cw = W / 8, ch = H / 8;
+  std::memset(part, 0, (size_t)cw * ch);
+  // Iterative bottom-up: the least cost of every node of every level.
+  std::vector<std::vector<uint64_t>> node(nl);
+  std::vector<std::vector<uint8_t>> split(nl);
+  for (int l = nl - 1; l >= 0; --l) {
+    int N = sizes[l], gx = (W + N - 1) / N, gy = (H + N - 1) / N;
+    node[l].assign((size_t)gx * gy, UINT64_MAX);
+    split[l].assign((size_t)gx * gy, 0);
+    for (int y = 0; y < gy; ++y)
+      for (int x = 0; x < gx; ++x) {
+        int px = x * N, py = y * N;
+        bool exists = px + N <= W && py + N <= H;
+        uint64_t own = exists ? cost[base[l] + y * nbx[l] + x] : UINT64_MAX;
+        uint64_t sp = UINT64_MAX;
+        if (l + 1 < nl) {
+          int M = sizes[l + 1], cgx = (W + M - 1) / M;
+          sp = 0;
+          for (int yy = py; yy < py + N && sp != UINT64_MAX; yy += M)
+            for (int xx = px; xx < px + N; xx += M) {
+              if (xx >= W || yy >= H) continue;
+              uint64_t cc = node[l + 1][(size_t)(yy / M) * cgx + xx / M];
+              if (cc == UINT64_MAX) {
+                sp = UINT64_MAX;
+                break;
+              }
+              sp += cc;
+            }
+        }
+        bool s = sp < own;
+        split[l][(size_t)y * gx + x] = s;
+        node[l][(size_t)y * gx + x] = s ? sp : own;
+      }
+  }
+  // Top-down marking of the chosen sizes.
+  std::vector<std::tuple<int, int, int>> st;
+  int N0 = sizes[0];
+  for (int y = 0; y < H; y += N0)
+    for (int x = 0; x < W; x += N0) st.emplace_back(0, x, y);
+  while (!st.empty()) {
+    auto [l, px, py] = st.back();
+    st.pop_back();
+    int N = sizes[l], gx = (W + N - 1) / N;
+    size_t idx = (size_t)(py / N) * gx + px / N;
+    if (split[l][idx]) {
+      int M = sizes[l + 1];
+      for (int yy = py; yy < py + N; yy += M)
+        for (int xx = px; xx < px + N; xx += M)
+          if (xx < W && yy < H) st.emplace_back(l + 1, xx, yy);
+    } else if (px + N <= W && py + N <= H && node[l][idx] != UINT64_MAX) {
+      int lg = 31 - __builtin_clz((unsigned)N);
+      for (int yy = py / 8; yy < (py + N) / 8 && yy < ch; ++yy)
+        for (int xx = px / 8; xx < (px + N) / 8 && xx < cw; ++xx) part[yy * cw + xx] = (uint8_t)lg;
+    }
+  }
+  return 0;
+}
+
+int rme_last_stats(void* ctx, rme_stats* s) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !s) return RME_EINVAL;
+  *s = c->last;
+  return 0;
+}
+
+int rme_chroma_predict(void* ctx, int32_t ref_id, int32_t nblocks, const int32_t* blocks, const rme_mv* mvs,
+                       void* out, void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return RME_EINVAL;
+  return fail(c, RME_ENOSYS, "chroma prediction not built yet");
+}
+
+int rme_sad_batch(const void*, int64_t, const int64_t*, const void*, int64_t, const int64_t*, int32_t, int32_t, int32_t,
+                  int32_t, uint32_t*, void*) {
+  return RME_ENOSYS;
+}
+int rme_satd_batch(const void*, int64_t, const int64_t*, const void*, int64_t, const int64_t*, int32_t, int32_t,
+                   int32_t, int32_t, uint32_t*, void*) {
+  return RME_ENOSYS;
+}
+
+int rme_serve_start(void*, const rme_serve_opts*, void**) { return RME_ENOSYS; }
+int rme_serve_open_stream(void*, int32_t, const rme_picture_desc*, const rme_params*, int32_t) { return RME_ENOSYS; }
+int rme_serve_submit(void*, int32_t, const void*, rme_result*, int64_t*) { return RME_ENOSYS; }
+int rme_serve_poll(void*, rme_completion*, int32_t, int32_t*) { return RME_ENOSYS; }
+int rme_serve_close_stream(void*, int32_t) { return RME_ENOSYS; }
+int rme_serve_stop(void*) { return RME_ENOSYS; }
+
+}  // extern "C"

@@ -1,0 +1,86 @@
+// Internal structures shared by the host side (rme_capi.cu) and the kernels
+// (rme_planes.cu, rme_search.cu) of librivet_me.so. Not part of the ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/rivet_me.h"
+
+namespace rme {
+
+constexpr int kH264Pad = 32;  // h264/frame.rs LUMA_PAD
+constexpr int kHevcPad = 80;  // hevc/frame.rs LUMA_PAD
+constexpr int kChromaPadHevc = 40;
+constexpr int kChromaPadH264 = 16;
+constexpr int kMvSpan = 4096;  // h264_hpel.rs MV_SPAN
+constexpr int kMvTab = 2 * kMvSpan + 1;
+constexpr int kLamBits = 96;   // HEVC rate table entries (mv_bits <= 71)
+constexpr int kMaxLevels = 4;
+constexpr int kWarpsPerBlock = 8;
+constexpr uint32_t kSpinLimit = 1u << 22;  // bounded dependency waits
+
+// Device status word bits.
+constexpr uint32_t kStatusWaitTimeout = 1u;
+constexpr uint32_t kStatusBadTask = 2u;
+constexpr uint32_t kStatusBounds = 4u;
+
+// One picture's planes on the device: `nplanes` planes of rows x stride
+// samples, one allocation; `origin` is the offset of visible sample (0, 0)
+// within a plane. H.264 pictures hold G, b, h, j; HEVC pictures hold G and
+// the 15 fractional phases (index fy*4+fx).
+struct DevPlanes {
+  const void* base;
+  int64_t plane_elems;
+  int32_t stride;
+  int32_t origin;
+};
+
+// One frame of a launch, as the kernel reads it.
+struct FrameDesc {
+  int32_t codec, bd, mode, nref;
+  int32_t width, height;  // H.264: the coded (macroblock-rounded) size
+  int32_t pad;            // the reference's plane border (search semantics)
+  DevPlanes src;
+  DevPlanes ref[RME_MAX_REFS];
+  // HEVC
+  int32_t nlevels;
+  int32_t size[kMaxLevels], nbx[kMaxLevels], nby[kMaxLevels], base[kMaxLevels + 1];
+  int32_t search_range, search_rings, quarter_cross;
+  const uint32_t* lam_bits;  // (uint32)(lam * bits), bits < kLamBits
+  // H.264
+  const uint16_t* tab;       // MvCostTable
+  int32_t range, hpel_iters, qpel_iters, umh, qpel_diamond, dia, vr;
+  float refine_ratio;
+  uint32_t ref_cost[RME_MAX_REFS];
+  // GIVEN
+  const rme_job* jobs;
+  // outputs and dependency flags (one per result)
+  rme_result* out;
+  int32_t* flags;
+  int32_t epoch;
+  int32_t ntasks;
+};
+
+struct LaunchDesc {
+  const FrameDesc* frames;
+  const uint32_t* queue;  // (frame << 24) | task, topological order
+  int64_t total;
+  unsigned long long* head;
+  uint32_t* status;
+  unsigned long long* counters;  // [tasks, sad, satd, sad_samples, satd_samples]
+};
+
+// Launch wrappers (defined in the .cu files).
+cudaError_t launch_pad_plane(const void* src, int bd, int w, int h, int sstride, DevPlanes dst, int cw, int ch,
+                             int pad, cudaStream_t s);
+cudaError_t launch_h264_hpel(DevPlanes p, int bd, int cw, int ch, int pad, cudaStream_t s);
+cudaError_t launch_hevc_phases(DevPlanes p, int bd, int w, int h, int pad, cudaStream_t s);
+cudaError_t launch_search(const LaunchDesc& L, int bytes_per_sample_max, int grid, cudaStream_t s);
+int search_blocks_per_sm(int bytes_per_sample_max);
+cudaError_t launch_chroma(const void* cb, const void* cr, int bd, int codec, int cw, int ch, int cstride,
+                          int nblocks, const int32_t* blocks, const rme_mv* mvs, const int64_t* out_off, void* out,
+                          cudaStream_t s);
+cudaError_t launch_dist_batch(bool satd, const void* a, int64_t as, const int64_t* aoff, const void* b, int64_t bs,
+                              const int64_t* boff, int w, int h, int bd, int n, uint32_t* out, cudaStream_t s);
+
+}  // namespace rme

@@ -1,0 +1,169 @@
+"""Python host API over librivet_me.so.
+
+`MotionSearch` is the reference's motion-search entry point lifted to the
+batched boundary: upload pictures once (references get their search planes
+built on the device, as the encoders build `Hpel` / `HalfPlanes` once per
+reference picture), then search whole frames — STANDALONE (the library's
+own predictor rule) or GIVEN (one job per encoder call, carrying the
+predictors and seeds `p_mb` / `pick_pu` would pass) — or batches of frames
+in one persistent launch. Every call goes through the C ABI; there is no
+CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Sequence
+
+import numpy as np
+
+from . import capi
+
+
+class MotionSearch:
+    """One device context (rme_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = capi.lib()
+        h = C.c_void_p()
+        rc = self._lib.rme_ctx_create(C.byref(h), device)
+        if rc != 0:
+            raise RuntimeError(f"rme_ctx_create failed ({rc}): no usable CUDA device {device}")
+        self.ctx = h
+        self._desc = {}
+
+    def close(self) -> None:
+        if self.ctx:
+            self._lib.rme_ctx_destroy(self.ctx)
+            self.ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc: int) -> None:
+        capi.check(rc, self.ctx)
+
+    # ---- pictures ---------------------------------------------------------
+    def upload(self, pic_id: int, pic: np.ndarray, codec: int, bit_depth: int, as_ref: bool = True,
+               stream: int = 0) -> None:
+        pic = np.ascontiguousarray(pic)
+        want = np.uint8 if bit_depth == 8 else np.uint16
+        if pic.dtype != want:
+            raise ValueError(f"{bit_depth}-bit pictures are {np.dtype(want).name}")
+        h, w = pic.shape
+        d = capi.PictureDesc(codec, bit_depth, w, h, w)
+        self._check(self._lib.rme_picture_upload(self.ctx, pic_id, C.byref(d), capi.ptr(pic), int(as_ref),
+                                                 C.c_void_p(stream)))
+        self._desc[pic_id] = d
+
+    def upload_chroma(self, pic_id: int, cb: np.ndarray, cr: np.ndarray) -> None:
+        cb, cr = np.ascontiguousarray(cb), np.ascontiguousarray(cr)
+        self._check(self._lib.rme_picture_upload_chroma(self.ctx, pic_id, capi.ptr(cb), capi.ptr(cr),
+                                                        cb.shape[1], None))
+
+    def release(self, pic_id: int) -> None:
+        self._check(self._lib.rme_picture_release(self.ctx, pic_id))
+        self._desc.pop(pic_id, None)
+
+    def plane(self, pic_id: int, index: int) -> np.ndarray:
+        rows, cols = C.c_int32(), C.c_int32()
+        self._check(self._lib.rme_picture_download_plane(self.ctx, pic_id, index, None, C.byref(rows), C.byref(cols)))
+        d = self._desc[pic_id]
+        out = np.zeros((rows.value, cols.value), np.uint8 if d.bit_depth == 8 else np.uint16)
+        self._check(self._lib.rme_picture_download_plane(self.ctx, pic_id, index, capi.ptr(out), C.byref(rows),
+                                                         C.byref(cols)))
+        return out
+
+    def memory_used(self) -> int:
+        b = C.c_uint64()
+        self._check(self._lib.rme_memory_used(self.ctx, C.byref(b)))
+        return b.value
+
+    # ---- search -----------------------------------------------------------
+    @staticmethod
+    def _frame(src_id: int, ref_ids: Sequence[int], jobs: np.ndarray | None = None) -> capi.Frame:
+        f = capi.Frame()
+        f.src_id = src_id
+        f.nref = len(ref_ids)
+        for i, r in enumerate(ref_ids):
+            f.ref_ids[i] = r
+        if jobs is not None:
+            f.jobs = C.cast(jobs.ctypes.data, C.POINTER(capi.Job))
+            f.njobs = len(jobs)
+        return f
+
+    def result_count(self, src_id: int, ref_ids: Sequence[int], params: capi.Params,
+                     jobs: np.ndarray | None = None) -> int:
+        f = self._frame(src_id, ref_ids, jobs)
+        n = C.c_int32()
+        self._check(self._lib.rme_frame_result_count(self.ctx, C.byref(f), C.byref(params), C.byref(n)))
+        return n.value
+
+    def search(self, src_id: int, ref_ids: Sequence[int], params: capi.Params,
+               jobs: np.ndarray | None = None) -> np.ndarray:
+        """One frame; results as a structured array (capi.RESULT_DTYPE)."""
+        if jobs is not None:
+            jobs = np.ascontiguousarray(jobs, capi.JOB_DTYPE)
+        f = self._frame(src_id, ref_ids, jobs)
+        n = self.result_count(src_id, ref_ids, params, jobs)
+        out = np.zeros(n, capi.RESULT_DTYPE)
+        self._check(self._lib.rme_frame_search(self.ctx, C.byref(f), C.byref(params),
+                                               C.cast(out.ctypes.data, C.POINTER(capi.Result)), None))
+        return out
+
+    def search_batch(self, frames: Sequence[tuple[int, Sequence[int]]],
+                     params: capi.Params | Sequence[capi.Params]) -> list[np.ndarray]:
+        """Many STANDALONE frames (src_id, ref_ids) in one persistent launch."""
+        n = len(frames)
+        if isinstance(params, capi.Params):
+            params = [params] * n
+        fa = (capi.Frame * n)(*[self._frame(s, r) for s, r in frames])
+        pa = (capi.Params * n)(*params)
+        counts = [self.result_count(s, r, p) for (s, r), p in zip(frames, params)]
+        offs = np.zeros(n, np.int64)
+        offs[1:] = np.cumsum(counts)[:-1]
+        out = np.zeros(int(sum(counts)), capi.RESULT_DTYPE)
+        self._check(self._lib.rme_batch_search(self.ctx, fa, pa, n, C.cast(out.ctypes.data, C.POINTER(capi.Result)),
+                                               offs.ctypes.data_as(C.POINTER(C.c_int64)), None))
+        return [out[o:o + c] for o, c in zip(offs, counts)]
+
+    def stats(self) -> capi.Stats:
+        s = capi.Stats()
+        self._check(self._lib.rme_last_stats(self.ctx, C.byref(s)))
+        return s
+
+    def chroma_predict(self, ref_id: int, blocks: np.ndarray, mvs: np.ndarray) -> np.ndarray:
+        d = self._desc[ref_id]
+        blocks = np.ascontiguousarray(blocks, np.int32)
+        mvs = np.ascontiguousarray(mvs, np.int16)
+        n = int(sum((b[2] // 2) * (b[3] // 2) * 2 for b in blocks))
+        out = np.zeros(n, np.uint8 if d.bit_depth == 8 else np.uint16)
+        self._check(self._lib.rme_chroma_predict(self.ctx, ref_id, len(blocks),
+                                                 blocks.ctypes.data_as(C.POINTER(C.c_int32)),
+                                                 C.cast(mvs.ctypes.data, C.POINTER(capi.Mv)), capi.ptr(out), None))
+        return out
+
+
+def standalone_blocks(codec: int, width: int, height: int, bit_depth: int, params: capi.Params) -> np.ndarray:
+    d = capi.PictureDesc(codec, bit_depth, width, height, width)
+    n = C.c_int32()
+    capi.check(capi.lib().rme_standalone_blocks(C.byref(d), C.byref(params), None, C.byref(n)))
+    out = np.zeros((n.value, 4), np.int32)
+    capi.check(capi.lib().rme_standalone_blocks(C.byref(d), C.byref(params),
+                                                out.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(n)))
+    return out
+
+
+def hevc_decide(width: int, height: int, bit_depth: int, params: capi.Params, nref: int, res: np.ndarray):
+    """Chosen reference per block and the 8x8-cell map of chosen PU sizes (log2)."""
+    d = capi.PictureDesc(capi.RME_CODEC_HEVC, bit_depth, width, height, width)
+    nb = len(res) // nref
+    best = np.zeros(nb, np.int32)
+    part = np.zeros((height // 8, width // 8), np.uint8)
+    capi.check(capi.lib().rme_hevc_decide(C.byref(d), C.byref(params), nref,
+                                          C.cast(res.ctypes.data, C.POINTER(capi.Result)),
+                                          best.ctypes.data_as(C.POINTER(C.c_int32)),
+                                          part.ctypes.data_as(C.POINTER(C.c_uint8))))
+    return best, part

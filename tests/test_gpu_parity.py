@@ -1,0 +1,201 @@
+"""CUDA path against the oracle, bit for bit, through the C ABI.
+
+Every comparison is exact: the search is integer arithmetic end to end, so
+every vector, reference index, cost, SATD, whole-sample winner and
+candidate count must equal the oracle's on the same input.
+"""
+import numpy as np
+import pytest
+
+import oracle
+import rivet_h26x_codecs_b200.capi as capi
+import rivet_h26x_codecs_b200.synth as synth
+from _common import assert_results_equal, lcg_picture, random_jobs, random_picture, shifted
+
+H264, HEVC = capi.RME_CODEC_H264, capi.RME_CODEC_HEVC
+pytestmark = pytest.mark.gpu
+
+
+def _run(ms, codec, bd, src, refs, p, jobs=None, base=1000):
+    ms.upload(base, src, codec, bd, as_ref=False)
+    ids = []
+    for i, r in enumerate(refs):
+        ms.upload(base + 1 + i, r, codec, bd, as_ref=True)
+        ids.append(base + 1 + i)
+    got = ms.search(base, ids, p, jobs)
+    want = oracle.frame_search(codec, bd, src, refs, p, jobs)
+    return got, want
+
+
+# ---- planes -----------------------------------------------------------------
+@pytest.mark.parametrize("bd", [8, 10])
+def test_h264_half_planes_equal_the_oracles(ms, bd):
+    pic = lcg_picture(48, 40, 12345, bd)  # the reference test's plane (h264_hpel.rs:1033-1045)
+    ms.upload(1, pic, H264, bd, as_ref=True)
+    want = oracle.h264_planes(pic, bd)
+    rows, cols = want.shape[1:]
+    for k in range(4):
+        got = ms.plane(1, k)
+        assert got.shape == (rows, cols)
+        # b and j are computed where the six-tap window fits across; h and j
+        # where it fits down (hpel_planes' loops); elsewhere the reference
+        # copies G and the search never reads it.
+        ys = slice(2, rows - 3) if k in (2, 3) else slice(0, rows)
+        xs = slice(2, cols - 3) if k in (1, 3) else slice(0, cols)
+        np.testing.assert_array_equal(got[ys, xs], want[k][ys, xs], err_msg=f"plane {k}")
+
+
+@pytest.mark.parametrize("bd,w,h", [(8, 40, 24), (10, 72, 40), (8, 200, 136)])
+def test_hevc_phases_equal_the_oracles(ms, bd, w, h):
+    pic = lcg_picture(w, h, 7, bd) if w == 40 else random_picture(np.random.default_rng(w), w, h, bd)
+    ms.upload(2, pic, HEVC, bd, as_ref=True)
+    want, ext = oracle.hevc_planes(pic, bd, force_quarter=True)
+    pad = 80
+    sl = (slice(pad - ext, pad + h + ext), slice(pad - ext, pad + w + ext))
+    for k in range(16):
+        np.testing.assert_array_equal(ms.plane(2, k)[sl], want[k][sl], err_msg=f"phase {k}")
+
+
+# ---- H.264 ------------------------------------------------------------------
+def test_h264_cif_frame_matches_the_oracle(ms):
+    """The CIF P-frame workload: 396 macroblocks, medium MeCfg, QP 28."""
+    seq = synth.config0()
+    p = oracle.params(H264, 28)
+    got, want = _run(ms, H264, 8, seq.frames[1], [seq.frames[0]], p)
+    assert_results_equal(got, want, "H.264 CIF")
+
+
+@pytest.mark.parametrize("variant", ["medium", "umh", "dia", "qpel_diamond", "vr", "slow"])
+@pytest.mark.parametrize("bd", [8, 10])
+def test_h264_settings_match_the_oracle(ms, variant, bd):
+    rng = np.random.default_rng(hash((variant, bd)) & 0xFFFF)
+    ref0 = random_picture(rng, 160, 112, bd)
+    ref1 = shifted(ref0, 3, -2, rng, 2.0)
+    ref2 = shifted(ref0, -5, 4, rng, 2.0)
+    src = shifted(ref0, 6, 5, rng, 2.0)
+    kw = {"medium": {}, "umh": {"h264_umh": 1}, "dia": {"h264_dia": 1, "h264_hpel_iters": 1, "h264_qpel_iters": 1},
+          "qpel_diamond": {"h264_qpel_diamond": 1}, "vr": {"h264_vertical_range": 7},
+          "slow": {"h264_range": 24}}[variant]
+    p = oracle.params(H264, 30, **kw)
+    got, want = _run(ms, H264, bd, src, [ref0, ref1, ref2], p)
+    assert_results_equal(got, want, f"H.264 {variant} {bd}-bit")
+
+
+def test_h264_ragged_picture_size(ms):
+    """A picture that is not whole macroblocks (coded size rounded up)."""
+    rng = np.random.default_rng(5)
+    ref = random_picture(rng, 100, 70, 8)
+    src = shifted(ref, -3, 2, rng, 1.0)
+    got, want = _run(ms, H264, 8, src, [ref], oracle.params(H264, 26))
+    assert_results_equal(got, want, "H.264 100x70")
+
+
+@pytest.mark.parametrize("bd", [8, 10])
+def test_h264_given_jobs_match_the_oracle(ms, bd):
+    rng = np.random.default_rng(17 + bd)
+    ref0 = random_picture(rng, 128, 96, bd)
+    ref1 = shifted(ref0, 2, 1, rng, 1.0)
+    src = shifted(ref0, -4, 3, rng, 1.0)
+    p = oracle.params(H264, 27, predictor_mode=capi.RME_PRED_GIVEN)
+    jobs = random_jobs(rng, H264, 128, 96, 2, 300, sizes=((16, 16), (16, 8), (8, 16), (8, 8), (8, 4), (4, 8),
+                                                          (4, 4)))
+    got, want = _run(ms, H264, bd, src, [ref0, ref1], p, jobs)
+    assert_results_equal(got, want, f"H.264 GIVEN {bd}-bit")
+
+
+# ---- HEVC -------------------------------------------------------------------
+@pytest.mark.parametrize("variant", ["medium", "range64_rings", "cross", "levels"])
+@pytest.mark.parametrize("bd", [8, 10])
+def test_hevc_frames_match_the_oracle(ms, variant, bd):
+    seq = synth.make_sequence(HEVC, 256, 192, bd, 3, 100 + bd, 64, 64, 2.0 if bd == 8 else 6.0)
+    kw = {"medium": {}, "range64_rings": {"hevc_search_range": 64, "hevc_search_rings": 1},
+          "cross": {"hevc_quarter_cross": 1, "hevc_search_rings": 2}, "levels": {"hevc_pu_mask": 0b1010}}[variant]
+    p = oracle.params(HEVC, 32, **kw)
+    got, want = _run(ms, HEVC, bd, seq.frames[2], [seq.frames[1], seq.frames[0]], p)
+    assert_results_equal(got, want, f"HEVC {variant} {bd}-bit")
+
+
+@pytest.mark.parametrize("bd", [8, 10])
+def test_hevc_given_jobs_match_the_oracle(ms, bd):
+    rng = np.random.default_rng(99 + bd)
+    ref0 = random_picture(rng, 192, 128, bd)
+    ref1 = shifted(ref0, -7, 2, rng, 1.0)
+    src = shifted(ref0, 5, -6, rng, 1.0)
+    p = oracle.params(HEVC, 30, predictor_mode=capi.RME_PRED_GIVEN, hevc_search_rings=1)
+    jobs = random_jobs(rng, HEVC, 192, 128, 2, 400, spread=400)
+    got, want = _run(ms, HEVC, bd, src, [ref0, ref1], p, jobs)
+    assert_results_equal(got, want, f"HEVC GIVEN {bd}-bit")
+
+
+def test_hevc_1080p_frame_matches_the_oracle(ms):
+    """One frame of the 1080p workload at full size: 42,900 PUs x 2 refs."""
+    seq = synth.config1(nframes=3)
+    p = oracle.params(HEVC, 32, hevc_search_range=64)
+    got, want = _run(ms, HEVC, 8, seq.frames[2], [seq.frames[1], seq.frames[0]], p)
+    assert_results_equal(got, want, "HEVC 1080p")
+    st = ms.stats()
+    assert st.tasks == len(got)
+    assert st.sad_candidates == int(want["n_sad"].sum())
+    assert st.satd_candidates == int(want["n_satd"].sum())
+
+
+def test_batch_equals_the_frames_and_the_oracle(ms):
+    """Several frames of two formats in one persistent launch, twice (the
+    second launch replays the captured graph)."""
+    seq = synth.make_sequence(HEVC, 192, 128, 8, 5, 31, 64, 64, 2.0)
+    h264 = synth.make_sequence(H264, 96, 64, 8, 3, 32, 16, 32, 2.0)
+    ph = oracle.params(HEVC, 32, hevc_search_range=40)
+    p4 = oracle.params(H264, 28)
+    for i, f in enumerate(seq.frames):
+        ms.upload(300 + i, f, HEVC, 8, as_ref=True)
+    for i, f in enumerate(h264.frames):
+        ms.upload(400 + i, f, H264, 8, as_ref=True)
+    frames = [(300 + t, [300 + t - 1, 300 + t - 2]) for t in range(2, 5)] + [(402, [401, 400])]
+    params = [ph, ph, ph, p4]
+    for _ in range(2):
+        outs = ms.search_batch(frames, params)
+        for (s, refs), pp, got in zip(frames, params, outs):
+            single = ms.search(s, refs, pp)
+            assert_results_equal(got, single, f"batch vs single {s}")
+            seqf = seq.frames if s < 400 else h264.frames
+            base = 300 if s < 400 else 400
+            codec = HEVC if s < 400 else H264
+            want = oracle.frame_search(codec, 8, seqf[s - base], [seqf[r - base] for r in refs], pp)
+            assert_results_equal(got, want, f"batch vs oracle {s}")
+
+
+# ---- the reference's search-behaviour tests, through the library --------------
+def grating(w, h):
+    """The reference tests' triangle grating (h265_me.rs:4989-5026,
+    h264_me.rs:3698-3710): 40 + 4|x%25-12| + 3|y%27-13|."""
+    y, x = np.mgrid[0:h, 0:w]
+    return (40 + 4 * np.abs(x % 25 - 12) + 3 * np.abs(y % 27 - 13)).astype(np.uint8)
+
+
+def test_hevc_integral_translation_is_found_exactly(ms):
+    ref = grating(64, 32)
+    src = shifted(ref, -6, 4)
+    p = oracle.params(HEVC, 26, hevc_pu_mask=0b0100)  # 32x32 units, as the reference test's CTBs
+    got, want = _run(ms, HEVC, 8, src, [ref], p)
+    assert_results_equal(got, want, "translation")
+    assert (got["mvx"] == -24).all() and (got["mvy"] == 16).all(), got[["mvx", "mvy"]]
+
+
+def test_hevc_half_sample_translation_is_found_by_the_refinement(ms):
+    ref = grating(64, 32)
+    src = oracle.hevc_predict(ref, 8, 0, 0, 2, 0, 64, 32)  # the decoder's own (2, 0) interpolation
+    p = oracle.params(HEVC, 26, hevc_pu_mask=0b0010)
+    got, want = _run(ms, HEVC, 8, src, [ref], p)
+    assert_results_equal(got, want, "half-sample translation")
+    assert (got["mvx"] == 2).all() and (got["mvy"] == 0).all()
+    assert (got["satd"] == 0).all()
+
+
+@pytest.mark.parametrize("d", [(1, 0), (0, -1), (5, 3), (-7, 2), (3, -8), (8, 8), (-8, -8)])
+def test_h264_integral_translation_is_found_exactly(ms, d):
+    ref = grating(48, 48)
+    src = shifted(ref, *d)
+    got, want = _run(ms, H264, 8, src, [ref], oracle.params(H264, 26))
+    assert_results_equal(got, want, f"translation {d}")
+    centre = got[4]  # the middle macroblock of the 3x3 picture
+    assert (centre["mvx"], centre["mvy"]) == (d[0] * 4, d[1] * 4)
