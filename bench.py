@@ -1,0 +1,388 @@
+#!/usr/bin/env python
+"""Benchmark: 1080p HEVC motion estimation on B200.
+
+Workload (one step): a 1080p 8-bit HEVC sequence of 62 synthetic pictures
+(sinusoids + noise, 64x64-region motion in +-40 px at quarter samples,
+sigma-2 noise), of which the last 60 are searched, each against the two
+pictures before it: 2Nx2N prediction units 8x8..64x64 (42,900 per
+reference), +-64 whole-sample search, half- then quarter-sample SATD
+refinement, lambda at QP 32 (medium tier: no widening rings, Tune::lambda
+0.85), STANDALONE predictors. A step rebuilds the search planes of the 60
+new references (HalfPlanes::new's work) and searches the 60 frames in one
+persistent launch (the batched form). The working set (62 pictures x 16
+planes, 2.6 GB) is far larger than L2, so no flush is needed between steps.
+
+Lines printed (one JSON line each; rank 0 only):
+  default            the batched form: value = frames/s on the device with
+                     inputs resident; e2e = the same through the C ABI from
+                     pinned host memory (uploads + plane builds + search +
+                     results back inside the timed region); the plain
+                     per-frame path (one frame per call) beside it, p50/p99.
+  --impl reference   the reference's CPU path on the host cores: the
+                     oracle's C++ restatement (AVX2 distortion rungs), since
+                     the Rust crate cannot be built here.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WIDTH, HEIGHT, NFRAMES, NREF, QP, RANGE = 1920, 1080, 60, 2, 32, 64
+METRIC = "1080p HEVC ME frames/s (batched persistent launch; plain per-frame GPU path, p50/p99 beside it; bit-exact)"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu, self.proc, self.lines = gpu, None, []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_workload(rank: int):
+    from rivet_h26x_codecs_b200 import synth
+    seq = synth.make_sequence(synth.HEVC, WIDTH, HEIGHT, 8, NFRAMES + NREF, synth.seed_for(1, rank), 64, 160, 2.0)
+    return seq.frames
+
+
+def hevc_params(oracle_mod=None):
+    import rivet_h26x_codecs_b200.capi as capi
+    p = capi.default_params(capi.RME_CODEC_HEVC, QP) if oracle_mod is None else oracle_mod.params(capi.RME_CODEC_HEVC, QP)
+    p.hevc_search_range = RANGE
+    return p
+
+
+def cpu_baseline(frames, threads: int, simd: int = 1):
+    """The oracle (C++ restatement, AVX2 rungs) over `threads` frames on as
+    many host threads: frames/s including their reference plane builds."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    import rivet_h26x_codecs_b200.capi as capi
+    n = max(1, min(threads, len(frames) - NREF))
+    srcs = [frames[NREF + i] for i in range(n)]
+    refs = [[frames[NREF + i - 1 - r] for r in range(NREF)] for i in range(n)]
+    p = hevc_params(oracle)
+    _, secs, _ = oracle.frames_search_mt(capi.RME_CODEC_HEVC, 8, srcs, refs, p, simd=simd, threads=threads)
+    return n / secs, n, secs
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        dist.barrier()
+        torch.cuda.synchronize()
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    frames = make_workload(0)[: NREF + args.ref_frames]
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_baseline(frames, threads)
+    t0 = time.perf_counter()
+    done = 0
+    for _ in range(args.steps):
+        _, n, _ = cpu_baseline(frames, threads)
+        done += n
+    secs = time.perf_counter() - t0
+    fps = done / secs
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": "hevc-1080p-8bit-2ref-pu8to64-range64-qp32", "frames_per_step": done // args.steps,
+                   "note": "bounded sample: one 1080p frame per host thread per step"},
+        "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": threads, "kind": "port",
+                         "sample": f"{done // args.steps} frames of the 1080p workload per step, one per thread, "
+                                   "reference plane builds included"},
+        "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    import rivet_h26x_codecs_b200 as rme
+    import rivet_h26x_codecs_b200.capi as capi
+
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except (OSError, ValueError):
+        pass
+    t0 = time.perf_counter()
+    frames = make_workload(rank)
+    log(f"[rank {rank}] workload generated in {time.perf_counter() - t0:.1f}s")
+    ms = rme.MotionSearch(local)
+    p = hevc_params()
+    ids = list(range(len(frames)))
+    for i, f in zip(ids, frames):
+        ms.upload(i, f, capi.RME_CODEC_HEVC, 8, as_ref=True)
+    batch = [(t, [t - 1 - r for r in range(NREF)]) for t in range(NREF, len(frames))]
+    stream = torch.cuda.Stream(device=local)
+    sh = stream.cuda_stream
+
+    def step():
+        for t, _ in batch:
+            ms.build_planes(t, sh)
+        return ms.search_batch(batch, p, sh)
+
+    # ---- plain per-frame GPU path (one frame per call) -----------------------
+    for t, refs in batch[:3]:
+        ms.search(t, refs, p, stream=sh)
+    lat = []
+    plain_out = []
+    for t, refs in batch:
+        a = time.perf_counter()
+        plain_out.append(ms.search(t, refs, p, stream=sh))
+        lat.append(time.perf_counter() - a)
+    plain_fps = len(batch) / sum(lat)
+
+    # ---- batched, device-resident -------------------------------------------
+    for _ in range(max(args.warmup, 3)):
+        outs = step()
+    for o, q in zip(outs, plain_out):
+        if not (o == q).all():
+            raise SystemExit("batched results differ from the per-frame path")
+    stats = ms.stats()
+    kernel_ms_list = []
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+            kernel_ms_list.append(ms.stats().kernel_ms)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    elapsed = ev0.elapsed_time(ev1) / 1e3
+    barrier(world)
+    elapsed = max_over_ranks(elapsed, world)
+    frames_per_step = len(batch)
+    value = world * frames_per_step * args.steps / elapsed
+    clocks = clk.summary()
+
+    # ---- end to end through the C ABI from pinned host memory --------------------
+    pinned = []
+    for f in frames:
+        t = torch.empty(f.shape, dtype=torch.uint8, pin_memory=True)
+        t.numpy()[...] = f
+        pinned.append(t)
+    h2d = sum(int(f.nbytes) for f in frames)
+    d2h = sum(int(o.nbytes) for o in outs)
+
+    def e2e_step():
+        for i, t in zip(ids, pinned):
+            ms.upload(i, t.numpy(), capi.RME_CODEC_HEVC, 8, as_ref=True, stream=sh)
+        return ms.search_batch(batch, p, sh)
+
+    for _ in range(2):
+        e2e_step()
+    barrier(world)
+    a = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_out = e2e_step()
+    torch.cuda.synchronize()
+    e2e_secs = max_over_ranks(time.perf_counter() - a, world)
+    e2e_value = world * frames_per_step * args.steps / e2e_secs
+    for o, q in zip(e2e_out, plain_out):
+        if not (o == q).all():
+            raise SystemExit("end-to-end results differ from the per-frame path")
+
+    # ---- roofline ---------------------------------------------------------------
+    st = ms.stats()
+    kms = float(np.median(kernel_ms_list)) / 1e3
+    int_ops = 2 * st.sad_samples + 7 * st.satd_samples + st.satd_samples // 16
+    peak_ops = C_double = None
+    import ctypes as C
+    C_double = C.c_double()
+    if capi.lib().rme_probe_int_peak(local, C.byref(C_double)) == 0:
+        peak_ops = C_double.value
+    plane_bytes = (WIDTH + 160 + 63) // 64 * 64 * (HEIGHT + 160)  # one padded plane, 8-bit
+    alg_bytes = (len(frames) * 16 * plane_bytes + frames_per_step * WIDTH * HEIGHT
+                 + sum(int(o.nbytes) for o in outs))
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    roof = {
+        "bound": "int_alu",
+        "achieved": int_ops / kms / 1e12, "peak": (peak_ops or 0) / 1e12, "unit": "Tops/s",
+        "frac": (int_ops / kms / peak_ops) if peak_ops else None,
+        "peak_source": "measured: rme_probe_int_peak (32-bit add/shift/xor chains, all SMs)",
+        "algorithmic_int_ops_per_launch": int(int_ops),
+        "kernel_ms": kms * 1e3,
+        "traffic": None,
+        "hbm": {"achieved": alg_bytes / kms / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                "frac": alg_bytes / kms / 1e9 / hbm_peak, "algorithmic_bytes_per_launch": alg_bytes,
+                "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback"},
+    }
+    traffic_file = ROOT / "profiles" / "search_kernel_traffic.json"
+    if traffic_file.exists():
+        try:
+            tr = json.loads(traffic_file.read_text())
+            roof["traffic"] = tr.get("bytes_per_launch_1080p")
+        except ValueError:
+            pass
+
+    # ---- CPU baseline (bounded sample) ---------------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        fps_all, n_all, secs_all = cpu_baseline(frames, threads)
+        fps_1, _, _ = cpu_baseline(frames, 1)
+        cpu = {"value": fps_all, "unit": "frames/s", "cores": threads, "kind": "port",
+               "sample": f"{n_all} frames of the workload, one per host thread, AVX2 rungs, "
+                         "reference plane builds included",
+               "value_1_thread": fps_1}
+
+    if rank == 0:
+        lat_ms = np.array(lat) * 1e3
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": "hevc-1080p-8bit-2ref-pu8to64-range64-qp32", "frames_per_step": frames_per_step,
+                       "width": WIDTH, "height": HEIGHT, "refs": NREF, "pus_per_ref": int(stats.tasks // frames_per_step // NREF),
+                       "predictors": "standalone", "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2 (2.6 GB of planes)"},
+            "plain_per_frame": {"value": plain_fps, "unit": "frames/s", "p50_ms": float(np.percentile(lat_ms, 50)),
+                                "p99_ms": float(np.percentile(lat_ms, 99))},
+            "batched_latency_ms": elapsed / args.steps * 1e3,
+            "pu_cost_evals_per_s": (st.sad_candidates + st.satd_candidates) / kms * world,
+            "e2e": {"value": e2e_value, "unit": "frames/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "gpu_launches": args.steps * (frames_per_step + 1),
+        }), flush=True)
+    ms.close()
+
+
+def profile_case():
+    """One 1080p frame (2 references) searched twice through the per-frame
+    path: the case the ncu captures of the search kernel run on (about
+    130 MB on the device, inputs larger than L2)."""
+    import rivet_h26x_codecs_b200 as rme
+    import rivet_h26x_codecs_b200.capi as capi
+    from rivet_h26x_codecs_b200 import synth
+    seq = synth.make_sequence(synth.HEVC, WIDTH, HEIGHT, 8, 3, synth.seed_for(1), 64, 160, 2.0)
+    with rme.MotionSearch(0) as ms:
+        for i, f in enumerate(seq.frames):
+            ms.upload(i, f, capi.RME_CODEC_HEVC, 8, as_ref=True)
+        p = hevc_params()
+        for _ in range(2):
+            ms.search(2, [1, 0], p)
+    print("profile case done")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ref-frames", type=int, default=8, help="reference arm: frames per step sample")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="small case for ncu: 3 pictures, one frame searched twice, nothing else")
+    args = ap.parse_args()
+    world, rank, local = dist_setup(args)
+    if args.profile_case:
+        profile_case()
+        return
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

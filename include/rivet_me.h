@@ -194,6 +194,11 @@ int rme_picture_upload_chroma(void* ctx, int32_t pic_id, const void* cb,
 
 int rme_picture_release(void* ctx, int32_t pic_id);
 
+/* Rebuild the search planes of an uploaded reference from its resident
+ * integer plane, on `stream`, without waiting: the per-reference plane
+ * build (build_hpel / HalfPlanes::new) of a picture already in HBM. */
+int rme_picture_build_planes(void* ctx, int32_t pic_id, void* stream);
+
 /* Copy one search plane of an uploaded reference to the host: plane 0 is
  * the padded integer plane, H.264 planes 1..3 are b, h, j (Hpel::plane
  * 0..2), HEVC planes 1..15 the fractional phase fy*4+fx (HalfPlanes'
@@ -310,6 +315,13 @@ int rme_serve_submit(void* server, int32_t stream_id, const void* luma,
 int rme_serve_poll(void* server, rme_completion* done, int32_t max, int32_t* n);
 int rme_serve_close_stream(void* server, int32_t stream_id);
 int rme_serve_stop(void* server);
+
+/* ---- diagnostics ------------------------------------------------------------ */
+
+/* Measured 32-bit integer-ALU throughput of `device` (add/shift/xor chains
+ * over every SM), in operations per second: the roofline denominator of the
+ * search kernel, which is integer work with no tensor-core content. */
+int rme_probe_int_peak(int32_t device, double* ops_per_s);
 
 #ifdef __cplusplus
 }

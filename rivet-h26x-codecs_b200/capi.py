@@ -104,6 +104,7 @@ SIGNATURES = {
     "rme_picture_upload": (C.c_int, [_vp, _i32, C.POINTER(PictureDesc), _vp, _i32, _vp]),
     "rme_picture_upload_chroma": (C.c_int, [_vp, _i32, _vp, _vp, _i32, _vp]),
     "rme_picture_release": (C.c_int, [_vp, _i32]),
+    "rme_picture_build_planes": (C.c_int, [_vp, _i32, _vp]),
     "rme_picture_download_plane": (C.c_int, [_vp, _i32, _i32, _vp, C.POINTER(C.c_int32),
                                              C.POINTER(C.c_int32)]),
     "rme_memory_used": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
@@ -126,6 +127,7 @@ SIGNATURES = {
     "rme_serve_poll": (C.c_int, [_vp, C.POINTER(Completion), _i32, C.POINTER(C.c_int32)]),
     "rme_serve_close_stream": (C.c_int, [_vp, _i32]),
     "rme_serve_stop": (C.c_int, [_vp]),
+    "rme_probe_int_peak": (C.c_int, [_i32, C.POINTER(C.c_double)]),
 }
 
 PACKAGE_DIR = Path(__file__).resolve().parent

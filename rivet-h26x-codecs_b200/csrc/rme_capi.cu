@@ -63,12 +63,17 @@ uint32_t hevc_ref_idx_bits(int r, int nref) {
   return r < nref - 1 ? (uint32_t)(r + 1) : (uint32_t)r;
 }
 
+// Buffers that grow on demand. `generation` counts reallocations across all
+// of them, so launch graphs captured over an old buffer are never replayed.
+static uint64_t g_buffer_generation = 0;
+
 template <class T>
 struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
   cudaError_t ensure(size_t want) {
     if (want <= n) return cudaSuccess;
+    ++g_buffer_generation;
     if (p) cudaFree(p);
     p = nullptr;
     n = 0;
@@ -87,6 +92,7 @@ struct PinBuf {
   size_t n = 0;
   cudaError_t ensure(size_t want) {
     if (want <= n) return cudaSuccess;
+    ++g_buffer_generation;
     if (p) cudaFreeHost(p);
     p = nullptr;
     n = 0;
@@ -235,6 +241,9 @@ int check_params(Ctx* c, const rme_params* p, const rme_picture_desc& d) {
     if (p->h264_range < 0 || p->h264_range > 512 || p->h264_hpel_iters < 0 || p->h264_qpel_iters < 0 ||
         p->h264_hpel_iters > 64 || p->h264_qpel_iters > 64)
       return fail(c, RME_EINVAL, "bad H.264 MeCfg");
+    // vertical_search is range - 1 of a level's MaxVmvR >= 0: at least -1.
+    // (A window emptied by it still clamps every point inside the plane.)
+    if (p->h264_vertical_range < -1) return fail(c, RME_EINVAL, "h264_vertical_range below -1");
   } else {
     if (p->hevc_pad < 8 || p->hevc_pad > kHevcPad) return fail(c, RME_EINVAL, "hevc_pad must be 8..80");
     if (p->hevc_search_range < 0 || p->hevc_search_range > 1024 || p->hevc_search_rings < 0 ||
@@ -411,10 +420,15 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
     toff[i + 1] = toff[i] + ntask[i];
   }
   const int64_t total = toff[n];
-  if (total >= (1 << 24) * (int64_t)1 && n > 1) return fail(c, RME_EINVAL, "too many tasks in one launch");
+  for (int i = 0; i < n; ++i)
+    if (ntask[i] >= (1 << 24)) return fail(c, RME_EINVAL, "more than 2^24 tasks in one frame");
   CK(c->d_frames.ensure(n));
   CK(c->d_out.ensure(std::max<int64_t>(total, 1)));
+  int32_t* old_flags = c->d_flags.p;
   CK(c->d_flags.ensure(std::max<int64_t>(total, 1)));
+  // Fresh flag memory holds arbitrary words, any of which could equal an
+  // epoch: zero it (epochs start at 1).
+  if (c->d_flags.p != old_flags) c->epoch = 0;
   CK(c->d_queue.ensure(std::max<int64_t>(total, 1)));
   CK(c->d_jobs.ensure(std::max<int64_t>(jobs_off[n], 1)));
   CK(c->d_misc.ensure(8));
@@ -485,12 +499,15 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   if (!c->bps) c->bps = std::max(1, search_blocks_per_sm(2));
   int64_t want = (total + kWarpsPerBlock - 1) / kWarpsPerBlock;
   int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)c->nsm * c->bps, want));
-  auto enqueue = [&]() -> cudaError_t {
+  auto enqueue = [&](bool capturing) -> cudaError_t {
+    const unsigned rec = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
     cudaError_t e = cudaMemcpyAsync(c->d_frames.p, c->h_frames.p, sizeof(FrameDesc) * n, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(c->d_misc.p, 0, 8 * sizeof(unsigned long long), s);
-    if (e == cudaSuccess) e = cudaEventRecord(c->ev0, s);
+    // Under capture the records are external ones: they become event-record
+    // nodes, so the kernel's device time is measured on every replay.
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(c->ev0, s, rec);
     if (e == cudaSuccess) e = launch_search(L, 2, grid, s);
-    if (e == cudaSuccess) e = cudaEventRecord(c->ev1, s);
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(c->ev1, s, rec);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(c->h_out.p, c->d_out.p, sizeof(rme_result) * total, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess)
@@ -503,11 +520,12 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
     std::vector<int64_t> gsig = sig;
     gsig.push_back(total);
     gsig.push_back((int64_t)(uintptr_t)s);
+    gsig.push_back((int64_t)g_buffer_generation);
     Graph& g = c->graphs[gsig];
     if (!g.exec) {
       cudaGraph_t graph;
       CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-      cudaError_t e = enqueue();
+      cudaError_t e = enqueue(true);
       cudaError_t e2 = cudaStreamEndCapture(s, &graph);
       if (e != cudaSuccess) return cuda_fail(c, e, "graph capture");
       if (e2 != cudaSuccess) return cuda_fail(c, e2, "graph capture end");
@@ -520,12 +538,12 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
     }
     CK(cudaGraphLaunch(g.exec, s));
   } else {
-    CK(enqueue());
+    CK(enqueue(false));
   }
   CK(cudaStreamSynchronize(s));
   uint32_t status = (uint32_t)(c->h_misc.p[6] & 0xffffffffu);
   float ms = 0.0f;
-  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
   c->last.tasks = c->h_misc.p[1];
   c->last.sad_candidates = c->h_misc.p[2];
   c->last.satd_candidates = c->h_misc.p[3];
@@ -619,7 +637,16 @@ int rme_picture_upload(void* ctx, int32_t pic_id, const rme_picture_desc* d, con
   pic->planes.plane_elems = (int64_t)stride * rows;
   pic->planes.origin = pic->pad * stride + pic->pad;
   pic->bytes = (size_t)pic->planes.plane_elems * bps * pic->nplanes + 256;
-  CK(cudaMalloc(&pic->buf, pic->bytes));
+  // Re-uploading an id with the same format reuses its device buffer (a
+  // stream's picture slots are refilled every frame).
+  auto old = c->pics.find(pic_id);
+  if (old != c->pics.end() && old->second->bytes == pic->bytes && old->second->planes.stride == stride) {
+    CK(cudaStreamSynchronize(s));
+    pic->buf = old->second->buf;
+    old->second->buf = nullptr;
+  } else {
+    CK(cudaMalloc(&pic->buf, pic->bytes));
+  }
   pic->planes.base = pic->buf;
   size_t src_bytes = (size_t)d->width * d->height * bps;
   CK(c->d_stage.ensure(src_bytes));
@@ -636,7 +663,7 @@ int rme_picture_upload(void* ctx, int32_t pic_id, const rme_picture_desc* d, con
   // The staging buffer is reused by the next upload: finish this one.
   CK(cudaStreamSynchronize(s));
   float ms = 0.0f;
-  cudaEventElapsedTime(&ms, c->evp0, c->evp1);
+  CK(cudaEventElapsedTime(&ms, c->evp0, c->evp1));
   c->planes_ms_acc += ms;
   c->pics[pic_id] = std::move(pic);
   return 0;
@@ -672,6 +699,20 @@ int rme_picture_release(void* ctx, int32_t pic_id) {
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   c->pics.erase(it);
+  return 0;
+}
+
+int rme_picture_build_planes(void* ctx, int32_t pic_id, void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return RME_EINVAL;
+  Picture* p;
+  int rc = picture_of(c, pic_id, &p);
+  if (rc) return rc;
+  if (!p->is_ref) return fail(c, RME_EINVAL, "picture was uploaded without as_ref");
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  CK(cudaSetDevice(c->device));
+  if (p->d.codec == RME_CODEC_H264) CK(launch_h264_hpel(p->planes, p->d.bit_depth, p->cw, p->ch, p->pad, s));
+  else CK(launch_hevc_phases(p->planes, p->d.bit_depth, p->cw, p->ch, p->pad, s));
   return 0;
 }
 

@@ -1009,8 +1009,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) search_kernel(LaunchDesc 
 int search_blocks_per_sm(int) {
   int n = 0;
   size_t smem = sizeof(WarpSmem) * kWarpsPerBlock;
-  cudaFuncSetAttribute(search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, search_kernel, kWarpsPerBlock * 32, smem);
+  if (cudaFuncSetAttribute(search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, search_kernel, kWarpsPerBlock * 32, smem) != cudaSuccess)
+    return 1;
   return n;
 }
 

@@ -63,6 +63,10 @@ class MotionSearch:
         self._check(self._lib.rme_picture_upload_chroma(self.ctx, pic_id, capi.ptr(cb), capi.ptr(cr),
                                                         cb.shape[1], None))
 
+    def build_planes(self, pic_id: int, stream: int = 0) -> None:
+        """Rebuild a resident reference's search planes (asynchronous)."""
+        self._check(self._lib.rme_picture_build_planes(self.ctx, pic_id, C.c_void_p(stream)))
+
     def release(self, pic_id: int) -> None:
         self._check(self._lib.rme_picture_release(self.ctx, pic_id))
         self._desc.pop(pic_id, None)
@@ -102,7 +106,7 @@ class MotionSearch:
         return n.value
 
     def search(self, src_id: int, ref_ids: Sequence[int], params: capi.Params,
-               jobs: np.ndarray | None = None) -> np.ndarray:
+               jobs: np.ndarray | None = None, stream: int = 0) -> np.ndarray:
         """One frame; results as a structured array (capi.RESULT_DTYPE)."""
         if jobs is not None:
             jobs = np.ascontiguousarray(jobs, capi.JOB_DTYPE)
@@ -110,11 +114,11 @@ class MotionSearch:
         n = self.result_count(src_id, ref_ids, params, jobs)
         out = np.zeros(n, capi.RESULT_DTYPE)
         self._check(self._lib.rme_frame_search(self.ctx, C.byref(f), C.byref(params),
-                                               C.cast(out.ctypes.data, C.POINTER(capi.Result)), None))
+                                               C.cast(out.ctypes.data, C.POINTER(capi.Result)), C.c_void_p(stream)))
         return out
 
     def search_batch(self, frames: Sequence[tuple[int, Sequence[int]]],
-                     params: capi.Params | Sequence[capi.Params]) -> list[np.ndarray]:
+                     params: capi.Params | Sequence[capi.Params], stream: int = 0) -> list[np.ndarray]:
         """Many STANDALONE frames (src_id, ref_ids) in one persistent launch."""
         n = len(frames)
         if isinstance(params, capi.Params):
@@ -126,7 +130,7 @@ class MotionSearch:
         offs[1:] = np.cumsum(counts)[:-1]
         out = np.zeros(int(sum(counts)), capi.RESULT_DTYPE)
         self._check(self._lib.rme_batch_search(self.ctx, fa, pa, n, C.cast(out.ctypes.data, C.POINTER(capi.Result)),
-                                               offs.ctypes.data_as(C.POINTER(C.c_int64)), None))
+                                               offs.ctypes.data_as(C.POINTER(C.c_int64)), C.c_void_p(stream)))
         return [out[o:o + c] for o, c in zip(offs, counts)]
 
     def stats(self) -> capi.Stats:
