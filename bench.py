@@ -341,21 +341,27 @@ def run_ours(args, world, rank, local):
     ms.close()
 
 
-def profile_case():
-    """One 1080p frame (2 references) searched twice through the per-frame
-    path: the case the ncu captures of the search kernel run on (about
-    130 MB on the device, inputs larger than L2)."""
+def profile_case(kind: str):
+    """The cases the ncu captures of the search kernel run on: one 1080p
+    frame (2 references, about 130 MB on the device) through the per-frame
+    path, or 8 frames (10 pictures, about 420 MB) in one batched launch;
+    each searched twice. Inputs are larger than L2 in both."""
     import rivet_h26x_codecs_b200 as rme
     import rivet_h26x_codecs_b200.capi as capi
     from rivet_h26x_codecs_b200 import synth
-    seq = synth.make_sequence(synth.HEVC, WIDTH, HEIGHT, 8, 3, synth.seed_for(1), 64, 160, 2.0)
+    n = 3 if kind == "frame" else 10
+    seq = synth.make_sequence(synth.HEVC, WIDTH, HEIGHT, 8, n, synth.seed_for(1), 64, 160, 2.0)
     with rme.MotionSearch(0) as ms:
         for i, f in enumerate(seq.frames):
             ms.upload(i, f, capi.RME_CODEC_HEVC, 8, as_ref=True)
         p = hevc_params()
         for _ in range(2):
-            ms.search(2, [1, 0], p)
-    print("profile case done")
+            if kind == "frame":
+                ms.search(2, [1, 0], p)
+            else:
+                ms.search_batch([(t, [t - 1, t - 2]) for t in range(2, n)], p)
+        st = ms.stats()
+        print(f"profile case {kind}: kernel {st.kernel_ms:.3f} ms, tasks {st.tasks}")
 
 
 def main():
@@ -366,12 +372,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--ref-frames", type=int, default=8, help="reference arm: frames per step sample")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--profile-case", action="store_true",
-                    help="small case for ncu: 3 pictures, one frame searched twice, nothing else")
+    ap.add_argument("--profile-case", choices=["frame", "batch"], default=None,
+                    help="small case for ncu: one frame (3 pictures) or a batch of 8 frames, searched twice")
     args = ap.parse_args()
     world, rank, local = dist_setup(args)
     if args.profile_case:
-        profile_case()
+        profile_case(args.profile_case)
         return
     try:
         if args.impl == "reference":

@@ -131,7 +131,9 @@ SIGNATURES = {
 }
 
 PACKAGE_DIR = Path(__file__).resolve().parent
-LIB_PATH = PACKAGE_DIR / "librivet_me.so"
+# RIVET_ME_LIB selects another build of the same library (e.g. a variant
+# compiled with other settings); by default the in-tree build is loaded.
+LIB_PATH = Path(os.environ.get("RIVET_ME_LIB", PACKAGE_DIR / "librivet_me.so"))
 
 _lib = None
 

@@ -122,14 +122,14 @@ struct Picture {
 };
 
 struct Tables {
-  uint16_t* tab = nullptr;       // H.264
-  uint32_t* lam_bits = nullptr;  // HEVC
-  float lam = 0.0f;
+  uint16_t* tab = nullptr;  // H.264 MvCostTable
+  float lam = 0.0f;         // the Lagrangian (H.264 lambda_satd; HEVC lam)
 };
 
-struct Order {  // task order of one frame shape, and the keys it sorts by
-  std::vector<uint32_t> tasks;
-  std::vector<uint32_t> keys;
+struct Deps {  // the dependency structure of one frame shape
+  int32_t* pending = nullptr;    // device: per task, how many tasks it reads
+  std::vector<uint32_t> ready;   // tasks that read none, in order
+  size_t ntasks = 0;
 };
 
 struct Graph {
@@ -138,37 +138,37 @@ struct Graph {
 };
 
 struct Ctx {
-  int device = 0, nsm = 0, bps = 0;
+  int device = 0, nsm = 0, bps8 = 0, bps16 = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp0 = nullptr, evp1 = nullptr;
   std::map<int, std::unique_ptr<Picture>> pics;
   std::map<std::tuple<int, int, int, uint32_t>, Tables> tables;
-  std::map<std::vector<int64_t>, Order> orders;
+  std::map<std::vector<int64_t>, Deps> deps;
   std::string err;
-  int32_t epoch = 0;
+  uint32_t epoch = 0;
   rme_stats last{};
   // launch buffers
   DevBuf<FrameDesc> d_frames;
-  DevBuf<uint32_t> d_queue;
+  DevBuf<unsigned long long> d_ready;  // the dataflow queue's slots
   DevBuf<rme_result> d_out;
-  DevBuf<int32_t> d_flags;
+  DevBuf<int32_t> d_pending;
   DevBuf<rme_job> d_jobs;
   DevBuf<unsigned long long> d_misc;  // head, counters[5], status
   DevBuf<uint8_t> d_stage;            // upload staging
   PinBuf<FrameDesc> h_frames;
   PinBuf<rme_result> h_out;
   PinBuf<unsigned long long> h_misc;
-  std::vector<uint32_t> queue_key;  // identity of what d_queue holds
-  std::vector<int64_t> queue_sig;
+  PinBuf<unsigned long long> h_init;  // [misc header | initial queue entries]
+
   std::map<std::vector<int64_t>, Graph> graphs;
   float planes_ms_acc = 0.0f;
   ~Ctx() {
     for (auto& g : graphs)
       if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
-    for (auto& t : tables) {
+    for (auto& d : deps)
+      if (d.second.pending) cudaFree(d.second.pending);
+    for (auto& t : tables)
       if (t.second.tab) cudaFree(t.second.tab);
-      if (t.second.lam_bits) cudaFree(t.second.lam_bits);
-    }
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (evp0) cudaEventDestroy(evp0);
@@ -276,48 +276,55 @@ const Tables* get_tables(Ctx* c, const rme_params* p, int bd, int* rc) {
       return nullptr;
     }
   } else {
-    std::vector<uint32_t> lb(kLamBits);
-    float lam = hevc_lambda(p->qp, bd, scale);
-    for (int b = 0; b < kLamBits; ++b) lb[b] = (uint32_t)(lam * (float)b);
-    t.lam = lam;
-    cudaError_t e = cudaMalloc(&t.lam_bits, kLamBits * sizeof(uint32_t));
-    if (e == cudaSuccess) e = cudaMemcpy(t.lam_bits, lb.data(), kLamBits * sizeof(uint32_t), cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) {
-      *rc = cuda_fail(c, e, "table upload");
-      return nullptr;
-    }
+    t.lam = hevc_lambda(p->qp, bd, scale);
   }
   return &(c->tables[key] = t);
 }
 
-// The STANDALONE task order of a frame shape: tasks sorted by a wavefront
-// key under which every task comes after the tasks it reads (HEVC: the
-// 8x8-unit anti-diagonal of the block's corner, larger blocks first at a
-// tie, so left, upper and enclosing blocks precede; H.264: mx + 2 my, so
-// A, B, C and D precede).
-const Order& get_order(Ctx* c, const rme_picture_desc& d, const rme_params* p, int nref) {
+// The STANDALONE dependency structure of a frame shape: per task how many
+// other tasks' results it reads (HEVC: the left and upper blocks of its
+// level, the enclosing block of the next larger evaluated size; H.264: the
+// A, B, C and D macroblocks), and the tasks that read none. The kernel
+// releases exactly these edges (rme_search.cu), so every count reaches zero.
+const Deps* get_deps(Ctx* c, const rme_picture_desc& d, const rme_params* p, int nref, int* rc) {
   std::vector<int64_t> sig = {d.codec, d.width, d.height, nref, d.codec == RME_CODEC_HEVC ? p->hevc_pu_mask : 0};
-  auto it = c->orders.find(sig);
-  if (it != c->orders.end()) return it->second;
-  Order o;
-  std::vector<int32_t> blocks(4 * (size_t)count_blocks(&d, p, nullptr));
-  int nb = count_blocks(&d, p, blocks.data());
-  int per = d.codec == RME_CODEC_H264 ? 1 : nref;
-  std::vector<std::pair<uint32_t, uint32_t>> kt;
-  kt.reserve((size_t)nb * per);
-  for (int b = 0; b < nb; ++b) {
-    int x = blocks[4 * b], y = blocks[4 * b + 1];
-    uint32_t key = d.codec == RME_CODEC_H264 ? (uint32_t)(x / 16 + 2 * (y / 16)) : (uint32_t)(x / 8 + y / 8);
-    for (int r = 0; r < per; ++r) kt.push_back({key, (uint32_t)(b * per + r)});
+  auto it = c->deps.find(sig);
+  if (it != c->deps.end()) return &it->second;
+  std::vector<int32_t> pend;
+  Deps dp;
+  if (d.codec == RME_CODEC_H264) {
+    const int mbw = (d.width + 15) / 16, mbh = (d.height + 15) / 16;
+    for (int my = 0; my < mbh; ++my)
+      for (int mx = 0; mx < mbw; ++mx)
+        pend.push_back((mx > 0) + (my > 0) + (my > 0 && mx + 1 < mbw) + (mx > 0 && my > 0));
+  } else {
+    int sizes[4];
+    const int nl = level_sizes(p, sizes);
+    for (int l = 0; l < nl; ++l) {
+      const int N = sizes[l], nbx = d.width / N, nby = d.height / N;
+      for (int by = 0; by < nby; ++by)
+        for (int bx = 0; bx < nbx; ++bx) {
+          bool parent = false;
+          if (l > 0) {
+            const int Np = sizes[l - 1];
+            parent = bx * N / Np < d.width / Np && by * N / Np < d.height / Np;
+          }
+          for (int r = 0; r < nref; ++r) pend.push_back((bx > 0) + (by > 0) + parent);
+        }
+    }
   }
-  std::stable_sort(kt.begin(), kt.end(), [](auto& a, auto& b) { return a.first < b.first; });
-  o.tasks.resize(kt.size());
-  o.keys.resize(kt.size());
-  for (size_t i = 0; i < kt.size(); ++i) {
-    o.tasks[i] = kt[i].second;
-    o.keys[i] = kt[i].first;
+  for (size_t t = 0; t < pend.size(); ++t)
+    if (pend[t] == 0) dp.ready.push_back((uint32_t)t);
+  dp.ntasks = pend.size();
+  cudaError_t e = cudaMalloc(&dp.pending, std::max<size_t>(pend.size(), 1) * sizeof(int32_t));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(dp.pending, pend.data(), pend.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    if (dp.pending) cudaFree(dp.pending);
+    *rc = cuda_fail(c, e, "dependency template");
+    return nullptr;
   }
-  return c->orders[sig] = std::move(o);
+  return &(c->deps[sig] = std::move(dp));
 }
 
 int picture_of(Ctx* c, int id, Picture** out) {
@@ -359,7 +366,7 @@ int make_frame(Ctx* c, const rme_frame* f, const rme_params* p, FrameDesc* fd, r
     fd->search_range = p->hevc_search_range;
     fd->search_rings = p->hevc_search_rings;
     fd->quarter_cross = p->hevc_quarter_cross;
-    fd->lam_bits = t->lam_bits;
+    fd->lam = t->lam;
     int sizes[4];
     fd->nlevels = level_sizes(p, sizes);
     for (int l = 0; l < fd->nlevels; ++l) {
@@ -399,7 +406,7 @@ int make_frame(Ctx* c, const rme_frame* f, const rme_params* p, FrameDesc* fd, r
     *ntasks = fd->codec == RME_CODEC_H264 ? nb : nb * f->nref;
   }
   fd->out = dout;
-  fd->flags = dflags;
+  fd->pending = dflags;
   fd->ntasks = *ntasks;
   return 0;
 }
@@ -422,40 +429,61 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   const int64_t total = toff[n];
   for (int i = 0; i < n; ++i)
     if (ntask[i] >= (1 << 24)) return fail(c, RME_EINVAL, "more than 2^24 tasks in one frame");
+  // `out` may be device memory: the kernels then write it directly.
+  cudaPointerAttributes pa{};
+  const bool dev_out = cudaPointerGetAttributes(&pa, out) == cudaSuccess && pa.type == cudaMemoryTypeDevice;
+  cudaGetLastError();  // a host pointer unknown to CUDA is not an error here
   CK(c->d_frames.ensure(n));
-  CK(c->d_out.ensure(std::max<int64_t>(total, 1)));
-  int32_t* old_flags = c->d_flags.p;
-  CK(c->d_flags.ensure(std::max<int64_t>(total, 1)));
-  // Fresh flag memory holds arbitrary words, any of which could equal an
-  // epoch: zero it (epochs start at 1).
-  if (c->d_flags.p != old_flags) c->epoch = 0;
-  CK(c->d_queue.ensure(std::max<int64_t>(total, 1)));
+  if (!dev_out) CK(c->d_out.ensure(std::max<int64_t>(total, 1)));
+  CK(c->d_pending.ensure(std::max<int64_t>(total, 1)));
+  unsigned long long* old_ready = c->d_ready.p;
+  CK(c->d_ready.ensure(std::max<int64_t>(total, 1)));
+  // Fresh slot memory may hold any word, an epoch's among them: zero it
+  // (epochs start at 1).
+  if (c->d_ready.p != old_ready) c->epoch = 0;
   CK(c->d_jobs.ensure(std::max<int64_t>(jobs_off[n], 1)));
-  CK(c->d_misc.ensure(8));
-  CK(c->h_out.ensure(std::max<int64_t>(total, 1)));
-  CK(c->h_misc.ensure(8));
-  if (c->epoch == 0) CK(cudaMemsetAsync(c->d_flags.p, 0, c->d_flags.n * sizeof(int32_t), s));
-  ++c->epoch;
-  if (c->epoch == INT32_MAX) {
-    c->epoch = 1;
-    CK(cudaMemsetAsync(c->d_flags.p, 0, c->d_flags.n * sizeof(int32_t), s));
+  CK(c->d_misc.ensure(16));
+  if (!dev_out) CK(c->h_out.ensure(std::max<int64_t>(total, 1)));
+  CK(c->h_misc.ensure(16));
+  if (c->epoch == 0 || c->epoch == 0xffffffffu) {
+    CK(cudaMemsetAsync(c->d_ready.p, 0, c->d_ready.n * sizeof(unsigned long long), s));
+    c->epoch = 0;
   }
-  // Pass 2: device pointers, queue.
+  ++c->epoch;
+  // Pass 2: device pointers; the queue's initial entries (8-bit frames'
+  // tasks first, then deeper ones: each part is one kernel launch of its
+  // own sample width, with its own part of the slots).
   std::vector<int64_t> sig;
   sig.push_back(n);
+  sig.push_back(dev_out);
+  std::vector<unsigned long long> init[2];
+  int64_t part_tasks[2] = {0, 0};
+  for (int i = 0; i < n; ++i) part_tasks[c->h_frames.p[i].bd > 8] += ntask[i];
+  std::vector<std::pair<const int32_t*, int>> pend_copies;  // (template, frame)
   for (int i = 0; i < n; ++i) {
     FrameDesc& fd = c->h_frames.p[i];
-    fd.out = c->d_out.p + toff[i];
-    fd.flags = c->d_flags.p + toff[i];
-    fd.epoch = c->epoch;
+    const int wide = fd.bd > 8;
+    fd.out = dev_out ? out + (offsets ? offsets[i] : toff[i]) : c->d_out.p + toff[i];
+    fd.pending = c->d_pending.p + toff[i];
+    const unsigned long long tag = ((unsigned long long)c->epoch << 32) | ((unsigned long long)i << 24);
     if (params[i].predictor_mode == RME_PRED_GIVEN) {
       fd.jobs = c->d_jobs.p + jobs_off[i];
       if (frames[i].njobs > 0)
         CK(cudaMemcpyAsync(c->d_jobs.p + jobs_off[i], frames[i].jobs, sizeof(rme_job) * frames[i].njobs,
                            cudaMemcpyHostToDevice, s));
+      for (int t = 0; t < ntask[i]; ++t) init[wide].push_back(tag | (uint32_t)t);
       sig.push_back(-1);
       sig.push_back(frames[i].njobs);
+      sig.push_back(fd.bd);
     } else {
+      Picture* src;
+      picture_of(c, frames[i].src_id, &src);
+      int rc = 0;
+      const Deps* dp = get_deps(c, src->d, &params[i], frames[i].nref, &rc);
+      if (!dp) return rc;
+      pend_copies.emplace_back(dp->pending, i);
+      for (uint32_t t : dp->ready) init[wide].push_back(tag | t);
+      sig.push_back(fd.bd);
       sig.push_back(fd.codec);
       sig.push_back(fd.width);
       sig.push_back(fd.height);
@@ -463,55 +491,65 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
       sig.push_back(params[i].hevc_pu_mask);
     }
   }
-  if (sig != c->queue_sig) {
-    // The merged queue: every frame's tasks in its own order, frames
-    // interleaved by their progress through that order (key / max key),
-    // so the launch advances all frames' wavefronts together.
-    std::vector<std::tuple<double, int, uint32_t>> all;
-    all.reserve(total);
-    for (int i = 0; i < n; ++i) {
-      if (params[i].predictor_mode == RME_PRED_GIVEN) {
-        for (int t = 0; t < ntask[i]; ++t) all.emplace_back((double)t / std::max(ntask[i], 1), i, (uint32_t)t);
-        continue;
-      }
-      Picture* src;
-      picture_of(c, frames[i].src_id, &src);
-      const Order& o = get_order(c, src->d, &params[i], frames[i].nref);
-      double mk = o.keys.empty() ? 1.0 : (double)o.keys.back() + 1.0;
-      for (size_t k = 0; k < o.tasks.size(); ++k) all.emplace_back((double)o.keys[k] / mk, i, o.tasks[k]);
-    }
-    if (n > 1) std::stable_sort(all.begin(), all.end(), [](auto& a, auto& b) {
-      return std::get<0>(a) < std::get<0>(b) || (std::get<0>(a) == std::get<0>(b) && std::get<1>(a) < std::get<1>(b));
+  // Frames' first tasks interleaved, so every frame starts at once.
+  for (int w = 0; w < 2; ++w)
+    std::stable_sort(init[w].begin(), init[w].end(), [](unsigned long long a, unsigned long long b) {
+      return (a & 0xffffffu) < (b & 0xffffffu);
     });
-    std::vector<uint32_t> q(total);
-    for (int64_t k = 0; k < total; ++k) q[k] = ((uint32_t)std::get<1>(all[k]) << 24) | std::get<2>(all[k]);
-    CK(cudaMemcpyAsync(c->d_queue.p, q.data(), sizeof(uint32_t) * total, cudaMemcpyHostToDevice, s));
-    CK(cudaStreamSynchronize(s));
-    c->queue_sig = sig;
-  }
-  LaunchDesc L;
-  L.frames = c->d_frames.p;
-  L.queue = c->d_queue.p;
-  L.total = total;
-  L.head = c->d_misc.p;
-  L.counters = c->d_misc.p + 1;
-  L.status = reinterpret_cast<uint32_t*>(c->d_misc.p + 6);
-  if (!c->bps) c->bps = std::max(1, search_blocks_per_sm(2));
-  int64_t want = (total + kWarpsPerBlock - 1) / kWarpsPerBlock;
-  int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)c->nsm * c->bps, want));
+  const int64_t n8 = part_tasks[0], n16 = part_tasks[1];
+  const size_t ninit = init[0].size() + init[1].size();
+  // h_init: [head8, tail8, head16, tail16, counters x5, status, epoch, pad x5 | entries]
+  CK(c->h_init.ensure(16 + ninit));
+  unsigned long long* hi = c->h_init.p;
+  std::memset(hi, 0, 16 * sizeof(unsigned long long));
+  hi[1] = init[0].size();
+  hi[3] = init[1].size();
+  hi[10] = c->epoch;
+  std::memcpy(hi + 16, init[0].data(), init[0].size() * sizeof(unsigned long long));
+  std::memcpy(hi + 16 + init[0].size(), init[1].data(), init[1].size() * sizeof(unsigned long long));
+  LaunchDesc L8, L16;
+  L8.frames = L16.frames = c->d_frames.p;
+  L8.ready = c->d_ready.p;
+  L16.ready = c->d_ready.p + n8;
+  L8.total = n8;
+  L16.total = n16;
+  L8.head = c->d_misc.p;
+  L8.tail = c->d_misc.p + 1;
+  L16.head = c->d_misc.p + 2;
+  L16.tail = c->d_misc.p + 3;
+  L8.counters = L16.counters = c->d_misc.p + 4;
+  L8.status = L16.status = reinterpret_cast<uint32_t*>(c->d_misc.p + 9);
+  L8.epoch = L16.epoch = reinterpret_cast<const uint32_t*>(c->d_misc.p + 10);
+  if (!c->bps8) c->bps8 = search_blocks_per_sm(1);
+  if (!c->bps16) c->bps16 = search_blocks_per_sm(2);
+  auto grid_for = [&](int64_t tasks, int bps) {
+    int64_t want = (tasks + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    return (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)c->nsm * bps, want));
+  };
+  const size_t n0 = init[0].size(), n1 = init[1].size();
   auto enqueue = [&](bool capturing) -> cudaError_t {
     const unsigned rec = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
     cudaError_t e = cudaMemcpyAsync(c->d_frames.p, c->h_frames.p, sizeof(FrameDesc) * n, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(c->d_misc.p, 0, 8 * sizeof(unsigned long long), s);
-    // Under capture the records are external ones: they become event-record
-    // nodes, so the kernel's device time is measured on every replay.
-    if (e == cudaSuccess) e = cudaEventRecordWithFlags(c->ev0, s, rec);
-    if (e == cudaSuccess) e = launch_search(L, 2, grid, s);
-    if (e == cudaSuccess) e = cudaEventRecordWithFlags(c->ev1, s, rec);
+    for (auto& pc : pend_copies)
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(c->d_pending.p + toff[pc.second], pc.first, sizeof(int32_t) * ntask[pc.second],
+                            cudaMemcpyDeviceToDevice, s);
     if (e == cudaSuccess)
+      e = cudaMemcpyAsync(c->d_misc.p, hi, 16 * sizeof(unsigned long long), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && n0)
+      e = cudaMemcpyAsync(c->d_ready.p, hi + 16, n0 * sizeof(unsigned long long), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && n1)
+      e = cudaMemcpyAsync(c->d_ready.p + n8, hi + 16 + n0, n1 * sizeof(unsigned long long), cudaMemcpyHostToDevice, s);
+    // Under capture the records are external ones: they become event-record
+    // nodes, so the kernels' device time is measured on every replay.
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(c->ev0, s, rec);
+    if (e == cudaSuccess && n8 > 0) e = launch_search(L8, 1, grid_for(n8, c->bps8), s);
+    if (e == cudaSuccess && n16 > 0) e = launch_search(L16, 2, grid_for(n16, c->bps16), s);
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(c->ev1, s, rec);
+    if (e == cudaSuccess && !dev_out)
       e = cudaMemcpyAsync(c->h_out.p, c->d_out.p, sizeof(rme_result) * total, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(c->h_misc.p, c->d_misc.p, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
+      e = cudaMemcpyAsync(c->h_misc.p, c->d_misc.p, 16 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
     return e;
   };
   bool has_given = false;
@@ -519,6 +557,8 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   if (use_graph && !has_given) {
     std::vector<int64_t> gsig = sig;
     gsig.push_back(total);
+    gsig.push_back((int64_t)n0);
+    gsig.push_back((int64_t)n1);
     gsig.push_back((int64_t)(uintptr_t)s);
     gsig.push_back((int64_t)g_buffer_generation);
     Graph& g = c->graphs[gsig];
@@ -541,18 +581,22 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
     CK(enqueue(false));
   }
   CK(cudaStreamSynchronize(s));
-  uint32_t status = (uint32_t)(c->h_misc.p[6] & 0xffffffffu);
+  uint32_t status = (uint32_t)(c->h_misc.p[9] & 0xffffffffu);
   float ms = 0.0f;
   CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
-  c->last.tasks = c->h_misc.p[1];
-  c->last.sad_candidates = c->h_misc.p[2];
-  c->last.satd_candidates = c->h_misc.p[3];
-  c->last.sad_samples = c->h_misc.p[4];
-  c->last.satd_samples = c->h_misc.p[5];
+  c->last.tasks = c->h_misc.p[4];
+  c->last.sad_candidates = c->h_misc.p[5];
+  c->last.satd_candidates = c->h_misc.p[6];
+  c->last.sad_samples = c->h_misc.p[7];
+  c->last.satd_samples = c->h_misc.p[8];
   c->last.kernel_ms = ms;
   c->last.planes_ms = c->planes_ms_acc;
   c->planes_ms_acc = 0.0f;
   if (status) return fail(c, RME_EDEVICE, "device status " + std::to_string(status));
+  if (c->last.tasks != (unsigned long long)total)
+    return fail(c, RME_EDEVICE, "the launch ran " + std::to_string(c->last.tasks) + " of " + std::to_string(total) +
+                                    " tasks");
+  if (dev_out) return 0;
   for (int i = 0; i < n; ++i) {
     int64_t off = offsets ? offsets[i] : toff[i];
     std::memcpy(out + off, c->h_out.p + toff[i], sizeof(rme_result) * ntask[i]);

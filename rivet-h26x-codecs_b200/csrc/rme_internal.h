@@ -14,7 +14,6 @@ constexpr int kChromaPadHevc = 40;
 constexpr int kChromaPadH264 = 16;
 constexpr int kMvSpan = 4096;  // h264_hpel.rs MV_SPAN
 constexpr int kMvTab = 2 * kMvSpan + 1;
-constexpr int kLamBits = 96;   // HEVC rate table entries (mv_bits <= 71)
 constexpr int kMaxLevels = 4;
 constexpr int kWarpsPerBlock = 8;
 constexpr uint32_t kSpinLimit = 1u << 22;  // bounded dependency waits
@@ -46,7 +45,7 @@ struct FrameDesc {
   int32_t nlevels;
   int32_t size[kMaxLevels], nbx[kMaxLevels], nby[kMaxLevels], base[kMaxLevels + 1];
   int32_t search_range, search_rings, quarter_cross;
-  const uint32_t* lam_bits;  // (uint32)(lam * bits), bits < kLamBits
+  float lam;                 // SATD Lagrangian (rate = (lam * bits as f32) as u32)
   // H.264
   const uint16_t* tab;       // MvCostTable
   int32_t range, hpel_iters, qpel_iters, umh, qpel_diamond, dia, vr;
@@ -54,20 +53,26 @@ struct FrameDesc {
   uint32_t ref_cost[RME_MAX_REFS];
   // GIVEN
   const rme_job* jobs;
-  // outputs and dependency flags (one per result)
+  // outputs, and per task the count of its unfinished dependencies
   rme_result* out;
-  int32_t* flags;
-  int32_t epoch;
+  int32_t* pending;
   int32_t ntasks;
 };
 
+// A launch's dataflow queue: a task is pushed when its last dependency
+// finishes (the frames' dependency-free tasks are pushed by the host), and
+// warps pop in push order. Slots hold (epoch << 32) | (frame << 24) | task,
+// so a slot of an earlier launch never reads as filled.
 struct LaunchDesc {
   const FrameDesc* frames;
-  const uint32_t* queue;  // (frame << 24) | task, topological order
-  int64_t total;
-  unsigned long long* head;
+  unsigned long long* ready;     // capacity `total`
+  int64_t total;                 // tasks of this launch (= pushes = pops)
+  unsigned long long* head;      // next slot to pop
+  unsigned long long* tail;      // next slot to push (starts at the host's count)
   uint32_t* status;
   unsigned long long* counters;  // [tasks, sad, satd, sad_samples, satd_samples]
+  const uint32_t* epoch;         // this launch's epoch (device memory: a
+                                 // replayed graph keeps its arguments)
 };
 
 // Launch wrappers (defined in the .cu files).

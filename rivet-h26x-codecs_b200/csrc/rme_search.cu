@@ -18,13 +18,15 @@
 //          its three-new-points continuation, the square; half- then
 //          quarter-sample rings that skip points within one step of the
 //          previous centre; SAD / SATD + MvCostTable rate, strict <.
-// The reference scores one candidate at a time; here a warp scores every
-// candidate of a step together (they are all known before the step: each
-// ring is around a centre fixed for the step) and then accepts them in the
-// reference's order with its strict <, so the chosen vector, its cost and
-// the candidate counts are the reference's (the sum for a candidate does
-// not depend on when it is taken, and a point equal to the current best
-// has the best cost, so a strict < never takes it).
+//
+// The reference scores one candidate at a time and takes it when strictly
+// cheaper than the best so far. Every candidate of a step is known before
+// the step (each ring is around a centre fixed for the step), so here a
+// warp scores them together: a group of lanes per candidate computes its
+// distortion and its rate, and the step's outcome is the warp minimum —
+// the lowest-indexed candidate among those of least cost, taken when below
+// the best. That is exactly the sequential strict-< walk: it ends on the
+// least cost, and on the first candidate reaching it.
 //
 // Distortion: 8-bit SAD is __vsadu4 over four packed samples, 10/12-bit
 // __vsadu2 over two (packed 16-bit lanes); SATD is the 4x4 Hadamard of
@@ -35,12 +37,13 @@
 //
 // Scheduling: in STANDALONE mode a task's seeds come from other tasks'
 // results (its left and upper neighbours at the same size, the enclosing
-// block one size up; H.264: the A, B, C / D macroblocks). The queue lists
-// every frame's tasks in an order where each task comes after everything
-// it reads, so a warp that claims a task only ever waits on tasks claimed
-// earlier by warps that are running; each wait is bounded (kSpinLimit
-// polls with backoff) and a wait that runs out sets a status bit the host
-// turns into RME_EDEVICE instead of hanging.
+// block one size up; H.264: the A, B, C and D macroblocks). Each task has a
+// count of those; a finishing task decrements its readers' counts and
+// pushes onto the launch's ready queue each one it brings to zero, so a
+// warp only ever takes a task whose inputs are complete. The only wait is
+// for the queue itself (a slot not yet pushed: nothing is ready anywhere);
+// it is bounded (kSpinLimit polls with backoff), and a wait that runs out
+// sets a status bit the host turns into RME_EDEVICE instead of hanging.
 #include <cuda_runtime.h>
 
 #include "rme_internal.h"
@@ -48,26 +51,40 @@
 namespace rme {
 namespace {
 
-constexpr int kMaxBlk = 64;
+// Resident blocks per SM the register allocation is bounded for (a build
+// setting: more blocks hide more latency, fewer leave more registers).
+#ifndef RME_MIN_BLOCKS
+#define RME_MIN_BLOCKS 3
+#endif
 
+constexpr int kMaxBlk = 64;
+constexpr uint32_t kInf = 0xffffffffu;
+constexpr unsigned kFull = 0xffffffffu;
+
+template <class S>
 struct alignas(16) WarpSmem {
-  uint32_t src[kMaxBlk * kMaxBlk / 2];  // source block as 32-bit words (row stride w*bytes/4)
-  int cx[32], cy[32];                   // candidates of the step
-  uint32_t cost[32];                    // their SAD or SATD
-  const void* p1[32];                   // SATD: first plane view of each candidate
-  const void* p2[32];                   //       second view to average with (H.264), or null
-  int tx[16], ty[16];                   // seed staging / tried
-  int n;
+  uint32_t src[kMaxBlk * kMaxBlk * sizeof(S) / 4];  // source block as words, row stride w*sizeof(S)/4
+  int ux[32], uy[32];                               // UMH candidates of a pass (in-order counting)
+  uint32_t uc[32];
+  unsigned long long cnt[5];                        // tasks, SAD / SATD candidates and samples
 };
 
 // ---- memory helpers --------------------------------------------------------
-__device__ __forceinline__ int ld_acquire(const int32_t* p) {
-  int v;
-  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+__device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
-__device__ __forceinline__ void st_release(int32_t* p, int v) {
-  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ void st_release64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+// Decrement with acquire-release order: the decrement that reaches zero
+// has observed every earlier decrementer's writes (their results), and its
+// push publishes them all to the task's popper.
+__device__ __forceinline__ int dec_acq_rel(int32_t* p) {
+  int old;
+  asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], -1;" : "=r"(old) : "l"(p) : "memory");
+  return old;
 }
 
 // Four 8-bit or two 16-bit samples starting at any sample address.
@@ -109,98 +126,163 @@ __device__ __forceinline__ uint32_t satd4x4(int d[16]) {
   return (sum + 1) >> 1;
 }
 
-// Lanes per candidate: the largest of 8/4/2/1 (SAD) or 4/2/1 (SATD) that
-// divides the candidate's work items, so each lane of a candidate's group
-// has the same number of items and a butterfly reduces the group.
-__device__ __forceinline__ int lanes_for(int items, int maxl) {
-  return (maxl >= 8 && (items & 7) == 0) ? 8 : ((items & 3) == 0 ? 4 : ((items & 1) == 0 ? 2 : 1));
+// Lanes per candidate for a step of n candidates: as many candidates per
+// pass as the step has (one pass when n <= 32), at most 32 lanes each.
+__device__ __forceinline__ int lanes_per(int n) { return n >= 32 ? 1 : 32 / max(n, 1); }
+
+// The sum over a group of `lpc` consecutive lanes (any width), in every
+// lane of the group.
+__device__ __forceinline__ uint32_t group_sum(uint32_t v, int lpc, int sub, int lane) {
+  for (int o = 1; o < lpc; o <<= 1) {
+    const uint32_t t = __shfl_down_sync(kFull, v, o);
+    if (sub + o < lpc) v += t;
+  }
+  return __shfl_sync(kFull, v, lane - sub);
 }
 
-// SAD of sm.cx/cy[0..n) (whole-sample offsets from the block at `org`).
-template <class S>
-__device__ __noinline__ void sad_batch(WarpSmem& sm, const S* org, int stride, int w, int h, int n, int lane) {
+// The warp's least cost and the lowest lane holding it. Lanes of one
+// candidate group hold the same cost, so that lane is the first lane of
+// the first candidate (in the step's order) reaching the least cost.
+struct Pick {
+  uint32_t cost;
+  int lane;
+};
+__device__ __forceinline__ Pick warp_min(uint32_t cost) {
+  uint32_t m = __reduce_min_sync(kFull, cost);
+  int l = __ffs(__ballot_sync(kFull, cost == m)) - 1;
+  return {m, l};
+}
+
+// N consecutive 32-bit words of samples starting at any sample address
+// (N + 1 aligned loads, all issued before any is used).
+template <int N>
+__device__ __forceinline__ void ldwords(const void* p, uint32_t (&out)[N]) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+  const uint32_t* q = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
+  const uint32_t sh = (uint32_t)(a & 3) * 8u;
+  uint32_t w[N + 1];
+#pragma unroll
+  for (int i = 0; i <= N; ++i) w[i] = __ldg(q + i);
+#pragma unroll
+  for (int i = 0; i < N; ++i) out[i] = __funnelshift_r(w[i], w[i + 1], sh);
+}
+
+// SAD of the candidate at whole-sample offset (fx, fy), split over the
+// group's lanes in chunks of CW words of a row, summed over the group.
+template <class S, int CW>
+__device__ __forceinline__ uint32_t sad_chunks(const uint32_t* src, int wr, int h, const S* rp, int stride, int lpc,
+                                               int sub) {
   constexpr int SPW = 4 / sizeof(S);
-  const int WR = w / SPW, IPC = WR * h;
-  const int LPC = lanes_for(IPC, 8), CPP = 32 / LPC, IPL = IPC / LPC;
-  const int sub = lane & (LPC - 1), grp = lane / LPC;
-  for (int c0 = 0; c0 < n; c0 += CPP) {
-    int c = c0 + grp;
-    uint32_t acc = 0;
-    if (c < n) {
-      const S* rp = org + (ptrdiff_t)sm.cy[c] * stride + sm.cx[c];
-      int row = sub / WR, wd = sub % WR;
-      for (int u = 0; u < IPL; ++u) {
-        acc += vsad(sm.src[row * WR + wd], ldw(rp + (ptrdiff_t)row * stride + wd * SPW), S());
-        wd += LPC;
-        while (wd >= WR) {
-          wd -= WR;
-          ++row;
-        }
+  const int nch = wr / CW, items = nch * h, rs = lpc / nch, cs = lpc % nch;
+  int row = sub / nch, col = sub % nch;
+  uint32_t acc = 0;
+  for (int i = sub; i < items; i += 2 * lpc) {
+    uint32_t a[CW], b[CW];
+    const int row2 = row + rs + (col + cs >= nch), col2 = (col + cs >= nch) ? col + cs - nch : col + cs;
+    const bool two = i + lpc < items;
+    ldwords<CW>(rp + (ptrdiff_t)row * stride + col * CW * SPW, a);
+    if (two) ldwords<CW>(rp + (ptrdiff_t)row2 * stride + col2 * CW * SPW, b);
+#pragma unroll
+    for (int k = 0; k < CW; ++k) acc += vsad(src[row * wr + col * CW + k], a[k], S());
+    if (two) {
+#pragma unroll
+      for (int k = 0; k < CW; ++k) acc += vsad(src[row2 * wr + col2 * CW + k], b[k], S());
+    }
+    row = row2 + rs;
+    col = col2 + cs;
+    if (col >= nch) {
+      col -= nch;
+      ++row;
+    }
+  }
+  return acc;
+}
+
+template <class S>
+__device__ __forceinline__ uint32_t group_sad(const uint32_t* src, int wr, int h, const S* org, int stride, int lpc,
+                                              int sub, int lane, bool ok, int fx, int fy) {
+  uint32_t acc = 0;
+  if (ok) {
+    const S* rp = org + (ptrdiff_t)fy * stride + fx;
+    if ((wr & 3) == 0) acc = sad_chunks<S, 4>(src, wr, h, rp, stride, lpc, sub);
+    else if ((wr & 1) == 0) acc = sad_chunks<S, 2>(src, wr, h, rp, stride, lpc, sub);
+    else acc = sad_chunks<S, 1>(src, wr, h, rp, stride, lpc, sub);
+  }
+  return group_sum(acc, lpc, sub, lane);
+}
+
+// SATD over strips of TS horizontally adjacent 4x4 tiles: the strip's four
+// rows of prediction samples are loaded (and averaged, H.264) first, then
+// each tile's Hadamard.
+template <class S, int TS>
+__device__ __forceinline__ uint32_t satd_strips(const uint32_t* src, int wr, int tw, int th, const S* p1,
+                                                const S* p2, int stride, int lpc, int sub) {
+  constexpr int SPW = 4 / sizeof(S);
+  constexpr int WPT = 4 / SPW;       // words per tile row
+  constexpr int WPS = TS * WPT;      // words per strip row
+  const int nspr = tw / TS, items = nspr * th;
+  uint32_t acc = 0;
+  for (int i = sub; i < items; i += lpc) {
+    const int ty = i / nspr, sx = i - ty * nspr;
+    uint32_t pw[4][WPS];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const ptrdiff_t off = (ptrdiff_t)(ty * 4 + r) * stride + sx * TS * 4;
+      ldwords<WPS>(p1 + off, pw[r]);
+      if (p2) {
+        uint32_t q[WPS];
+        ldwords<WPS>(p2 + off, q);
+#pragma unroll
+        for (int k = 0; k < WPS; ++k) pw[r][k] = vavg(pw[r][k], q[k], S());
       }
     }
-    for (int o = LPC >> 1; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (sub == 0 && c < n) sm.cost[c] = acc;
-  }
-  __syncwarp();
-}
-
-// SATD of the predictions sm.p1[k] (averaged with sm.p2[k] where set),
-// k < n, against the source block.
-template <class S>
-__device__ __noinline__ void satd_batch(WarpSmem& sm, int stride, int w, int h, int n, int lane) {
-  constexpr int SPW = 4 / sizeof(S);
-  const int WR = w / SPW, TW = w >> 2, TPC = TW * (h >> 2);
-  const int LPC = lanes_for(TPC, 4), CPP = 32 / LPC, IPL = TPC / LPC;
-  const int sub = lane & (LPC - 1), grp = lane / LPC;
-  for (int c0 = 0; c0 < n; c0 += CPP) {
-    int c = c0 + grp;
-    uint32_t acc = 0;
-    if (c < n) {
-      const S* a = (const S*)sm.p1[c];
-      const S* b = (const S*)sm.p2[c];
-      int ty = sub / TW, tx = sub % TW;
-      for (int u = 0; u < IPL; ++u) {
-        int d[16];
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          ptrdiff_t off = (ptrdiff_t)(ty * 4 + r) * stride + tx * 4;
-          const uint32_t* srow = &sm.src[(ty * 4 + r) * WR + tx * (4 / SPW)];
+    for (int t = 0; t < TS; ++t) {
+      int d[16];
 #pragma unroll
-          for (int k = 0; k < 4 / SPW; ++k) {
-            uint32_t pw = ldw(a + off + k * SPW);
-            if (b) pw = vavg(pw, ldw(b + off + k * SPW), S());
-            uint32_t sw = srow[k];
+      for (int r = 0; r < 4; ++r) {
+        const uint32_t* srow = &src[(ty * 4 + r) * wr + (sx * TS + t) * WPT];
 #pragma unroll
-            for (int e = 0; e < SPW; ++e) {
-              int sh = e * (32 / SPW);
-              uint32_t m = SPW == 4 ? 0xffu : 0xffffu;
-              d[r * 4 + k * SPW + e] = (int)((sw >> sh) & m) - (int)((pw >> sh) & m);
-            }
+        for (int k = 0; k < WPT; ++k) {
+          const uint32_t sw = srow[k], qw = pw[r][t * WPT + k];
+#pragma unroll
+          for (int e = 0; e < SPW; ++e) {
+            const int sh = e * (32 / SPW);
+            const uint32_t m = SPW == 4 ? 0xffu : 0xffffu;
+            d[r * 4 + k * SPW + e] = (int)((sw >> sh) & m) - (int)((qw >> sh) & m);
           }
         }
-        acc += satd4x4(d);
-        tx += LPC;
-        while (tx >= TW) {
-          tx -= TW;
-          ++ty;
-        }
       }
+      acc += satd4x4(d);
     }
-    for (int o = LPC >> 1; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (sub == 0 && c < n) sm.cost[c] = acc;
   }
-  __syncwarp();
+  return acc;
+}
+
+template <class S>
+__device__ __forceinline__ uint32_t group_satd(const uint32_t* src, int wr, int tw, int th, const S* p1, const S* p2,
+                                               int stride, int lpc, int sub, int lane, bool ok) {
+  // Strips of 16 bytes of prediction per row (four 8-bit tiles, two
+  // 16-bit ones) where the block is that wide.
+  constexpr int TSW = sizeof(S) == 1 ? 4 : 2;
+  uint32_t acc = 0;
+  if (ok) {
+    if (tw % TSW == 0) acc = satd_strips<S, TSW>(src, wr, tw, th, p1, p2, stride, lpc, sub);
+    else if ((tw & 1) == 0) acc = satd_strips<S, 2>(src, wr, tw, th, p1, p2, stride, lpc, sub);
+    else acc = satd_strips<S, 1>(src, wr, tw, th, p1, p2, stride, lpc, sub);
+  }
+  return group_sum(acc, lpc, sub, lane);
 }
 
 // The source block into shared memory as words.
 template <class S>
-__device__ __forceinline__ void stage_src(WarpSmem& sm, const S* org, int stride, int w, int h, int lane) {
+__device__ __forceinline__ void stage_src(uint32_t* dst, const S* org, int stride, int w, int h, int lane) {
   constexpr int SPW = 4 / sizeof(S);
-  const int WR = w / SPW;
+  const int wr = w / SPW;
   __syncwarp();
-  for (int i = lane; i < WR * h; i += 32) {
-    int row = i / WR, wd = i - row * WR;
-    sm.src[i] = ldw(org + (ptrdiff_t)row * stride + wd * SPW);
+  for (int i = lane; i < wr * h; i += 32) {
+    int row = i / wr, wd = i - row * wr;
+    dst[i] = ldw(org + (ptrdiff_t)row * stride + wd * SPW);
   }
   __syncwarp();
 }
@@ -210,30 +292,54 @@ __device__ __forceinline__ const S* plane_at(const DevPlanes& p, int plane, int 
   return (const S*)p.base + (int64_t)plane * p.plane_elems + p.origin + (int64_t)y * p.stride + x;
 }
 
-// Bounded wait for a dependency's flag (lane 0), then a warp barrier.
-__device__ __forceinline__ void wait_flag(const int32_t* f, int epoch, uint32_t* status, int lane) {
-  if (lane == 0) {
-    uint32_t ns = 32;
-    uint32_t it = 0;
-    while (ld_acquire(f) != epoch) {
-      if (++it >= kSpinLimit) {
-        atomicOr(status, kStatusWaitTimeout);
-        break;
-      }
-      __nanosleep(ns);
-      if (ns < 1024) ns <<= 1;
+// ---- dataflow queue ---------------------------------------------------------
+
+// Push task `t` of frame `f` (lane 0): its last dependency just finished.
+__device__ __forceinline__ void push_ready(const LaunchDesc& L, int f, int t) {
+  const unsigned long long idx = atomicAdd(L.tail, 1ull);
+  if (idx < (unsigned long long)L.total)
+    st_release64(L.ready + idx, ((unsigned long long)__ldg(L.epoch) << 32) | ((uint32_t)f << 24) | (uint32_t)t);
+  else
+    atomicOr(L.status, kStatusBadTask);
+}
+
+// One finished dependency of task `d` of frame `f` (lane 0).
+__device__ __forceinline__ void release(const LaunchDesc& L, const FrameDesc& F, int f, int d) {
+  if (dec_acq_rel(&F.pending[d]) == 1) push_ready(L, f, d);
+}
+
+// The entry in slot `idx` once pushed (lane 0; bounded wait with backoff),
+// or 0xffffffff when the wait runs out (status set).
+__device__ __forceinline__ uint32_t pop_slot(const LaunchDesc& L, unsigned long long idx, uint32_t epoch) {
+  uint32_t ns = 32, it = 0;
+  for (;;) {
+    const unsigned long long v = ld_acquire64(L.ready + idx);
+    if ((uint32_t)(v >> 32) == epoch) return (uint32_t)v;
+    if (++it >= kSpinLimit) {
+      atomicOr(L.status, kStatusWaitTimeout);
+      return 0xffffffffu;
     }
+    __nanosleep(ns);
+    if (ns < 256) ns <<= 1;
   }
-  __syncwarp();
 }
 
 __device__ __forceinline__ uint32_t ldcg_u32(const void* p) { return __ldcg((const unsigned int*)p); }
 __device__ __forceinline__ int mvx_of(uint32_t v) { return (int)(int16_t)(v & 0xffffu); }
 __device__ __forceinline__ int mvy_of(uint32_t v) { return (int)(int16_t)(v >> 16); }
 
-struct Counters {
-  unsigned long long tasks = 0, sad = 0, satd = 0, sad_samples = 0, satd_samples = 0;
-};
+// Per-warp totals of the work done, kept in shared memory (not registers)
+// and added to the launch's counters once at exit.
+template <class S>
+__device__ __forceinline__ void count_task(WarpSmem<S>& sm, int lane, uint32_t nsad, uint32_t nsatd, int area) {
+  if (lane == 0) {
+    sm.cnt[0] += 1;
+    sm.cnt[1] += nsad;
+    sm.cnt[2] += nsatd;
+    sm.cnt[3] += (unsigned long long)nsad * area;
+    sm.cnt[4] += (unsigned long long)nsatd * area;
+  }
+}
 
 __device__ __forceinline__ void write_result(rme_result* o, int mvx, int mvy, int ref, uint32_t cost, uint32_t satd,
                                              int imx, int imy, uint32_t icost, uint32_t nsad, uint32_t nsatd,
@@ -254,6 +360,7 @@ __device__ __forceinline__ void write_result(rme_result* o, int mvx, int mvy, in
   }
 }
 
+
 // ---- HEVC -------------------------------------------------------------------
 
 // mvd_component_bits (h265_search.rs:212-247) in closed form: 1 at zero,
@@ -263,18 +370,20 @@ __device__ __forceinline__ uint32_t hevc_cbits(int d) {
   uint32_t a = (uint32_t)abs(d);
   return a == 0 ? 1u : 3u + 2u * (31u - __clz(a));
 }
-__device__ __forceinline__ uint32_t hevc_rate(const FrameDesc& F, int mx, int my, const int pq[4]) {
-  uint32_t b0 = hevc_cbits(mx - pq[0]) + hevc_cbits(my - pq[1]);
-  uint32_t b1 = hevc_cbits(mx - pq[2]) + hevc_cbits(my - pq[3]);
-  uint32_t bits = min(b0, b1) + 1u;
-  return __ldg(&F.lam_bits[min(bits, (uint32_t)(kLamBits - 1))]);
+// (lam * mv_bits as f32) as u32 (h265_me.rs:3776, 3890): one IEEE
+// round-to-nearest multiply, truncated.
+__device__ __forceinline__ uint32_t hevc_rate(float lam, int mx, int my, int p0x, int p0y, int p1x, int p1y) {
+  uint32_t b0 = hevc_cbits(mx - p0x) + hevc_cbits(my - p0y);
+  uint32_t b1 = hevc_cbits(mx - p1x) + hevc_cbits(my - p1y);
+  return __float2uint_rz(__fmul_rn(lam, __uint2float_rn(min(b0, b1) + 1u)));
 }
 
 template <class S>
-__device__ void hevc_task(const FrameDesc& F, int t, WarpSmem& sm, int lane, uint32_t* status, Counters& cnt) {
+__device__ void hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, WarpSmem<S>& sm, int lane) {
   int r, x, y, w, h, ns;
-  int pq[4];
-  int32_t* flag = nullptr;
+  int p0x, p0y, p1x, p1y;
+  int sx = 0, sy = 0;  // this lane's seed (lane < ns)
+  int l = 0, lbx = 0, lby = 0, local = 0;  // STANDALONE: level and block
   rme_result* out;
   if (F.mode == RME_PRED_GIVEN) {
     const rme_job* j = &F.jobs[t];
@@ -284,266 +393,220 @@ __device__ void hevc_task(const FrameDesc& F, int t, WarpSmem& sm, int lane, uin
     w = j->w;
     h = j->h;
     ns = j->nseeds;
-    pq[0] = j->mvp[0].x;
-    pq[1] = j->mvp[0].y;
-    pq[2] = j->mvp[1].x;
-    pq[3] = j->mvp[1].y;
+    p0x = j->mvp[0].x;
+    p0y = j->mvp[0].y;
+    p1x = j->mvp[1].x;
+    p1y = j->mvp[1].y;
     if (lane < ns) {
-      sm.tx[lane] = j->seeds[lane].x;
-      sm.ty[lane] = j->seeds[lane].y;
+      sx = j->seeds[lane].x;
+      sy = j->seeds[lane].y;
     }
     out = &F.out[t];
   } else {
     r = t % F.nref;
-    int blk = t / F.nref, l = 0;
+    const int blk = t / F.nref;
     while (l + 1 < F.nlevels && blk >= F.base[l + 1]) ++l;
-    int local = blk - F.base[l], nbx = F.nbx[l];
-    int by = local / nbx, bx = local - by * nbx, N = F.size[l];
-    x = bx * N;
-    y = by * N;
+    local = blk - F.base[l];
+    const int nbx = F.nbx[l];
+    lby = local / nbx;
+    lbx = local - lby * nbx;
+    const int N = F.size[l];
+    x = lbx * N;
+    y = lby * N;
     w = h = N;
-    // AMVP pair from the left and upper results of this level, the parent
-    // seed from the enclosing block one evaluated size up.
-    int na = 0, ax = 0, ay = 0, bxv = 0, byv = 0;
-    if (bx > 0) {
-      int idx = (F.base[l] + local - 1) * F.nref + r;
-      wait_flag(&F.flags[idx], F.epoch, status, lane);
-      uint32_t v = ldcg_u32(&F.out[idx].mv);
+    // The AMVP pair from the left and upper results of this level, the
+    // parent seed from the enclosing block one evaluated size up (all of
+    // them finished: the task was queued after its last dependency).
+    int na = 0, ax = 0, ay = 0, cx = 0, cy = 0;
+    if (lbx > 0) {
+      const int idx = (F.base[l] + local - 1) * F.nref + r;
+      const uint32_t v = ldcg_u32(&F.out[idx].mv);
       ax = mvx_of(v);
       ay = mvy_of(v);
       na = 1;
     }
-    if (by > 0) {
-      int idx = (F.base[l] + local - nbx) * F.nref + r;
-      wait_flag(&F.flags[idx], F.epoch, status, lane);
-      uint32_t v = ldcg_u32(&F.out[idx].mv);
-      int qx = mvx_of(v), qy = mvy_of(v);
+    if (lby > 0) {
+      const int idx = (F.base[l] + local - nbx) * F.nref + r;
+      const uint32_t v = ldcg_u32(&F.out[idx].mv);
+      const int qx = mvx_of(v), qy = mvy_of(v);
       if (na == 0) {
         ax = qx;
         ay = qy;
         na = 1;
       } else if (qx != ax || qy != ay) {
-        bxv = qx;
-        byv = qy;
+        cx = qx;
+        cy = qy;
         na = 2;
       }
     }
-    pq[0] = na > 0 ? ax : 0;
-    pq[1] = na > 0 ? ay : 0;
-    pq[2] = na > 1 ? bxv : 0;
-    pq[3] = na > 1 ? byv : 0;
+    p0x = na > 0 ? ax : 0;
+    p0y = na > 0 ? ay : 0;
+    p1x = na > 1 ? cx : 0;
+    p1y = na > 1 ? cy : 0;
     ns = 3;
     int psx = 0, psy = 0;
-    bool parent = false;
     if (l > 0) {
-      int Np = F.size[l - 1], px = x / Np, py = y / Np;
+      const int Np = F.size[l - 1], px = x / Np, py = y / Np;
       if (px < F.nbx[l - 1] && py < F.nby[l - 1]) {
-        int idx = (F.base[l - 1] + py * F.nbx[l - 1] + px) * F.nref + r;
-        wait_flag(&F.flags[idx], F.epoch, status, lane);
-        uint32_t v = ldcg_u32(&F.out[idx].mv);
+        const int idx = (F.base[l - 1] + py * F.nbx[l - 1] + px) * F.nref + r;
+        const uint32_t v = ldcg_u32(&F.out[idx].mv);
         psx = mvx_of(v);
         psy = mvy_of(v);
-        parent = true;
+        ns = 4;
       }
     }
-    if (lane == 0) {
-      sm.tx[0] = 0;
-      sm.ty[0] = 0;
-      sm.tx[1] = pq[0];
-      sm.ty[1] = pq[1];
-      sm.tx[2] = pq[2];
-      sm.ty[2] = pq[3];
-      sm.tx[3] = psx;
-      sm.ty[3] = psy;
-    }
-    if (parent) ns = 4;
-    flag = &F.flags[t];
+    // seeds = [zero, mvp0, mvp1, parent] (h265_me.rs:1327-1348)
+    sx = lane == 1 ? p0x : lane == 2 ? p1x : lane == 3 ? psx : 0;
+    sy = lane == 1 ? p0y : lane == 2 ? p1y : lane == 3 ? psy : 0;
     out = &F.out[t];
   }
   const DevPlanes& R = F.ref[r];
-  const S* src = plane_at<S>(F.src, 0, x, y);
-  stage_src(sm, src, F.src.stride, w, h, lane);
+  stage_src<S>(sm.src, plane_at<S>(F.src, 0, x, y), F.src.stride, w, h, lane);
   const S* org = plane_at<S>(R, 0, x, y);
   const int stride = R.stride;
+  constexpr int SPW = 4 / sizeof(S);
+  const int wr = w / SPW, tw = w >> 2, th = h >> 2;
   const int padm = F.pad - 4;  // h265_search.rs MARGIN
   const int lox = -padm - x, hix = F.width + padm - w - x, loy = -padm - y, hiy = F.height + padm - h - y;
+  const float lam = F.lam;
   uint32_t nsad = 0, nsatd = 0;
 
-  // Seeds: >> 2, clamp_pos, dedupe through tried[16] (h265_me.rs:3785-3800).
-  if (lane == 0) {
-    int tx[16], ty[16];
+  // Seeds: >> 2, clamp_pos, dedupe (a seed equal to an earlier one is
+  // skipped: `tried`, h265_me.rs:3785-3800), scored in order.
+  const int qx = min(max(sx >> 2, lox), hix), qy = min(max(sy >> 2, loy), hiy);
+  bool dup = false;
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      tx[i] = INT32_MIN;
-      ty[i] = 0;
-    }
-    int n = 0;
-    for (int i = 0; i < ns; ++i) {
-      int cx = min(max(sm.tx[i] >> 2, lox), hix), cy = min(max(sm.ty[i] >> 2, loy), hiy);
-      bool seen = false;
-#pragma unroll
-      for (int k = 0; k < 16; ++k) seen |= (tx[k] == cx && ty[k] == cy);
-      if (seen) continue;
-#pragma unroll
-      for (int k = 0; k < 16; ++k)
-        if (k == i) {
-          tx[k] = cx;
-          ty[k] = cy;
-        }
-      sm.cx[n] = cx;
-      sm.cy[n] = cy;
-      ++n;
-    }
-    sm.n = n;
+  for (int j = 0; j < RME_MAX_SEEDS; ++j) {
+    const int ox = __shfl_sync(kFull, qx, j), oy = __shfl_sync(kFull, qy, j);
+    dup |= j < lane && ox == qx && oy == qy;
   }
-  __syncwarp();
-  int n = sm.n;
-  sad_batch<S>(sm, org, stride, w, h, n, lane);
+  const uint32_t keep = __ballot_sync(kFull, lane < ns && !dup);
+  const int nk = __popc(keep);
   int bx = 0, by = 0;
-  uint32_t bcost = 0xffffffffu;
-  for (int k = 0; k < n; ++k) {
-    uint32_t c = sm.cost[k] + hevc_rate(F, sm.cx[k] * 4, sm.cy[k] * 4, pq);
-    if (c < bcost) {
-      bcost = c;
-      bx = sm.cx[k];
-      by = sm.cy[k];
+  uint32_t bcost = kInf;
+  {
+    const int lpc = lanes_per(nk), cpp = 32 / lpc, sub = lane % lpc;
+    for (int c0 = 0; c0 < nk; c0 += cpp) {
+      const int c = lane / lpc < cpp ? c0 + lane / lpc : nk;
+      const bool ok = c < nk;
+      const int from = ok ? __fns(keep, 0, c + 1) : 0;
+      const int fx = __shfl_sync(kFull, qx, from), fy = __shfl_sync(kFull, qy, from);
+      const uint32_t s = group_sad<S>(sm.src, wr, h, org, stride, lpc, sub, lane, ok, fx, fy);
+      const uint32_t cost = ok ? s + hevc_rate(lam, fx * 4, fy * 4, p0x, p0y, p1x, p1y) : kInf;
+      const Pick p = warp_min(cost);
+      if (p.cost < bcost) {
+        bcost = p.cost;
+        bx = __shfl_sync(kFull, fx, p.lane);
+        by = __shfl_sync(kFull, fy, p.lane);
+      }
     }
   }
-  nsad += n;
+  nsad += nk;
   const int ox = bx, oy = by, range = F.search_range;
   auto inside = [&](int cx, int cy) {
     return abs(cx - ox) <= range && abs(cy - oy) <= range && cx >= lox && cx <= hix && cy >= loy && cy <= hiy;
   };
+  const int lpc4 = lanes_per(4), g4 = lane / lpc4, sub4 = lane % lpc4;
+  const int dx4 = g4 == 0 ? 1 : g4 == 1 ? -1 : 0, dy4 = g4 == 2 ? 1 : g4 == 3 ? -1 : 0;
   int rings = 0;
   for (;;) {
+    // The small diamond from a fixed `from` per round.
     for (int it = 0; it < 2 * range; ++it) {
-      int fx = bx, fy = by;
-      __syncwarp();
-      // Lanes 0..3 each own one diamond point; the valid ones are packed
-      // in order.
-      int dxs = lane == 0 ? 1 : lane == 1 ? -1 : 0, dys = lane == 2 ? 1 : lane == 3 ? -1 : 0;
-      bool ok = lane < 4 && inside(fx + dxs, fy + dys);
-      uint32_t m = __ballot_sync(0xffffffffu, ok);
-      if (ok) {
-        int pos = __popc(m & ((1u << lane) - 1));
-        sm.cx[pos] = fx + dxs;
-        sm.cy[pos] = fy + dys;
-      }
-      __syncwarp();
-      int nd = __popc(m);
-      sad_batch<S>(sm, org, stride, w, h, nd, lane);
-      bool improved = false;
-      for (int k = 0; k < nd; ++k) {
-        uint32_t c = sm.cost[k] + hevc_rate(F, sm.cx[k] * 4, sm.cy[k] * 4, pq);
-        if (c < bcost) {
-          bcost = c;
-          bx = sm.cx[k];
-          by = sm.cy[k];
-          improved = true;
-        }
-      }
-      nsad += nd;
-      if (!improved) break;
+      const int fx = bx + dx4, fy = by + dy4;
+      const bool ok = g4 < 4 && inside(fx, fy);
+      const uint32_t s = group_sad<S>(sm.src, wr, h, org, stride, lpc4, sub4, lane, ok, fx, fy);
+      const uint32_t cost = ok ? s + hevc_rate(lam, fx * 4, fy * 4, p0x, p0y, p1x, p1y) : kInf;
+      nsad += __popc(__ballot_sync(kFull, ok && sub4 == 0));
+      const Pick p = warp_min(cost);
+      if (!(p.cost < bcost)) break;
+      bcost = p.cost;
+      bx = __shfl_sync(kFull, fx, p.lane);
+      by = __shfl_sync(kFull, fy, p.lane);
     }
     if (rings >= F.search_rings) break;
     ++rings;
-    int fx = bx, fy = by;
-    __syncwarp();
-    // Square rings at 4, 8, 16: 24 points, in the reference's order.
-    int rr = lane < 8 ? 4 : lane < 16 ? 8 : 16, k8 = lane & 7;
-    int dxs = (k8 == 0 || k8 == 4 || k8 == 6) ? rr : (k8 == 1 || k8 == 5 || k8 == 7) ? -rr : 0;
-    int dys = (k8 == 2 || k8 == 4 || k8 == 5) ? rr : (k8 == 3 || k8 == 6 || k8 == 7) ? -rr : 0;
-    bool ok = lane < 24 && inside(fx + dxs, fy + dys);
-    uint32_t m = __ballot_sync(0xffffffffu, ok);
-    if (ok) {
-      int pos = __popc(m & ((1u << lane) - 1));
-      sm.cx[pos] = fx + dxs;
-      sm.cy[pos] = fy + dys;
-    }
-    __syncwarp();
-    int nr = __popc(m);
-    sad_batch<S>(sm, org, stride, w, h, nr, lane);
+    // Square rings at 4, 8, 16 around the settled point: 24 points, in the
+    // reference's order; a better one restarts the descent.
+    const int cxr = bx, cyr = by;
+    const int lpc = lanes_per(24), cpp = 32 / lpc, sub = lane % lpc;
     bool moved = false;
-    for (int k = 0; k < nr; ++k) {
-      uint32_t c = sm.cost[k] + hevc_rate(F, sm.cx[k] * 4, sm.cy[k] * 4, pq);
-      if (c < bcost) {
-        bcost = c;
-        bx = sm.cx[k];
-        by = sm.cy[k];
+    for (int c0 = 0; c0 < 24; c0 += cpp) {
+      const int c = lane / lpc < cpp ? c0 + lane / lpc : 24, rr = c < 8 ? 4 : c < 16 ? 8 : 16, k8 = c & 7;
+      const int dx = (k8 == 0 || k8 == 4 || k8 == 6) ? rr : (k8 == 1 || k8 == 5 || k8 == 7) ? -rr : 0;
+      const int dy = (k8 == 2 || k8 == 4 || k8 == 5) ? rr : (k8 == 3 || k8 == 6 || k8 == 7) ? -rr : 0;
+      const int fx = cxr + dx, fy = cyr + dy;
+      const bool ok = c < 24 && inside(fx, fy);
+      const uint32_t s = group_sad<S>(sm.src, wr, h, org, stride, lpc, sub, lane, ok, fx, fy);
+      const uint32_t cost = ok ? s + hevc_rate(lam, fx * 4, fy * 4, p0x, p0y, p1x, p1y) : kInf;
+      nsad += __popc(__ballot_sync(kFull, ok && sub == 0));
+      const Pick p = warp_min(cost);
+      if (p.cost < bcost) {
+        bcost = p.cost;
+        bx = __shfl_sync(kFull, fx, p.lane);
+        by = __shfl_sync(kFull, fy, p.lane);
         moved = true;
       }
     }
-    nsad += nr;
     if (!moved) break;
   }
   const uint32_t int_cost = bcost;
   const int imx = bx * 4, imy = by * 4;
 
-  // refine_subpel: the start and the half-sample ring in one batch, then
-  // the quarter-sample ring around the winner.
-  auto set_cand = [&](int k, int mx, int my) {
-    sm.cx[k] = mx;
-    sm.cy[k] = my;
-    sm.p1[k] = plane_at<S>(R, (my & 3) * 4 + (mx & 3), x + (mx >> 2), y + (my >> 2));
-    sm.p2[k] = nullptr;
-  };
-  __syncwarp();
-  if (lane < 9) {
-    // k = 0: the start; k = 1..8: dy in {-2,0,2} outer, dx inner, centre skipped.
-    int q = lane == 0 ? 4 : (lane <= 4 ? lane - 1 : lane);
-    set_cand(lane, imx + (q % 3 - 1) * 2, imy + (q / 3 - 1) * 2);
-  }
-  __syncwarp();
-  satd_batch<S>(sm, stride, w, h, 9, lane);
+  // refine_subpel: candidate 0 the start, 1..8 the half-sample ring (dy in
+  // {-2,0,2} outer, dx inner, centre skipped), in one step; then the
+  // quarter-sample ring around the winner.
   int bmx = imx, bmy = imy;
-  uint32_t bsatd = sm.cost[0];
-  uint32_t bc = bsatd + hevc_rate(F, imx, imy, pq);
-  for (int k = 1; k < 9; ++k) {
-    uint32_t c = sm.cost[k] + hevc_rate(F, sm.cx[k], sm.cy[k], pq);
-    if (c < bc) {
-      bc = c;
-      bsatd = sm.cost[k];
-      bmx = sm.cx[k];
-      bmy = sm.cy[k];
-    }
-  }
-  nsatd += 9;
+  uint32_t bc = kInf, bsatd = 0;
   {
-    int cmx = bmx, cmy = bmy;
-    __syncwarp();
-    bool cross = F.quarter_cross != 0;
-    int q = lane < 4 ? lane : lane + 1;  // ring positions 0..8 minus the centre
-    int dx = q % 3 - 1, dy = q / 3 - 1;
-    bool ok = lane < 8 && !(cross && dx != 0 && dy != 0);
-    uint32_t m = __ballot_sync(0xffffffffu, ok);
-    if (ok) set_cand(__popc(m & ((1u << lane) - 1)), (int)(int16_t)(cmx + dx), (int)(int16_t)(cmy + dy));
-    __syncwarp();
-    int nq = __popc(m);
-    satd_batch<S>(sm, stride, w, h, nq, lane);
-    for (int k = 0; k < nq; ++k) {
-      uint32_t c = sm.cost[k] + hevc_rate(F, sm.cx[k], sm.cy[k], pq);
-      if (c < bc) {
-        bc = c;
-        bsatd = sm.cost[k];
-        bmx = sm.cx[k];
-        bmy = sm.cy[k];
-      }
+    const int lpc = lanes_per(9), sub = lane % lpc, c = lane / lpc;
+    const int q = c == 0 ? 4 : (c <= 4 ? c - 1 : c);
+    const int mx = imx + (q % 3 - 1) * 2, my = imy + (q / 3 - 1) * 2;
+    const bool ok = c < 9;
+    const S* p1 = plane_at<S>(R, (my & 3) * 4 + (mx & 3), x + (mx >> 2), y + (my >> 2));
+    const uint32_t s = group_satd<S>(sm.src, wr, tw, th, p1, nullptr, stride, lpc, sub, lane, ok);
+    const uint32_t cost = ok ? s + hevc_rate(lam, mx, my, p0x, p0y, p1x, p1y) : kInf;
+    const Pick p = warp_min(cost);
+    bc = p.cost;
+    bsatd = __shfl_sync(kFull, s, p.lane);
+    bmx = __shfl_sync(kFull, mx, p.lane);
+    bmy = __shfl_sync(kFull, my, p.lane);
+    nsatd += 9;
+  }
+  {
+    const bool cross = F.quarter_cross != 0;
+    const int lpc = lanes_per(8), sub = lane % lpc, c = lane / lpc;
+    const int q = c < 4 ? c : c + 1;
+    const int dx = q % 3 - 1, dy = q / 3 - 1;
+    const bool ok = c < 8 && !(cross && dx != 0 && dy != 0);
+    const int mx = (int)(int16_t)(bmx + dx), my = (int)(int16_t)(bmy + dy);
+    const S* p1 = plane_at<S>(R, (my & 3) * 4 + (mx & 3), x + (mx >> 2), y + (my >> 2));
+    const uint32_t s = group_satd<S>(sm.src, wr, tw, th, p1, nullptr, stride, lpc, sub, lane, ok);
+    const uint32_t cost = ok ? s + hevc_rate(lam, mx, my, p0x, p0y, p1x, p1y) : kInf;
+    nsatd += __popc(__ballot_sync(kFull, ok && sub == 0));
+    const Pick p = warp_min(cost);
+    if (p.cost < bc) {
+      bc = p.cost;
+      bsatd = __shfl_sync(kFull, s, p.lane);
+      bmx = __shfl_sync(kFull, mx, p.lane);
+      bmy = __shfl_sync(kFull, my, p.lane);
     }
-    nsatd += nq;
   }
   write_result(out, bmx, bmy, r, bc, bsatd, imx, imy, int_cost, nsad, nsatd, lane);
-  if (flag) {
-    __syncwarp();
-    if (lane == 0) {
-      __threadfence();
-      st_release(flag, F.epoch);
+  if (F.mode != RME_PRED_GIVEN && lane == 0) {
+    // The tasks reading this result: right and lower neighbours of this
+    // level, the blocks of the next evaluated size inside this one.
+    __threadfence();
+    if (lbx + 1 < F.nbx[l]) release(L, F, f, (F.base[l] + local + 1) * F.nref + r);
+    if (lby + 1 < F.nby[l]) release(L, F, f, (F.base[l] + local + F.nbx[l]) * F.nref + r);
+    if (l + 1 < F.nlevels) {
+      const int N = F.size[l], M = F.size[l + 1];
+      const int cx1 = min((lbx + 1) * N / M, F.nbx[l + 1]), cy1 = min((lby + 1) * N / M, F.nby[l + 1]);
+      for (int cy = lby * N / M; cy < cy1; ++cy)
+        for (int cx = lbx * N / M; cx < cx1; ++cx)
+          release(L, F, f, (F.base[l + 1] + cy * F.nbx[l + 1] + cx) * F.nref + r);
     }
   }
-  cnt.tasks += 1;
-  cnt.sad += nsad;
-  cnt.satd += nsatd;
-  cnt.sad_samples += (unsigned long long)nsad * w * h;
-  cnt.satd_samples += (unsigned long long)nsatd * w * h;
+  count_task(sm, lane, nsad, nsatd, w * h);
 }
 
 // ---- H.264 ------------------------------------------------------------------
@@ -562,176 +625,180 @@ __constant__ int8_t c_hex12[12][2] = {{-2, 1}, {-2, -1}, {2, 1},  {2, -1}, {-1, 
 
 struct H264Blk {
   int x, y, w, h;
-  int px, py;       // predictor (quarter samples)
+  int px, py;          // predictor (quarter samples)
   int lx, hx, ly, hy;  // search_bounds
+  int wr, ipc, tw, th, tpc;
 };
 
 __device__ __forceinline__ uint32_t h264_rate(const FrameDesc& F, const H264Blk& B, int qx, int qy) {
-  int dx = min(max(qx - B.px, -kMvSpan), kMvSpan), dy = min(max(qy - B.py, -kMvSpan), kMvSpan);
+  const int dx = min(max(qx - B.px, -kMvSpan), kMvSpan), dy = min(max(qy - B.py, -kMvSpan), kMvSpan);
   return (uint32_t)__ldg(&F.tab[dx + kMvSpan]) + (uint32_t)__ldg(&F.tab[dy + kMvSpan]);
 }
 
-// ring(): points around a fixed centre c (offsets from `offs` of length
-// nof, lane k owns offset k), inside the box and not the centre, scored
-// together, accepted in order; returns the offset index of the last
-// point taken or -1.
-template <class S>
-__device__ int h264_ring(const FrameDesc& F, const H264Blk& B, WarpSmem& sm, const S* org, int stride, int lane,
-                         int cx, int cy, int ox, int oy, bool valid_lane, int box[4], int& bx, int& by,
-                         uint32_t& bcost, uint32_t& nsad) {
-  __syncwarp();
-  int fx = cx + ox, fy = cy + oy;
-  bool ok = valid_lane && fx >= box[0] && fx <= box[1] && fy >= box[2] && fy <= box[3] && !(fx == cx && fy == cy);
-  uint32_t m = __ballot_sync(0xffffffffu, ok);
-  if (ok) {
-    int pos = __popc(m & ((1u << lane) - 1));
-    sm.cx[pos] = fx;
-    sm.cy[pos] = fy;
-    sm.tx[pos] = lane;
-  }
-  __syncwarp();
-  int n = __popc(m);
-  sad_batch<S>(sm, org, stride, B.w, B.h, n, lane);
+// ring(): up to n points around a fixed centre (candidate c at offset
+// off(c)), those inside the box and not the centre, scored in one step;
+// returns the index of the point taken, or -1.
+template <class S, class Off>
+__device__ __forceinline__ int h264_ring(const FrameDesc& F, const H264Blk& B, WarpSmem<S>& sm, const S* org,
+                                         int stride, int lane, int n, Off off, const int box[4], int& bx, int& by,
+                                         uint32_t& bcost, uint32_t& nsad) {
+  const int cx = bx, cy = by;
+  const int lpc = lanes_per(n), cpp = 32 / lpc, sub = lane % lpc;
   int moved = -1;
-  for (int k = 0; k < n; ++k) {
-    uint32_t c = sm.cost[k] + h264_rate(F, B, sm.cx[k] * 4, sm.cy[k] * 4);
-    if (c < bcost) {
-      bcost = c;
-      bx = sm.cx[k];
-      by = sm.cy[k];
-      moved = sm.tx[k];
+  for (int c0 = 0; c0 < n; c0 += cpp) {
+    const int c = lane / lpc < cpp ? c0 + lane / lpc : n;
+    int ox = 0, oy = 0;
+    off(c < n ? c : 0, ox, oy);
+    const int fx = cx + ox, fy = cy + oy;
+    const bool ok = c < n && fx >= box[0] && fx <= box[1] && fy >= box[2] && fy <= box[3] && !(fx == cx && fy == cy);
+    const uint32_t s = group_sad<S>(sm.src, B.wr, B.h, org, stride, lpc, sub, lane, ok, fx, fy);
+    const uint32_t cost = ok ? s + h264_rate(F, B, fx * 4, fy * 4) : kInf;
+    nsad += __popc(__ballot_sync(kFull, ok && sub == 0));
+    const Pick p = warp_min(cost);
+    if (p.cost < bcost) {
+      bcost = p.cost;
+      bx = __shfl_sync(kFull, fx, p.lane);
+      by = __shfl_sync(kFull, fy, p.lane);
+      moved = __shfl_sync(kFull, c, p.lane);
     }
   }
-  nsad += n;
   return moved;
 }
 
-// Search::int_search (h264_hpel.rs:789-952) for one reference: lane k
+// Search::int_search (h264_hpel.rs:789-952) for one reference: lane k + 1
 // holds candidate k of `ncand` (quarter samples).
 template <class S>
-__device__ void h264_int_search(const FrameDesc& F, const H264Blk& B, WarpSmem& sm, int lane, const DevPlanes& R,
+__device__ void h264_int_search(const FrameDesc& F, const H264Blk& B, WarpSmem<S>& sm, int lane, const DevPlanes& R,
                                 int ncand, int cand_x, int cand_y, int& imx, int& imy, uint32_t& icost,
                                 uint32_t& nsad) {
   const S* org = plane_at<S>(R, 0, B.x, B.y);
   const int stride = R.stride;
-  auto clampf = [&](int m, int lo, int hi) { return min(max((m + 2) >> 2, lo), hi); };
-  int bx = clampf(B.px, B.lx, B.hx), by = clampf(B.py, B.ly, B.hy);
-  // The predictor and the distinct candidates (tried[12]), in order.
-  __syncwarp();
-  int fx = clampf(cand_x, B.lx, B.hx), fy = clampf(cand_y, B.ly, B.hy);
-  if (lane < ncand) {
-    sm.tx[lane] = fx;
-    sm.ty[lane] = fy;
+  // Candidate list: slot 0 the rounded, clamped predictor; slot k >= 1 the
+  // candidate k-1, skipped when it equals the predictor's point or an
+  // earlier candidate's (`tried`).
+  const int pxr = min(max((B.px + 2) >> 2, B.lx), B.hx), pyr = min(max((B.py + 2) >> 2, B.ly), B.hy);
+  const int cl = lane - 1;
+  const int qx = lane == 0 ? pxr : min(max((cand_x + 2) >> 2, B.lx), B.hx);
+  const int qy = lane == 0 ? pyr : min(max((cand_y + 2) >> 2, B.ly), B.hy);
+  bool skip = lane > 0 && (qx == pxr && qy == pyr);
+#pragma unroll
+  for (int j = 1; j <= 8; ++j) {
+    const int ox = __shfl_sync(kFull, qx, j), oy = __shfl_sync(kFull, qy, j);
+    skip |= j < lane && ox == qx && oy == qy;
   }
-  __syncwarp();
-  if (lane == 0) {
-    int tx[12], ty[12], nt = 0, n = 1;
-    sm.cx[0] = bx;
-    sm.cy[0] = by;
-    for (int i = 0; i < ncand; ++i) {
-      int qx = sm.tx[i], qy = sm.ty[i];
-      bool seen = qx == bx && qy == by;
-      for (int k = 0; k < nt; ++k) seen |= (tx[k] == qx && ty[k] == qy);
-      if (seen) continue;
-      if (nt < 12) {
-        tx[nt] = qx;
-        ty[nt] = qy;
-        ++nt;
+  const uint32_t keep = __ballot_sync(kFull, (lane == 0 || cl < ncand) && !skip);
+  const int nk = __popc(keep);
+  int bx = pxr, by = pyr;
+  uint32_t bcost = kInf;
+  {
+    const int lpc = lanes_per(nk), cpp = 32 / lpc, sub = lane % lpc;
+    for (int c0 = 0; c0 < nk; c0 += cpp) {
+      const int c = lane / lpc < cpp ? c0 + lane / lpc : nk;
+      const bool ok = c < nk;
+      const int from = ok ? __fns(keep, 0, c + 1) : 0;
+      const int fx = __shfl_sync(kFull, qx, from), fy = __shfl_sync(kFull, qy, from);
+      const uint32_t s = group_sad<S>(sm.src, B.wr, B.h, org, stride, lpc, sub, lane, ok, fx, fy);
+      const uint32_t cost = ok ? s + h264_rate(F, B, fx * 4, fy * 4) : kInf;
+      const Pick p = warp_min(cost);
+      if (p.cost < bcost) {
+        bcost = p.cost;
+        bx = __shfl_sync(kFull, fx, p.lane);
+        by = __shfl_sync(kFull, fy, p.lane);
       }
-      sm.cx[n] = qx;
-      sm.cy[n] = qy;
-      ++n;
-    }
-    sm.n = n;
-  }
-  __syncwarp();
-  int n = sm.n;
-  sad_batch<S>(sm, org, stride, B.w, B.h, n, lane);
-  uint32_t bcost = sm.cost[0] + h264_rate(F, B, bx * 4, by * 4);
-  for (int k = 1; k < n; ++k) {
-    uint32_t c = sm.cost[k] + h264_rate(F, B, sm.cx[k] * 4, sm.cy[k] * 4);
-    if (c < bcost) {
-      bcost = c;
-      bx = sm.cx[k];
-      by = sm.cy[k];
     }
   }
-  nsad += n;
+  nsad += nk;
   const int range = F.range;
-  int box[4] = {max(bx - range, B.lx), min(bx + range, B.hx), max(by - range, B.ly), min(by + range, B.hy)};
+  const int box[4] = {max(bx - range, B.lx), min(bx + range, B.hx), max(by - range, B.ly), min(by + range, B.hy)};
   if (F.umh) {
     // The cross r = 2, 4, .. range then 12-point hexagon rings r = 4, 8, ..
     // range around the fixed start, each point taken by try_at: skipped
-    // when outside the box or equal to the best so far, else scored.
+    // (and not scored) when outside the box or equal to the best so far.
     const int cx = bx, cy = by;
     const int ncross = 4 * (range / 2), nhex = 12 * (range / 4), total = ncross + nhex;
     for (int c0 = 0; c0 < total; c0 += 32) {
-      __syncwarp();
-      int i = c0 + lane, qx = 0, qy = 0;
+      const int i = c0 + lane;
+      int qx2 = 0, qy2 = 0;
       bool ok = i < total;
       if (ok) {
         if (i < ncross) {
-          int rr = 2 * (i / 4 + 1), k = i & 3;
-          qx = cx + (k == 0 ? -rr : k == 1 ? rr : 0);
-          qy = cy + (k == 2 ? -rr : k == 3 ? rr : 0);
+          const int rr = 2 * (i / 4 + 1), k = i & 3;
+          qx2 = cx + (k == 0 ? -rr : k == 1 ? rr : 0);
+          qy2 = cy + (k == 2 ? -rr : k == 3 ? rr : 0);
         } else {
-          int j = i - ncross, rr = 4 * (j / 12 + 1), k = j % 12;
-          qx = cx + c_hex12[k][0] * rr / 2;
-          qy = cy + c_hex12[k][1] * rr / 2;
+          const int j = i - ncross, rr = 4 * (j / 12 + 1), k = j % 12;
+          qx2 = cx + c_hex12[k][0] * rr / 2;
+          qy2 = cy + c_hex12[k][1] * rr / 2;
         }
-        ok = qx >= box[0] && qx <= box[1] && qy >= box[2] && qy <= box[3];
+        ok = qx2 >= box[0] && qx2 <= box[1] && qy2 >= box[2] && qy2 <= box[3];
       }
-      uint32_t m = __ballot_sync(0xffffffffu, ok);
-      if (ok) {
-        int pos = __popc(m & ((1u << lane) - 1));
-        sm.cx[pos] = qx;
-        sm.cy[pos] = qy;
-      }
+      const uint32_t s = group_sad<S>(sm.src, B.wr, B.h, org, stride, 1, 0, lane, ok, qx2, qy2);
+      const uint32_t cost = ok ? s + h264_rate(F, B, qx2 * 4, qy2 * 4) : kInf;
+      // In-order walk for the count of points scored (equal-to-best ones
+      // are not); the outcome is the step's least cost, first reached.
       __syncwarp();
-      int nb = __popc(m);
-      sad_batch<S>(sm, org, stride, B.w, B.h, nb, lane);
-      for (int k = 0; k < nb; ++k) {
-        if (sm.cx[k] == bx && sm.cy[k] == by) continue;
-        ++nsad;
-        uint32_t c = sm.cost[k] + h264_rate(F, B, sm.cx[k] * 4, sm.cy[k] * 4);
-        if (c < bcost) {
-          bcost = c;
-          bx = sm.cx[k];
-          by = sm.cy[k];
+      sm.ux[lane] = qx2;
+      sm.uy[lane] = qy2;
+      sm.uc[lane] = ok ? cost : kInf;
+      __syncwarp();
+      int wx = bx, wy = by;
+      uint32_t wc = bcost, scored = 0;
+      const int np = min(32, total - c0);
+      for (int k = 0; k < np; ++k) {
+        const uint32_t ck = sm.uc[k];
+        if (ck == kInf) continue;
+        const int kx = sm.ux[k], ky = sm.uy[k];
+        if (kx == wx && ky == wy) continue;
+        ++scored;
+        if (ck < wc) {
+          wc = ck;
+          wx = kx;
+          wy = ky;
         }
       }
+      nsad += scored;
+      bx = wx;
+      by = wy;
+      bcost = wc;
     }
   }
   if (F.dia) {
     for (int it = 0; it < range; ++it) {
-      int cx = bx, cy = by;
-      int ox = lane == 0 ? -1 : lane == 1 ? 1 : 0, oy = lane == 2 ? -1 : lane == 3 ? 1 : 0;
-      h264_ring<S>(F, B, sm, org, stride, lane, cx, cy, ox, oy, lane < 4, box, bx, by, bcost, nsad);
+      const int cx = bx, cy = by;
+      h264_ring<S>(F, B, sm, org, stride, lane, 4,
+                   [](int c, int& ox, int& oy) {
+                     ox = c == 0 ? -1 : c == 1 ? 1 : 0;
+                     oy = c == 2 ? -1 : c == 3 ? 1 : 0;
+                   },
+                   box, bx, by, bcost, nsad);
       if (bx == cx && by == cy) break;
     }
   } else {
-    int cx = bx, cy = by;
-    int k6 = lane < 6 ? lane : 0;
-    int dir = h264_ring<S>(F, B, sm, org, stride, lane, cx, cy, c_hex[k6][0], c_hex[k6][1], lane < 6, box, bx, by,
-                           bcost, nsad);
+    int dir = h264_ring<S>(F, B, sm, org, stride, lane, 6,
+                           [](int c, int& ox, int& oy) {
+                             ox = c_hex[c][0];
+                             oy = c_hex[c][1];
+                           },
+                           box, bx, by, bcost, nsad);
     int it = 1;
     while (dir != -1 && it < range) {
-      cx = bx;
-      cy = by;
-      int ks = lane == 0 ? (dir + 5) % 6 : lane == 1 ? dir : (dir + 1) % 6;
-      int moved = h264_ring<S>(F, B, sm, org, stride, lane, cx, cy, c_hex[ks][0], c_hex[ks][1], lane < 3, box, bx,
-                               by, bcost, nsad);
-      if (moved == -1) {
-        dir = -1;
-      } else {
-        dir = moved == 0 ? (dir + 5) % 6 : moved == 1 ? dir : (dir + 1) % 6;
-      }
+      const int d = dir;
+      const int moved = h264_ring<S>(F, B, sm, org, stride, lane, 3,
+                                     [d](int c, int& ox, int& oy) {
+                                       const int k = c == 0 ? (d + 5) % 6 : c == 1 ? d : (d + 1) % 6;
+                                       ox = c_hex[k][0];
+                                       oy = c_hex[k][1];
+                                     },
+                                     box, bx, by, bcost, nsad);
+      dir = moved == -1 ? -1 : (moved == 0 ? (d + 5) % 6 : moved == 1 ? d : (d + 1) % 6);
       ++it;
     }
-    cx = bx;
-    cy = by;
-    int k8 = lane & 7;
-    h264_ring<S>(F, B, sm, org, stride, lane, cx, cy, c_sq[k8][0], c_sq[k8][1], lane < 8, box, bx, by, bcost, nsad);
+    h264_ring<S>(F, B, sm, org, stride, lane, 8,
+                 [](int c, int& ox, int& oy) {
+                   ox = c_sq[c][0];
+                   oy = c_sq[c][1];
+                 },
+                 box, bx, by, bcost, nsad);
   }
   imx = bx * 4;
   imy = by * 4;
@@ -740,22 +807,14 @@ __device__ void h264_int_search(const FrameDesc& F, const H264Blk& B, WarpSmem& 
 
 // Search::refine (h264_hpel.rs:956-1021) from (smx, smy): the start, then
 // `hpel` rings of half-sample points and `qpel` of quarter-sample points
-// (the start scored in the same batch as the first ring).
+// (the start scored in the same step as the first ring).
 template <class S>
-__device__ void h264_refine(const FrameDesc& F, const H264Blk& B, WarpSmem& sm, int lane, const DevPlanes& R, int smx,
+__device__ void h264_refine(const FrameDesc& F, const H264Blk& B, WarpSmem<S>& sm, int lane, const DevPlanes& R, int smx,
                             int smy, int hpel, int qpel, int& omx, int& omy, uint32_t& osatd, uint32_t& ocost,
                             uint32_t& nsatd) {
   const int qlx = B.lx * 4, qhx = B.hx * 4, qly = B.ly * 4, qhy = B.hy * 4;
-  auto set_cand = [&](int k, int mx, int my) {
-    int xi = B.x + (mx >> 2), yi = B.y + (my >> 2);
-    const int8_t* q = c_h264_qpel[(my & 3) * 4 + (mx & 3)];
-    sm.cx[k] = mx;
-    sm.cy[k] = my;
-    sm.p1[k] = plane_at<S>(R, q[0], xi + q[1], yi + q[2]);
-    sm.p2[k] = q[3] < 0 ? nullptr : plane_at<S>(R, q[3], xi + q[4], yi + q[5]);
-  };
   int bmx = smx, bmy = smy;
-  uint32_t bsatd = 0, bc = 0;
+  uint32_t bsatd = 0, bc = kInf;
   bool first = true;
   for (int s = 0; s < 2; ++s) {
     const int step = s == 0 ? 2 : 1, iters = s == 0 ? hpel : qpel;
@@ -765,33 +824,35 @@ __device__ void h264_refine(const FrameDesc& F, const H264Blk& B, WarpSmem& sm, 
     for (int it = 0; it < iters || first; ++it) {
       const int cmx = bmx, cmy = bmy;
       const bool ring = it < iters;
-      __syncwarp();
-      // slot 0: the start (first batch only); then the ring's points.
-      const int base = first ? 1 : 0;
-      const int kk = lane & 7;
-      const int mx = (int)(int16_t)(cmx + c_ring[kk][0] * step), my = (int)(int16_t)(cmy + c_ring[kk][1] * step);
-      const bool ok = ring && lane < pts && mx >= qlx && mx <= qhx && my >= qly && my <= qhy &&
-                      !(has_prev && abs(mx - prevx) <= step && abs(my - prevy) <= step);
-      const uint32_t m = __ballot_sync(0xffffffffu, ok);
-      if (ok) set_cand(base + __popc(m & ((1u << lane) - 1)), mx, my);
-      if (first && lane == 31) set_cand(0, cmx, cmy);
-      __syncwarp();
-      const int nr = __popc(m), ntot = base + nr;
-      satd_batch<S>(sm, R.stride, B.w, B.h, ntot, lane);
-      if (first) {
-        bsatd = sm.cost[0];
-        bc = bsatd + h264_rate(F, B, cmx, cmy);
+      // Candidate 0 the start (first step only), then the ring's points.
+      const int base = first ? 1 : 0, n = base + (ring ? pts : 0);
+      const int lpc = lanes_per(n), sub = lane % lpc, c = lane / lpc;
+      const int k = c - base;
+      int mx = cmx, my = cmy;
+      bool ok;
+      if (k < 0) {
+        ok = c < n;
+      } else {
+        const int kk = k & 7;
+        mx = (int)(int16_t)(cmx + c_ring[kk][0] * step);
+        my = (int)(int16_t)(cmy + c_ring[kk][1] * step);
+        ok = c < n && mx >= qlx && mx <= qhx && my >= qly && my <= qhy &&
+             !(has_prev && abs(mx - prevx) <= step && abs(my - prevy) <= step);
       }
-      for (int k = base; k < ntot; ++k) {
-        uint32_t c = sm.cost[k] + h264_rate(F, B, sm.cx[k], sm.cy[k]);
-        if (c < bc) {
-          bc = c;
-          bsatd = sm.cost[k];
-          bmx = sm.cx[k];
-          bmy = sm.cy[k];
-        }
+      const int xi = B.x + (mx >> 2), yi = B.y + (my >> 2);
+      const int8_t* q = c_h264_qpel[(my & 3) * 4 + (mx & 3)];
+      const S* p1 = plane_at<S>(R, q[0], xi + q[1], yi + q[2]);
+      const S* p2 = q[3] < 0 ? nullptr : plane_at<S>(R, q[3], xi + q[4], yi + q[5]);
+      const uint32_t sv = group_satd<S>(sm.src, B.wr, B.tw, B.th, p1, p2, R.stride, lpc, sub, lane, ok);
+      const uint32_t cost = ok ? sv + h264_rate(F, B, mx, my) : kInf;
+      nsatd += __popc(__ballot_sync(kFull, ok && sub == 0));
+      const Pick p = warp_min(cost);
+      if (p.cost < bc) {
+        bc = p.cost;
+        bsatd = __shfl_sync(kFull, sv, p.lane);
+        bmx = __shfl_sync(kFull, mx, p.lane);
+        bmy = __shfl_sync(kFull, my, p.lane);
       }
-      nsatd += ntot;
       first = false;
       if (!ring) break;
       if (bmx == cmx && bmy == cmy) break;
@@ -817,7 +878,7 @@ __device__ __forceinline__ void median_mvp(Nb a, Nb b, Nb c, int ref, int& ox, i
     b = a;
     c = a;
   }
-  bool ma = a.ref == ref, mb = b.ref == ref, mc = c.ref == ref;
+  const bool ma = a.ref == ref, mb = b.ref == ref, mc = c.ref == ref;
   if (ma && !mb && !mc) {
     ox = a.x;
     oy = a.y;
@@ -834,27 +895,33 @@ __device__ __forceinline__ void median_mvp(Nb a, Nb b, Nb c, int ref, int& ox, i
 }
 
 template <class S>
-__device__ void h264_task(const FrameDesc& F, int t, WarpSmem& sm, int lane, uint32_t* status, Counters& cnt) {
+__device__ void h264_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, WarpSmem<S>& sm, int lane) {
   H264Blk B;
   uint32_t nsad = 0, nsatd = 0;
-  auto bounds = [&](int x, int y, int w, int h) {  // search_bounds (h264_hpel.rs:476-488)
+  auto shape = [&](int x, int y, int w, int h) {  // search_bounds (h264_hpel.rs:476-488)
+    B.x = x;
+    B.y = y;
+    B.w = w;
+    B.h = h;
     B.lx = 4 - F.pad - x;
     B.hx = F.width + F.pad - (w + 4) - x;
     B.ly = max(4 - F.pad - y, -F.vr);
     B.hy = min(F.height + F.pad - (h + 4) - y, F.vr);
+    B.wr = w * (int)sizeof(S) / 4;
+    B.ipc = B.wr * h;
+    B.tw = w >> 2;
+    B.th = h >> 2;
+    B.tpc = B.tw * B.th;
   };
   if (F.mode == RME_PRED_GIVEN) {
     const rme_job* j = &F.jobs[t];
-    B.x = j->x;
-    B.y = j->y;
-    B.w = j->w;
-    B.h = j->h;
+    shape(j->x, j->y, j->w, j->h);
     B.px = j->mvp[0].x;
     B.py = j->mvp[0].y;
-    bounds(B.x, B.y, B.w, B.h);
-    int nc = j->nseeds;
-    int cx = lane < nc ? j->seeds[lane].x : 0, cy = lane < nc ? j->seeds[lane].y : 0;
-    stage_src(sm, plane_at<S>(F.src, 0, B.x, B.y), F.src.stride, B.w, B.h, lane);
+    const int nc = j->nseeds;
+    const int cx = lane >= 1 && lane - 1 < nc ? j->seeds[lane - 1].x : 0;
+    const int cy = lane >= 1 && lane - 1 < nc ? j->seeds[lane - 1].y : 0;
+    stage_src<S>(sm.src, plane_at<S>(F.src, 0, B.x, B.y), F.src.stride, B.w, B.h, lane);
     int mx, my, imx, imy;
     uint32_t sat, c, ic;
     const bool score = (j->flags & RME_JOB_SCORE_ONLY) != 0;
@@ -866,36 +933,33 @@ __device__ void h264_task(const FrameDesc& F, int t, WarpSmem& sm, int lane, uin
     // p_mb's search section (h264_analyse.rs:1884-1975) with the
     // neighbours' final 16x16 results as the motion context.
     const int mbw = F.width / 16, mx = t % mbw, my = t / mbw;
-    B.x = mx * 16;
-    B.y = my * 16;
-    B.w = B.h = 16;
-    bounds(B.x, B.y, 16, 16);
+    shape(mx * 16, my * 16, 16, 16);
     auto nb = [&](int qx, int qy) {
       Nb m{false, -1, 0, 0};
       if (qx < 0 || qy < 0 || qx >= mbw) return m;
-      int idx = qy * mbw + qx;
-      wait_flag(&F.flags[idx], F.epoch, status, lane);
-      uint32_t v = ldcg_u32(&F.out[idx].mv);
+      const int idx = qy * mbw + qx;
+      const uint32_t v = ldcg_u32(&F.out[idx].mv);
       m.avail = true;
       m.ref = (int)ldcg_u32(&F.out[idx].ref);
       m.x = mvx_of(v);
       m.y = mvy_of(v);
       return m;
     };
-    Nb A = nb(mx - 1, my), Bn = nb(mx, my - 1), C = nb(mx + 1, my - 1), D = nb(mx - 1, my - 1);
-    Nb Cc = C.avail ? C : D;
+    const Nb A = nb(mx - 1, my), Bn = nb(mx, my - 1), C = nb(mx + 1, my - 1), D = nb(mx - 1, my - 1);
+    const Nb Cc = C.avail ? C : D;
     // p_skip_mv (h264/mb.rs:1235-1246)
     int skx = 0, sky = 0;
     if (A.avail && Bn.avail && !(A.ref == 0 && A.x == 0 && A.y == 0) && !(Bn.ref == 0 && Bn.x == 0 && Bn.y == 0))
       median_mvp(A, Bn, Cc, 0, skx, sky);
-    // cands = [skip_mv, 0, distinct A, B, C vectors] (h264_pic.rs:713-751)
+    // cands = [skip_mv, 0, distinct A, B, C vectors] (h264_pic.rs:713-751);
+    // lane k + 1 holds candidate k.
     int ncx[8], ncy[8], nc = 0;
     ncx[nc] = skx;
     ncy[nc++] = sky;
     ncx[nc] = 0;
     ncy[nc++] = 0;
     {
-      Nb q[3] = {A, Bn, C};
+      const Nb q[3] = {A, Bn, C};
       int vx[4], vy[4], nn = 0;
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
@@ -912,9 +976,9 @@ __device__ void h264_task(const FrameDesc& F, int t, WarpSmem& sm, int lane, uin
         ncy[nc++] = vy[k];
       }
     }
-    stage_src(sm, plane_at<S>(F.src, 0, B.x, B.y), F.src.stride, 16, 16, lane);
+    stage_src<S>(sm.src, plane_at<S>(F.src, 0, B.x, B.y), F.src.stride, 16, 16, lane);
     int mv16x = 0, mv16y = 0, r16 = 0, mi16x = 0, mi16y = 0;
-    uint32_t c16 = 0xffffffffu, s16 = 0, ci16 = 0, int16 = 0xffffffffu;
+    uint32_t c16 = kInf, s16 = 0, ci16 = 0, int16 = kInf;
     for (int r = 0; r < F.nref; ++r) {
       int prx, pry;
       median_mvp(A, Bn, Cc, r, prx, pry);
@@ -922,13 +986,13 @@ __device__ void h264_task(const FrameDesc& F, int t, WarpSmem& sm, int lane, uin
         ncx[nc] = prx;
         ncy[nc] = pry;
       }
-      int k = r > 0 ? min(nc + 1, 8) : nc;
+      const int k = r > 0 ? min(nc + 1, 8) : nc;
       B.px = prx;
       B.py = pry;
       int cx = 0, cy = 0;
 #pragma unroll
       for (int i = 0; i < 8; ++i)
-        if (lane == i) {
+        if (lane == i + 1) {
           cx = ncx[i];
           cy = ncy[i];
         }
@@ -957,70 +1021,86 @@ __device__ void h264_task(const FrameDesc& F, int t, WarpSmem& sm, int lane, uin
       }
     }
     write_result(&F.out[t], mv16x, mv16y, r16, c16, s16, mi16x, mi16y, ci16, nsad, nsatd, lane);
-    __syncwarp();
     if (lane == 0) {
+      // The macroblocks whose A, B, C or D this one is.
+      const int mbh = F.height / 16;
       __threadfence();
-      st_release(&F.flags[t], F.epoch);
+      if (mx + 1 < mbw) release(L, F, f, t + 1);
+      if (my + 1 < mbh) {
+        if (mx > 0) release(L, F, f, t + mbw - 1);
+        release(L, F, f, t + mbw);
+        if (mx + 1 < mbw) release(L, F, f, t + mbw + 1);
+      }
     }
   }
-  cnt.tasks += 1;
-  cnt.sad += nsad;
-  cnt.satd += nsatd;
-  cnt.sad_samples += (unsigned long long)nsad * B.w * B.h;
-  cnt.satd_samples += (unsigned long long)nsatd * B.w * B.h;
+  count_task(sm, lane, nsad, nsatd, B.w * B.h);
 }
 
-__global__ void __launch_bounds__(kWarpsPerBlock * 32) search_kernel(LaunchDesc L) {
+template <class S>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, RME_MIN_BLOCKS) search_kernel(LaunchDesc L) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  WarpSmem& sm = reinterpret_cast<WarpSmem*>(smem_raw)[warp];
-  Counters cnt;
+  WarpSmem<S>& sm = reinterpret_cast<WarpSmem<S>*>(smem_raw)[warp];
+  if (lane < 5) sm.cnt[lane] = 0;
+  __syncwarp();
+  const uint32_t epoch = __ldg(L.epoch);
   for (;;) {
-    unsigned long long g = 0;
-    if (lane == 0) g = atomicAdd(L.head, 1ull);
-    g = __shfl_sync(0xffffffffu, g, 0);
-    if (g >= (unsigned long long)L.total) break;
-    uint32_t e = __ldg(&L.queue[g]);
-    const FrameDesc& F = L.frames[e >> 24];
-    int t = (int)(e & 0xffffffu);
-    if (t >= F.ntasks) {
+    unsigned long long idx = 0;
+    if (lane == 0) idx = atomicAdd(L.head, 1ull);
+    idx = __shfl_sync(kFull, idx, 0);
+    if (idx >= (unsigned long long)L.total) break;
+    uint32_t e = 0;
+    if (lane == 0) e = pop_slot(L, idx, epoch);
+    e = __shfl_sync(kFull, e, 0);
+    __syncwarp();
+    if (e == 0xffffffffu) continue;  // the wait ran out (status set)
+    const int f = (int)(e >> 24), t = (int)(e & 0xffffffu);
+    const FrameDesc& F = L.frames[f];
+    // A task of the other sample width, or past its frame, is a host bug:
+    // flag it and skip it rather than read out of bounds.
+    if (t >= F.ntasks || (sizeof(S) == 1) != (F.bd == 8)) {
       if (lane == 0) atomicOr(L.status, kStatusBadTask);
       continue;
     }
-    if (F.codec == RME_CODEC_HEVC) {
-      if (F.bd == 8) hevc_task<uint8_t>(F, t, sm, lane, L.status, cnt);
-      else hevc_task<uint16_t>(F, t, sm, lane, L.status, cnt);
-    } else {
-      if (F.bd == 8) h264_task<uint8_t>(F, t, sm, lane, L.status, cnt);
-      else h264_task<uint16_t>(F, t, sm, lane, L.status, cnt);
-    }
+    if (F.codec == RME_CODEC_HEVC) hevc_task<S>(L, F, f, t, sm, lane);
+    else h264_task<S>(L, F, f, t, sm, lane);
   }
-  if (lane == 0) {
-    atomicAdd(&L.counters[0], cnt.tasks);
-    atomicAdd(&L.counters[1], cnt.sad);
-    atomicAdd(&L.counters[2], cnt.satd);
-    atomicAdd(&L.counters[3], cnt.sad_samples);
-    atomicAdd(&L.counters[4], cnt.satd_samples);
-  }
+  __syncwarp();
+  if (lane < 5) atomicAdd(&L.counters[lane], sm.cnt[lane]);
+}
+
+template <class S>
+size_t smem_bytes() {
+  return sizeof(WarpSmem<S>) * kWarpsPerBlock;
+}
+
+template <class S>
+int blocks_per_sm() {
+  int n = 0;
+  cudaError_t e = cudaFuncSetAttribute(search_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem_bytes<S>());
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, search_kernel<S>, kWarpsPerBlock * 32, smem_bytes<S>());
+  return e == cudaSuccess && n > 0 ? n : 1;
+}
+
+template <class S>
+cudaError_t launch(const LaunchDesc& L, int grid, cudaStream_t s) {
+  cudaError_t e = cudaFuncSetAttribute(search_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem_bytes<S>());
+  if (e != cudaSuccess) return e;
+  search_kernel<S><<<grid, kWarpsPerBlock * 32, smem_bytes<S>(), s>>>(L);
+  return cudaGetLastError();
 }
 
 }  // namespace
 
-int search_blocks_per_sm(int) {
-  int n = 0;
-  size_t smem = sizeof(WarpSmem) * kWarpsPerBlock;
-  if (cudaFuncSetAttribute(search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, search_kernel, kWarpsPerBlock * 32, smem) != cudaSuccess)
-    return 1;
-  return n;
+int search_blocks_per_sm(int bytes_per_sample) {
+  return bytes_per_sample == 1 ? blocks_per_sm<uint8_t>() : blocks_per_sm<uint16_t>();
 }
 
-cudaError_t launch_search(const LaunchDesc& L, int, int grid, cudaStream_t s) {
-  size_t smem = sizeof(WarpSmem) * kWarpsPerBlock;
-  cudaError_t e = cudaFuncSetAttribute(search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  search_kernel<<<grid, kWarpsPerBlock * 32, smem, s>>>(L);
-  return cudaGetLastError();
+cudaError_t launch_search(const LaunchDesc& L, int bytes_per_sample, int grid, cudaStream_t s) {
+  return bytes_per_sample == 1 ? launch<uint8_t>(L, grid, s) : launch<uint16_t>(L, grid, s);
 }
 
 }  // namespace rme
