@@ -316,6 +316,39 @@ int rme_serve_poll(void* server, rme_completion* done, int32_t max, int32_t* n);
 int rme_serve_close_stream(void* server, int32_t stream_id);
 int rme_serve_stop(void* server);
 
+/* ---- search without allocating --------------------------------------------- */
+
+/* One picture's planes in device memory the caller owns, in the layout the
+ * library keeps them (rme_picture_download_plane returns the same samples):
+ * `nplanes` consecutive planes `plane_elems` samples apart, each padded by
+ * `pad` samples on every side and `stride` samples per row; plane 0 is the
+ * integer plane, then H.264's b, h, j or HEVC's fractional phases 1..15.
+ * `base` (16-byte aligned) points at row 0, column 0 of plane 0, and the
+ * memory must extend 16 bytes past the last plane. */
+typedef struct {
+  const void* base;
+  int64_t plane_elems;
+  int32_t stride;
+  int32_t pad;
+} rme_plane_set;
+
+/* No counterpart in the reference (its search runs on the CPU and borrows
+ * slices). A GIVEN-mode search that allocates no device memory, for callers
+ * that cannot call cudaMalloc: a plugin whose host pipeline owns all of the
+ * GPU's memory, or a latency-bound loop that cannot afford the device-wide
+ * synchronisation of an allocation. Inputs and outputs are the caller's:
+ * `src` (plane 0 read) and `refs[nref]` (all planes read) as above, `jobs`
+ * and `out` (njobs each) in device memory. The same results as
+ * rme_frame_search in GIVEN mode. The search's scratch lives in a fixed
+ * 576 KiB device array inside the library, held on every device it is used
+ * on until the process exits: at most 65536 jobs per call (RME_EINVAL
+ * beyond). The first call on a device looks the array up (do it before any
+ * stream capture); calls share the array, so calls that overlap on the GPU
+ * race and must be serialised. Synchronous on `stream`. */
+int rme_search_given_noalloc(const rme_picture_desc* d, const rme_params* p, const rme_plane_set* src,
+                             const rme_plane_set* refs, int32_t nref, const rme_job* jobs, int32_t njobs,
+                             rme_result* out, void* stream);
+
 /* ---- diagnostics ------------------------------------------------------------ */
 
 /* Measured 32-bit integer-ALU throughput of `device` (add/shift/xor chains

@@ -68,6 +68,10 @@ class Frame(C.Structure):
                 ("jobs", C.POINTER(Job)), ("njobs", C.c_int32)]
 
 
+class PlaneSet(C.Structure):
+    _fields_ = [("base", C.c_void_p), ("plane_elems", C.c_int64), ("stride", C.c_int32), ("pad", C.c_int32)]
+
+
 class Stats(C.Structure):
     _fields_ = [("tasks", C.c_uint64), ("sad_candidates", C.c_uint64),
                 ("satd_candidates", C.c_uint64), ("sad_samples", C.c_uint64),
@@ -128,6 +132,8 @@ SIGNATURES = {
     "rme_serve_close_stream": (C.c_int, [_vp, _i32]),
     "rme_serve_stop": (C.c_int, [_vp]),
     "rme_probe_int_peak": (C.c_int, [_i32, C.POINTER(C.c_double)]),
+    "rme_search_given_noalloc": (C.c_int, [C.POINTER(PictureDesc), C.POINTER(Params), C.POINTER(PlaneSet),
+                                           C.POINTER(PlaneSet), _i32, _vp, _i32, _vp, _vp]),
 }
 
 PACKAGE_DIR = Path(__file__).resolve().parent
