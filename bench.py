@@ -138,22 +138,29 @@ def dist_setup(args):
     return world, rank, local
 
 
-def max_over_ranks(x: float, world: int) -> float:
+def max_over_ranks(x: float, world: int, device: str = "cuda") -> float:
+    """The slowest rank's time: replicas are timed as a whole job."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
 
-def barrier(world: int):
+def barrier(world: int, device: str = "cuda"):
     if world > 1:
         import torch
         import torch.distributed as dist
         dist.barrier()
-        torch.cuda.synchronize()
+        if device == "cuda":
+            torch.cuda.synchronize()
+
+
+def job_rate(world: int, frames_per_step: int, steps: int, seconds: float) -> float:
+    """Whole-job frames/s: every rank searches its own frames (weak scaling)."""
+    return world * frames_per_step * steps / seconds
 
 
 def run_reference(args, world, rank):
@@ -244,7 +251,7 @@ def run_ours(args, world, rank, local):
     barrier(world)
     elapsed = max_over_ranks(elapsed, world)
     frames_per_step = len(batch)
-    value = world * frames_per_step * args.steps / elapsed
+    value = job_rate(world, frames_per_step, args.steps, elapsed)
     clocks = clk.summary()
 
     # ---- end to end through the C ABI from pinned host memory --------------------
@@ -269,7 +276,7 @@ def run_ours(args, world, rank, local):
         e2e_out = e2e_step()
     torch.cuda.synchronize()
     e2e_secs = max_over_ranks(time.perf_counter() - a, world)
-    e2e_value = world * frames_per_step * args.steps / e2e_secs
+    e2e_value = job_rate(world, frames_per_step, args.steps, e2e_secs)
     for o, q in zip(e2e_out, plain_out):
         if not (o == q).all():
             raise SystemExit("end-to-end results differ from the per-frame path")

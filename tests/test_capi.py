@@ -1,0 +1,106 @@
+"""The C ABI without a GPU: every declared entry point is exported and bound,
+and the host-side logic (defaults, the STANDALONE block enumeration, the
+decision over results) equals the oracle's."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle
+import rivet_h26x_codecs_b200.capi as capi
+import rivet_h26x_codecs_b200.host as host
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "rivet_me.h"
+
+
+def declared():
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    return sorted(set(re.findall(r"\b(rme_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_the_library_exports_every_declared_entry_point():
+    names = declared()
+    assert len(names) >= 25
+    lib = capi.lib()
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(names) == set(capi.SIGNATURES), set(names) ^ set(capi.SIGNATURES)
+
+
+def test_struct_layouts_match_the_header():
+    assert C.sizeof(capi.Mv) == 4
+    assert C.sizeof(capi.Result) == 32
+    assert C.sizeof(capi.Job) == 28 + 4 * 2 + 4 * capi.RME_MAX_SEEDS
+    assert C.sizeof(capi.Params) == 19 * 4
+
+
+def test_defaults_are_the_oracles():
+    for codec, qp in [(capi.RME_CODEC_H264, 28), (capi.RME_CODEC_HEVC, 32)]:
+        a, b = capi.default_params(codec, qp), oracle.params(codec, qp)
+        for name, _ in capi.Params._fields_:
+            assert getattr(a, name) == getattr(b, name), name
+
+
+@pytest.mark.parametrize("codec,w,h,mask", [(capi.RME_CODEC_HEVC, 1920, 1080, 0xF), (capi.RME_CODEC_HEVC, 200, 136, 0b1010),
+                                            (capi.RME_CODEC_H264, 352, 288, 0), (capi.RME_CODEC_H264, 100, 70, 0)])
+def test_standalone_blocks_are_the_oracles(codec, w, h, mask):
+    p = capi.default_params(codec, 30)
+    if mask:
+        p.hevc_pu_mask = mask
+    got = host.standalone_blocks(codec, w, h, 8, p)
+    d = capi.PictureDesc(codec, 8, w, h, w)
+    want = oracle.standalone_blocks(d, p)
+    np.testing.assert_array_equal(got, want)
+    if (codec, w, h, mask) == (capi.RME_CODEC_HEVC, 1920, 1080, 0xF):
+        assert len(got) == 32400 + 8040 + 1980 + 480
+
+
+@pytest.mark.parametrize("w,h,mask,nref", [(1920, 1080, 0xF, 2), (200, 136, 0xF, 3), (136, 200, 0b1011, 1)])
+def test_the_hevc_decision_is_the_oracles(w, h, mask, nref):
+    p = capi.default_params(capi.RME_CODEC_HEVC, 32)
+    p.hevc_pu_mask = mask
+    nb = len(host.standalone_blocks(capi.RME_CODEC_HEVC, w, h, 8, p))
+    rng = np.random.default_rng(w + h + nref)
+    res = np.zeros(nb * nref, capi.RESULT_DTYPE)
+    res["cost"] = rng.integers(0, 5000, size=len(res))
+    res["cost"][: len(res) // 2 * 2: 2] = res["cost"][1: len(res) // 2 * 2: 2]  # ties between references
+    best, part = host.hevc_decide(w, h, 8, p, nref, res)
+    d = capi.PictureDesc(capi.RME_CODEC_HEVC, 8, w, h, w)
+    obest, opart = oracle.hevc_decide(d, p, nref, res)
+    np.testing.assert_array_equal(best, obest)
+    np.testing.assert_array_equal(part, opart)
+    assert set(np.unique(part)) <= {0, 3, 4, 5, 6}
+
+
+def test_a_context_without_a_device_fails_cleanly():
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a device is present")
+    except ImportError:
+        pass
+    h = C.c_void_p()
+    assert capi.lib().rme_ctx_create(C.byref(h), 0) == capi.RME_ECUDA
+
+
+def test_invalid_arguments_are_refused_without_a_device():
+    lib = capi.lib()
+    n = C.c_int32()
+    bad = capi.PictureDesc(7, 8, 64, 64, 64)
+    assert lib.rme_standalone_blocks(C.byref(bad), C.byref(capi.default_params(1, 30)), None, C.byref(n)) == capi.RME_EINVAL
+    deep = capi.PictureDesc(1, 16, 64, 64, 64)
+    assert lib.rme_standalone_blocks(C.byref(deep), C.byref(capi.default_params(1, 30)), None, C.byref(n)) == capi.RME_EINVAL
+    d = capi.PictureDesc(1, 8, 64, 64, 64)
+    p = capi.default_params(1, 30)
+    p.predictor_mode = capi.RME_PRED_GIVEN
+    ps = capi.PlaneSet(16, 224 * 224, 224, 80)
+    refs = (capi.PlaneSet * 1)(ps)
+    # the search without allocation refuses more jobs than its fixed scratch holds
+    assert lib.rme_search_given_noalloc(C.byref(d), C.byref(p), C.byref(ps), refs, 1, C.c_void_p(16), 65537,
+                                        C.c_void_p(16), None) == capi.RME_EINVAL
+    # and a misaligned plane
+    mis = capi.PlaneSet(18, 224 * 224, 224, 80)
+    assert lib.rme_search_given_noalloc(C.byref(d), C.byref(p), C.byref(mis), refs, 1, C.c_void_p(16), 4,
+                                        C.c_void_p(16), None) == capi.RME_EINVAL

@@ -199,3 +199,19 @@ def test_h264_integral_translation_is_found_exactly(ms, d):
     assert_results_equal(got, want, f"translation {d}")
     centre = got[4]  # the middle macroblock of the 3x3 picture
     assert (centre["mvx"], centre["mvy"]) == (d[0] * 4, d[1] * 4)
+
+
+# ---- the committed golden fixtures ------------------------------------------------
+@pytest.mark.parametrize("name", ["h264_96x64_medium", "h264_96x64_umh", "hevc_128x96_medium",
+                                  "hevc_128x96_rings_cross", "hevc_96x64_10bit"])
+def test_the_gpu_reproduces_the_golden_fixtures(ms, name):
+    from pathlib import Path
+    z = np.load(Path(__file__).resolve().parent / "golden" / f"{name}.npz")
+    codec, bd = int(z["codec"]), int(z["bit_depth"])
+    p = oracle.params(codec, int(z["qp"]), **dict(eval(str(z["params"]))))
+    ms.upload(900, z["src"], codec, bd, as_ref=False)
+    refs = list(z["refs"])
+    for i, r in enumerate(refs):
+        ms.upload(901 + i, r, codec, bd, as_ref=True)
+    got = ms.search(900, [901 + i for i in range(len(refs))], p)
+    assert_results_equal(got, z["results"].view(capi.RESULT_DTYPE), name)
