@@ -431,8 +431,11 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
     if (ntask[i] >= (1 << 24)) return fail(c, RME_EINVAL, "more than 2^24 tasks in one frame");
   // `out` may be device memory: the kernels then write it directly.
   cudaPointerAttributes pa{};
-  const bool dev_out = cudaPointerGetAttributes(&pa, out) == cudaSuccess && pa.type == cudaMemoryTypeDevice;
+  // Pinned host memory takes the results straight from the device buffer.
+  const bool known = cudaPointerGetAttributes(&pa, out) == cudaSuccess;
   cudaGetLastError();  // a host pointer unknown to CUDA is not an error here
+  const bool dev_out = known && pa.type == cudaMemoryTypeDevice;
+  const bool pinned_out = known && pa.type == cudaMemoryTypeHost;
   CK(c->d_frames.ensure(n));
   if (!dev_out) CK(c->d_out.ensure(std::max<int64_t>(total, 1)));
   CK(c->d_pending.ensure(std::max<int64_t>(total, 1)));
@@ -443,7 +446,7 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   if (c->d_ready.p != old_ready) c->epoch = 0;
   CK(c->d_jobs.ensure(std::max<int64_t>(jobs_off[n], 1)));
   CK(c->d_misc.ensure(16));
-  if (!dev_out) CK(c->h_out.ensure(std::max<int64_t>(total, 1)));
+  if (!dev_out && !pinned_out) CK(c->h_out.ensure(std::max<int64_t>(total, 1)));
   CK(c->h_misc.ensure(16));
   if (c->epoch == 0 || c->epoch == 0xffffffffu) {
     CK(cudaMemsetAsync(c->d_ready.p, 0, c->d_ready.n * sizeof(unsigned long long), s));
@@ -455,7 +458,7 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   // own sample width, with its own part of the slots).
   std::vector<int64_t> sig;
   sig.push_back(n);
-  sig.push_back(dev_out);
+  sig.push_back(dev_out + 2 * pinned_out);
   std::vector<unsigned long long> init[2];
   int64_t part_tasks[2] = {0, 0};
   for (int i = 0; i < n; ++i) part_tasks[c->h_frames.p[i].bd > 8] += ntask[i];
@@ -546,7 +549,7 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
     if (e == cudaSuccess && n8 > 0) e = launch_search(L8, 1, grid_for(n8, c->bps8), s);
     if (e == cudaSuccess && n16 > 0) e = launch_search(L16, 2, grid_for(n16, c->bps16), s);
     if (e == cudaSuccess) e = cudaEventRecordWithFlags(c->ev1, s, rec);
-    if (e == cudaSuccess && !dev_out)
+    if (e == cudaSuccess && !dev_out && !pinned_out)
       e = cudaMemcpyAsync(c->h_out.p, c->d_out.p, sizeof(rme_result) * total, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(c->h_misc.p, c->d_misc.p, 16 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
@@ -580,6 +583,18 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   } else {
     CK(enqueue(false));
   }
+  if (pinned_out) {
+    // One copy per run of frames whose results are contiguous in `out`.
+    for (int i = 0; i < n;) {
+      int j = i + 1;
+      while (j < n && (!offsets || offsets[j] == offsets[i] + (toff[j] - toff[i]))) ++j;
+      const int64_t off = offsets ? offsets[i] : toff[i];
+      if (toff[j] > toff[i])
+        CK(cudaMemcpyAsync(out + off, c->d_out.p + toff[i], sizeof(rme_result) * (toff[j] - toff[i]),
+                           cudaMemcpyDeviceToHost, s));
+      i = j;
+    }
+  }
   CK(cudaStreamSynchronize(s));
   uint32_t status = (uint32_t)(c->h_misc.p[9] & 0xffffffffu);
   float ms = 0.0f;
@@ -596,7 +611,7 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   if (c->last.tasks != (unsigned long long)total)
     return fail(c, RME_EDEVICE, "the launch ran " + std::to_string(c->last.tasks) + " of " + std::to_string(total) +
                                     " tasks");
-  if (dev_out) return 0;
+  if (dev_out || pinned_out) return 0;
   for (int i = 0; i < n; ++i) {
     int64_t off = offsets ? offsets[i] : toff[i];
     std::memcpy(out + off, c->h_out.p + toff[i], sizeof(rme_result) * ntask[i]);

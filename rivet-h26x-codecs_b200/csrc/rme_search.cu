@@ -416,19 +416,26 @@ __device__ void hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t,
     w = h = N;
     // The AMVP pair from the left and upper results of this level, the
     // parent seed from the enclosing block one evaluated size up (all of
-    // them finished: the task was queued after its last dependency).
+    // them finished: the task was queued after its last dependency). Lanes
+    // 0, 1, 2 load them together.
+    int didx = -1;
+    if (lane == 0 && lbx > 0) didx = (F.base[l] + local - 1) * F.nref + r;
+    if (lane == 1 && lby > 0) didx = (F.base[l] + local - nbx) * F.nref + r;
+    if (lane == 2 && l > 0) {
+      const int Np = F.size[l - 1], px = x / Np, py = y / Np;
+      if (px < F.nbx[l - 1] && py < F.nby[l - 1]) didx = (F.base[l - 1] + py * F.nbx[l - 1] + px) * F.nref + r;
+    }
+    const uint32_t dv = didx >= 0 ? ldcg_u32(&F.out[didx].mv) : 0u;
+    const uint32_t have = __ballot_sync(kFull, didx >= 0);
+    const uint32_t va = __shfl_sync(kFull, dv, 0), vb = __shfl_sync(kFull, dv, 1), vp = __shfl_sync(kFull, dv, 2);
     int na = 0, ax = 0, ay = 0, cx = 0, cy = 0;
-    if (lbx > 0) {
-      const int idx = (F.base[l] + local - 1) * F.nref + r;
-      const uint32_t v = ldcg_u32(&F.out[idx].mv);
-      ax = mvx_of(v);
-      ay = mvy_of(v);
+    if (have & 1u) {
+      ax = mvx_of(va);
+      ay = mvy_of(va);
       na = 1;
     }
-    if (lby > 0) {
-      const int idx = (F.base[l] + local - nbx) * F.nref + r;
-      const uint32_t v = ldcg_u32(&F.out[idx].mv);
-      const int qx = mvx_of(v), qy = mvy_of(v);
+    if (have & 2u) {
+      const int qx = mvx_of(vb), qy = mvy_of(vb);
       if (na == 0) {
         ax = qx;
         ay = qy;
@@ -443,18 +450,8 @@ __device__ void hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t,
     p0y = na > 0 ? ay : 0;
     p1x = na > 1 ? cx : 0;
     p1y = na > 1 ? cy : 0;
-    ns = 3;
-    int psx = 0, psy = 0;
-    if (l > 0) {
-      const int Np = F.size[l - 1], px = x / Np, py = y / Np;
-      if (px < F.nbx[l - 1] && py < F.nby[l - 1]) {
-        const int idx = (F.base[l - 1] + py * F.nbx[l - 1] + px) * F.nref + r;
-        const uint32_t v = ldcg_u32(&F.out[idx].mv);
-        psx = mvx_of(v);
-        psy = mvy_of(v);
-        ns = 4;
-      }
-    }
+    ns = (have & 4u) ? 4 : 3;
+    const int psx = mvx_of(vp), psy = mvy_of(vp);
     // seeds = [zero, mvp0, mvp1, parent] (h265_me.rs:1327-1348)
     sx = lane == 1 ? p0x : lane == 2 ? p1x : lane == 3 ? psx : 0;
     sy = lane == 1 ? p0y : lane == 2 ? p1y : lane == 3 ? psy : 0;
@@ -592,18 +589,31 @@ __device__ void hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t,
     }
   }
   write_result(out, bmx, bmy, r, bc, bsatd, imx, imy, int_cost, nsad, nsatd, lane);
-  if (F.mode != RME_PRED_GIVEN && lane == 0) {
+  if (F.mode != RME_PRED_GIVEN) {
     // The tasks reading this result: right and lower neighbours of this
-    // level, the blocks of the next evaluated size inside this one.
-    __threadfence();
-    if (lbx + 1 < F.nbx[l]) release(L, F, f, (F.base[l] + local + 1) * F.nref + r);
-    if (lby + 1 < F.nby[l]) release(L, F, f, (F.base[l] + local + F.nbx[l]) * F.nref + r);
+    // level, the blocks of the next evaluated size inside this one. Lane 0's
+    // result is fenced, then each lane releases one of them.
+    if (lane == 0) __threadfence();
+    __syncwarp();
+    int ncx = 0, ncy = 0, cx0 = 0, cy0 = 0;
     if (l + 1 < F.nlevels) {
       const int N = F.size[l], M = F.size[l + 1];
-      const int cx1 = min((lbx + 1) * N / M, F.nbx[l + 1]), cy1 = min((lby + 1) * N / M, F.nby[l + 1]);
-      for (int cy = lby * N / M; cy < cy1; ++cy)
-        for (int cx = lbx * N / M; cx < cx1; ++cx)
-          release(L, F, f, (F.base[l + 1] + cy * F.nbx[l + 1] + cx) * F.nref + r);
+      cx0 = lbx * N / M;
+      cy0 = lby * N / M;
+      ncx = max(0, min((lbx + 1) * N / M, F.nbx[l + 1]) - cx0);
+      ncy = max(0, min((lby + 1) * N / M, F.nby[l + 1]) - cy0);
+    }
+    for (int k = lane; k < 2 + ncx * ncy; k += 32) {
+      int dtask = -1;
+      if (k == 0) {
+        if (lbx + 1 < F.nbx[l]) dtask = (F.base[l] + local + 1) * F.nref + r;
+      } else if (k == 1) {
+        if (lby + 1 < F.nby[l]) dtask = (F.base[l] + local + F.nbx[l]) * F.nref + r;
+      } else {
+        const int c = k - 2, cy = cy0 + c / ncx, cx = cx0 + c % ncx;
+        dtask = (F.base[l + 1] + cy * F.nbx[l + 1] + cx) * F.nref + r;
+      }
+      if (dtask >= 0) release(L, F, f, dtask);
     }
   }
   count_task(sm, lane, nsad, nsatd, w * h);
@@ -934,18 +944,37 @@ __device__ void h264_task(const LaunchDesc& L, const FrameDesc& F, int f, int t,
     // neighbours' final 16x16 results as the motion context.
     const int mbw = F.width / 16, mx = t % mbw, my = t / mbw;
     shape(mx * 16, my * 16, 16, 16);
-    auto nb = [&](int qx, int qy) {
+    // Lanes 0..3 load the A, B, C, D neighbours' results together.
+    int nqx = mx, nqy = my;
+    if (lane == 0) nqx = mx - 1;
+    if (lane == 1) nqy = my - 1;
+    if (lane == 2) {
+      nqx = mx + 1;
+      nqy = my - 1;
+    }
+    if (lane == 3) {
+      nqx = mx - 1;
+      nqy = my - 1;
+    }
+    const bool nok = lane < 4 && nqx >= 0 && nqy >= 0 && nqx < mbw;
+    uint32_t nmv = 0, nref = 0;
+    if (nok) {
+      nmv = ldcg_u32(&F.out[nqy * mbw + nqx].mv);
+      nref = ldcg_u32(reinterpret_cast<const uint32_t*>(&F.out[nqy * mbw + nqx].ref));
+    }
+    const uint32_t navail = __ballot_sync(kFull, nok);
+    auto nb = [&](int k) {
       Nb m{false, -1, 0, 0};
-      if (qx < 0 || qy < 0 || qx >= mbw) return m;
-      const int idx = qy * mbw + qx;
-      const uint32_t v = ldcg_u32(&F.out[idx].mv);
+      const uint32_t v = __shfl_sync(kFull, nmv, k);
+      const int rf = (int)__shfl_sync(kFull, nref, k);
+      if (!((navail >> k) & 1u)) return m;
       m.avail = true;
-      m.ref = (int)ldcg_u32(&F.out[idx].ref);
+      m.ref = rf;
       m.x = mvx_of(v);
       m.y = mvy_of(v);
       return m;
     };
-    const Nb A = nb(mx - 1, my), Bn = nb(mx, my - 1), C = nb(mx + 1, my - 1), D = nb(mx - 1, my - 1);
+    const Nb A = nb(0), Bn = nb(1), C = nb(2), D = nb(3);
     const Nb Cc = C.avail ? C : D;
     // p_skip_mv (h264/mb.rs:1235-1246)
     int skx = 0, sky = 0;
@@ -1021,17 +1050,26 @@ __device__ void h264_task(const LaunchDesc& L, const FrameDesc& F, int f, int t,
       }
     }
     write_result(&F.out[t], mv16x, mv16y, r16, c16, s16, mi16x, mi16y, ci16, nsad, nsatd, lane);
+    // The macroblocks whose A, B, C or D this one is, one per lane.
+    const int mbh = F.height / 16;
+    if (lane == 0) __threadfence();
+    __syncwarp();
+    bool rel = false;
+    int dtask = 0;
     if (lane == 0) {
-      // The macroblocks whose A, B, C or D this one is.
-      const int mbh = F.height / 16;
-      __threadfence();
-      if (mx + 1 < mbw) release(L, F, f, t + 1);
-      if (my + 1 < mbh) {
-        if (mx > 0) release(L, F, f, t + mbw - 1);
-        release(L, F, f, t + mbw);
-        if (mx + 1 < mbw) release(L, F, f, t + mbw + 1);
-      }
+      rel = mx + 1 < mbw;
+      dtask = t + 1;
+    } else if (lane == 1) {
+      rel = my + 1 < mbh && mx > 0;
+      dtask = t + mbw - 1;
+    } else if (lane == 2) {
+      rel = my + 1 < mbh;
+      dtask = t + mbw;
+    } else if (lane == 3) {
+      rel = my + 1 < mbh && mx + 1 < mbw;
+      dtask = t + mbw + 1;
     }
+    if (rel) release(L, F, f, dtask);
   }
   count_task(sm, lane, nsad, nsatd, B.w * B.h);
 }

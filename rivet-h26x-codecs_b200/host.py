@@ -118,8 +118,15 @@ class MotionSearch:
         return out
 
     def search_batch(self, frames: Sequence[tuple[int, Sequence[int]]],
-                     params: capi.Params | Sequence[capi.Params], stream: int = 0) -> list[np.ndarray]:
-        """Many STANDALONE frames (src_id, ref_ids) in one persistent launch."""
+                     params: capi.Params | Sequence[capi.Params], stream: int = 0, out=None) -> list:
+        """Many STANDALONE frames (src_id, ref_ids) in one persistent launch.
+
+        `out` is where the results go: None (a new host array), a structured
+        array of capi.RESULT_DTYPE, or a tensor (device memory, or pinned
+        host memory) of at least 32 bytes per result. Device memory keeps the
+        results on the device; pinned memory takes them in one direct copy.
+        Returns one view of `out` per frame (tensor views are uint8 bytes).
+        """
         n = len(frames)
         if isinstance(params, capi.Params):
             params = [params] * n
@@ -128,10 +135,33 @@ class MotionSearch:
         counts = [self.result_count(s, r, p) for (s, r), p in zip(frames, params)]
         offs = np.zeros(n, np.int64)
         offs[1:] = np.cumsum(counts)[:-1]
-        out = np.zeros(int(sum(counts)), capi.RESULT_DTYPE)
-        self._check(self._lib.rme_batch_search(self.ctx, fa, pa, n, C.cast(out.ctypes.data, C.POINTER(capi.Result)),
+        total = int(sum(counts))
+        rsize = capi.RESULT_DTYPE.itemsize
+        if out is None:
+            out = np.zeros(total, capi.RESULT_DTYPE)
+        if hasattr(out, "data_ptr"):
+            nbytes = out.numel() * out.element_size()
+            if nbytes < total * rsize:
+                raise ValueError(f"out holds {nbytes} bytes, the results need {total * rsize}")
+            addr = out.data_ptr()
+        else:
+            if out.dtype != capi.RESULT_DTYPE or out.size < total or not out.flags.c_contiguous:
+                raise ValueError("out must be a contiguous RESULT_DTYPE array of at least the result count")
+            addr = out.ctypes.data
+        self._check(self._lib.rme_batch_search(self.ctx, fa, pa, n, C.cast(C.c_void_p(addr), C.POINTER(capi.Result)),
                                                offs.ctypes.data_as(C.POINTER(C.c_int64)), C.c_void_p(stream)))
+        if hasattr(out, "data_ptr"):
+            import torch
+            flat = out.view(-1).view(torch.uint8)
+            return [flat[o * rsize:(o + c) * rsize] for o, c in zip(offs, counts)]
         return [out[o:o + c] for o, c in zip(offs, counts)]
+
+    def batch_result_count(self, frames: Sequence[tuple[int, Sequence[int]]],
+                           params: capi.Params | Sequence[capi.Params]) -> int:
+        """Results a search_batch of these frames returns (all frames)."""
+        if isinstance(params, capi.Params):
+            params = [params] * len(frames)
+        return int(sum(self.result_count(s, r, p) for (s, r), p in zip(frames, params)))
 
     def stats(self) -> capi.Stats:
         s = capi.Stats()

@@ -164,6 +164,30 @@ def test_batch_equals_the_frames_and_the_oracle(ms):
             assert_results_equal(got, want, f"batch vs oracle {s}")
 
 
+def test_batch_results_into_device_and_pinned_memory(ms):
+    """The batched search writing its results to a device tensor (they stay
+    there) and to pinned host memory (one direct copy) equals the host-array
+    form."""
+    import torch
+    seq = synth.make_sequence(HEVC, 192, 128, 8, 4, 33, 64, 64, 2.0)
+    p = oracle.params(HEVC, 30)
+    for i, f in enumerate(seq.frames):
+        ms.upload(500 + i, f, HEVC, 8, as_ref=True)
+    frames = [(500 + t, [500 + t - 1]) for t in range(1, 4)]
+    want = ms.search_batch(frames, p)
+    n = ms.batch_result_count(frames, p)
+    dev = torch.zeros(n * 32 + 64, dtype=torch.uint8, device="cuda:0")
+    pin = torch.zeros(n * 32, dtype=torch.uint8, pin_memory=True)
+    for _ in range(2):
+        got_dev = ms.search_batch(frames, p, out=dev)
+        got_pin = ms.search_batch(frames, p, out=pin)
+        for w, d, q in zip(want, got_dev, got_pin):
+            assert_results_equal(d.cpu().numpy().view(capi.RESULT_DTYPE), w, "device out")
+            assert_results_equal(q.numpy().view(capi.RESULT_DTYPE), w, "pinned out")
+    with pytest.raises(ValueError):
+        ms.search_batch(frames, p, out=torch.zeros(n * 32 - 1, dtype=torch.uint8, device="cuda:0"))
+
+
 # ---- the reference's search-behaviour tests, through the library --------------
 def grating(w, h):
     """The reference tests' triangle grating (h265_me.rs:4989-5026,
