@@ -31,6 +31,17 @@ using namespace rme;
 
 namespace {
 
+// A launch's tasks split into parts by kind, one search kernel each:
+// part = 2 * (deeper than 8 bits) + (H.264).
+constexpr int kParts = 4;
+// The launch header in device memory (u64 words): head and tail of each
+// part's queue, then the counters, the status word and the epoch.
+constexpr int kMiscCounters = 8, kMiscStatus = 13, kMiscEpoch = 14;
+
+int part_of(const FrameDesc& fd) { return 2 * (fd.bd > 8) + (fd.codec == RME_CODEC_H264); }
+int part_bytes(int k) { return k >= 2 ? 2 : 1; }
+int part_codec(int k) { return (k & 1) ? RME_CODEC_H264 : RME_CODEC_HEVC; }
+
 // ---- Lagrangian tables -------------------------------------------------------
 float h264_mvd_bits(int d) {  // h264_hpel.rs:407-429
   uint32_t a = (uint32_t)std::abs(d);
@@ -138,8 +149,13 @@ struct Graph {
 };
 
 struct Ctx {
-  int device = 0, nsm = 0, bps8 = 0, bps16 = 0;
+  int device = 0, nsm = 0;
+  int bps[kParts] = {0, 0, 0, 0};  // resident search blocks per SM, per part
   cudaStream_t stream = nullptr;
+  // The parts of a launch after the first run on streams of their own,
+  // forked from and joined back to the caller's stream.
+  cudaStream_t aux[kParts] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev_fork = nullptr, ev_join[kParts] = {nullptr, nullptr, nullptr, nullptr};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp0 = nullptr, evp1 = nullptr;
   std::map<int, std::unique_ptr<Picture>> pics;
   std::map<std::tuple<int, int, int, uint32_t>, Tables> tables;
@@ -153,7 +169,7 @@ struct Ctx {
   DevBuf<rme_result> d_out;
   DevBuf<int32_t> d_pending;
   DevBuf<rme_job> d_jobs;
-  DevBuf<unsigned long long> d_misc;  // head, counters[5], status
+  DevBuf<unsigned long long> d_misc;  // the launch header (kMisc*)
   DevBuf<uint8_t> d_stage;            // upload staging
   PinBuf<FrameDesc> h_frames;
   PinBuf<rme_result> h_out;
@@ -173,6 +189,11 @@ struct Ctx {
     if (ev1) cudaEventDestroy(ev1);
     if (evp0) cudaEventDestroy(evp0);
     if (evp1) cudaEventDestroy(evp1);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    for (int k = 0; k < kParts; ++k) {
+      if (ev_join[k]) cudaEventDestroy(ev_join[k]);
+      if (aux[k]) cudaStreamDestroy(aux[k]);
+    }
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -459,13 +480,13 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   std::vector<int64_t> sig;
   sig.push_back(n);
   sig.push_back(dev_out + 2 * pinned_out);
-  std::vector<unsigned long long> init[2];
-  int64_t part_tasks[2] = {0, 0};
-  for (int i = 0; i < n; ++i) part_tasks[c->h_frames.p[i].bd > 8] += ntask[i];
+  std::vector<unsigned long long> init[kParts];
+  int64_t part_tasks[kParts] = {0, 0, 0, 0};
+  for (int i = 0; i < n; ++i) part_tasks[part_of(c->h_frames.p[i])] += ntask[i];
   std::vector<std::pair<const int32_t*, int>> pend_copies;  // (template, frame)
   for (int i = 0; i < n; ++i) {
     FrameDesc& fd = c->h_frames.p[i];
-    const int wide = fd.bd > 8;
+    const int part = part_of(fd);
     fd.out = dev_out ? out + (offsets ? offsets[i] : toff[i]) : c->d_out.p + toff[i];
     fd.pending = c->d_pending.p + toff[i];
     const unsigned long long tag = ((unsigned long long)c->epoch << 32) | ((unsigned long long)i << 24);
@@ -474,7 +495,7 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
       if (frames[i].njobs > 0)
         CK(cudaMemcpyAsync(c->d_jobs.p + jobs_off[i], frames[i].jobs, sizeof(rme_job) * frames[i].njobs,
                            cudaMemcpyHostToDevice, s));
-      for (int t = 0; t < ntask[i]; ++t) init[wide].push_back(tag | (uint32_t)t);
+      for (int t = 0; t < ntask[i]; ++t) init[part].push_back(tag | (uint32_t)t);
       sig.push_back(-1);
       sig.push_back(frames[i].njobs);
       sig.push_back(fd.bd);
@@ -485,7 +506,7 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
       const Deps* dp = get_deps(c, src->d, &params[i], frames[i].nref, &rc);
       if (!dp) return rc;
       pend_copies.emplace_back(dp->pending, i);
-      for (uint32_t t : dp->ready) init[wide].push_back(tag | t);
+      for (uint32_t t : dp->ready) init[part].push_back(tag | t);
       sig.push_back(fd.bd);
       sig.push_back(fd.codec);
       sig.push_back(fd.width);
@@ -495,41 +516,51 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
     }
   }
   // Frames' first tasks interleaved, so every frame starts at once.
-  for (int w = 0; w < 2; ++w)
-    std::stable_sort(init[w].begin(), init[w].end(), [](unsigned long long a, unsigned long long b) {
+  for (int k = 0; k < kParts; ++k)
+    std::stable_sort(init[k].begin(), init[k].end(), [](unsigned long long a, unsigned long long b) {
       return (a & 0xffffffu) < (b & 0xffffffu);
     });
-  const int64_t n8 = part_tasks[0], n16 = part_tasks[1];
-  const size_t ninit = init[0].size() + init[1].size();
-  // h_init: [head8, tail8, head16, tail16, counters x5, status, epoch, pad x5 | entries]
+  // h_init: [head, tail of each part | counters x5, status, epoch, pad | entries]
+  size_t ninit = 0, init_off[kParts];
+  for (int k = 0; k < kParts; ++k) {
+    init_off[k] = ninit;
+    ninit += init[k].size();
+  }
   CK(c->h_init.ensure(16 + ninit));
   unsigned long long* hi = c->h_init.p;
   std::memset(hi, 0, 16 * sizeof(unsigned long long));
-  hi[1] = init[0].size();
-  hi[3] = init[1].size();
-  hi[10] = c->epoch;
-  std::memcpy(hi + 16, init[0].data(), init[0].size() * sizeof(unsigned long long));
-  std::memcpy(hi + 16 + init[0].size(), init[1].data(), init[1].size() * sizeof(unsigned long long));
-  LaunchDesc L8, L16;
-  L8.frames = L16.frames = c->d_frames.p;
-  L8.ready = c->d_ready.p;
-  L16.ready = c->d_ready.p + n8;
-  L8.total = n8;
-  L16.total = n16;
-  L8.head = c->d_misc.p;
-  L8.tail = c->d_misc.p + 1;
-  L16.head = c->d_misc.p + 2;
-  L16.tail = c->d_misc.p + 3;
-  L8.counters = L16.counters = c->d_misc.p + 4;
-  L8.status = L16.status = reinterpret_cast<uint32_t*>(c->d_misc.p + 9);
-  L8.epoch = L16.epoch = reinterpret_cast<const uint32_t*>(c->d_misc.p + 10);
-  if (!c->bps8) c->bps8 = search_blocks_per_sm(1);
-  if (!c->bps16) c->bps16 = search_blocks_per_sm(2);
+  hi[kMiscEpoch] = c->epoch;
+  LaunchDesc Ls[kParts];
+  int64_t slot0 = 0, slot_off[kParts];
+  for (int k = 0; k < kParts; ++k) {
+    hi[2 * k + 1] = init[k].size();
+    std::memcpy(hi + 16 + init_off[k], init[k].data(), init[k].size() * sizeof(unsigned long long));
+    slot_off[k] = slot0;
+    LaunchDesc& L = Ls[k];
+    L.frames = c->d_frames.p;
+    L.ready = c->d_ready.p + slot0;
+    L.total = part_tasks[k];
+    L.head = c->d_misc.p + 2 * k;
+    L.tail = c->d_misc.p + 2 * k + 1;
+    L.counters = c->d_misc.p + kMiscCounters;
+    L.status = reinterpret_cast<uint32_t*>(c->d_misc.p + kMiscStatus);
+    L.epoch = reinterpret_cast<const uint32_t*>(c->d_misc.p + kMiscEpoch);
+    slot0 += part_tasks[k];
+    if (part_tasks[k] > 0 && !c->bps[k]) c->bps[k] = search_blocks_per_sm(part_bytes(k), part_codec(k));
+  }
+  int nparts = 0, order[kParts];
+  for (int k = 0; k < kParts; ++k)
+    if (part_tasks[k] > 0) order[nparts++] = k;
+  for (int j = 1; j < nparts; ++j) {
+    if (!c->aux[j]) CK(cudaStreamCreateWithFlags(&c->aux[j], cudaStreamNonBlocking));
+    if (!c->ev_join[j]) CK(cudaEventCreateWithFlags(&c->ev_join[j], cudaEventDisableTiming));
+  }
+  if (nparts > 1 && !c->ev_fork) CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
   auto grid_for = [&](int64_t tasks, int bps) {
     int64_t want = (tasks + kWarpsPerBlock - 1) / kWarpsPerBlock;
     return (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)c->nsm * bps, want));
   };
-  const size_t n0 = init[0].size(), n1 = init[1].size();
+  sig.push_back(nparts);
   auto enqueue = [&](bool capturing) -> cudaError_t {
     const unsigned rec = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
     cudaError_t e = cudaMemcpyAsync(c->d_frames.p, c->h_frames.p, sizeof(FrameDesc) * n, cudaMemcpyHostToDevice, s);
@@ -539,15 +570,24 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
                             cudaMemcpyDeviceToDevice, s);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(c->d_misc.p, hi, 16 * sizeof(unsigned long long), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess && n0)
-      e = cudaMemcpyAsync(c->d_ready.p, hi + 16, n0 * sizeof(unsigned long long), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess && n1)
-      e = cudaMemcpyAsync(c->d_ready.p + n8, hi + 16 + n0, n1 * sizeof(unsigned long long), cudaMemcpyHostToDevice, s);
+    for (int k = 0; k < kParts; ++k)
+      if (e == cudaSuccess && !init[k].empty())
+        e = cudaMemcpyAsync(c->d_ready.p + slot_off[k], hi + 16 + init_off[k],
+                            init[k].size() * sizeof(unsigned long long), cudaMemcpyHostToDevice, s);
     // Under capture the records are external ones: they become event-record
     // nodes, so the kernels' device time is measured on every replay.
     if (e == cudaSuccess) e = cudaEventRecordWithFlags(c->ev0, s, rec);
-    if (e == cudaSuccess && n8 > 0) e = launch_search(L8, 1, grid_for(n8, c->bps8), s);
-    if (e == cudaSuccess && n16 > 0) e = launch_search(L16, 2, grid_for(n16, c->bps16), s);
+    // Parts after the first run concurrently on the auxiliary streams
+    // (parallel branches of a captured graph).
+    if (e == cudaSuccess && nparts > 1) e = cudaEventRecord(c->ev_fork, s);
+    for (int j = 0; j < nparts && e == cudaSuccess; ++j) {
+      const int k = order[j];
+      cudaStream_t sk = j == 0 ? s : c->aux[j];
+      if (j > 0) e = cudaStreamWaitEvent(sk, c->ev_fork, 0);
+      if (e == cudaSuccess) e = launch_search(Ls[k], part_bytes(k), part_codec(k), grid_for(part_tasks[k], c->bps[k]), sk);
+      if (e == cudaSuccess && j > 0) e = cudaEventRecord(c->ev_join[j], sk);
+    }
+    for (int j = 1; j < nparts && e == cudaSuccess; ++j) e = cudaStreamWaitEvent(s, c->ev_join[j], 0);
     if (e == cudaSuccess) e = cudaEventRecordWithFlags(c->ev1, s, rec);
     if (e == cudaSuccess && !dev_out && !pinned_out)
       e = cudaMemcpyAsync(c->h_out.p, c->d_out.p, sizeof(rme_result) * total, cudaMemcpyDeviceToHost, s);
@@ -560,8 +600,7 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   if (use_graph && !has_given) {
     std::vector<int64_t> gsig = sig;
     gsig.push_back(total);
-    gsig.push_back((int64_t)n0);
-    gsig.push_back((int64_t)n1);
+    for (int k = 0; k < kParts; ++k) gsig.push_back((int64_t)init[k].size());
     gsig.push_back((int64_t)(uintptr_t)s);
     gsig.push_back((int64_t)g_buffer_generation);
     Graph& g = c->graphs[gsig];
@@ -596,14 +635,14 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
     }
   }
   CK(cudaStreamSynchronize(s));
-  uint32_t status = (uint32_t)(c->h_misc.p[9] & 0xffffffffu);
+  uint32_t status = (uint32_t)(c->h_misc.p[kMiscStatus] & 0xffffffffu);
   float ms = 0.0f;
   CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
-  c->last.tasks = c->h_misc.p[4];
-  c->last.sad_candidates = c->h_misc.p[5];
-  c->last.satd_candidates = c->h_misc.p[6];
-  c->last.sad_samples = c->h_misc.p[7];
-  c->last.satd_samples = c->h_misc.p[8];
+  c->last.tasks = c->h_misc.p[kMiscCounters];
+  c->last.sad_candidates = c->h_misc.p[kMiscCounters + 1];
+  c->last.satd_candidates = c->h_misc.p[kMiscCounters + 2];
+  c->last.sad_samples = c->h_misc.p[kMiscCounters + 3];
+  c->last.satd_samples = c->h_misc.p[kMiscCounters + 4];
   c->last.kernel_ms = ms;
   c->last.planes_ms = c->planes_ms_acc;
   c->planes_ms_acc = 0.0f;

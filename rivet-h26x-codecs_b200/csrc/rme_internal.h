@@ -80,8 +80,10 @@ cudaError_t launch_pad_plane(const void* src, int bd, int w, int h, int sstride,
                              int pad, cudaStream_t s);
 cudaError_t launch_h264_hpel(DevPlanes p, int bd, int cw, int ch, int pad, cudaStream_t s);
 cudaError_t launch_hevc_phases(DevPlanes p, int bd, int w, int h, int pad, cudaStream_t s);
-cudaError_t launch_search(const LaunchDesc& L, int bytes_per_sample_max, int grid, cudaStream_t s);
-int search_blocks_per_sm(int bytes_per_sample_max);
+// The search over one kind of task (sample width, codec): `grid` persistent
+// blocks pulling from L's queue.
+cudaError_t launch_search(const LaunchDesc& L, int bytes_per_sample, int codec, int grid, cudaStream_t s);
+int search_blocks_per_sm(int bytes_per_sample, int codec);
 cudaError_t launch_chroma(const void* cb, const void* cr, int bd, int codec, int cw, int ch, int cstride,
                           int nblocks, const int32_t* blocks, const rme_mv* mvs, const int64_t* out_off, void* out,
                           cudaStream_t s);

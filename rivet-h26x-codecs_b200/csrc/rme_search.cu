@@ -1,5 +1,6 @@
-// The motion search on the device: one persistent launch, one warp per
-// (block, reference) task, tasks pulled from a device work queue.
+// The motion search on the device: one persistent launch per kind of task
+// (sample width, codec), one warp per (block, reference) task, tasks pulled
+// from a device work queue.
 //
 // What a task computes is the reference's search, step for step:
 //   HEVC   search_full   (encode/h265_me.rs:3749-3858): seeds rounded
@@ -1074,7 +1075,10 @@ __device__ void h264_task(const LaunchDesc& L, const FrameDesc& F, int f, int t,
   count_task(sm, lane, nsad, nsatd, B.w * B.h);
 }
 
-template <class S>
+// One kernel per (sample width, codec): a launch holds the tasks of one
+// kind, so each kernel carries only its codec's search (a smaller body
+// stays resident in the instruction caches).
+template <class S, int CODEC>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, RME_MIN_BLOCKS) search_kernel(LaunchDesc L) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1094,13 +1098,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, RME_MIN_BLOCKS) search_ke
     if (e == 0xffffffffu) continue;  // the wait ran out (status set)
     const int f = (int)(e >> 24), t = (int)(e & 0xffffffu);
     const FrameDesc& F = L.frames[f];
-    // A task of the other sample width, or past its frame, is a host bug:
-    // flag it and skip it rather than read out of bounds.
-    if (t >= F.ntasks || (sizeof(S) == 1) != (F.bd == 8)) {
+    // A task of another kind, or past its frame, is a host bug: flag it
+    // and skip it rather than read out of bounds.
+    if (t >= F.ntasks || (sizeof(S) == 1) != (F.bd == 8) || F.codec != CODEC) {
       if (lane == 0) atomicOr(L.status, kStatusBadTask);
       continue;
     }
-    if (F.codec == RME_CODEC_HEVC) hevc_task<S>(L, F, f, t, sm, lane);
+    if constexpr (CODEC == RME_CODEC_HEVC) hevc_task<S>(L, F, f, t, sm, lane);
     else h264_task<S>(L, F, f, t, sm, lane);
   }
   __syncwarp();
@@ -1112,33 +1116,40 @@ size_t smem_bytes() {
   return sizeof(WarpSmem<S>) * kWarpsPerBlock;
 }
 
-template <class S>
+template <class S, int CODEC>
 int blocks_per_sm() {
   int n = 0;
-  cudaError_t e = cudaFuncSetAttribute(search_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(search_kernel<S, CODEC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem_bytes<S>());
   if (e == cudaSuccess)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, search_kernel<S>, kWarpsPerBlock * 32, smem_bytes<S>());
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, search_kernel<S, CODEC>, kWarpsPerBlock * 32,
+                                                      smem_bytes<S>());
   return e == cudaSuccess && n > 0 ? n : 1;
 }
 
-template <class S>
+template <class S, int CODEC>
 cudaError_t launch(const LaunchDesc& L, int grid, cudaStream_t s) {
-  cudaError_t e = cudaFuncSetAttribute(search_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(search_kernel<S, CODEC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem_bytes<S>());
   if (e != cudaSuccess) return e;
-  search_kernel<S><<<grid, kWarpsPerBlock * 32, smem_bytes<S>(), s>>>(L);
+  search_kernel<S, CODEC><<<grid, kWarpsPerBlock * 32, smem_bytes<S>(), s>>>(L);
   return cudaGetLastError();
 }
 
 }  // namespace
 
-int search_blocks_per_sm(int bytes_per_sample) {
-  return bytes_per_sample == 1 ? blocks_per_sm<uint8_t>() : blocks_per_sm<uint16_t>();
+int search_blocks_per_sm(int bytes_per_sample, int codec) {
+  if (codec == RME_CODEC_HEVC)
+    return bytes_per_sample == 1 ? blocks_per_sm<uint8_t, RME_CODEC_HEVC>() : blocks_per_sm<uint16_t, RME_CODEC_HEVC>();
+  return bytes_per_sample == 1 ? blocks_per_sm<uint8_t, RME_CODEC_H264>() : blocks_per_sm<uint16_t, RME_CODEC_H264>();
 }
 
-cudaError_t launch_search(const LaunchDesc& L, int bytes_per_sample, int grid, cudaStream_t s) {
-  return bytes_per_sample == 1 ? launch<uint8_t>(L, grid, s) : launch<uint16_t>(L, grid, s);
+cudaError_t launch_search(const LaunchDesc& L, int bytes_per_sample, int codec, int grid, cudaStream_t s) {
+  if (codec == RME_CODEC_HEVC)
+    return bytes_per_sample == 1 ? launch<uint8_t, RME_CODEC_HEVC>(L, grid, s)
+                                 : launch<uint16_t, RME_CODEC_HEVC>(L, grid, s);
+  return bytes_per_sample == 1 ? launch<uint8_t, RME_CODEC_H264>(L, grid, s)
+                               : launch<uint16_t, RME_CODEC_H264>(L, grid, s);
 }
 
 }  // namespace rme
