@@ -347,7 +347,7 @@ struct H264Search {
       py[np] = fy;
       ++np;
     }
-    uint32_t sc[16];
+    uint32_t sc[16] = {};
     for (int k = 0; k < np; ++k) sc[k] = sad_full(px[k], py[k]);
     uint32_t bcost = sc[0];
     for (int k = 1; k < np; ++k)
