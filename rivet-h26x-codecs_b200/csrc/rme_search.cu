@@ -379,6 +379,86 @@ __device__ __forceinline__ uint32_t hevc_rate(float lam, int mx, int my, int p0x
   return __float2uint_rz(__fmul_rn(lam, __uint2float_rn(min(b0, b1) + 1u)));
 }
 
+// ---- HEVC scoring: one lane's part of a candidate ----------------------------
+//
+// A candidate is scored by a group of lanes. For SAD the group is eight
+// lanes and lane `sub` sums rows sub, sub + 8, ...; square blocks of the
+// STANDALONE sizes have their shape fixed at compile time (every load of a
+// row issued before any is used, no division between a step's loads and
+// its decision), other shapes go a word at a time.
+
+template <class S, int WR, int RPL>
+__device__ __forceinline__ uint32_t sad_rows_fixed(const uint32_t* src, const S* rp, int stride, int sub) {
+  constexpr int SPW = 4 / sizeof(S), CW = WR < 8 ? WR : 8, UNR = RPL < 2 ? RPL : 2;
+  uint32_t acc = 0;
+#pragma unroll UNR
+  for (int k = 0; k < RPL; ++k) {
+    const int row = sub + 8 * k;
+    const S* rr = rp + (ptrdiff_t)row * stride;
+    const uint32_t* sr = src + row * WR;
+#pragma unroll
+    for (int c = 0; c < WR; c += CW) {
+      uint32_t a[CW];
+      ldwords<CW>(rr + c * SPW, a);
+#pragma unroll
+      for (int j = 0; j < CW; ++j) acc += vsad(sr[c + j], a[j], S());
+    }
+  }
+  return acc;
+}
+
+template <class S>
+__device__ __forceinline__ uint32_t sad_part(const uint32_t* src, int w, int h, const S* rp, int stride, int sub) {
+  constexpr int SPW = 4 / sizeof(S);
+  if (w == h) {
+    if (w == 8) return sad_rows_fixed<S, 8 / SPW, 1>(src, rp, stride, sub);
+    if (w == 16) return sad_rows_fixed<S, 16 / SPW, 2>(src, rp, stride, sub);
+    if (w == 32) return sad_rows_fixed<S, 32 / SPW, 4>(src, rp, stride, sub);
+    if (w == 64) return sad_rows_fixed<S, 64 / SPW, 8>(src, rp, stride, sub);
+  }
+  const int wr = w / SPW;
+  uint32_t acc = 0;
+  for (int row = sub; row < h; row += 8)
+    for (int k = 0; k < wr; ++k) acc += vsad(src[row * wr + k], ldw(rp + (ptrdiff_t)row * stride + k * SPW), S());
+  return acc;
+}
+
+// SATD: lane `sub` of a group of G lanes takes the 4x4 tiles sub, sub + G,
+// ... (row-major over tw tiles per row) of the candidate whose prediction
+// starts at `pp`; each tile is the Hadamard of dsp/distortion.rs:326-381.
+template <class S>
+__device__ __forceinline__ uint32_t satd_part(const uint32_t* src, int wr, int tw, int ntiles, const S* pp, int stride,
+                                              int sub, int G) {
+  constexpr int SPW = 4 / sizeof(S), WPT = 4 / SPW;  // words per tile row
+  const bool pow2 = (tw & (tw - 1)) == 0;
+  const int sh = __ffs(tw) - 1;
+  uint32_t acc = 0;
+#pragma unroll 2
+  for (int t = sub; t < ntiles; t += G) {
+    const int ty = pow2 ? t >> sh : t / tw, tx = t - ty * tw;
+    uint32_t pw[4][WPT];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) ldwords<WPT>(pp + (ptrdiff_t)(ty * 4 + r) * stride + tx * 4, pw[r]);
+    int d[16];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const uint32_t* srow = &src[(ty * 4 + r) * wr + tx * WPT];
+#pragma unroll
+      for (int k = 0; k < WPT; ++k) {
+        const uint32_t sw = srow[k], qw = pw[r][k];
+#pragma unroll
+        for (int e = 0; e < SPW; ++e) {
+          const int shf = e * (32 / SPW);
+          const uint32_t m = SPW == 4 ? 0xffu : 0xffffu;
+          d[r * 4 + k * SPW + e] = (int)((sw >> shf) & m) - (int)((qw >> shf) & m);
+        }
+      }
+    }
+    acc += satd4x4(d);
+  }
+  return acc;
+}
+
 template <class S>
 __device__ void hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, WarpSmem<S>& sm, int lane) {
   int r, x, y, w, h, ns;
@@ -480,115 +560,128 @@ __device__ void hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t,
   }
   const uint32_t keep = __ballot_sync(kFull, lane < ns && !dup);
   const int nk = __popc(keep);
-  int bx = 0, by = 0;
+  const bool kept = (keep >> lane) & 1u;
+  const int rank = __popc(keep & ((1u << lane) - 1u));
+
+  // search_full as one loop of steps, each scoring four candidates (eight
+  // lanes each; group g = lane / 8): the seeds four at a time, then the
+  // small diamond rounds from a fixed `from`, then (search_rings) the 24
+  // ring points four at a time, a move restarting the diamond. One scoring
+  // site keeps the kernel's code small.
+  const int g = lane >> 3, sub = lane & 7;
+  const int range = F.search_range;
+  int bx = 0, by = 0, ox = 0, oy = 0, cxr = 0, cyr = 0;
   uint32_t bcost = kInf;
-  {
-    const int lpc = lanes_per(nk), cpp = 32 / lpc, sub = lane % lpc;
-    for (int c0 = 0; c0 < nk; c0 += cpp) {
-      const int c = lane / lpc < cpp ? c0 + lane / lpc : nk;
-      const bool ok = c < nk;
-      const int from = ok ? __fns(keep, 0, c + 1) : 0;
-      const int fx = __shfl_sync(kFull, qx, from), fy = __shfl_sync(kFull, qy, from);
-      const uint32_t s = group_sad<S>(sm.src, wr, h, org, stride, lpc, sub, lane, ok, fx, fy);
-      const uint32_t cost = ok ? s + hevc_rate(lam, fx * 4, fy * 4, p0x, p0y, p1x, p1y) : kInf;
-      const Pick p = warp_min(cost);
-      if (p.cost < bcost) {
-        bcost = p.cost;
-        bx = __shfl_sync(kFull, fx, p.lane);
-        by = __shfl_sync(kFull, fy, p.lane);
-      }
-    }
-  }
-  nsad += nk;
-  const int ox = bx, oy = by, range = F.search_range;
-  auto inside = [&](int cx, int cy) {
-    return abs(cx - ox) <= range && abs(cy - oy) <= range && cx >= lox && cx <= hix && cy >= loy && cy <= hiy;
-  };
-  const int lpc4 = lanes_per(4), g4 = lane / lpc4, sub4 = lane % lpc4;
-  const int dx4 = g4 == 0 ? 1 : g4 == 1 ? -1 : 0, dy4 = g4 == 2 ? 1 : g4 == 3 ? -1 : 0;
-  int rings = 0;
+  int state = nk > 0 ? 0 : 1, c0 = 0, it = 0, rings = 0;
+  bool moved = false;
   for (;;) {
-    // The small diamond from a fixed `from` per round.
-    for (int it = 0; it < 2 * range; ++it) {
-      const int fx = bx + dx4, fy = by + dy4;
-      const bool ok = g4 < 4 && inside(fx, fy);
-      const uint32_t s = group_sad<S>(sm.src, wr, h, org, stride, lpc4, sub4, lane, ok, fx, fy);
-      const uint32_t cost = ok ? s + hevc_rate(lam, fx * 4, fy * 4, p0x, p0y, p1x, p1y) : kInf;
-      nsad += __popc(__ballot_sync(kFull, ok && sub4 == 0));
-      const Pick p = warp_min(cost);
-      if (!(p.cost < bcost)) break;
+    if (state == 1 && it >= 2 * range) {  // the diamond has settled
+      if (rings >= F.search_rings) break;
+      ++rings;
+      state = 2;
+      c0 = 0;
+      moved = false;
+      cxr = bx;
+      cyr = by;
+    }
+    int fx, fy;
+    bool ok;
+    if (state == 0) {
+      // Candidate c0 + g: the kept seed of that rank.
+      const uint32_t m0 = __ballot_sync(kFull, kept && rank == c0), m1 = __ballot_sync(kFull, kept && rank == c0 + 1),
+                     m2 = __ballot_sync(kFull, kept && rank == c0 + 2),
+                     m3 = __ballot_sync(kFull, kept && rank == c0 + 3);
+      const uint32_t m = g == 0 ? m0 : g == 1 ? m1 : g == 2 ? m2 : m3;
+      ok = m != 0u;
+      const int from = ok ? __ffs(m) - 1 : 0;
+      fx = __shfl_sync(kFull, qx, from);
+      fy = __shfl_sync(kFull, qy, from);
+    } else {
+      if (state == 1) {  // (1,0), (-1,0), (0,1), (0,-1)
+        fx = bx + (g == 0 ? 1 : g == 1 ? -1 : 0);
+        fy = by + (g == 2 ? 1 : g == 3 ? -1 : 0);
+      } else {  // (r,0), (-r,0), (0,r), (0,-r), (r,r), (-r,r), (r,-r), (-r,-r) for r = 4, 8, 16
+        const int c = c0 + g, rr = c < 8 ? 4 : c < 16 ? 8 : 16, k8 = c & 7;
+        fx = cxr + ((k8 == 0 || k8 == 4 || k8 == 6) ? rr : (k8 == 1 || k8 == 5 || k8 == 7) ? -rr : 0);
+        fy = cyr + ((k8 == 2 || k8 == 4 || k8 == 5) ? rr : (k8 == 3 || k8 == 6 || k8 == 7) ? -rr : 0);
+      }
+      ok = abs(fx - ox) <= range && abs(fy - oy) <= range && fx >= lox && fx <= hix && fy >= loy && fy <= hiy;
+      nsad += __popc(__ballot_sync(kFull, ok && sub == 0));
+    }
+    uint32_t part = ok ? sad_part<S>(sm.src, w, h, org + (ptrdiff_t)fy * stride + fx, stride, sub) : 0u;
+    part += __shfl_xor_sync(kFull, part, 4);
+    part += __shfl_xor_sync(kFull, part, 2);
+    part += __shfl_xor_sync(kFull, part, 1);
+    const uint32_t cost = ok ? part + hevc_rate(lam, fx * 4, fy * 4, p0x, p0y, p1x, p1y) : kInf;
+    const Pick p = warp_min(cost);
+    const bool better = p.cost < bcost;
+    if (better) {
       bcost = p.cost;
       bx = __shfl_sync(kFull, fx, p.lane);
       by = __shfl_sync(kFull, fy, p.lane);
     }
-    if (rings >= F.search_rings) break;
-    ++rings;
-    // Square rings at 4, 8, 16 around the settled point: 24 points, in the
-    // reference's order; a better one restarts the descent.
-    const int cxr = bx, cyr = by;
-    const int lpc = lanes_per(24), cpp = 32 / lpc, sub = lane % lpc;
-    bool moved = false;
-    for (int c0 = 0; c0 < 24; c0 += cpp) {
-      const int c = lane / lpc < cpp ? c0 + lane / lpc : 24, rr = c < 8 ? 4 : c < 16 ? 8 : 16, k8 = c & 7;
-      const int dx = (k8 == 0 || k8 == 4 || k8 == 6) ? rr : (k8 == 1 || k8 == 5 || k8 == 7) ? -rr : 0;
-      const int dy = (k8 == 2 || k8 == 4 || k8 == 5) ? rr : (k8 == 3 || k8 == 6 || k8 == 7) ? -rr : 0;
-      const int fx = cxr + dx, fy = cyr + dy;
-      const bool ok = c < 24 && inside(fx, fy);
-      const uint32_t s = group_sad<S>(sm.src, wr, h, org, stride, lpc, sub, lane, ok, fx, fy);
-      const uint32_t cost = ok ? s + hevc_rate(lam, fx * 4, fy * 4, p0x, p0y, p1x, p1y) : kInf;
-      nsad += __popc(__ballot_sync(kFull, ok && sub == 0));
-      const Pick p = warp_min(cost);
-      if (p.cost < bcost) {
-        bcost = p.cost;
-        bx = __shfl_sync(kFull, fx, p.lane);
-        by = __shfl_sync(kFull, fy, p.lane);
-        moved = true;
+    if (state == 0) {
+      c0 += 4;
+      if (c0 >= nk) {  // the descent is confined to +-range of the best seed
+        nsad += nk;
+        ox = bx;
+        oy = by;
+        state = 1;
+        it = 0;
+      }
+    } else if (state == 1) {
+      it = better ? it + 1 : 2 * range;
+    } else {
+      moved |= better;
+      c0 += 4;
+      if (c0 >= 24) {
+        if (!moved) break;
+        state = 1;
+        it = 0;
       }
     }
-    if (!moved) break;
   }
   const uint32_t int_cost = bcost;
   const int imx = bx * 4, imy = by * 4;
 
   // refine_subpel: candidate 0 the start, 1..8 the half-sample ring (dy in
   // {-2,0,2} outer, dx inner, centre skipped), in one step; then the
-  // quarter-sample ring around the winner.
+  // quarter-sample ring around the winner (the cross only when asked).
+  // Passes: candidates 0..7 of the half step (four lanes each), candidate 8
+  // (all lanes), the quarter step's 8 (four lanes each); a later pass wins
+  // only when strictly cheaper, as in the reference's in-order walk.
   int bmx = imx, bmy = imy;
   uint32_t bc = kInf, bsatd = 0;
-  {
-    const int lpc = lanes_per(9), sub = lane % lpc, c = lane / lpc;
-    const int q = c == 0 ? 4 : (c <= 4 ? c - 1 : c);
-    const int mx = imx + (q % 3 - 1) * 2, my = imy + (q / 3 - 1) * 2;
-    const bool ok = c < 9;
-    const S* p1 = plane_at<S>(R, (my & 3) * 4 + (mx & 3), x + (mx >> 2), y + (my >> 2));
-    const uint32_t s = group_satd<S>(sm.src, wr, tw, th, p1, nullptr, stride, lpc, sub, lane, ok);
-    const uint32_t cost = ok ? s + hevc_rate(lam, mx, my, p0x, p0y, p1x, p1y) : kInf;
-    const Pick p = warp_min(cost);
-    bc = p.cost;
-    bsatd = __shfl_sync(kFull, s, p.lane);
-    bmx = __shfl_sync(kFull, mx, p.lane);
-    bmy = __shfl_sync(kFull, my, p.lane);
-    nsatd += 9;
-  }
-  {
-    const bool cross = F.quarter_cross != 0;
-    const int lpc = lanes_per(8), sub = lane % lpc, c = lane / lpc;
-    const int q = c < 4 ? c : c + 1;
-    const int dx = q % 3 - 1, dy = q / 3 - 1;
-    const bool ok = c < 8 && !(cross && dx != 0 && dy != 0);
-    const int mx = (int)(int16_t)(bmx + dx), my = (int)(int16_t)(bmy + dy);
-    const S* p1 = plane_at<S>(R, (my & 3) * 4 + (mx & 3), x + (mx >> 2), y + (my >> 2));
-    const uint32_t s = group_satd<S>(sm.src, wr, tw, th, p1, nullptr, stride, lpc, sub, lane, ok);
-    const uint32_t cost = ok ? s + hevc_rate(lam, mx, my, p0x, p0y, p1x, p1y) : kInf;
-    nsatd += __popc(__ballot_sync(kFull, ok && sub == 0));
+  const int ntiles = tw * th;
+  for (int pass = 0; pass < 3; ++pass) {
+    const int G = pass == 1 ? 32 : 4, c = pass == 1 ? 8 : lane >> 2, gsub = pass == 1 ? lane : lane & 3;
+    int mx, my;
+    bool ok;
+    if (pass < 2) {
+      const int q = c == 0 ? 4 : (c <= 4 ? c - 1 : c);
+      mx = imx + (q % 3 - 1) * 2;
+      my = imy + (q / 3 - 1) * 2;
+      ok = true;
+    } else {
+      const int q = c < 4 ? c : c + 1, dx = q % 3 - 1, dy = q / 3 - 1;
+      mx = (int)(int16_t)(bmx + dx);
+      my = (int)(int16_t)(bmy + dy);
+      ok = !(F.quarter_cross != 0 && dx != 0 && dy != 0);
+      nsatd += __popc(__ballot_sync(kFull, ok && gsub == 0));
+    }
+    const S* pp = plane_at<S>(R, (my & 3) * 4 + (mx & 3), x + (mx >> 2), y + (my >> 2));
+    uint32_t part = ok ? satd_part<S>(sm.src, wr, tw, ntiles, pp, stride, gsub, G) : 0u;
+    for (int o = G >> 1; o > 0; o >>= 1) part += __shfl_xor_sync(kFull, part, o);
+    const uint32_t cost = ok ? part + hevc_rate(lam, mx, my, p0x, p0y, p1x, p1y) : kInf;
     const Pick p = warp_min(cost);
     if (p.cost < bc) {
       bc = p.cost;
-      bsatd = __shfl_sync(kFull, s, p.lane);
+      bsatd = __shfl_sync(kFull, part, p.lane);
       bmx = __shfl_sync(kFull, mx, p.lane);
       bmy = __shfl_sync(kFull, my, p.lane);
     }
   }
+  nsatd += 9;
   write_result(out, bmx, bmy, r, bc, bsatd, imx, imy, int_cost, nsad, nsatd, lane);
   if (F.mode != RME_PRED_GIVEN) {
     // The tasks reading this result: right and lower neighbours of this
