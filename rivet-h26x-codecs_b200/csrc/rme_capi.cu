@@ -171,6 +171,10 @@ struct Ctx {
   DevBuf<rme_job> d_jobs;
   DevBuf<unsigned long long> d_misc;  // the launch header (kMisc*)
   DevBuf<uint8_t> d_stage;            // upload staging
+  DevBuf<int32_t> d_cblk;             // chroma: blocks, vectors, output offsets, output
+  DevBuf<rme_mv> d_cmv;
+  DevBuf<int64_t> d_coff;
+  DevBuf<uint8_t> d_cout;
   PinBuf<FrameDesc> h_frames;
   PinBuf<rme_result> h_out;
   PinBuf<unsigned long long> h_misc;
@@ -973,16 +977,81 @@ int rme_chroma_predict(void* ctx, int32_t ref_id, int32_t nblocks, const int32_t
                        void* out, void* stream) {
   Ctx* c = (Ctx*)ctx;
   if (!c) return RME_EINVAL;
-  return fail(c, RME_ENOSYS, "chroma prediction not built yet");
+  Picture* p;
+  int rc = picture_of(c, ref_id, &p);
+  if (rc) return rc;
+  if (!p->chroma) return fail(c, RME_EINVAL, "no chroma uploaded for this picture");
+  if (nblocks < 0 || (nblocks > 0 && (!blocks || !mvs || !out))) return fail(c, RME_EINVAL, "bad block list");
+  if (nblocks == 0) return 0;
+  std::vector<int64_t> off(nblocks);
+  int64_t total = 0;
+  for (int i = 0; i < nblocks; ++i) {
+    const int32_t* b = blocks + 4 * i;
+    if (b[0] < 0 || b[1] < 0 || b[2] < 2 || b[3] < 2 || b[2] > 128 || b[3] > 128 || b[0] + b[2] > p->d.width ||
+        b[1] + b[3] > p->d.height)
+      return fail(c, RME_EINVAL, "block " + std::to_string(i) + " outside the picture");
+    off[i] = total;
+    total += 2 * (int64_t)(b[2] / 2) * (b[3] / 2);
+  }
+  const int bps = p->d.bit_depth == 8 ? 1 : 2;
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  CK(cudaSetDevice(c->device));
+  cudaPointerAttributes pa{};
+  const bool dev_out = cudaPointerGetAttributes(&pa, out) == cudaSuccess && pa.type == cudaMemoryTypeDevice;
+  cudaGetLastError();
+  CK(c->d_cblk.ensure(4 * (int64_t)nblocks));
+  CK(c->d_cmv.ensure(nblocks));
+  CK(c->d_coff.ensure(nblocks));
+  if (!dev_out) CK(c->d_cout.ensure(total * bps));
+  CK(cudaMemcpyAsync(c->d_cblk.p, blocks, sizeof(int32_t) * 4 * nblocks, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(c->d_cmv.p, mvs, sizeof(rme_mv) * nblocks, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(c->d_coff.p, off.data(), sizeof(int64_t) * nblocks, cudaMemcpyHostToDevice, s));
+  const int cw = p->d.width / 2, ch = p->d.height / 2;
+  const uint8_t* cb = (const uint8_t*)p->chroma;
+  const uint8_t* cr = cb + (size_t)cw * ch * bps;
+  void* dst = dev_out ? out : (void*)c->d_cout.p;
+  CK(launch_chroma(cb, cr, p->d.bit_depth, p->d.codec, cw, ch, cw, nblocks, c->d_cblk.p, c->d_cmv.p, c->d_coff.p, dst,
+                   s));
+  if (!dev_out) CK(cudaMemcpyAsync(out, c->d_cout.p, (size_t)total * bps, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return 0;
 }
 
-int rme_sad_batch(const void*, int64_t, const int64_t*, const void*, int64_t, const int64_t*, int32_t, int32_t, int32_t,
-                  int32_t, uint32_t*, void*) {
-  return RME_ENOSYS;
+namespace {
+bool device_accessible(const void* ptr, int* dev) {
+  cudaPointerAttributes pa{};
+  const bool ok = ptr && cudaPointerGetAttributes(&pa, ptr) == cudaSuccess &&
+                  (pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged);
+  cudaGetLastError();
+  if (ok && dev) *dev = pa.device;
+  return ok;
 }
-int rme_satd_batch(const void*, int64_t, const int64_t*, const void*, int64_t, const int64_t*, int32_t, int32_t,
-                   int32_t, int32_t, uint32_t*, void*) {
-  return RME_ENOSYS;
+
+int dist_batch(bool satd, const void* a, int64_t as, const int64_t* aoff, const void* b, int64_t bs,
+               const int64_t* boff, int32_t w, int32_t h, int32_t bd, int32_t n, uint32_t* out, void* stream) {
+  if (n < 0 || w < 1 || h < 1 || w > 256 || h > 256 || bd < 8 || bd > 14 || as < w || bs < w) return RME_EINVAL;
+  if (satd && ((w & 3) || (h & 3))) return RME_EINVAL;
+  if (n == 0) return 0;
+  int dev = 0;
+  if (!device_accessible(a, &dev) || !device_accessible(b, nullptr) || !device_accessible(aoff, nullptr) ||
+      !device_accessible(boff, nullptr) || !device_accessible(out, nullptr))
+    return RME_EINVAL;
+  if (cudaSetDevice(dev) != cudaSuccess) return RME_ECUDA;
+  return launch_dist_batch(satd, a, as, aoff, b, bs, boff, w, h, bd, n, out, (cudaStream_t)stream) == cudaSuccess
+             ? 0
+             : RME_ECUDA;
+}
+}  // namespace
+
+int rme_sad_batch(const void* a, int64_t a_stride, const int64_t* a_off, const void* b, int64_t b_stride,
+                  const int64_t* b_off, int32_t w, int32_t h, int32_t bit_depth, int32_t n, uint32_t* out,
+                  void* stream) {
+  return dist_batch(false, a, a_stride, a_off, b, b_stride, b_off, w, h, bit_depth, n, out, stream);
+}
+int rme_satd_batch(const void* a, int64_t a_stride, const int64_t* a_off, const void* b, int64_t b_stride,
+                   const int64_t* b_off, int32_t w, int32_t h, int32_t bit_depth, int32_t n, uint32_t* out,
+                   void* stream) {
+  return dist_batch(true, a, a_stride, a_off, b, b_stride, b_off, w, h, bit_depth, n, out, stream);
 }
 
 int rme_serve_start(void*, const rme_serve_opts*, void**) { return RME_ENOSYS; }

@@ -201,3 +201,20 @@ def hevc_decide(width: int, height: int, bit_depth: int, params: capi.Params, nr
                                           best.ctypes.data_as(C.POINTER(C.c_int32)),
                                           part.ctypes.data_as(C.POINTER(C.c_uint8))))
     return best, part
+
+
+def distortion_batch(kind: str, a, a_stride: int, a_off, b, b_stride: int, b_off, w: int, h: int, bit_depth: int,
+                     out, stream: int = 0):
+    """The batched SadFn / SatdFn: out[i] = sad|satd of the w x h blocks at
+    a + a_off[i] and b + b_off[i] (strides in samples). `a`, `b`, the
+    offsets (int64) and `out` (32-bit) are device tensors; asynchronous on
+    `stream`. Returns `out`."""
+    lib = capi.lib()
+    fn = lib.rme_sad_batch if kind == "sad" else lib.rme_satd_batch
+    n = out.numel()
+    rc = fn(C.c_void_p(a.data_ptr()), a_stride, C.c_void_p(a_off.data_ptr()), C.c_void_p(b.data_ptr()), b_stride,
+            C.c_void_p(b_off.data_ptr()), w, h, bit_depth, n, C.cast(C.c_void_p(out.data_ptr()), C.POINTER(C.c_uint32)),
+            C.c_void_p(stream))
+    if rc != 0:
+        raise RuntimeError(f"rme_{kind}_batch failed: {rc}")
+    return out

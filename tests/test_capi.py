@@ -104,3 +104,19 @@ def test_invalid_arguments_are_refused_without_a_device():
     mis = capi.PlaneSet(18, 224 * 224, 224, 80)
     assert lib.rme_search_given_noalloc(C.byref(d), C.byref(p), C.byref(mis), refs, 1, C.c_void_p(16), 4,
                                         C.c_void_p(16), None) == capi.RME_EINVAL
+
+
+def test_distortion_batches_refuse_host_memory():
+    """The batched distortion entry points take device pointers only: host
+    arrays (or no device at all) are refused before any launch."""
+    a = np.zeros((16, 16), np.uint8)
+    off = np.zeros(1, np.int64)
+    out = np.zeros(1, np.uint32)
+    lib = capi.lib()
+    for fn in (lib.rme_sad_batch, lib.rme_satd_batch):
+        rc = fn(capi.ptr(a), 16, off.ctypes.data, capi.ptr(a), 16, off.ctypes.data, 8, 8, 8, 1,
+                out.ctypes.data_as(C.POINTER(C.c_uint32)), None)
+        assert rc == capi.RME_EINVAL
+    # satd needs whole 4x4 tiles
+    assert lib.rme_satd_batch(None, 16, None, None, 16, None, 6, 8, 8, 0, None, None) == capi.RME_EINVAL
+    assert lib.rme_sad_batch(None, 16, None, None, 16, None, 6, 8, 8, 0, None, None) == 0

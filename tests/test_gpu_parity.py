@@ -188,6 +188,60 @@ def test_batch_results_into_device_and_pinned_memory(ms):
         ms.search_batch(frames, p, out=torch.zeros(n * 32 - 1, dtype=torch.uint8, device="cuda:0"))
 
 
+# ---- chroma of chosen vectors and the batched distortion kernels ------------------
+@pytest.mark.parametrize("codec,bd", [(HEVC, 8), (HEVC, 10), (H264, 8), (H264, 10)])
+def test_chroma_prediction_matches_the_oracle(ms, codec, bd):
+    """4:2:0 chroma of chosen luma vectors: HEVC's 4-tap eighth-sample
+    filter with uni rounding, H.264's bilinear weights; vectors reaching far
+    outside the picture read the edge-replicated planes."""
+    import torch
+    rng = np.random.default_rng(70 + 2 * bd + codec)
+    W, H = 96, 64
+    luma = random_picture(rng, W, H, bd)
+    cb, cr = random_picture(rng, W // 2, H // 2, bd), random_picture(rng, W // 2, H // 2, bd)
+    ms.upload(700, luma, codec, bd, as_ref=True)
+    ms.upload_chroma(700, cb, cr)
+    sizes = [(8, 8), (16, 16), (32, 32), (64, 64), (16, 8), (8, 16), (4, 4), (2, 2), (12, 6)]
+    blocks, mvs = [], []
+    for i in range(300):
+        bw, bh = sizes[i % len(sizes)]
+        blocks.append((rng.integers(0, W - bw + 1), rng.integers(0, H - bh + 1), bw, bh))
+        spread = 40 if i % 3 else 600
+        mvs.append(rng.integers(-spread, spread + 1, size=2))
+    blocks, mvs = np.array(blocks, np.int32), np.array(mvs, np.int16)
+    want = oracle.chroma_predict(codec, bd, W, H, cb, cr, blocks, mvs)
+    got = ms.chroma_predict(700, blocks, mvs)
+    np.testing.assert_array_equal(got, want)
+    ms.release(700)
+
+
+@pytest.mark.parametrize("bd", [8, 10])
+@pytest.mark.parametrize("kind", ["sad", "satd"])
+def test_distortion_batches_match_the_oracle(kind, bd):
+    """rme_sad_batch / rme_satd_batch over device buffers equal the
+    reference's size-generic kernels block for block."""
+    import torch
+    import rivet_h26x_codecs_b200.host as host
+    rng = np.random.default_rng(90 + bd + (kind == "satd"))
+    A, B = random_picture(rng, 160, 120, bd), random_picture(rng, 160, 120, bd)
+    view = np.uint8 if bd == 8 else np.int16
+    da = torch.from_numpy(A.view(view).copy()).cuda()
+    db = torch.from_numpy(B.view(view).copy()).cuda()
+    shapes = [(4, 4), (8, 8), (16, 16), (64, 64), (8, 4), (16, 12), (32, 64)] + ([(3, 5), (7, 1)] if kind == "sad" else [])
+    for w, h in shapes:
+        n = 97
+        ax, ay = rng.integers(0, 160 - w + 1, n), rng.integers(0, 120 - h + 1, n)
+        bx, by = rng.integers(0, 160 - w + 1, n), rng.integers(0, 120 - h + 1, n)
+        aoff = torch.from_numpy((ay * 160 + ax).astype(np.int64)).cuda()
+        boff = torch.from_numpy((by * 160 + bx).astype(np.int64)).cuda()
+        out = torch.zeros(n, dtype=torch.int32, device="cuda")
+        host.distortion_batch(kind, da, 160, aoff, db, 160, boff, w, h, bd, out)
+        got = out.cpu().numpy().view(np.uint32)
+        fn = oracle.sad if kind == "sad" else oracle.satd
+        want = [fn(bd, A[ay[i]:ay[i] + h, ax[i]:ax[i] + w], B[by[i]:by[i] + h, bx[i]:bx[i] + w]) for i in range(n)]
+        np.testing.assert_array_equal(got, np.array(want, np.uint32), f"{kind} {w}x{h}")
+
+
 # ---- the reference's search-behaviour tests, through the library --------------
 def grating(w, h):
     """The reference tests' triangle grating (h265_me.rs:4989-5026,
