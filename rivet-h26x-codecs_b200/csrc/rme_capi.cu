@@ -1054,11 +1054,4 @@ int rme_satd_batch(const void* a, int64_t a_stride, const int64_t* a_off, const 
   return dist_batch(true, a, a_stride, a_off, b, b_stride, b_off, w, h, bit_depth, n, out, stream);
 }
 
-int rme_serve_start(void*, const rme_serve_opts*, void**) { return RME_ENOSYS; }
-int rme_serve_open_stream(void*, int32_t, const rme_picture_desc*, const rme_params*, int32_t) { return RME_ENOSYS; }
-int rme_serve_submit(void*, int32_t, const void*, rme_result*, int64_t*) { return RME_ENOSYS; }
-int rme_serve_poll(void*, rme_completion*, int32_t, int32_t*) { return RME_ENOSYS; }
-int rme_serve_close_stream(void*, int32_t) { return RME_ENOSYS; }
-int rme_serve_stop(void*) { return RME_ENOSYS; }
-
 }  // extern "C"

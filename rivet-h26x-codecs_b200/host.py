@@ -218,3 +218,69 @@ def distortion_batch(kind: str, a, a_stride: int, a_off, b, b_stride: int, b_off
     if rc != 0:
         raise RuntimeError(f"rme_{kind}_batch failed: {rc}")
     return out
+
+
+class Server:
+    """The serving loop (rme_serve_*) on its own context: per-frame ME
+    requests of many streams, batched into persistent launches as they
+    arrive; each stream's reference pictures stay resident. The context is
+    the server's while it runs."""
+
+    def __init__(self, ms: MotionSearch, hbm_budget_bytes: int, max_frames_per_launch: int = 32,
+                 max_streams: int = 256):
+        self._lib = capi.lib()
+        self.ms = ms
+        o = capi.ServeOpts(hbm_budget_bytes, max_frames_per_launch, max_streams)
+        h = C.c_void_p()
+        capi.check(self._lib.rme_serve_start(ms.ctx, C.byref(o), C.byref(h)))
+        self.h = h
+        self._streams = {}
+        self._out = {}
+
+    def open_stream(self, stream_id: int, codec: int, bit_depth: int, width: int, height: int,
+                    params: capi.Params, nref: int) -> int:
+        """Admit a stream; returns 0, or RME_EBUSY when the budget is spent."""
+        d = capi.PictureDesc(codec, bit_depth, width, height, width)
+        rc = self._lib.rme_serve_open_stream(self.h, stream_id, C.byref(d), C.byref(params), nref)
+        if rc == 0:
+            nb = len(standalone_blocks(codec, width, height, bit_depth, params))
+            self._streams[stream_id] = [codec, nb, nref, 0]
+        elif rc != capi.RME_EBUSY:
+            capi.check(rc)
+        return rc
+
+    def submit(self, stream_id: int, luma: np.ndarray) -> int:
+        """Queue one frame (copied before return); returns the request id."""
+        codec, nb, nref, seen = self._streams[stream_id]
+        nr = min(nref, seen)
+        count = nb if codec == capi.RME_CODEC_H264 else nb * nr
+        out = np.zeros(max(count, 1), capi.RESULT_DTYPE) if nr else None
+        rid = C.c_int64()
+        luma = np.ascontiguousarray(luma)
+        capi.check(self._lib.rme_serve_submit(self.h, stream_id, capi.ptr(luma),
+                                              C.cast(out.ctypes.data, C.POINTER(capi.Result)) if out is not None
+                                              else None, C.byref(rid)))
+        self._streams[stream_id][3] = seen + 1
+        self._out[rid.value] = out[:count] if out is not None else np.zeros(0, capi.RESULT_DTYPE)
+        return rid.value
+
+    def poll(self, max_n: int = 4096) -> list[dict]:
+        """Completed requests since the last poll: dicts with the request id,
+        stream, status, submit and done times (s) and the results."""
+        buf = (capi.Completion * max_n)()
+        n = C.c_int32()
+        capi.check(self._lib.rme_serve_poll(self.h, buf, max_n, C.byref(n)))
+        done = []
+        for c in buf[:n.value]:
+            done.append({"id": c.request_id, "stream": c.stream_id, "status": c.status, "submit_s": c.submit_s,
+                         "done_s": c.done_s, "results": self._out.pop(c.request_id)})
+        return done
+
+    def close_stream(self, stream_id: int) -> None:
+        capi.check(self._lib.rme_serve_close_stream(self.h, stream_id))
+        self._streams.pop(stream_id, None)
+
+    def stop(self) -> None:
+        if self.h:
+            capi.check(self._lib.rme_serve_stop(self.h))
+            self.h = None

@@ -120,3 +120,16 @@ def test_distortion_batches_refuse_host_memory():
     # satd needs whole 4x4 tiles
     assert lib.rme_satd_batch(None, 16, None, None, 16, None, 6, 8, 8, 0, None, None) == capi.RME_EINVAL
     assert lib.rme_sad_batch(None, 16, None, None, 16, None, 6, 8, 8, 0, None, None) == 0
+
+
+def test_the_serving_loop_validates_its_arguments():
+    lib = capi.lib()
+    h = C.c_void_p()
+    o = capi.ServeOpts(1 << 30, 8, 4)
+    assert lib.rme_serve_start(None, C.byref(o), C.byref(h)) == capi.RME_EINVAL
+    bad = capi.ServeOpts(1 << 30, 0, 4)  # no frames per launch
+    assert lib.rme_serve_start(C.c_void_p(16), C.byref(bad), C.byref(h)) == capi.RME_EINVAL
+    n = C.c_int32()
+    assert lib.rme_serve_poll(None, None, 0, C.byref(n)) == capi.RME_EINVAL
+    assert lib.rme_serve_submit(None, 1, None, None, None) == capi.RME_EINVAL
+    assert lib.rme_serve_stop(None) == capi.RME_EINVAL
