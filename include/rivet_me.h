@@ -162,7 +162,8 @@ typedef struct {
   uint64_t sad_samples;      /* sum over SAD candidates of w*h              */
   uint64_t satd_samples;     /* sum over SATD candidates of w*h             */
   float    kernel_ms;        /* device time of the search launch(es)        */
-  float    planes_ms;        /* device time of the plane builds             */
+  float    planes_ms;        /* device time from the first upload since the
+                                previous search to the end of the last one  */
 } rme_stats;
 
 /* ---- lifecycle ---------------------------------------------------------- */
@@ -301,8 +302,10 @@ typedef struct {
 } rme_completion;
 
 int rme_serve_start(void* ctx, const rme_serve_opts* o, void** server);
-/* Admit a stream of one format and settings; refused with RME_EBUSY when
- * its resident pictures would pass the budget. */
+/* Admit a stream of one format and settings (STANDALONE predictors, 1..4
+ * references); refused with RME_EBUSY when its resident pictures would pass
+ * the budget. A stream holds nref + 4 pictures: up to four of its frames
+ * join one launch. */
 int rme_serve_open_stream(void* server, int32_t stream_id, const rme_picture_desc* d,
                           const rme_params* p, int32_t nref);
 /* Submit one frame of a stream: its luma (host memory, copied before

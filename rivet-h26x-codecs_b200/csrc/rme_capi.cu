@@ -85,10 +85,10 @@ struct DevBuf {
   cudaError_t ensure(size_t want) {
     if (want <= n) return cudaSuccess;
     ++g_buffer_generation;
+    const size_t grow = std::max(want, n * 3 / 2);  // geometric: few reallocations
     if (p) cudaFree(p);
     p = nullptr;
     n = 0;
-    size_t grow = std::max(want, n * 3 / 2);
     cudaError_t e = cudaMalloc(&p, grow * sizeof(T) + 64);
     if (e == cudaSuccess) n = grow;
     return e;
@@ -104,10 +104,10 @@ struct PinBuf {
   cudaError_t ensure(size_t want) {
     if (want <= n) return cudaSuccess;
     ++g_buffer_generation;
+    const size_t grow = std::max(want, n * 3 / 2);
     if (p) cudaFreeHost(p);
     p = nullptr;
     n = 0;
-    size_t grow = std::max(want, n * 3 / 2);
     cudaError_t e = cudaMallocHost(&p, grow * sizeof(T) + 64);
     if (e == cudaSuccess) n = grow;
     return e;
@@ -145,7 +145,7 @@ struct Deps {  // the dependency structure of one frame shape
 
 struct Graph {
   cudaGraphExec_t exec = nullptr;
-  size_t nframes = 0, total = 0;
+  int seen = 0;  // launches of this shape so far: captured on the second
 };
 
 struct Ctx {
@@ -170,7 +170,6 @@ struct Ctx {
   DevBuf<int32_t> d_pending;
   DevBuf<rme_job> d_jobs;
   DevBuf<unsigned long long> d_misc;  // the launch header (kMisc*)
-  DevBuf<uint8_t> d_stage;            // upload staging
   DevBuf<int32_t> d_cblk;             // chroma: blocks, vectors, output offsets, output
   DevBuf<rme_mv> d_cmv;
   DevBuf<int64_t> d_coff;
@@ -181,7 +180,7 @@ struct Ctx {
   PinBuf<unsigned long long> h_init;  // [misc header | initial queue entries]
 
   std::map<std::vector<int64_t>, Graph> graphs;
-  float planes_ms_acc = 0.0f;
+  bool planes_pending = false;  // uploads recorded between evp0 and evp1 since the last search
   ~Ctx() {
     for (auto& g : graphs)
       if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
@@ -608,7 +607,11 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
     gsig.push_back((int64_t)(uintptr_t)s);
     gsig.push_back((int64_t)g_buffer_generation);
     Graph& g = c->graphs[gsig];
-    if (!g.exec) {
+    // A shape is captured when it comes a second time (a one-off batch,
+    // common in serving, is not worth a capture).
+    if (!g.exec && ++g.seen < 2) {
+      CK(enqueue(false));
+    } else if (!g.exec) {
       cudaGraph_t graph;
       CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       cudaError_t e = enqueue(true);
@@ -622,7 +625,7 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
         return cuda_fail(c, e, "graph instantiate");
       }
     }
-    CK(cudaGraphLaunch(g.exec, s));
+    if (g.exec) CK(cudaGraphLaunch(g.exec, s));
   } else {
     CK(enqueue(false));
   }
@@ -648,8 +651,15 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   c->last.sad_samples = c->h_misc.p[kMiscCounters + 3];
   c->last.satd_samples = c->h_misc.p[kMiscCounters + 4];
   c->last.kernel_ms = ms;
-  c->last.planes_ms = c->planes_ms_acc;
-  c->planes_ms_acc = 0.0f;
+  c->last.planes_ms = 0.0f;
+  if (c->planes_pending) {
+    // Device time from the first upload since the previous search to the
+    // end of the last one (the uploads' stream precedes this search's).
+    cudaEventSynchronize(c->evp1);
+    if (cudaEventElapsedTime(&c->last.planes_ms, c->evp0, c->evp1) != cudaSuccess) c->last.planes_ms = 0.0f;
+    cudaGetLastError();
+    c->planes_pending = false;
+  }
   if (status) return fail(c, RME_EDEVICE, "device status " + std::to_string(status));
   if (c->last.tasks != (unsigned long long)total)
     return fail(c, RME_EDEVICE, "the launch ran " + std::to_string(c->last.tasks) + " of " + std::to_string(total) +
@@ -740,33 +750,31 @@ int rme_picture_upload(void* ctx, int32_t pic_id, const rme_picture_desc* d, con
   pic->planes.origin = pic->pad * stride + pic->pad;
   pic->bytes = (size_t)pic->planes.plane_elems * bps * pic->nplanes + 256;
   // Re-uploading an id with the same format reuses its device buffer (a
-  // stream's picture slots are refilled every frame).
+  // stream's picture slots are refilled every frame). Work already queued
+  // on the picture is ordered before the refill by the stream.
   auto old = c->pics.find(pic_id);
   if (old != c->pics.end() && old->second->bytes == pic->bytes && old->second->planes.stride == stride) {
-    CK(cudaStreamSynchronize(s));
     pic->buf = old->second->buf;
     old->second->buf = nullptr;
   } else {
+    if (old != c->pics.end()) CK(cudaStreamSynchronize(s));
     CK(cudaMalloc(&pic->buf, pic->bytes));
   }
   pic->planes.base = pic->buf;
-  size_t src_bytes = (size_t)d->width * d->height * bps;
-  CK(c->d_stage.ensure(src_bytes));
-  CK(cudaMemcpy2DAsync(c->d_stage.p, (size_t)d->width * bps, luma, (size_t)d->stride * bps, (size_t)d->width * bps,
-                       d->height, cudaMemcpyHostToDevice, s));
-  CK(cudaEventRecord(c->evp0, s));
-  CK(launch_pad_plane(c->d_stage.p, d->bit_depth, d->width, d->height, d->width, pic->planes, pic->cw, pic->ch,
-                      pic->pad, s));
+  // The visible picture straight into plane 0, then its border in place:
+  // nothing is staged, so nothing waits (a pageable source is consumed
+  // before the copy call returns; a pinned one is read on the stream).
+  uint8_t* origin = (uint8_t*)pic->buf + (size_t)pic->planes.origin * bps;
+  if (!c->planes_pending) CK(cudaEventRecord(c->evp0, s));
+  CK(cudaMemcpy2DAsync(origin, (size_t)stride * bps, luma, (size_t)d->stride * bps, (size_t)d->width * bps, d->height,
+                       cudaMemcpyHostToDevice, s));
+  CK(launch_pad_plane(origin, d->bit_depth, d->width, d->height, stride, pic->planes, pic->cw, pic->ch, pic->pad, s));
   if (as_ref) {
     if (h264) CK(launch_h264_hpel(pic->planes, d->bit_depth, pic->cw, pic->ch, pic->pad, s));
     else CK(launch_hevc_phases(pic->planes, d->bit_depth, pic->cw, pic->ch, pic->pad, s));
   }
   CK(cudaEventRecord(c->evp1, s));
-  // The staging buffer is reused by the next upload: finish this one.
-  CK(cudaStreamSynchronize(s));
-  float ms = 0.0f;
-  CK(cudaEventElapsedTime(&ms, c->evp0, c->evp1));
-  c->planes_ms_acc += ms;
+  c->planes_pending = true;
   c->pics[pic_id] = std::move(pic);
   return 0;
 }

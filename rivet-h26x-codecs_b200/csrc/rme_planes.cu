@@ -28,6 +28,9 @@ __global__ void pad_plane_kernel(const S* __restrict__ src, int w, int h, int ss
   int x = blockIdx.x * blockDim.x + threadIdx.x;
   int y = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= pcol || y >= prow) return;
+  // In place (src is the plane's own visible picture): only the border is
+  // written, and it reads only the visible picture.
+  if (src == dst + (int64_t)pad * dstride + pad && x >= pad && x < pad + w && y >= pad && y < pad + h) return;
   int sx = min(max(x - pad, 0), w - 1);
   int sy = min(max(y - pad, 0), h - 1);
   dst[(int64_t)y * dstride + x] = src[(int64_t)sy * sstride + sx];

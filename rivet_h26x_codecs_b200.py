@@ -13,4 +13,4 @@ from rivet_h26x_codecs_b200.capi import (  # noqa: E402,F401
     RME_CODEC_H264, RME_CODEC_HEVC, RME_PRED_GIVEN, RME_PRED_STANDALONE, default_params, lib,
 )
 
-from rivet_h26x_codecs_b200.host import MotionSearch, hevc_decide, standalone_blocks  # noqa: E402,F401
+from rivet_h26x_codecs_b200.host import MotionSearch, Server, distortion_batch, hevc_decide, standalone_blocks  # noqa: E402,F401,E501

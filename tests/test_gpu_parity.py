@@ -140,8 +140,8 @@ def test_hevc_1080p_frame_matches_the_oracle(ms):
 
 
 def test_batch_equals_the_frames_and_the_oracle(ms):
-    """Several frames of two formats in one persistent launch, twice (the
-    second launch replays the captured graph)."""
+    """Several frames of two formats in one persistent launch, three times
+    (the second launch captures a graph, the third replays it)."""
     seq = synth.make_sequence(HEVC, 192, 128, 8, 5, 31, 64, 64, 2.0)
     h264 = synth.make_sequence(H264, 96, 64, 8, 3, 32, 16, 32, 2.0)
     ph = oracle.params(HEVC, 32, hevc_search_range=40)
@@ -152,7 +152,7 @@ def test_batch_equals_the_frames_and_the_oracle(ms):
         ms.upload(400 + i, f, H264, 8, as_ref=True)
     frames = [(300 + t, [300 + t - 1, 300 + t - 2]) for t in range(2, 5)] + [(402, [401, 400])]
     params = [ph, ph, ph, p4]
-    for _ in range(2):
+    for _ in range(3):
         outs = ms.search_batch(frames, params)
         for (s, refs), pp, got in zip(frames, params, outs):
             single = ms.search(s, refs, pp)

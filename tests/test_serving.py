@@ -101,7 +101,9 @@ def test_results_are_the_same_alone_and_in_the_mix():
 
 def test_admission_is_bounded_by_the_budget():
     with host.MotionSearch(0) as ms:
-        one = 16 * (1920 + 160 + 127) // 128 * 128 * (1080 + 160) * 3  # three 1080p pictures' planes, roughly
+        # A stream holds nref + 4 pictures of 16 padded planes (rows of 128-byte multiples).
+        picture = ((1920 + 160 + 127) // 128 * 128) * (1080 + 160) * 16 + 256
+        one = picture * (2 + 4)
         srv = host.Server(ms, hbm_budget_bytes=int(one * 1.5), max_frames_per_launch=4)
         try:
             p = _params(HEVC, 32)
