@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -150,7 +151,15 @@ struct Graph {
 
 struct Ctx {
   int device = 0, nsm = 0;
-  int bps[kParts] = {0, 0, 0, 0};  // resident search blocks per SM, per part
+  int bps[kParts][kSearchVariants] = {};  // resident search blocks per SM, per part and variant
+  // The tuner: per (part, log2 of its task count), each occupancy variant
+  // is timed on one real launch of that class, then the fastest is kept.
+  struct Tune {
+    int best = -1, tried = 0;
+    float ms[kSearchVariants] = {};
+  };
+  std::map<std::pair<int, int>, Tune> tune;
+  bool tune_on = true;
   cudaStream_t stream = nullptr;
   // The parts of a launch after the first run on streams of their own,
   // forked from and joined back to the caller's stream.
@@ -549,7 +558,26 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
     L.status = reinterpret_cast<uint32_t*>(c->d_misc.p + kMiscStatus);
     L.epoch = reinterpret_cast<const uint32_t*>(c->d_misc.p + kMiscEpoch);
     slot0 += part_tasks[k];
-    if (part_tasks[k] > 0 && !c->bps[k]) c->bps[k] = search_blocks_per_sm(part_bytes(k), part_codec(k));
+  }
+  int nparts_used = 0;
+  for (int k = 0; k < kParts; ++k) nparts_used += part_tasks[k] > 0;
+  int variant[kParts];
+  Ctx::Tune* tuning = nullptr;  // the class this launch times, if any
+  for (int k = 0; k < kParts; ++k) {
+    variant[k] = kDefaultVariant;
+    if (part_tasks[k] == 0) continue;
+    if (c->tune_on) {
+      const int bucket = 63 - __builtin_clzll((unsigned long long)part_tasks[k]);
+      Ctx::Tune& T = c->tune[{k, bucket}];
+      if (T.best >= 0) {
+        variant[k] = T.best;
+      } else if (nparts_used == 1) {  // one kind in the launch: its time is the part's
+        variant[k] = T.tried;
+        tuning = &T;
+      }
+    }
+    if (!c->bps[k][variant[k]]) c->bps[k][variant[k]] = search_blocks_per_sm(part_bytes(k), part_codec(k), variant[k]);
+    sig.push_back(variant[k]);
   }
   int nparts = 0, order[kParts];
   for (int k = 0; k < kParts; ++k)
@@ -587,7 +615,9 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
       const int k = order[j];
       cudaStream_t sk = j == 0 ? s : c->aux[j];
       if (j > 0) e = cudaStreamWaitEvent(sk, c->ev_fork, 0);
-      if (e == cudaSuccess) e = launch_search(Ls[k], part_bytes(k), part_codec(k), grid_for(part_tasks[k], c->bps[k]), sk);
+      if (e == cudaSuccess)
+        e = launch_search(Ls[k], part_bytes(k), part_codec(k), variant[k], grid_for(part_tasks[k], c->bps[k][variant[k]]),
+                          sk);
       if (e == cudaSuccess && j > 0) e = cudaEventRecord(c->ev_join[j], sk);
     }
     for (int j = 1; j < nparts && e == cudaSuccess; ++j) e = cudaStreamWaitEvent(s, c->ev_join[j], 0);
@@ -651,6 +681,11 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   c->last.sad_samples = c->h_misc.p[kMiscCounters + 3];
   c->last.satd_samples = c->h_misc.p[kMiscCounters + 4];
   c->last.kernel_ms = ms;
+  if (tuning && tuning->best < 0) {
+    tuning->ms[tuning->tried++] = ms;
+    if (tuning->tried == kSearchVariants)
+      tuning->best = (int)(std::min_element(tuning->ms, tuning->ms + kSearchVariants) - tuning->ms);
+  }
   c->last.planes_ms = 0.0f;
   if (c->planes_pending) {
     // Device time from the first upload since the previous search to the
@@ -708,6 +743,8 @@ int rme_ctx_create(void** out, int32_t device) {
   if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return RME_ECUDA;
   c->nsm = nsm;
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return RME_ECUDA;
+  // RME_TUNE=0 keeps every launch on the default occupancy variant.
+  if (const char* t = std::getenv("RME_TUNE")) c->tune_on = t[0] != '0';
   if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
       cudaEventCreate(&c->evp0) != cudaSuccess || cudaEventCreate(&c->evp1) != cudaSuccess)
     return RME_ECUDA;

@@ -81,9 +81,12 @@ cudaError_t launch_pad_plane(const void* src, int bd, int w, int h, int sstride,
 cudaError_t launch_h264_hpel(DevPlanes p, int bd, int cw, int ch, int pad, cudaStream_t s);
 cudaError_t launch_hevc_phases(DevPlanes p, int bd, int w, int h, int pad, cudaStream_t s);
 // The search over one kind of task (sample width, codec): `grid` persistent
-// blocks pulling from L's queue.
-cudaError_t launch_search(const LaunchDesc& L, int bytes_per_sample, int codec, int grid, cudaStream_t s);
-int search_blocks_per_sm(int bytes_per_sample, int codec);
+// blocks pulling from L's queue. `variant` picks the kernel's occupancy
+// bound: 0, 1, 2 for 2, 3, 4 resident blocks per SM (1 is the default).
+constexpr int kSearchVariants = 3, kDefaultVariant = 1;
+cudaError_t launch_search(const LaunchDesc& L, int bytes_per_sample, int codec, int variant, int grid,
+                          cudaStream_t s);
+int search_blocks_per_sm(int bytes_per_sample, int codec, int variant);
 cudaError_t launch_chroma(const void* cb, const void* cr, int bd, int codec, int cw, int ch, int cstride,
                           int nblocks, const int32_t* blocks, const rme_mv* mvs, const int64_t* out_off, void* out,
                           cudaStream_t s);

@@ -191,8 +191,8 @@ extern "C" int rme_search_given_noalloc(const rme_picture_desc* d, const rme_par
   int nsm = 0;
   if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return RME_ECUDA;
   const int64_t want = ((int64_t)njobs + kWarpsPerBlock - 1) / kWarpsPerBlock;
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)nsm * search_blocks_per_sm(bytes, d->codec), want));
-  if (launch_search(L, bytes, d->codec, grid, s) != cudaSuccess) return RME_ECUDA;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)nsm * search_blocks_per_sm(bytes, d->codec, kDefaultVariant), want));
+  if (launch_search(L, bytes, d->codec, kDefaultVariant, grid, s) != cudaSuccess) return RME_ECUDA;
   if (cudaMemcpyAsync(misc, d_misc, sizeof(misc), cudaMemcpyDeviceToHost, s) != cudaSuccess) return RME_ECUDA;
   if (cudaStreamSynchronize(s) != cudaSuccess) return RME_ECUDA;
   if ((uint32_t)misc[9] != 0 || misc[4] != (unsigned long long)njobs) return RME_EDEVICE;

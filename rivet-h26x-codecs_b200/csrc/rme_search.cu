@@ -52,11 +52,6 @@
 namespace rme {
 namespace {
 
-// Resident blocks per SM the register allocation is bounded for (a build
-// setting: more blocks hide more latency, fewer leave more registers).
-#ifndef RME_MIN_BLOCKS
-#define RME_MIN_BLOCKS 3
-#endif
 
 constexpr int kMaxBlk = 64;
 constexpr uint32_t kInf = 0xffffffffu;
@@ -1168,11 +1163,15 @@ __device__ void h264_task(const LaunchDesc& L, const FrameDesc& F, int f, int t,
   count_task(sm, lane, nsad, nsatd, B.w * B.h);
 }
 
-// One kernel per (sample width, codec): a launch holds the tasks of one
-// kind, so each kernel carries only its codec's search (a smaller body
-// stays resident in the instruction caches).
-template <class S, int CODEC>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, RME_MIN_BLOCKS) search_kernel(LaunchDesc L) {
+// One kernel per (sample width, codec, occupancy variant): a launch holds
+// the tasks of one kind, so each kernel carries only its codec's search (a
+// smaller body stays resident in the instruction caches). MINB is the
+// number of resident blocks the register allocation is bounded for: 2
+// leaves more registers per thread (a single frame's dependency chain runs
+// faster), 4 keeps more warps resident (large batches hide more latency);
+// the host's tuner picks per kind and launch size.
+template <class S, int CODEC, int MINB>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, MINB) search_kernel(LaunchDesc L) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   WarpSmem<S>& sm = reinterpret_cast<WarpSmem<S>*>(smem_raw)[warp];
@@ -1209,40 +1208,53 @@ size_t smem_bytes() {
   return sizeof(WarpSmem<S>) * kWarpsPerBlock;
 }
 
-template <class S, int CODEC>
+template <class S, int CODEC, int MINB>
 int blocks_per_sm() {
   int n = 0;
-  cudaError_t e = cudaFuncSetAttribute(search_kernel<S, CODEC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(search_kernel<S, CODEC, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem_bytes<S>());
   if (e == cudaSuccess)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, search_kernel<S, CODEC>, kWarpsPerBlock * 32,
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, search_kernel<S, CODEC, MINB>, kWarpsPerBlock * 32,
                                                       smem_bytes<S>());
   return e == cudaSuccess && n > 0 ? n : 1;
 }
 
-template <class S, int CODEC>
+template <class S, int CODEC, int MINB>
 cudaError_t launch(const LaunchDesc& L, int grid, cudaStream_t s) {
-  cudaError_t e = cudaFuncSetAttribute(search_kernel<S, CODEC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(search_kernel<S, CODEC, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem_bytes<S>());
   if (e != cudaSuccess) return e;
-  search_kernel<S, CODEC><<<grid, kWarpsPerBlock * 32, smem_bytes<S>(), s>>>(L);
+  search_kernel<S, CODEC, MINB><<<grid, kWarpsPerBlock * 32, smem_bytes<S>(), s>>>(L);
   return cudaGetLastError();
+}
+
+template <class S, int CODEC>
+int bps_variant(int v) {
+  return v == 0 ? blocks_per_sm<S, CODEC, 2>() : v == 2 ? blocks_per_sm<S, CODEC, 4>() : blocks_per_sm<S, CODEC, 3>();
+}
+template <class S, int CODEC>
+cudaError_t launch_variant(const LaunchDesc& L, int v, int grid, cudaStream_t s) {
+  return v == 0 ? launch<S, CODEC, 2>(L, grid, s) : v == 2 ? launch<S, CODEC, 4>(L, grid, s)
+                                                           : launch<S, CODEC, 3>(L, grid, s);
 }
 
 }  // namespace
 
-int search_blocks_per_sm(int bytes_per_sample, int codec) {
+int search_blocks_per_sm(int bytes_per_sample, int codec, int variant) {
   if (codec == RME_CODEC_HEVC)
-    return bytes_per_sample == 1 ? blocks_per_sm<uint8_t, RME_CODEC_HEVC>() : blocks_per_sm<uint16_t, RME_CODEC_HEVC>();
-  return bytes_per_sample == 1 ? blocks_per_sm<uint8_t, RME_CODEC_H264>() : blocks_per_sm<uint16_t, RME_CODEC_H264>();
+    return bytes_per_sample == 1 ? bps_variant<uint8_t, RME_CODEC_HEVC>(variant)
+                                 : bps_variant<uint16_t, RME_CODEC_HEVC>(variant);
+  return bytes_per_sample == 1 ? bps_variant<uint8_t, RME_CODEC_H264>(variant)
+                               : bps_variant<uint16_t, RME_CODEC_H264>(variant);
 }
 
-cudaError_t launch_search(const LaunchDesc& L, int bytes_per_sample, int codec, int grid, cudaStream_t s) {
+cudaError_t launch_search(const LaunchDesc& L, int bytes_per_sample, int codec, int variant, int grid,
+                          cudaStream_t s) {
   if (codec == RME_CODEC_HEVC)
-    return bytes_per_sample == 1 ? launch<uint8_t, RME_CODEC_HEVC>(L, grid, s)
-                                 : launch<uint16_t, RME_CODEC_HEVC>(L, grid, s);
-  return bytes_per_sample == 1 ? launch<uint8_t, RME_CODEC_H264>(L, grid, s)
-                               : launch<uint16_t, RME_CODEC_H264>(L, grid, s);
+    return bytes_per_sample == 1 ? launch_variant<uint8_t, RME_CODEC_HEVC>(L, variant, grid, s)
+                                 : launch_variant<uint16_t, RME_CODEC_HEVC>(L, variant, grid, s);
+  return bytes_per_sample == 1 ? launch_variant<uint8_t, RME_CODEC_H264>(L, variant, grid, s)
+                               : launch_variant<uint16_t, RME_CODEC_H264>(L, variant, grid, s);
 }
 
 }  // namespace rme
