@@ -49,7 +49,8 @@ def shifted(pic: np.ndarray, dx: int, dy: int, rng: np.random.Generator | None =
 
 def random_jobs(rng: np.random.Generator, codec: int, w: int, h: int, nref: int, n: int,
                 sizes=((8, 8), (16, 16), (16, 8), (8, 16), (32, 32), (64, 64), (4, 4), (8, 4), (4, 8), (32, 16),
-                       (16, 64), (64, 16), (12, 16), (16, 12)),
+                       (16, 64), (64, 16), (12, 16), (16, 12), (64, 48), (48, 64), (32, 24), (24, 32), (32, 8),
+                       (8, 32)),
                 spread: int = 120) -> np.ndarray:
     jobs = np.zeros(n, capi.JOB_DTYPE)
     max_seeds = 8 if codec == capi.RME_CODEC_H264 else capi.RME_MAX_SEEDS
