@@ -139,6 +139,52 @@ def test_hevc_1080p_frame_matches_the_oracle(ms):
     assert st.satd_candidates == int(want["n_satd"].sum())
 
 
+def test_hevc_4k_10bit_four_references_match_the_oracle(ms):
+    """One frame of the 2160p 10-bit workload (config 2 without AMP): four
+    references, +-128, 10-bit samples, 4x the PUs of 1080p."""
+    seq = synth.config2(nframes=5)
+    p = oracle.params(HEVC, 32, hevc_search_range=128)
+    f = seq.frames
+    got, want = _run(ms, HEVC, 10, f[4], [f[3], f[2], f[1], f[0]], p, base=2000)
+    assert_results_equal(got, want, "HEVC 2160p 10-bit 4 refs")
+    for i in range(2000, 2005):
+        ms.release(i)
+
+
+def test_mixed_stream_batch_equals_the_per_frame_path(ms):
+    """The batched form's mix (config 3): H.264 360p 8-bit, HEVC 720p 8-bit,
+    HEVC 1080p 10-bit and HEVC 2160p 8-bit streams, two references each and
+    ranges 32 / 64 / 64 / 128, one frame of each in one launch (two kinds of
+    8-bit task and one 16-bit kind, concurrent); every frame equals its
+    per-frame search, and the two smaller ones the oracle."""
+    kinds = [(H264, 8, 640, 360, 32), (HEVC, 8, 1280, 720, 64), (HEVC, 10, 1920, 1080, 64), (HEVC, 8, 3840, 2160, 128)]
+    frames, params, pics = [], [], {}
+    for k, (codec, bd, w, h, rng_) in enumerate(kinds):
+        seq = synth.stream_sequence(codec, w, h, bd, 3, k)
+        base = 3000 + 10 * k
+        for t, fr in enumerate(seq.frames):
+            ms.upload(base + t, fr, codec, bd, as_ref=True)
+        pics[k] = seq.frames
+        frames.append((base + 2, [base + 1, base]))
+        p = oracle.params(codec, 30)
+        if codec == HEVC:
+            p.hevc_search_range = rng_
+        else:
+            p.h264_range = rng_
+        params.append(p)
+    for _ in range(2):
+        outs = ms.search_batch(frames, params)
+        for (s_id, refs), pp, got in zip(frames, params, outs):
+            assert_results_equal(got, ms.search(s_id, refs, pp), f"mix vs per-frame {s_id}")
+    for k in (0, 1):
+        codec, bd = kinds[k][0], kinds[k][1]
+        want = oracle.frame_search(codec, bd, pics[k][2], [pics[k][1], pics[k][0]], params[k])
+        assert_results_equal(outs[k], want, f"mix vs oracle {k}")
+    for k in range(4):
+        for t in range(3):
+            ms.release(3000 + 10 * k + t)
+
+
 def test_batch_equals_the_frames_and_the_oracle(ms):
     """Several frames of two formats in one persistent launch, three times
     (the second launch captures a graph, the third replays it)."""
