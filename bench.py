@@ -367,7 +367,7 @@ def run_ours(args, world, rank, local):
 
 
 def run_served(frames, capacity_fps: float, loads=(0.2, 0.5, 0.8, 1.0, 1.2), seconds: float = 2.0,
-               warm_s: float = 0.5, local: int = 0) -> dict:
+               warm_s: float = 0.5, local: int = 0, max_batch: int = 64) -> dict:
     """The serving loop under Poisson load: streams of the 1080p workload at
     30 frames/s each, the total rate a fraction of the measured batched
     capacity; per-frame latency is submit -> results complete (host clock,
@@ -384,10 +384,14 @@ def run_served(frames, capacity_fps: float, loads=(0.2, 0.5, 0.8, 1.0, 1.2), sec
         rate = load * capacity_fps
         nstreams = max(1, int(round(rate / 30.0)))
         with rme.MotionSearch(local) as ms:
-            srv = rme.Server(ms, hbm_budget_bytes=120 << 30, max_frames_per_launch=64, max_streams=1024)
+            srv = rme.Server(ms, hbm_budget_bytes=120 << 30, max_frames_per_launch=max_batch, max_streams=1024)
             try:
                 for sid in range(nstreams):
                     assert srv.open_stream(sid, capi.RME_CODEC_HEVC, 8, WIDTH, HEIGHT, p, NREF) == 0
+                # Each stream's client reuses a ring of result buffers (as an
+                # encoder reuses its motion field), touched once here.
+                count = 42900 * NREF
+                bufs = {sid: [np.zeros(count, capi.RESULT_DTYPE) for _ in range(8)] for sid in range(nstreams)}
                 # Fill every stream's picture ring once (allocations, not timed).
                 nxt = {}
                 for sid in range(nstreams):
@@ -413,7 +417,7 @@ def run_served(frames, capacity_fps: float, loads=(0.2, 0.5, 0.8, 1.0, 1.2), sec
                     while time.perf_counter() - t0 < at:
                         done += srv.poll()
                         time.sleep(0.0002)
-                    rid = srv.submit(sid, frames[(sid * 7 + nxt[sid]) % len(frames)])
+                    rid = srv.submit(sid, frames[(sid * 7 + nxt[sid]) % len(frames)], out=bufs[sid][nxt[sid] % 8])
                     nxt[sid] += 1
                     if at >= warm_s:
                         measured.add(rid)

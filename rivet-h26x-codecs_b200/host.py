@@ -249,12 +249,25 @@ class Server:
             capi.check(rc)
         return rc
 
-    def submit(self, stream_id: int, luma: np.ndarray) -> int:
-        """Queue one frame (copied before return); returns the request id."""
+    def result_count(self, stream_id: int) -> int:
+        """Results the stream's next submitted frame will have."""
         codec, nb, nref, seen = self._streams[stream_id]
         nr = min(nref, seen)
-        count = nb if codec == capi.RME_CODEC_H264 else nb * nr
-        out = np.zeros(max(count, 1), capi.RESULT_DTYPE) if nr else None
+        return 0 if nr == 0 else nb if codec == capi.RME_CODEC_H264 else nb * nr
+
+    def submit(self, stream_id: int, luma: np.ndarray, out: np.ndarray | None = None) -> int:
+        """Queue one frame (copied before return); returns the request id.
+        The results land in `out` (a RESULT_DTYPE array of at least
+        result_count(stream_id) entries that the caller reuses, as an encoder
+        reuses its motion field) or in a new array."""
+        codec, nb, nref, seen = self._streams[stream_id]
+        nr = min(nref, seen)
+        count = self.result_count(stream_id)
+        if out is not None:
+            if out.dtype != capi.RESULT_DTYPE or out.size < count or not out.flags.c_contiguous:
+                raise ValueError("out must be a contiguous RESULT_DTYPE array of the frame's result count")
+        elif nr:
+            out = np.zeros(max(count, 1), capi.RESULT_DTYPE)
         rid = C.c_int64()
         luma = np.ascontiguousarray(luma)
         capi.check(self._lib.rme_serve_submit(self.h, stream_id, capi.ptr(luma),
