@@ -502,6 +502,8 @@ __device__ void hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t,
       if (px < F.nbx[l - 1] && py < F.nby[l - 1]) didx = (F.base[l - 1] + py * F.nbx[l - 1] + px) * F.nref + r;
     }
     const uint32_t dv = didx >= 0 ? ldcg_u32(&F.out[didx].mv) : 0u;
+    // The source block is staged while those loads are in flight.
+    stage_src<S>(sm.src, plane_at<S>(F.src, 0, x, y), F.src.stride, w, h, lane);
     const uint32_t have = __ballot_sync(kFull, didx >= 0);
     const uint32_t va = __shfl_sync(kFull, dv, 0), vb = __shfl_sync(kFull, dv, 1), vp = __shfl_sync(kFull, dv, 2);
     int na = 0, ax = 0, ay = 0, cx = 0, cy = 0;
@@ -534,7 +536,7 @@ __device__ void hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t,
     out = &F.out[t];
   }
   const DevPlanes& R = F.ref[r];
-  stage_src<S>(sm.src, plane_at<S>(F.src, 0, x, y), F.src.stride, w, h, lane);
+  if (F.mode == RME_PRED_GIVEN) stage_src<S>(sm.src, plane_at<S>(F.src, 0, x, y), F.src.stride, w, h, lane);
   const S* org = plane_at<S>(R, 0, x, y);
   const int stride = R.stride;
   constexpr int SPW = 4 / sizeof(S);
