@@ -62,8 +62,11 @@ extern "C" {
  * GIVEN:      the caller passes one rme_job per (block, reference) with its
  *             predictor(s) and candidate seeds — one encoder call exactly.
  * STANDALONE: the library derives them from the frame's own results in a
- *             fixed order (a wavefront), the rule restated in DESIGN.md
- *             and in the oracle; used for whole-frame throughput runs.   */
+ *             fixed order (a wavefront): HEVC, per reference and size
+ *             level, the AMVP pair of the left and upper blocks' results
+ *             and the enclosing block's result as the parent seed; H.264,
+ *             p_mb's candidates over the A, B, C, D macroblocks' results.
+ *             Used for whole-frame throughput runs.                      */
 #define RME_PRED_GIVEN       0
 #define RME_PRED_STANDALONE  1
 
@@ -111,8 +114,10 @@ typedef struct {
   float   hevc_lambda_scale;
   int32_t hevc_pad;
   int32_t hevc_pu_mask;       /* STANDALONE: bit k -> 2Nx2N PUs of 8<<k     */
-  int32_t hevc_amp;           /* STANDALONE: also the AMP shapes 2NxnU,
-                                 2NxnD, nLx2N, nRx2N of every size >= 16   */
+  int32_t hevc_amp;           /* STANDALONE: also the AMP units of every
+                                 CU of size >= 16: bit 0 2NxnU, 1 2NxnD,
+                                 2 nLx2N, 3 nRx2N (each CU's two units,
+                                 searched from the CU's 2Nx2N result)      */
 } rme_params;
 
 /* One search job (GIVEN mode): a block, the reference it searches, its
@@ -221,7 +226,9 @@ int rme_frame_result_count(void* ctx, const rme_frame* f, const rme_params* p,
                            int32_t* count);
 
 /* The STANDALONE blocks of a frame, in result order (HEVC: size levels from
- * the largest, raster order within a level; H.264: macroblock raster).
+ * the largest, raster order within a level, then the AMP units hevc_amp
+ * asks for: per level of 16 or more, per CU in raster order, per mode in
+ * bit order, the top/left unit then the other; H.264: macroblock raster).
  * `blocks` receives 4 int32 per block (x, y, w, h); pass NULL to get the
  * count only. */
 int rme_standalone_blocks(const rme_picture_desc* d, const rme_params* p,

@@ -29,8 +29,27 @@ int level_sizes(const rme_params* p, int* sizes) {  // largest first
   return n;
 }
 
+// The two PUs of an asymmetric partition of the N x N CU at (x, y): mode
+// bit 0 2NxnU, 1 2NxnD, 2 nLx2N, 3 nRx2N (H.265 Table 7-10), part 0 the
+// top/left unit.
+void amp_pu(int mode, int part, int x, int y, int N, int32_t* b) {
+  const int q = N / 4;
+  b[0] = x;
+  b[1] = y;
+  b[2] = N;
+  b[3] = N;
+  switch (mode) {
+    case 0: b[3] = part ? 3 * q : q; b[1] = part ? y + q : y; break;
+    case 1: b[3] = part ? q : 3 * q; b[1] = part ? y + 3 * q : y; break;
+    case 2: b[2] = part ? 3 * q : q; b[0] = part ? x + q : x; break;
+    default: b[2] = part ? q : 3 * q; b[0] = part ? x + 3 * q : x; break;
+  }
+}
+
 // HEVC STANDALONE blocks: per size level (largest first), the 2Nx2N PUs
-// that lie wholly inside the picture, raster order.
+// that lie wholly inside the picture, raster order; then, where asked
+// (hevc_amp), per level of 16 or more, per such CU in raster order, per
+// enabled AMP mode (bit order), its two PUs.
 int hevc_blocks(int W, int H, const rme_params* p, int32_t* blocks) {
   int sizes[4], nl = level_sizes(p, sizes), n = 0;
   for (int l = 0; l < nl; ++l) {
@@ -45,6 +64,15 @@ int hevc_blocks(int W, int H, const rme_params* p, int32_t* blocks) {
         }
         ++n;
       }
+  }
+  for (int l = 0; l < nl && sizes[l] >= 16; ++l) {
+    int N = sizes[l];
+    for (int by = 0; by + N <= H; by += N)
+      for (int bx = 0; bx + N <= W; bx += N)
+        for (int m = 0; m < 4; ++m)
+          if ((p->hevc_amp >> m) & 1)
+            for (int k = 0; k < 2; ++k, ++n)
+              if (blocks) amp_pu(m, k, bx, by, N, blocks + 4 * n);
   }
   return n;
 }
@@ -337,6 +365,29 @@ void hevc_frame(const Dist<S>& dist, const S* src, int W, int H, ptrdiff_t ss, i
           hevc_one(dist, *refs[r], bd, src, ss, bx * N, by * N, N, N, lam, p, mvp, seeds, ns, r, at(l, bx, by, r));
         }
   }
+  // AMP (hevc_amp): each CU's two units per enabled mode, searched from the
+  // CU's own 2Nx2N result `own` — the parts search's own seed first
+  // (pick_pu under part_seeded, h265_me.rs:1327-1348) — with the AMVP pair
+  // [own, 0] (two zeros when own is zero): seeds [own, mvp0, mvp1].
+  size_t k = base[nl];
+  for (int l = 0; l < nl && sizes[l] >= 16; ++l) {
+    int N = sizes[l];
+    for (int by = 0; by < nby[l]; ++by)
+      for (int bx = 0; bx < nbx[l]; ++bx)
+        for (int m = 0; m < 4; ++m)
+          if ((p->hevc_amp >> m) & 1)
+            for (int part = 0; part < 2; ++part, ++k) {
+              int32_t b[4];
+              amp_pu(m, part, bx * N, by * N, N, b);
+              for (int r = 0; r < nref; ++r) {
+                Mv own(at(l, bx, by, r).mv.x, at(l, bx, by, r).mv.y);
+                Mv mvp[2] = {own, Mv()};
+                Mv seeds[3] = {own, mvp[0], mvp[1]};
+                hevc_one(dist, *refs[r], bd, src, ss, b[0], b[1], b[2], b[3], lam, p, mvp, seeds, 3, r,
+                         out[k * nref + r]);
+              }
+            }
+  }
 }
 
 template <class S>
@@ -523,8 +574,9 @@ int orc_hevc_decide(const rme_picture_desc* d, const rme_params* p, int32_t nref
     nby[l] = H / sizes[l];
     base[l + 1] = base[l] + nbx[l] * nby[l];
   }
-  std::vector<uint64_t> cost(base[nl]);
-  for (int b = 0; b < base[nl]; ++b) {
+  const int nb_all = hevc_blocks(W, H, p, nullptr);
+  std::vector<uint64_t> cost(nb_all);
+  for (int b = 0; b < nb_all; ++b) {
     int br = 0;
     uint64_t bc = UINT64_MAX;
     for (int r = 0; r < nref; ++r) {

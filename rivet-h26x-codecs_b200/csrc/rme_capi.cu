@@ -236,6 +236,22 @@ int level_sizes(const rme_params* p, int* sizes) {
   return n;
 }
 
+// The two units of an asymmetric partition of the N x N CU at (x, y): mode
+// bit 0 2NxnU, 1 2NxnD, 2 nLx2N, 3 nRx2N, part 0 the top/left unit.
+void amp_unit(int mode, int part, int x, int y, int N, int32_t* b) {
+  const int q = N / 4;
+  b[0] = x;
+  b[1] = y;
+  b[2] = b[3] = N;
+  if (mode < 2) {
+    b[3] = (part == (mode == 0)) ? 3 * q : q;
+    if (part) b[1] = y + (mode == 0 ? q : 3 * q);
+  } else {
+    b[2] = (part == (mode == 2)) ? 3 * q : q;
+    if (part) b[0] = x + (mode == 2 ? q : 3 * q);
+  }
+}
+
 int count_blocks(const rme_picture_desc* d, const rme_params* p, int32_t* blocks) {
   int n = 0;
   if (d->codec == RME_CODEC_H264) {
@@ -260,6 +276,17 @@ int count_blocks(const rme_picture_desc* d, const rme_params* p, int32_t* blocks
           blocks[4 * n + 2] = blocks[4 * n + 3] = N;
         }
   }
+  // AMP units: per level of 16 or more, per CU, per enabled mode, two units.
+  if (p->predictor_mode == RME_PRED_STANDALONE)
+    for (int l = 0; l < nl && sizes[l] >= 16; ++l) {
+      int N = sizes[l];
+      for (int by = 0; by + N <= d->height; by += N)
+        for (int bx = 0; bx + N <= d->width; bx += N)
+          for (int m = 0; m < 4; ++m)
+            if ((p->hevc_amp >> m) & 1)
+              for (int k = 0; k < 2; ++k, ++n)
+                if (blocks) amp_unit(m, k, bx, by, N, blocks + 4 * n);
+    }
   return n;
 }
 
@@ -284,7 +311,7 @@ int check_params(Ctx* c, const rme_params* p, const rme_picture_desc& d) {
       return fail(c, RME_EINVAL, "bad HEVC search settings");
     if (p->predictor_mode == RME_PRED_STANDALONE && ((p->hevc_pu_mask & 0xF) == 0 || (p->hevc_pu_mask & ~0xF)))
       return fail(c, RME_EINVAL, "hevc_pu_mask must select sizes among 8..64");
-    if (p->hevc_amp) return fail(c, RME_ENOSYS, "AMP shapes in STANDALONE mode are not built");
+    if (p->hevc_amp & ~0xF) return fail(c, RME_EINVAL, "hevc_amp selects among four AMP modes");
   }
   return 0;
 }
@@ -320,7 +347,8 @@ const Tables* get_tables(Ctx* c, const rme_params* p, int bd, int* rc) {
 // A, B, C and D macroblocks), and the tasks that read none. The kernel
 // releases exactly these edges (rme_search.cu), so every count reaches zero.
 const Deps* get_deps(Ctx* c, const rme_picture_desc& d, const rme_params* p, int nref, int* rc) {
-  std::vector<int64_t> sig = {d.codec, d.width, d.height, nref, d.codec == RME_CODEC_HEVC ? p->hevc_pu_mask : 0};
+  std::vector<int64_t> sig = {d.codec, d.width, d.height, nref, d.codec == RME_CODEC_HEVC ? p->hevc_pu_mask : 0,
+                              d.codec == RME_CODEC_HEVC ? p->hevc_amp : 0};
   auto it = c->deps.find(sig);
   if (it != c->deps.end()) return &it->second;
   std::vector<int32_t> pend;
@@ -345,6 +373,9 @@ const Deps* get_deps(Ctx* c, const rme_picture_desc& d, const rme_params* p, int
           for (int r = 0; r < nref; ++r) pend.push_back((bx > 0) + (by > 0) + parent);
         }
     }
+    // An AMP unit reads its CU's 2Nx2N result.
+    const int namp = count_blocks(&d, p, nullptr) - (int)(pend.size() / nref);
+    for (int k = 0; k < namp * nref; ++k) pend.push_back(1);
   }
   for (size_t t = 0; t < pend.size(); ++t)
     if (pend[t] == 0) dp.ready.push_back((uint32_t)t);
@@ -407,6 +438,15 @@ int make_frame(Ctx* c, const rme_frame* f, const rme_params* p, FrameDesc* fd, r
       fd->nbx[l] = src->d.width / sizes[l];
       fd->nby[l] = src->d.height / sizes[l];
       fd->base[l + 1] = fd->base[l] + fd->nbx[l] * fd->nby[l];
+    }
+    if (p->predictor_mode == RME_PRED_STANDALONE && p->hevc_amp) {
+      fd->amp = p->hevc_amp;
+      fd->amp_nmodes = __builtin_popcount((unsigned)p->hevc_amp);
+      fd->amp_base[0] = fd->base[fd->nlevels];
+      while (fd->amp_nlev < fd->nlevels && fd->size[fd->amp_nlev] >= 16) {
+        const int l = fd->amp_nlev++;
+        fd->amp_base[l + 1] = fd->amp_base[l] + fd->nbx[l] * fd->nby[l] * 2 * fd->amp_nmodes;
+      }
     }
   } else {
     fd->pad = p->h264_pad;
@@ -938,8 +978,9 @@ int rme_hevc_decide(const rme_picture_desc* d, const rme_params* p, int32_t nref
     nby[l] = H / sizes[l];
     base[l + 1] = base[l] + nbx[l] * nby[l];
   }
-  std::vector<uint64_t> cost(base[nl]);
-  for (int b = 0; b < base[nl]; ++b) {
+  const int nb_all = count_blocks(d, p, nullptr);  // AMP units included
+  std::vector<uint64_t> cost(nb_all);
+  for (int b = 0; b < nb_all; ++b) {
     int br = 0;
     uint64_t bc = UINT64_MAX;
     for (int r = 0; r < nref; ++r) {

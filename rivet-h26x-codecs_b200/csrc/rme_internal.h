@@ -46,6 +46,11 @@ struct FrameDesc {
   int32_t size[kMaxLevels], nbx[kMaxLevels], nby[kMaxLevels], base[kMaxLevels + 1];
   int32_t search_range, search_rings, quarter_cross;
   float lam;                 // SATD Lagrangian (rate = (lam * bits as f32) as u32)
+  // STANDALONE AMP: mode bits, their count, the levels that have AMP units
+  // (the first amp_nlev: sizes of 16 or more), and per such level the block
+  // index of its first AMP unit (amp_base[0] = base[nlevels]).
+  int32_t amp, amp_nmodes, amp_nlev;
+  int32_t amp_base[kMaxLevels + 1];
   // H.264
   const uint16_t* tab;       // MvCostTable
   int32_t range, hpel_iters, qpel_iters, umh, qpel_diamond, dia, vr;

@@ -460,6 +460,7 @@ __device__ void hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t,
   int p0x, p0y, p1x, p1y;
   int sx = 0, sy = 0;  // this lane's seed (lane < ns)
   int l = 0, lbx = 0, lby = 0, local = 0;  // STANDALONE: level and block
+  bool amp_unit = false;                   // STANDALONE: an AMP unit
   rme_result* out;
   if (F.mode == RME_PRED_GIVEN) {
     const rme_job* j = &F.jobs[t];
@@ -480,6 +481,48 @@ __device__ void hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t,
     out = &F.out[t];
   } else {
     r = t % F.nref;
+    const int blk = t / F.nref;
+    amp_unit = blk >= F.base[F.nlevels];
+  }
+  if (amp_unit) {
+    // An AMP unit (after every 2Nx2N block): its level, CU, mode and part.
+    // It is searched from its CU's own 2Nx2N result: AMVP pair [own, 0],
+    // seeds [own, mvp0, mvp1] (the parts search's own seed first).
+    const int blk = t / F.nref;
+    int la = 0;
+    while (la + 1 < F.amp_nlev && blk >= F.amp_base[la + 1]) ++la;
+    const int per = 2 * F.amp_nmodes, j = blk - F.amp_base[la], cu = j / per, rem = j - cu * per;
+    int mode = 0;
+    for (int b = 0, k = rem >> 1; b < 4; ++b)
+      if ((F.amp >> b) & 1) {
+        if (k == 0) {
+          mode = b;
+          break;
+        }
+        --k;
+      }
+    const int part = rem & 1, N = F.size[la], q = N / 4;
+    const int cby = cu / F.nbx[la], cbx = cu - cby * F.nbx[la];
+    x = cbx * N;
+    y = cby * N;
+    w = h = N;
+    if (mode < 2) {
+      h = (part == (mode == 0)) ? 3 * q : q;
+      if (part) y += mode == 0 ? q : 3 * q;
+    } else {
+      w = (part == (mode == 2)) ? 3 * q : q;
+      if (part) x += mode == 2 ? q : 3 * q;
+    }
+    const uint32_t ov = ldcg_u32(&F.out[(F.base[la] + cu) * F.nref + r].mv);
+    stage_src<S>(sm.src, plane_at<S>(F.src, 0, x, y), F.src.stride, w, h, lane);
+    p0x = mvx_of(ov);
+    p0y = mvy_of(ov);
+    p1x = p1y = 0;
+    ns = 3;
+    sx = lane == 0 || lane == 1 ? p0x : 0;
+    sy = lane == 0 || lane == 1 ? p0y : 0;
+    out = &F.out[t];
+  } else if (F.mode != RME_PRED_GIVEN) {
     const int blk = t / F.nref;
     while (l + 1 < F.nlevels && blk >= F.base[l + 1]) ++l;
     local = blk - F.base[l];
@@ -680,10 +723,11 @@ __device__ void hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t,
   }
   nsatd += 9;
   write_result(out, bmx, bmy, r, bc, bsatd, imx, imy, int_cost, nsad, nsatd, lane);
-  if (F.mode != RME_PRED_GIVEN) {
+  if (F.mode != RME_PRED_GIVEN && !amp_unit) {
     // The tasks reading this result: right and lower neighbours of this
-    // level, the blocks of the next evaluated size inside this one. Lane 0's
-    // result is fenced, then each lane releases one of them.
+    // level, the blocks of the next evaluated size inside this one, this
+    // CU's AMP units. Lane 0's result is fenced, then each lane releases one
+    // of them.
     if (lane == 0) __threadfence();
     __syncwarp();
     int ncx = 0, ncy = 0, cx0 = 0, cy0 = 0;
@@ -694,15 +738,18 @@ __device__ void hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t,
       ncx = max(0, min((lbx + 1) * N / M, F.nbx[l + 1]) - cx0);
       ncy = max(0, min((lby + 1) * N / M, F.nby[l + 1]) - cy0);
     }
-    for (int k = lane; k < 2 + ncx * ncy; k += 32) {
+    const int namp = l < F.amp_nlev ? 2 * F.amp_nmodes : 0, nch = ncx * ncy;
+    for (int k = lane; k < 2 + nch + namp; k += 32) {
       int dtask = -1;
       if (k == 0) {
         if (lbx + 1 < F.nbx[l]) dtask = (F.base[l] + local + 1) * F.nref + r;
       } else if (k == 1) {
         if (lby + 1 < F.nby[l]) dtask = (F.base[l] + local + F.nbx[l]) * F.nref + r;
-      } else {
+      } else if (k < 2 + nch) {
         const int c = k - 2, cy = cy0 + c / ncx, cx = cx0 + c % ncx;
         dtask = (F.base[l + 1] + cy * F.nbx[l + 1] + cx) * F.nref + r;
+      } else {
+        dtask = (F.amp_base[l] + local * namp + (k - 2 - nch)) * F.nref + r;
       }
       if (dtask >= 0) release(L, F, f, dtask);
     }

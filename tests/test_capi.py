@@ -43,24 +43,38 @@ def test_defaults_are_the_oracles():
             assert getattr(a, name) == getattr(b, name), name
 
 
-@pytest.mark.parametrize("codec,w,h,mask", [(capi.RME_CODEC_HEVC, 1920, 1080, 0xF), (capi.RME_CODEC_HEVC, 200, 136, 0b1010),
-                                            (capi.RME_CODEC_H264, 352, 288, 0), (capi.RME_CODEC_H264, 100, 70, 0)])
-def test_standalone_blocks_are_the_oracles(codec, w, h, mask):
+@pytest.mark.parametrize("codec,w,h,mask,amp", [(capi.RME_CODEC_HEVC, 1920, 1080, 0xF, 0),
+                                                (capi.RME_CODEC_HEVC, 200, 136, 0b1010, 0),
+                                                (capi.RME_CODEC_HEVC, 200, 136, 0xF, 0b0101),
+                                                (capi.RME_CODEC_HEVC, 136, 200, 0b0111, 0xF),
+                                                (capi.RME_CODEC_H264, 352, 288, 0, 0), (capi.RME_CODEC_H264, 100, 70, 0, 0)])
+def test_standalone_blocks_are_the_oracles(codec, w, h, mask, amp):
     p = capi.default_params(codec, 30)
     if mask:
         p.hevc_pu_mask = mask
+    p.hevc_amp = amp
     got = host.standalone_blocks(codec, w, h, 8, p)
     d = capi.PictureDesc(codec, 8, w, h, w)
     want = oracle.standalone_blocks(d, p)
     np.testing.assert_array_equal(got, want)
     if (codec, w, h, mask) == (capi.RME_CODEC_HEVC, 1920, 1080, 0xF):
         assert len(got) == 32400 + 8040 + 1980 + 480
+    if amp:  # two units per enabled mode of every CU of 16 or more, each half of its CU's area
+        nmodes = bin(amp).count("1")
+        cus = got[got[:, 2] == got[:, 3]]
+        big = cus[cus[:, 2] >= 16]
+        assert len(got) == len(cus) + 2 * nmodes * len(big)
+        units = got[len(cus):]
+        assert (units[0::2, 2] * units[0::2, 3] + units[1::2, 2] * units[1::2, 3] ==
+                np.repeat(big[:, 2] ** 2, nmodes)).all()
 
 
-@pytest.mark.parametrize("w,h,mask,nref", [(1920, 1080, 0xF, 2), (200, 136, 0xF, 3), (136, 200, 0b1011, 1)])
-def test_the_hevc_decision_is_the_oracles(w, h, mask, nref):
+@pytest.mark.parametrize("w,h,mask,nref,amp", [(1920, 1080, 0xF, 2, 0), (200, 136, 0xF, 3, 0), (136, 200, 0b1011, 1, 0),
+                                               (200, 136, 0xF, 2, 0b0101)])
+def test_the_hevc_decision_is_the_oracles(w, h, mask, nref, amp):
     p = capi.default_params(capi.RME_CODEC_HEVC, 32)
     p.hevc_pu_mask = mask
+    p.hevc_amp = amp
     nb = len(host.standalone_blocks(capi.RME_CODEC_HEVC, w, h, 8, p))
     rng = np.random.default_rng(w + h + nref)
     res = np.zeros(nb * nref, capi.RESULT_DTYPE)

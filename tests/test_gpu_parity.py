@@ -104,12 +104,16 @@ def test_h264_given_jobs_match_the_oracle(ms, bd):
 
 
 # ---- HEVC -------------------------------------------------------------------
-@pytest.mark.parametrize("variant", ["medium", "range64_rings", "cross", "levels"])
+@pytest.mark.parametrize("variant", ["medium", "range64_rings", "cross", "levels", "amp", "amp_all_levels"])
 @pytest.mark.parametrize("bd", [8, 10])
 def test_hevc_frames_match_the_oracle(ms, variant, bd):
+    """STANDALONE frames under the search settings, size levels and AMP
+    units (2NxnU + nLx2N as the 2160p workload asks, or all four modes over
+    a subset of levels), against the oracle."""
     seq = synth.make_sequence(HEVC, 256, 192, bd, 3, 100 + bd, 64, 64, 2.0 if bd == 8 else 6.0)
     kw = {"medium": {}, "range64_rings": {"hevc_search_range": 64, "hevc_search_rings": 1},
-          "cross": {"hevc_quarter_cross": 1, "hevc_search_rings": 2}, "levels": {"hevc_pu_mask": 0b1010}}[variant]
+          "cross": {"hevc_quarter_cross": 1, "hevc_search_rings": 2}, "levels": {"hevc_pu_mask": 0b1010},
+          "amp": {"hevc_amp": 0b0101}, "amp_all_levels": {"hevc_amp": 0xF, "hevc_pu_mask": 0b0111}}[variant]
     p = oracle.params(HEVC, 32, **kw)
     got, want = _run(ms, HEVC, bd, seq.frames[2], [seq.frames[1], seq.frames[0]], p)
     assert_results_equal(got, want, f"HEVC {variant} {bd}-bit")
@@ -140,10 +144,10 @@ def test_hevc_1080p_frame_matches_the_oracle(ms):
 
 
 def test_hevc_4k_10bit_four_references_match_the_oracle(ms):
-    """One frame of the 2160p 10-bit workload (config 2 without AMP): four
-    references, +-128, 10-bit samples, 4x the PUs of 1080p."""
+    """One frame of the 2160p 10-bit workload: four references, +-128,
+    10-bit samples, 2Nx2N PUs 8..64 plus the 2NxnU and nLx2N units."""
     seq = synth.config2(nframes=5)
-    p = oracle.params(HEVC, 32, hevc_search_range=128)
+    p = oracle.params(HEVC, 32, hevc_search_range=128, hevc_amp=0b0101)
     f = seq.frames
     got, want = _run(ms, HEVC, 10, f[4], [f[3], f[2], f[1], f[0]], p, base=2000)
     assert_results_equal(got, want, "HEVC 2160p 10-bit 4 refs")
