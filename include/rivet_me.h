@@ -326,6 +326,36 @@ int rme_serve_poll(void* server, rme_completion* done, int32_t max, int32_t* n);
 int rme_serve_close_stream(void* server, int32_t stream_id);
 int rme_serve_stop(void* server);
 
+/* ---- lookahead at half resolution ------------------------------------------- */
+
+/* The HEVC encoder's lookahead (quantiser propagation) measures at half
+ * resolution: each picture reduced to 8 bits as 2x2 means, costed in 8x8
+ * blocks (16x16 of the picture). These are its ME kernels, batched per
+ * picture (encode/h265_cutree.rs). */
+
+/* Build (or rebuild) a resident picture's half-resolution plane and its
+ * blocks' intra costs: LowRes::new + intra_cost (h265_cutree.rs:61-140).
+ * Synchronous. */
+int rme_lowres_build(void* ctx, int32_t pic_id, void* stream);
+
+/* Its block grid and (when `intra` is not NULL) the intra cost per block,
+ * raster order. */
+int rme_lowres_info(void* ctx, int32_t pic_id, int32_t* bw, int32_t* bh, uint32_t* intra);
+
+/* search (h265_cutree.rs:152-216) of every block of `cur_id` against
+ * `ref_id`: seeds zero, left and above vectors, a cross descent at steps 4,
+ * 2, 1 within +-16 of the best seed, SAD + 2 * min(|dx| + |dy|, 32); per
+ * block the winner's SATD (`cost`), its vector in half-resolution samples,
+ * and (when `nsad` is not NULL) the SADs scored. Host outputs, synchronous. */
+int rme_lowres_search(void* ctx, int32_t cur_id, int32_t ref_id, uint32_t* cost, rme_mv* mv, uint32_t* nsad,
+                      void* stream);
+
+/* bi_cost (h265_cutree.rs:222-243) of every block: the SATD against the
+ * rounded average of its blocks displaced by mv0 in r0 and mv1 in r1.
+ * Host inputs and output, synchronous. */
+int rme_lowres_bi_cost(void* ctx, int32_t cur_id, int32_t r0_id, const rme_mv* mv0, int32_t r1_id,
+                       const rme_mv* mv1, uint32_t* cost, void* stream);
+
 /* ---- search without allocating --------------------------------------------- */
 
 /* One picture's planes in device memory the caller owns, in the layout the

@@ -494,6 +494,164 @@ uint32_t hevc_ref_idx_bits(int r, int nref) {  // ref_idx_lX, truncated unary, c
 
 }  // namespace
 
+namespace {
+
+// ---- lookahead (HEVC cutree) at half resolution -------------------------------
+// encode/h265_cutree.rs: B = 8, PAD = 24, RANGE = 16.
+constexpr int LA_B = 8, LA_PAD = 24, LA_RANGE = 16;
+
+struct LowRes {
+  std::vector<uint8_t> luma;
+  int stride = 0, w = 0, h = 0, bw = 0, bh = 0;
+  std::vector<uint32_t> intra;
+  ptrdiff_t off(int x, int y) const { return (ptrdiff_t)(y + LA_PAD) * stride + x + LA_PAD; }
+};
+
+// LowRes::new (h265_cutree.rs:61-110): each sample the mean of a 2x2
+// square of the picture (clamped at its edges), shifted to 8 bits, over
+// whole 8x8 blocks; the padding edge-replicated.
+template <class S>
+LowRes lowres_new(const S* y, int w, int h, ptrdiff_t ys, int bd) {
+  LowRes L;
+  const int lw = (w + 1) / 2, lh = (h + 1) / 2;
+  L.bw = (lw + LA_B - 1) / LA_B;
+  L.bh = (lh + LA_B - 1) / LA_B;
+  const int pw = L.bw * LA_B, ph = L.bh * LA_B;
+  L.w = pw;
+  L.h = ph;
+  L.stride = pw + 2 * LA_PAD;
+  L.luma.assign((size_t)L.stride * (ph + 2 * LA_PAD), 0);
+  const int shift = bd - 8;
+  auto at = [&](int x, int y0) { return (int)y[(ptrdiff_t)std::min(y0, h - 1) * ys + std::min(x, w - 1)]; };
+  for (int yy = 0; yy < ph; ++yy)
+    for (int xx = 0; xx < pw; ++xx) {
+      const int x2 = 2 * std::min(xx, lw - 1), y2 = 2 * std::min(yy, lh - 1);
+      const int sum = at(x2, y2) + at(x2 + 1, y2) + at(x2, y2 + 1) + at(x2 + 1, y2 + 1);
+      L.luma[(size_t)(yy + LA_PAD) * L.stride + xx + LA_PAD] = (uint8_t)std::min(((sum + 2) >> 2) >> shift, 255);
+    }
+  for (int yy = LA_PAD; yy < LA_PAD + ph; ++yy) {
+    uint8_t* row = &L.luma[(size_t)yy * L.stride];
+    std::fill(row, row + LA_PAD, row[LA_PAD]);
+    std::fill(row + LA_PAD + pw, row + L.stride, row[LA_PAD + pw - 1]);
+  }
+  for (int yy = 0; yy < LA_PAD; ++yy) {
+    std::memcpy(&L.luma[(size_t)yy * L.stride], &L.luma[(size_t)LA_PAD * L.stride], L.stride);
+    std::memcpy(&L.luma[(size_t)(LA_PAD + ph + yy) * L.stride], &L.luma[(size_t)(LA_PAD + ph - 1) * L.stride],
+                L.stride);
+  }
+  // intra_cost (h265_cutree.rs:118-140): the least SATD of a flat (DC of
+  // the 8 samples above and 8 left), a horizontal and a vertical
+  // prediction; floored at 2 * B.
+  L.intra.resize((size_t)L.bw * L.bh);
+  for (int b = 0; b < L.bw * L.bh; ++b) {
+    const int x = (b % L.bw) * LA_B, yb = (b / L.bw) * LA_B;
+    const ptrdiff_t o = L.off(x, yb);
+    const uint8_t* src = &L.luma[o];
+    int top[LA_B], left[LA_B], st = 0;
+    for (int i = 0; i < LA_B; ++i) {
+      top[i] = L.luma[o - L.stride + i];
+      left[i] = L.luma[o + (ptrdiff_t)i * L.stride - 1];
+      st += top[i] + left[i];
+    }
+    uint8_t pred[LA_B * LA_B];
+    std::fill(pred, pred + LA_B * LA_B, (uint8_t)((st + LA_B) / (2 * LA_B)));
+    uint32_t best = satd_scalar<uint8_t>(src, L.stride, pred, LA_B, LA_B, LA_B);
+    for (int i = 0; i < LA_B * LA_B; ++i) pred[i] = (uint8_t)left[i / LA_B];
+    best = std::min(best, satd_scalar<uint8_t>(src, L.stride, pred, LA_B, LA_B, LA_B));
+    for (int i = 0; i < LA_B * LA_B; ++i) pred[i] = (uint8_t)top[i % LA_B];
+    best = std::min(best, satd_scalar<uint8_t>(src, L.stride, pred, LA_B, LA_B, LA_B));
+    L.intra[b] = std::max(best, (uint32_t)(LA_B * 2));
+  }
+  return L;
+}
+
+// search (h265_cutree.rs:152-216): per block in raster order, seeds zero,
+// left and above vectors (scored in order, strict <, within the padded
+// plane); a cross descent at steps 4, 2, 1 from a fixed `from` per round,
+// confined to +-RANGE around the best seed; SAD + 2 * min(|dx| + |dy|, 32);
+// the winner's SATD as the cost.
+void lowres_search(const LowRes& cur, const LowRes& refp, uint32_t* cost, rme_mv* mv, uint32_t* nsad) {
+  const int n = cur.bw * cur.bh, lim = LA_PAD - 1;
+  for (int b = 0; b < n; ++b) {
+    const int bx = b % cur.bw, by = b / cur.bw, x = bx * LA_B, y = by * LA_B;
+    const uint8_t* src = &cur.luma[cur.off(x, y)];
+    uint32_t count = 0;
+    auto ok = [&](int dx, int dy) {
+      return x + dx >= -lim && y + dy >= -lim && x + dx + LA_B <= refp.w + lim && y + dy + LA_B <= refp.h + lim;
+    };
+    auto sad = [&](int dx, int dy) {
+      ++count;
+      return sad_scalar<uint8_t>(src, cur.stride, &refp.luma[refp.off(x + dx, y + dy)], refp.stride, LA_B, LA_B) +
+             2u * (uint32_t)std::min(std::abs(dx) + std::abs(dy), 32);
+    };
+    int sx[3] = {0, 0, 0}, sy[3] = {0, 0, 0}, ns = 1;
+    if (bx > 0) {
+      sx[ns] = mv[b - 1].x;
+      sy[ns++] = mv[b - 1].y;
+    }
+    if (by > 0) {
+      sx[ns] = mv[b - cur.bw].x;
+      sy[ns++] = mv[b - cur.bw].y;
+    }
+    int bxm = 0, bym = 0;
+    uint32_t bc = UINT32_MAX;
+    for (int k = 0; k < ns; ++k)
+      if (ok(sx[k], sy[k])) {
+        const uint32_t c = sad(sx[k], sy[k]);
+        if (c < bc) {
+          bc = c;
+          bxm = sx[k];
+          bym = sy[k];
+        }
+      }
+    const int cx = bxm, cy = bym;
+    for (int step : {4, 2, 1}) {
+      for (;;) {
+        const int fx = bxm, fy = bym;
+        const int dirs[4][2] = {{step, 0}, {-step, 0}, {0, step}, {0, -step}};
+        for (auto& d : dirs) {
+          const int dx = fx + d[0], dy = fy + d[1];
+          if (std::abs(dx - cx) > LA_RANGE || std::abs(dy - cy) > LA_RANGE || !ok(dx, dy)) continue;
+          const uint32_t c = sad(dx, dy);
+          if (c < bc) {
+            bc = c;
+            bxm = dx;
+            bym = dy;
+          }
+        }
+        if (bxm == fx && bym == fy) break;
+      }
+    }
+    cost[b] = satd_scalar<uint8_t>(src, cur.stride, &refp.luma[refp.off(x + bxm, y + bym)], refp.stride, LA_B, LA_B);
+    mv[b].x = (int16_t)bxm;
+    mv[b].y = (int16_t)bym;
+    if (nsad) nsad[b] = count;
+  }
+}
+
+// bi_cost (h265_cutree.rs:222-243): SATD against the rounded average of
+// the two displaced blocks.
+uint32_t lowres_bi_cost(const LowRes& cur, const LowRes& r0, rme_mv m0, const LowRes& r1, rme_mv m1, int b) {
+  const int x = (b % cur.bw) * LA_B, y = (b / cur.bw) * LA_B;
+  const ptrdiff_t o0 = r0.off(x + m0.x, y + m0.y), o1 = r1.off(x + m1.x, y + m1.y);
+  uint8_t pred[LA_B * LA_B];
+  for (int yy = 0; yy < LA_B; ++yy)
+    for (int xx = 0; xx < LA_B; ++xx)
+      pred[yy * LA_B + xx] =
+          (uint8_t)((r0.luma[o0 + (ptrdiff_t)yy * r0.stride + xx] + r1.luma[o1 + (ptrdiff_t)yy * r1.stride + xx] + 1) >> 1);
+  return satd_scalar<uint8_t>(&cur.luma[cur.off(x, y)], cur.stride, pred, LA_B, LA_B, LA_B);
+}
+
+template <class S>
+LowRes lowres_of(const rme_picture_desc* d, const void* luma) {
+  return lowres_new<S>((const S*)luma, d->width, d->height, d->stride, d->bit_depth);
+}
+LowRes lowres_any(const rme_picture_desc* d, const void* luma) {
+  return d->bit_depth == 8 ? lowres_of<uint8_t>(d, luma) : lowres_of<uint16_t>(d, luma);
+}
+
+}  // namespace
+
 extern "C" {
 
 void orc_params_default(rme_params* p, int32_t codec, int32_t qp) {
@@ -772,6 +930,39 @@ int orc_chroma_predict(const rme_picture_desc* d, const void* cb, const void* cr
   };
   if (d->bit_depth == 8) run(uint8_t{});
   else run(uint16_t{});
+  return 0;
+}
+
+// The lookahead's half-resolution plane (padded, stride returned) and
+// per-block intra costs of one picture.
+int orc_lowres(const rme_picture_desc* d, const void* luma, uint8_t* plane, int32_t* stride, int32_t* rows,
+               uint32_t* intra, int32_t* nblocks) {
+  if (!valid_desc(d) || !luma) return RME_EINVAL;
+  LowRes L = lowres_any(d, luma);
+  if (stride) *stride = L.stride;
+  if (rows) *rows = L.h + 2 * LA_PAD;
+  if (nblocks) *nblocks = L.bw * L.bh;
+  if (plane) std::memcpy(plane, L.luma.data(), L.luma.size());
+  if (intra) std::memcpy(intra, L.intra.data(), L.intra.size() * sizeof(uint32_t));
+  return 0;
+}
+
+// The lookahead's search of `cur` against `ref` (both full-resolution
+// pictures of one format), and optionally the bi cost against a second
+// reference with vectors mv1.
+int orc_lowres_search(const rme_picture_desc* d, const void* cur, const void* ref, uint32_t* cost, rme_mv* mv,
+                      uint32_t* nsad) {
+  if (!valid_desc(d) || !cur || !ref) return RME_EINVAL;
+  LowRes C = lowres_any(d, cur), R = lowres_any(d, ref);
+  lowres_search(C, R, cost, mv, nsad);
+  return 0;
+}
+
+int orc_lowres_bi_cost(const rme_picture_desc* d, const void* cur, const void* r0, const rme_mv* mv0, const void* r1,
+                       const rme_mv* mv1, uint32_t* cost) {
+  if (!valid_desc(d) || !cur || !r0 || !r1) return RME_EINVAL;
+  LowRes C = lowres_any(d, cur), A = lowres_any(d, r0), B = lowres_any(d, r1);
+  for (int b = 0; b < C.bw * C.bh; ++b) cost[b] = lowres_bi_cost(C, A, mv0[b], B, mv1[b], b);
   return 0;
 }
 

@@ -45,6 +45,11 @@ _SIGS = {
                                    C.c_int32, C.c_int32, C.c_void_p]),
     "orc_chroma_predict": (C.c_int, [_PD, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_int32),
                                      C.POINTER(capi.Mv), C.c_void_p]),
+    "orc_lowres": (C.c_int, [_PD, C.c_void_p, C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_void_p,
+                             C.POINTER(C.c_int32)]),
+    "orc_lowres_search": (C.c_int, [_PD, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "orc_lowres_bi_cost": (C.c_int, [_PD, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p]),
 }
 
 _lib = None
@@ -198,4 +203,36 @@ def chroma_predict(codec, bit_depth, luma_w, luma_h, cb, cr, blocks: np.ndarray,
                                   len(blocks), blocks.ctypes.data_as(C.POINTER(C.c_int32)),
                                   C.cast(mvs.ctypes.data, C.POINTER(capi.Mv)), out.ctypes.data)
     assert rc == 0
+    return out
+
+
+def lowres(pic: np.ndarray, bit_depth: int):
+    """The lookahead's half-resolution plane (padded) and intra costs."""
+    d = desc(capi.RME_CODEC_HEVC, pic, bit_depth)
+    stride, rows, n = C.c_int32(), C.c_int32(), C.c_int32()
+    assert lib().orc_lowres(C.byref(d), pic.ctypes.data, None, C.byref(stride), C.byref(rows), None, C.byref(n)) == 0
+    plane = np.zeros((rows.value, stride.value), np.uint8)
+    intra = np.zeros(n.value, np.uint32)
+    assert lib().orc_lowres(C.byref(d), pic.ctypes.data, plane.ctypes.data, None, None, intra.ctypes.data, None) == 0
+    return plane, intra
+
+
+def lowres_search(cur: np.ndarray, ref: np.ndarray, bit_depth: int):
+    d = desc(capi.RME_CODEC_HEVC, cur, bit_depth)
+    n = C.c_int32()
+    assert lib().orc_lowres(C.byref(d), cur.ctypes.data, None, None, None, None, C.byref(n)) == 0
+    cost, nsad = np.zeros(n.value, np.uint32), np.zeros(n.value, np.uint32)
+    mv = np.zeros((n.value, 2), np.int16)
+    assert lib().orc_lowres_search(C.byref(d), cur.ctypes.data, ref.ctypes.data, cost.ctypes.data, mv.ctypes.data,
+                                   nsad.ctypes.data) == 0
+    return cost, mv, nsad
+
+
+def lowres_bi_cost(cur, r0, mv0, r1, mv1, bit_depth):
+    d = desc(capi.RME_CODEC_HEVC, cur, bit_depth)
+    mv0 = np.ascontiguousarray(mv0, np.int16)
+    mv1 = np.ascontiguousarray(mv1, np.int16)
+    out = np.zeros(len(mv0), np.uint32)
+    assert lib().orc_lowres_bi_cost(C.byref(d), cur.ctypes.data, r0.ctypes.data, mv0.ctypes.data, r1.ctypes.data,
+                                    mv1.ctypes.data, out.ctypes.data) == 0
     return out

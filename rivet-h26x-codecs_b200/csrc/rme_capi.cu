@@ -127,9 +127,12 @@ struct Picture {
   bool is_ref = false;
   void* chroma = nullptr;  // cb then cr, unpadded (cw/2 x ch/2), packed
   size_t chroma_bytes = 0;
+  void* lowres = nullptr;  // the lookahead's half-resolution plane, then its intra costs
+  LowresDesc lr{};
   ~Picture() {
     if (buf) cudaFree(buf);
     if (chroma) cudaFree(chroma);
+    if (lowres) cudaFree(lowres);
   }
 };
 
@@ -179,6 +182,11 @@ struct Ctx {
   DevBuf<int32_t> d_pending;
   DevBuf<rme_job> d_jobs;
   DevBuf<unsigned long long> d_misc;  // the launch header (kMisc*)
+  DevBuf<int32_t> d_lorder;           // lookahead: claim order (per block shape), done flags, results
+  std::pair<int, int> lorder_shape{0, 0};
+  DevBuf<int32_t> d_ldone;
+  DevBuf<uint32_t> d_lcost, d_lsad;
+  DevBuf<rme_mv> d_lmv, d_lmv2;
   DevBuf<int32_t> d_cblk;             // chroma: blocks, vectors, output offsets, output
   DevBuf<rme_mv> d_cmv;
   DevBuf<int64_t> d_coff;
@@ -1138,6 +1146,131 @@ int rme_satd_batch(const void* a, int64_t a_stride, const int64_t* a_off, const 
                    const int64_t* b_off, int32_t w, int32_t h, int32_t bit_depth, int32_t n, uint32_t* out,
                    void* stream) {
   return dist_batch(true, a, a_stride, a_off, b, b_stride, b_off, w, h, bit_depth, n, out, stream);
+}
+
+// ---- lookahead at half resolution (h265_cutree.rs) ---------------------------
+
+int rme_lowres_build(void* ctx, int32_t pic_id, void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return RME_EINVAL;
+  Picture* p;
+  int rc = picture_of(c, pic_id, &p);
+  if (rc) return rc;
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  CK(cudaSetDevice(c->device));
+  LowresDesc L{};
+  const int lw = (p->d.width + 1) / 2, lh = (p->d.height + 1) / 2;
+  L.bw = (lw + 7) / 8;
+  L.bh = (lh + 7) / 8;
+  L.pw = L.bw * 8;
+  L.ph = L.bh * 8;
+  L.stride = L.pw + 2 * kLowresPad;
+  const size_t plane = (size_t)L.stride * (L.ph + 2 * kLowresPad), intra = sizeof(uint32_t) * L.bw * L.bh;
+  if (!p->lowres) CK(cudaMalloc(&p->lowres, plane + 256 + intra));
+  L.plane = (uint8_t*)p->lowres;
+  L.intra = (uint32_t*)((uint8_t*)p->lowres + (plane + 255) / 256 * 256);
+  p->lr = L;
+  CK(launch_lowres_build(p->planes, p->d.bit_depth, p->d.width, p->d.height, L, s));
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+int rme_lowres_info(void* ctx, int32_t pic_id, int32_t* bw, int32_t* bh, uint32_t* intra) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return RME_EINVAL;
+  Picture* p;
+  int rc = picture_of(c, pic_id, &p);
+  if (rc) return rc;
+  if (!p->lowres) return fail(c, RME_EINVAL, "no half-resolution plane: call rme_lowres_build");
+  if (bw) *bw = p->lr.bw;
+  if (bh) *bh = p->lr.bh;
+  if (intra) CK(cudaMemcpy(intra, p->lr.intra, sizeof(uint32_t) * p->lr.bw * p->lr.bh, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+namespace {
+int lowres_pair(Ctx* c, int32_t a, int32_t b, Picture** pa, Picture** pb) {
+  int rc = picture_of(c, a, pa);
+  if (!rc) rc = picture_of(c, b, pb);
+  if (rc) return rc;
+  if (!(*pa)->lowres || !(*pb)->lowres) return fail(c, RME_EINVAL, "no half-resolution plane: call rme_lowres_build");
+  if ((*pa)->lr.bw != (*pb)->lr.bw || (*pa)->lr.bh != (*pb)->lr.bh)
+    return fail(c, RME_EINVAL, "half-resolution sizes differ");
+  return 0;
+}
+}  // namespace
+
+int rme_lowres_search(void* ctx, int32_t cur_id, int32_t ref_id, uint32_t* cost, rme_mv* mv, uint32_t* nsad,
+                      void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !cost || !mv) return RME_EINVAL;
+  Picture *pc, *pr;
+  int rc = lowres_pair(c, cur_id, ref_id, &pc, &pr);
+  if (rc) return rc;
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  CK(cudaSetDevice(c->device));
+  const int bw = pc->lr.bw, bh = pc->lr.bh, n = bw * bh;
+  // Claim order: anti-diagonals, each block after its left and above ones.
+  if (c->lorder_shape != std::make_pair(bw, bh)) {
+    std::vector<int32_t> order;
+    order.reserve(n);
+    for (int d = 0; d <= bw + bh - 2; ++d)
+      for (int by = std::max(0, d - bw + 1); by <= std::min(d, bh - 1); ++by) order.push_back((by << 16) | (d - by));
+    CK(c->d_lorder.ensure(n));
+    CK(cudaMemcpy(c->d_lorder.p, order.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+    c->lorder_shape = {bw, bh};
+  }
+  CK(c->d_ldone.ensure(n + 8));
+  CK(c->d_lcost.ensure(n));
+  CK(c->d_lsad.ensure(n));
+  CK(c->d_lmv.ensure(n));
+  // done flags, then the claim counter and the status word (one memset).
+  CK(cudaMemsetAsync(c->d_ldone.p, 0, sizeof(int32_t) * (n + 8), s));
+  const int ci = (n + 3) & ~1;  // an 8-byte aligned word after the flags
+  unsigned long long* counter = reinterpret_cast<unsigned long long*>(c->d_ldone.p + ci);
+  uint32_t* status = reinterpret_cast<uint32_t*>(c->d_ldone.p + ci + 2);
+  const int grid = std::max(1, std::min(c->nsm * 4, (n + 7) / 8));
+  CK(launch_lowres_search(pc->lr, pr->lr, c->d_lorder.p, c->d_ldone.p, counter, status, c->d_lcost.p, c->d_lmv.p,
+                          c->d_lsad.p, grid, s));
+  uint32_t st = 0;
+  CK(cudaMemcpyAsync(cost, c->d_lcost.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(mv, c->d_lmv.p, sizeof(rme_mv) * n, cudaMemcpyDeviceToHost, s));
+  if (nsad) CK(cudaMemcpyAsync(nsad, c->d_lsad.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&st, status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (st) return fail(c, RME_EDEVICE, "device status " + std::to_string(st));
+  return 0;
+}
+
+int rme_lowres_bi_cost(void* ctx, int32_t cur_id, int32_t r0_id, const rme_mv* mv0, int32_t r1_id, const rme_mv* mv1,
+                       uint32_t* cost, void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !mv0 || !mv1 || !cost) return RME_EINVAL;
+  Picture *pc, *p0, *p1;
+  int rc = lowres_pair(c, cur_id, r0_id, &pc, &p0);
+  if (!rc) rc = lowres_pair(c, cur_id, r1_id, &pc, &p1);
+  if (rc) return rc;
+  const int n = pc->lr.bw * pc->lr.bh;
+  // Every displaced block must stay in the padded plane (the search's own
+  // vectors always do).
+  for (int i = 0; i < n; ++i) {
+    const int x = (i % pc->lr.bw) * 8, y = (i / pc->lr.bw) * 8;
+    for (const rme_mv* m : {mv0 + i, mv1 + i})
+      if (x + m->x < -kLowresPad || y + m->y < -kLowresPad || x + m->x + 8 > pc->lr.pw + kLowresPad ||
+          y + m->y + 8 > pc->lr.ph + kLowresPad)
+        return fail(c, RME_EINVAL, "vector of block " + std::to_string(i) + " leaves the padded plane");
+  }
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  CK(cudaSetDevice(c->device));
+  CK(c->d_lmv.ensure(n));
+  CK(c->d_lmv2.ensure(n));
+  CK(c->d_lcost.ensure(n));
+  CK(cudaMemcpyAsync(c->d_lmv.p, mv0, sizeof(rme_mv) * n, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(c->d_lmv2.p, mv1, sizeof(rme_mv) * n, cudaMemcpyHostToDevice, s));
+  CK(launch_lowres_bi(pc->lr, p0->lr, p1->lr, c->d_lmv.p, c->d_lmv2.p, c->d_lcost.p, s));
+  CK(cudaMemcpyAsync(cost, c->d_lcost.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return 0;
 }
 
 }  // extern "C"

@@ -85,6 +85,21 @@ cudaError_t launch_pad_plane(const void* src, int bd, int w, int h, int sstride,
                              int pad, cudaStream_t s);
 cudaError_t launch_h264_hpel(DevPlanes p, int bd, int cw, int ch, int pad, cudaStream_t s);
 cudaError_t launch_hevc_phases(DevPlanes p, int bd, int w, int h, int pad, cudaStream_t s);
+// The lookahead's half-resolution plane of a picture (h265_cutree.rs LowRes):
+// 8-bit, whole 8x8 blocks (pw x ph), padded by kLowresPad on every side.
+constexpr int kLowresPad = 24, kLowresRange = 16;
+struct LowresDesc {
+  uint8_t* plane;   // (ph + 2 pad) rows of `stride` bytes
+  uint32_t* intra;  // per block, raster
+  int32_t stride, pw, ph, bw, bh;
+};
+cudaError_t launch_lowres_build(const DevPlanes& pic, int bd, int w, int h, const LowresDesc& L, cudaStream_t s);
+cudaError_t launch_lowres_search(const LowresDesc& cur, const LowresDesc& ref, const int32_t* order, int32_t* done,
+                                 unsigned long long* counter, uint32_t* status, uint32_t* cost, rme_mv* mv,
+                                 uint32_t* nsad, int grid, cudaStream_t s);
+cudaError_t launch_lowres_bi(const LowresDesc& cur, const LowresDesc& r0, const LowresDesc& r1, const rme_mv* m0,
+                             const rme_mv* m1, uint32_t* cost, cudaStream_t s);
+
 // The search over one kind of task (sample width, codec): `grid` persistent
 // blocks pulling from L's queue. `variant` picks the kernel's occupancy
 // bound: 0, 1, 2 for 2, 3, 4 resident blocks per SM (1 is the default).

@@ -1,0 +1,290 @@
+// The lookahead's motion estimation at half resolution (the HEVC encoder's
+// quantiser propagation, encode/h265_cutree.rs): the half-resolution plane
+// of a picture and its blocks' intra costs (LowRes::new, intra_cost), the
+// per-block motion search against a reference (search) and the SATD
+// against the average of two displaced blocks (bi_cost).
+//
+// The search reads the left and above blocks' vectors as seeds, so its
+// blocks form a wavefront. Warps claim blocks in anti-diagonal order from
+// one counter and wait (bounded) for the two blocks they read: every block
+// a warp waits for was claimed earlier by a running warp, so the wait
+// always ends unless a wait bound runs out, which sets the status word.
+#include <cuda_runtime.h>
+
+#include "rme_internal.h"
+
+namespace rme {
+namespace {
+
+constexpr unsigned kAll = 0xffffffffu;
+
+// LowRes::new (h265_cutree.rs:61-110): the 2x2 mean of the picture
+// (clamped at its edges) shifted to 8 bits, over whole 8x8 blocks, the
+// border replicated: every padded position is the value of its clamped
+// position.
+template <class S>
+__global__ void lowres_build_kernel(const S* __restrict__ pic, int pstride, int w, int h, int bd, LowresDesc L) {
+  const int X = blockIdx.x * blockDim.x + threadIdx.x, Y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int rows = L.ph + 2 * kLowresPad;
+  if (X >= L.stride || Y >= rows) return;
+  const int lw = (w + 1) / 2, lh = (h + 1) / 2;
+  const int xx = min(max(X - kLowresPad, 0), L.pw - 1), yy = min(max(Y - kLowresPad, 0), L.ph - 1);
+  const int x2 = 2 * min(xx, lw - 1), y2 = 2 * min(yy, lh - 1);
+  auto at = [&](int x, int y) { return (int)pic[(ptrdiff_t)min(y, h - 1) * pstride + min(x, w - 1)]; };
+  const int s = at(x2, y2) + at(x2 + 1, y2) + at(x2, y2 + 1) + at(x2 + 1, y2 + 1);
+  L.plane[(ptrdiff_t)Y * L.stride + X] = (uint8_t)min(((s + 2) >> 2) >> (bd - 8), 255);
+}
+
+__device__ uint32_t satd8x8_u8(const uint8_t* a, int as, const uint8_t* b, int bs) {
+  uint32_t total = 0;
+  for (int ty = 0; ty < 2; ++ty)
+    for (int tx = 0; tx < 2; ++tx) {
+      int d[16];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+          d[r * 4 + c] = (int)a[(ty * 4 + r) * as + tx * 4 + c] - (int)b[(ty * 4 + r) * bs + tx * 4 + c];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int p = d[i * 4], q = d[i * 4 + 1], u = d[i * 4 + 2], v = d[i * 4 + 3];
+        const int s0 = p + v, s1 = q + u, s2 = q - u, s3 = p - v;
+        d[i * 4] = s0 + s1;
+        d[i * 4 + 1] = s3 + s2;
+        d[i * 4 + 2] = s0 - s1;
+        d[i * 4 + 3] = s3 - s2;
+      }
+      uint32_t sum = 0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int p = d[j], q = d[4 + j], u = d[8 + j], v = d[12 + j];
+        const int s0 = p + v, s1 = q + u, s2 = q - u, s3 = p - v;
+        sum += abs(s0 + s1) + abs(s3 + s2) + abs(s0 - s1) + abs(s3 - s2);
+      }
+      total += (sum + 1) >> 1;
+    }
+  return total;
+}
+
+// intra_cost (h265_cutree.rs:118-140), one thread per block: the least SATD
+// of the flat, horizontal and vertical predictions from the samples above
+// and left, floored at 16.
+__global__ void lowres_intra_kernel(LowresDesc L) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= L.bw * L.bh) return;
+  const int x = (b % L.bw) * 8, y = (b / L.bw) * 8;
+  const uint8_t* src = L.plane + (ptrdiff_t)(y + kLowresPad) * L.stride + x + kLowresPad;
+  uint8_t top[8], left[8];
+  int st = 0;
+  for (int i = 0; i < 8; ++i) {
+    top[i] = src[i - L.stride];
+    left[i] = src[(ptrdiff_t)i * L.stride - 1];
+    st += top[i] + left[i];
+  }
+  uint8_t pred[64];
+  const uint8_t dc = (uint8_t)((st + 8) / 16);
+  for (int i = 0; i < 64; ++i) pred[i] = dc;
+  uint32_t best = satd8x8_u8(src, L.stride, pred, 8);
+  for (int i = 0; i < 64; ++i) pred[i] = left[i / 8];
+  best = min(best, satd8x8_u8(src, L.stride, pred, 8));
+  for (int i = 0; i < 64; ++i) pred[i] = top[i % 8];
+  best = min(best, satd8x8_u8(src, L.stride, pred, 8));
+  L.intra[b] = max(best, 16u);
+}
+
+__device__ __forceinline__ uint32_t ld_acquire32(const int32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release32(int32_t* p, int32_t v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// A bounded wait (lane 0) for block b to be done.
+__device__ __forceinline__ bool wait_done(const int32_t* done, int b, uint32_t* status) {
+  uint32_t ns = 32;
+  for (uint32_t it = 0; it < kSpinLimit; ++it) {
+    if (ld_acquire32(done + b)) return true;
+    __nanosleep(ns);
+    if (ns < 256) ns <<= 1;
+  }
+  atomicOr(status, kStatusWaitTimeout);
+  return false;
+}
+
+// Eight bytes of a row at any byte address (three aligned loads).
+__device__ __forceinline__ void ld8(const uint8_t* p, uint32_t& a, uint32_t& b) {
+  const uintptr_t u = reinterpret_cast<uintptr_t>(p);
+  const uint32_t* q = reinterpret_cast<const uint32_t*>(u & ~uintptr_t(3));
+  const uint32_t sh = (uint32_t)(u & 3) * 8u;
+  const uint32_t w0 = __ldg(q), w1 = __ldg(q + 1), w2 = __ldg(q + 2);
+  a = __funnelshift_r(w0, w1, sh);
+  b = __funnelshift_r(w1, w2, sh);
+}
+
+struct Pick2 {
+  uint32_t cost;
+  int lane;
+};
+__device__ __forceinline__ Pick2 argmin(uint32_t c) {
+  const uint32_t m = __reduce_min_sync(kAll, c);
+  return {m, __ffs(__ballot_sync(kAll, c == m)) - 1};
+}
+
+// search (h265_cutree.rs:152-216), one warp per block: four candidates per
+// step (group g = lane / 8, lane sub = row), the first least cost taken when
+// strictly below the best, as the reference's in-order scoring.
+__global__ void __launch_bounds__(256) lowres_search_kernel(LowresDesc cur, LowresDesc ref, const int32_t* order,
+                                                            int32_t* done, unsigned long long* counter,
+                                                            uint32_t* status, uint32_t* cost, rme_mv* mv,
+                                                            uint32_t* nsad_out) {
+  const int lane = threadIdx.x & 31, g = lane >> 3, sub = lane & 7;
+  const int n = cur.bw * cur.bh, lim = kLowresPad - 1;
+  for (;;) {
+    unsigned long long i = 0;
+    if (lane == 0) i = atomicAdd(counter, 1ull);
+    i = __shfl_sync(kAll, i, 0);
+    if (i >= (unsigned long long)n) break;
+    const int packed = __ldg(order + i), bx = packed & 0xffff, by = packed >> 16, b = by * cur.bw + bx;
+    if (lane == 0) {
+      if (bx > 0) wait_done(done, b - 1, status);
+      if (by > 0) wait_done(done, b - cur.bw, status);
+    }
+    __syncwarp();
+    const int x = bx * 8, y = by * 8;
+    const uint8_t* src = cur.plane + (ptrdiff_t)(y + kLowresPad) * cur.stride + x + kLowresPad;
+    const uint8_t* rb = ref.plane + (ptrdiff_t)(y + kLowresPad) * ref.stride + x + kLowresPad;
+    // This lane's source row (8-byte aligned: x, the pad and the stride
+    // are multiples of 8).
+    const uint32_t s0 = *reinterpret_cast<const uint32_t*>(src + (ptrdiff_t)sub * cur.stride);
+    const uint32_t s1 = *reinterpret_cast<const uint32_t*>(src + (ptrdiff_t)sub * cur.stride + 4);
+    auto inplane = [&](int dx, int dy) {
+      return x + dx >= -lim && y + dy >= -lim && x + dx + 8 <= ref.pw + lim && y + dy + 8 <= ref.ph + lim;
+    };
+    auto score = [&](bool ok, int dx, int dy) -> uint32_t {
+      uint32_t part = 0;
+      if (ok) {
+        uint32_t a, c;
+        ld8(rb + (ptrdiff_t)(dy + sub) * ref.stride + dx, a, c);
+        part = __vsadu4(s0, a) + __vsadu4(s1, c);
+      }
+      part += __shfl_xor_sync(kAll, part, 4);
+      part += __shfl_xor_sync(kAll, part, 2);
+      part += __shfl_xor_sync(kAll, part, 1);
+      return ok ? part + 2u * (uint32_t)min(abs(dx) + abs(dy), 32) : 0xffffffffu;
+    };
+    // Seeds: zero, the left block's vector, the above block's.
+    uint32_t lv = 0, av = 0;
+    if (bx > 0) lv = __ldcg(reinterpret_cast<const unsigned int*>(mv + b - 1));
+    if (by > 0) av = __ldcg(reinterpret_cast<const unsigned int*>(mv + b - cur.bw));
+    const int ns = 1 + (bx > 0) + (by > 0);
+    const uint32_t sv = g == 0 ? 0u : g == 1 ? (bx > 0 ? lv : av) : av;
+    int dx = (int)(int16_t)(sv & 0xffffu), dy = (int)(int16_t)(sv >> 16);
+    bool ok = g < ns && inplane(dx, dy);
+    uint32_t nsad = __popc(__ballot_sync(kAll, ok && sub == 0));
+    Pick2 p = argmin(score(ok, dx, dy));
+    uint32_t bc = p.cost;
+    int bxm = __shfl_sync(kAll, dx, p.lane), bym = __shfl_sync(kAll, dy, p.lane);
+    if (bc == 0xffffffffu) bxm = bym = 0;  // no seed in the plane
+    const int cx = bxm, cy = bym;
+    for (int step = 4; step >= 1; step >>= 1) {
+      for (;;) {
+        dx = bxm + (g == 0 ? step : g == 1 ? -step : 0);
+        dy = bym + (g == 2 ? step : g == 3 ? -step : 0);
+        ok = abs(dx - cx) <= kLowresRange && abs(dy - cy) <= kLowresRange && inplane(dx, dy);
+        nsad += __popc(__ballot_sync(kAll, ok && sub == 0));
+        p = argmin(score(ok, dx, dy));
+        if (!(p.cost < bc)) break;
+        bc = p.cost;
+        bxm = __shfl_sync(kAll, dx, p.lane);
+        bym = __shfl_sync(kAll, dy, p.lane);
+      }
+    }
+    // The winner's SATD: tile `lane` of the four (lanes 0..3).
+    uint32_t sat = 0;
+    if (lane < 4) {
+      const int tx = lane & 1, ty = lane >> 1;
+      int d[16];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const uint8_t* sr = src + (ptrdiff_t)(ty * 4 + r) * cur.stride + tx * 4;
+        const uint8_t* pr = rb + (ptrdiff_t)(bym + ty * 4 + r) * ref.stride + bxm + tx * 4;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) d[r * 4 + c] = (int)sr[c] - (int)pr[c];
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int a0 = d[k * 4], a1 = d[k * 4 + 1], a2 = d[k * 4 + 2], a3 = d[k * 4 + 3];
+        const int t0 = a0 + a3, t1 = a1 + a2, t2 = a1 - a2, t3 = a0 - a3;
+        d[k * 4] = t0 + t1;
+        d[k * 4 + 1] = t3 + t2;
+        d[k * 4 + 2] = t0 - t1;
+        d[k * 4 + 3] = t3 - t2;
+      }
+      uint32_t sum = 0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int a0 = d[j], a1 = d[4 + j], a2 = d[8 + j], a3 = d[12 + j];
+        const int t0 = a0 + a3, t1 = a1 + a2, t2 = a1 - a2, t3 = a0 - a3;
+        sum += abs(t0 + t1) + abs(t3 + t2) + abs(t0 - t1) + abs(t3 - t2);
+      }
+      sat = (sum + 1) >> 1;
+    }
+    sat += __shfl_xor_sync(kAll, sat, 1);
+    sat += __shfl_xor_sync(kAll, sat, 2);
+    if (lane == 0) {
+      cost[b] = sat;
+      mv[b].x = (int16_t)bxm;
+      mv[b].y = (int16_t)bym;
+      if (nsad_out) nsad_out[b] = nsad;
+      __threadfence();
+      st_release32(done + b, 1);
+    }
+    __syncwarp();
+  }
+}
+
+// bi_cost (h265_cutree.rs:222-243), one thread per block.
+__global__ void lowres_bi_kernel(LowresDesc cur, LowresDesc r0, LowresDesc r1, const rme_mv* m0, const rme_mv* m1,
+                                 uint32_t* cost) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= cur.bw * cur.bh) return;
+  const int x = (b % cur.bw) * 8, y = (b / cur.bw) * 8;
+  const uint8_t* a = r0.plane + (ptrdiff_t)(y + m0[b].y + kLowresPad) * r0.stride + x + m0[b].x + kLowresPad;
+  const uint8_t* c = r1.plane + (ptrdiff_t)(y + m1[b].y + kLowresPad) * r1.stride + x + m1[b].x + kLowresPad;
+  uint8_t pred[64];
+  for (int yy = 0; yy < 8; ++yy)
+    for (int xx = 0; xx < 8; ++xx)
+      pred[yy * 8 + xx] = (uint8_t)(((int)a[(ptrdiff_t)yy * r0.stride + xx] + c[(ptrdiff_t)yy * r1.stride + xx] + 1) >> 1);
+  cost[b] = satd8x8_u8(cur.plane + (ptrdiff_t)(y + kLowresPad) * cur.stride + x + kLowresPad, cur.stride, pred, 8);
+}
+
+}  // namespace
+
+cudaError_t launch_lowres_build(const DevPlanes& pic, int bd, int w, int h, const LowresDesc& L, cudaStream_t s) {
+  dim3 blk(32, 8), grd((L.stride + 31) / 32, (L.ph + 2 * kLowresPad + 7) / 8);
+  if (bd == 8)
+    lowres_build_kernel<uint8_t><<<grd, blk, 0, s>>>((const uint8_t*)pic.base + pic.origin, pic.stride, w, h, bd, L);
+  else
+    lowres_build_kernel<uint16_t><<<grd, blk, 0, s>>>((const uint16_t*)pic.base + pic.origin, pic.stride, w, h, bd, L);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  lowres_intra_kernel<<<(L.bw * L.bh + 127) / 128, 128, 0, s>>>(L);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lowres_search(const LowresDesc& cur, const LowresDesc& ref, const int32_t* order, int32_t* done,
+                                 unsigned long long* counter, uint32_t* status, uint32_t* cost, rme_mv* mv,
+                                 uint32_t* nsad, int grid, cudaStream_t s) {
+  lowres_search_kernel<<<grid, 256, 0, s>>>(cur, ref, order, done, counter, status, cost, mv, nsad);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lowres_bi(const LowresDesc& cur, const LowresDesc& r0, const LowresDesc& r1, const rme_mv* m0,
+                             const rme_mv* m1, uint32_t* cost, cudaStream_t s) {
+  lowres_bi_kernel<<<(cur.bw * cur.bh + 127) / 128, 128, 0, s>>>(cur, r0, r1, m0, m1, cost);
+  return cudaGetLastError();
+}
+
+}  // namespace rme

@@ -163,6 +163,40 @@ class MotionSearch:
             params = [params] * len(frames)
         return int(sum(self.result_count(s, r, p) for (s, r), p in zip(frames, params)))
 
+    # ---- lookahead at half resolution --------------------------------------
+    def lowres_build(self, pic_id: int) -> None:
+        """The picture's half-resolution plane and intra costs (on the device)."""
+        self._check(self._lib.rme_lowres_build(self.ctx, pic_id, None))
+
+    def lowres_intra(self, pic_id: int) -> np.ndarray:
+        bw, bh = C.c_int32(), C.c_int32()
+        self._check(self._lib.rme_lowres_info(self.ctx, pic_id, C.byref(bw), C.byref(bh), None))
+        out = np.zeros(bw.value * bh.value, np.uint32)
+        self._check(self._lib.rme_lowres_info(self.ctx, pic_id, None, None,
+                                              out.ctypes.data_as(C.POINTER(C.c_uint32))))
+        return out
+
+    def lowres_search(self, cur_id: int, ref_id: int):
+        """(cost, mv (n x 2 int16), nsad) per half-resolution block."""
+        bw, bh = C.c_int32(), C.c_int32()
+        self._check(self._lib.rme_lowres_info(self.ctx, cur_id, C.byref(bw), C.byref(bh), None))
+        n = bw.value * bh.value
+        cost, nsad = np.zeros(n, np.uint32), np.zeros(n, np.uint32)
+        mv = np.zeros((n, 2), np.int16)
+        self._check(self._lib.rme_lowres_search(self.ctx, cur_id, ref_id, cost.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                                C.cast(mv.ctypes.data, C.POINTER(capi.Mv)),
+                                                nsad.ctypes.data_as(C.POINTER(C.c_uint32)), None))
+        return cost, mv, nsad
+
+    def lowres_bi_cost(self, cur_id: int, r0_id: int, mv0: np.ndarray, r1_id: int, mv1: np.ndarray) -> np.ndarray:
+        mv0 = np.ascontiguousarray(mv0, np.int16)
+        mv1 = np.ascontiguousarray(mv1, np.int16)
+        out = np.zeros(len(mv0), np.uint32)
+        self._check(self._lib.rme_lowres_bi_cost(self.ctx, cur_id, r0_id, C.cast(mv0.ctypes.data, C.POINTER(capi.Mv)),
+                                                 r1_id, C.cast(mv1.ctypes.data, C.POINTER(capi.Mv)),
+                                                 out.ctypes.data_as(C.POINTER(C.c_uint32)), None))
+        return out
+
     def stats(self) -> capi.Stats:
         s = capi.Stats()
         self._check(self._lib.rme_last_stats(self.ctx, C.byref(s)))
