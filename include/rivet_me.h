@@ -328,31 +328,46 @@ int rme_serve_stop(void* server);
 
 /* ---- lookahead at half resolution ------------------------------------------- */
 
-/* The HEVC encoder's lookahead (quantiser propagation) measures at half
- * resolution: each picture reduced to 8 bits as 2x2 means, costed in 8x8
- * blocks (16x16 of the picture). These are its ME kernels, batched per
- * picture (encode/h265_cutree.rs). */
+/* Both encoders' lookaheads (quantiser propagation) measure at half
+ * resolution, in 8x8 blocks (16x16 of the picture), one set of kernels per
+ * codec chosen by the picture's codec:
+ *  - HEVC (encode/h265_cutree.rs): the picture reduced to 8 bits as 2x2
+ *    means over ceil(w/2) x ceil(h/2), whole blocks;
+ *  - H.264 (encode/h264_lookahead.rs): 2x2 means at the stream's sample
+ *    depth, one block per macroblock.
+ * Both planes are padded by 24 replicated samples. Batched per picture. */
 
 /* Build (or rebuild) a resident picture's half-resolution plane and its
- * blocks' intra costs: LowRes::new + intra_cost (h265_cutree.rs:61-140).
- * Synchronous. */
+ * blocks' intra costs: HEVC LowRes::new + intra_cost (h265_cutree.rs:61-140,
+ * the least SATD of DC, H and V floored at 16); H.264 Lookahead::add +
+ * intra_costs (h264_lookahead.rs:87-222, the least SATD of DC, V, H and the
+ * edge blend, plus 12). Synchronous. */
 int rme_lowres_build(void* ctx, int32_t pic_id, void* stream);
 
 /* Its block grid and (when `intra` is not NULL) the intra cost per block,
  * raster order. */
 int rme_lowres_info(void* ctx, int32_t pic_id, int32_t* bw, int32_t* bh, uint32_t* intra);
 
-/* search (h265_cutree.rs:152-216) of every block of `cur_id` against
- * `ref_id`: seeds zero, left and above vectors, a cross descent at steps 4,
- * 2, 1 within +-16 of the best seed, SAD + 2 * min(|dx| + |dy|, 32); per
- * block the winner's SATD (`cost`), its vector in half-resolution samples,
- * and (when `nsad` is not NULL) the SADs scored. Host outputs, synchronous. */
+/* The block search of every block of `cur_id` against `ref_id` (both built
+ * with rme_lowres_build, same codec and size), the left and above blocks'
+ * vectors as candidates:
+ *  - HEVC search (h265_cutree.rs:152-216): seeds zero, left, above; a cross
+ *    descent at steps 4, 2, 1 within +-16 of the best seed;
+ *    SAD + 2 * min(|dx| + |dy|, 32);
+ *  - H.264 search (h264_lookahead.rs:227-376): zero, then left and above
+ *    clamped to the window (16 samples into the border, 32 at most);
+ *    hexagon steps (at most 16), then the eight-point square;
+ *    SAD + 2 * min(|dx| + |dy|, 64).
+ * Per block the winner's SATD (`cost`), its vector in half-resolution
+ * samples, and (when `nsad` is not NULL) the SADs the reference scores.
+ * Host outputs, synchronous. */
 int rme_lowres_search(void* ctx, int32_t cur_id, int32_t ref_id, uint32_t* cost, rme_mv* mv, uint32_t* nsad,
                       void* stream);
 
-/* bi_cost (h265_cutree.rs:222-243) of every block: the SATD against the
- * rounded average of its blocks displaced by mv0 in r0 and mv1 in r1.
- * Host inputs and output, synchronous. */
+/* The average-of-two cost of every block (HEVC bi_cost,
+ * h265_cutree.rs:222-243; H.264 estimate, h264_lookahead.rs:417-432): the
+ * SATD against the rounded average of its blocks displaced by mv0 in r0 and
+ * mv1 in r1. Host inputs and output, synchronous. */
 int rme_lowres_bi_cost(void* ctx, int32_t cur_id, int32_t r0_id, const rme_mv* mv0, int32_t r1_id,
                        const rme_mv* mv1, uint32_t* cost, void* stream);
 

@@ -642,12 +642,194 @@ uint32_t lowres_bi_cost(const LowRes& cur, const LowRes& r0, rme_mv m0, const Lo
   return satd_scalar<uint8_t>(&cur.luma[cur.off(x, y)], cur.stride, pred, LA_B, LA_B, LA_B);
 }
 
+// ---- lookahead (H.264) at half resolution -----------------------------------
+// encode/h264_lookahead.rs: PAD = 24, RANGE = 16; the plane keeps the
+// stream's sample type.
+template <class S>
+struct LowResS {
+  Plane<S> low;
+  int bw = 0, bh = 0;
+  std::vector<uint32_t> intra;
+};
+
+// Lookahead::add (h264_lookahead.rs:87-117): each sample the rounded mean
+// of the 2x2 square of the picture at (2x, 2y), clamped to the picture,
+// over the macroblock grid (8 samples per macroblock); the border
+// replicated (extend_edges).
+template <class S>
+LowResS<S> lowres_h264(const S* y, int w, int h, ptrdiff_t ys) {
+  LowResS<S> L;
+  L.bw = (w + 15) / 16;
+  L.bh = (h + 15) / 16;
+  const int lw = L.bw * 8, lh = L.bh * 8;
+  std::vector<S> flat((size_t)lw * lh);
+  for (int yy = 0; yy < lh; ++yy) {
+    const int y0 = std::min(2 * yy, h - 1), y1 = std::min(2 * yy + 1, h - 1);
+    for (int xx = 0; xx < lw; ++xx) {
+      const int x0 = std::min(2 * xx, w - 1), x1 = std::min(2 * xx + 1, w - 1);
+      const int s = (int)y[y0 * ys + x0] + y[y0 * ys + x1] + y[y1 * ys + x0] + y[y1 * ys + x1];
+      flat[(size_t)yy * lw + xx] = (S)((s + 2) >> 2);
+    }
+  }
+  L.low = Plane<S>(lw, lh, LA_PAD);
+  L.low.load(flat.data(), lw);
+  // intra_costs (h264_lookahead.rs:146-222): DC from the neighbours there
+  // are (the block's own mean with none), the vertical and horizontal
+  // predictions where their edge exists, the bilinear blend of both edges;
+  // the least SATD, plus 12.
+  L.intra.resize((size_t)L.bw * L.bh);
+  for (int by = 0; by < L.bh; ++by)
+    for (int bx = 0; bx < L.bw; ++bx) {
+      const int x = bx * 8, yb = by * 8;
+      const S* src = &L.low.data[L.low.offset(x, yb)];
+      const ptrdiff_t st = L.low.stride;
+      int t[8], l[8];
+      for (int i = 0; i < 8; ++i) {
+        t[i] = L.low.data[L.low.offset(x + i, yb - 1)];
+        l[i] = L.low.data[L.low.offset(x - 1, yb + i)];
+      }
+      const bool ht = by > 0, hl = bx > 0;
+      int dc;
+      if (ht && hl) {
+        int sum = 8;
+        for (int i = 0; i < 8; ++i) sum += t[i] + l[i];
+        dc = sum >> 4;
+      } else if (ht || hl) {
+        int sum = 4;
+        for (int i = 0; i < 8; ++i) sum += ht ? t[i] : l[i];
+        dc = sum >> 3;
+      } else {
+        int sum = 32;
+        for (int yy = 0; yy < 8; ++yy)
+          for (int xx = 0; xx < 8; ++xx) sum += src[yy * st + xx];
+        dc = sum >> 6;
+      }
+      S pred[64];
+      std::fill(pred, pred + 64, (S)dc);
+      uint32_t best = satd_scalar<S>(src, st, pred, 8, 8, 8);
+      if (ht) {
+        for (int i = 0; i < 64; ++i) pred[i] = (S)t[i % 8];
+        best = std::min(best, satd_scalar<S>(src, st, pred, 8, 8, 8));
+      }
+      if (hl) {
+        for (int i = 0; i < 64; ++i) pred[i] = (S)l[i / 8];
+        best = std::min(best, satd_scalar<S>(src, st, pred, 8, 8, 8));
+      }
+      if (ht && hl) {
+        for (int yy = 0; yy < 8; ++yy)
+          for (int xx = 0; xx < 8; ++xx)
+            pred[yy * 8 + xx] = (S)((t[xx] * (8 - yy) + l[yy] * (8 - xx) + t[7] * yy + l[7] * xx + 8) >> 4);
+        best = std::min(best, satd_scalar<S>(src, st, pred, 8, 8, 8));
+      }
+      L.intra[(size_t)by * L.bw + bx] = best + 12;
+    }
+  return L;
+}
+
+// Lookahead::search (h264_lookahead.rs:227-376) for every block in raster
+// order, the candidates being the left and above blocks' vectors (zero where
+// there is no such block): SAD + 2 * min(|mx| + |my|, 64) from the zero
+// vector; each candidate clamped to the window and scored unless it is the
+// best's point; the hexagon with its three-new-points continuation, at
+// most RANGE rounds; the square; the winner's SATD.
+template <class S>
+void lowres_search_h264(const LowResS<S>& cur, const LowResS<S>& refp, uint32_t* cost, rme_mv* mv, uint32_t* nsad) {
+  static const int HEX[6][2] = {{-2, 0}, {-1, -2}, {1, -2}, {2, 0}, {1, 2}, {-1, 2}};
+  static const int SQ[8][2] = {{-1, -1}, {0, -1}, {1, -1}, {-1, 0}, {1, 0}, {-1, 1}, {0, 1}, {1, 1}};
+  const int lim = LA_PAD - 8, n = cur.bw * cur.bh;
+  for (int b = 0; b < n; ++b) {
+    const int bx = b % cur.bw, by = b / cur.bw, x = bx * 8, y = by * 8;
+    const S* src = &cur.low.data[cur.low.offset(x, y)];
+    const ptrdiff_t cs = cur.low.stride, rs = refp.low.stride;
+    const int lx = std::max(-x - lim, -LA_RANGE * 2), hx = std::min(cur.low.width - 8 - x + lim, LA_RANGE * 2);
+    const int ly = std::max(-y - lim, -LA_RANGE * 2), hy = std::min(cur.low.height - 8 - y + lim, LA_RANGE * 2);
+    uint32_t count = 0;
+    auto sad = [&](int mx, int my) {
+      ++count;
+      return sad_scalar<S>(src, cs, &refp.low.data[refp.low.offset(x + mx, y + my)], rs, 8, 8) +
+             2u * (uint32_t)std::min(std::abs(mx) + std::abs(my), 64);
+    };
+    int bmx = 0, bmy = 0;
+    uint32_t bc = sad(0, 0);
+    const int cand[2][2] = {{bx > 0 ? mv[b - 1].x : 0, bx > 0 ? mv[b - 1].y : 0},
+                            {by > 0 ? mv[b - cur.bw].x : 0, by > 0 ? mv[b - cur.bw].y : 0}};
+    for (auto& c : cand) {
+      const int cx = std::clamp(c[0], lx, hx), cy = std::clamp(c[1], ly, hy);
+      if (cx != bmx || cy != bmy) {
+        const uint32_t v = sad(cx, cy);
+        if (v < bc) {
+          bc = v;
+          bmx = cx;
+          bmy = cy;
+        }
+      }
+    }
+    int from = -1;
+    for (int it = 0; it < LA_RANGE; ++it) {
+      const int cx = bmx, cy = bmy;
+      int step = -1;
+      uint32_t live = 0x3f;
+      if (from >= 0) {
+        const uint32_t r = 7u << (from + 5);
+        live = (r | r >> 6 | r >> 12) & 0x3f;
+      }
+      for (int k = 0; k < 6; ++k) {
+        const int mx = cx + HEX[k][0], my = cy + HEX[k][1];
+        if (!((live >> k) & 1) || mx < lx || mx > hx || my < ly || my > hy) continue;
+        const uint32_t v = sad(mx, my);
+        if (v < bc) {
+          bc = v;
+          bmx = mx;
+          bmy = my;
+          step = k;
+        }
+      }
+      if (bmx == cx && bmy == cy) break;
+      from = step;
+    }
+    const int cx = bmx, cy = bmy;
+    for (auto& q : SQ) {
+      const int mx = cx + q[0], my = cy + q[1];
+      if (mx < lx || mx > hx || my < ly || my > hy) continue;
+      const uint32_t v = sad(mx, my);
+      if (v < bc) {
+        bc = v;
+        bmx = mx;
+        bmy = my;
+      }
+    }
+    cost[b] = satd_scalar<S>(src, cs, &refp.low.data[refp.low.offset(x + bmx, y + bmy)], rs, 8, 8);
+    mv[b].x = (int16_t)bmx;
+    mv[b].y = (int16_t)bmy;
+    if (nsad) nsad[b] = count;
+  }
+}
+
+// The average-of-two cost of estimate() (h264_lookahead.rs:417-432).
+template <class S>
+uint32_t lowres_bi_h264(const LowResS<S>& cur, const LowResS<S>& r0, rme_mv m0, const LowResS<S>& r1, rme_mv m1,
+                        int b) {
+  const int x = (b % cur.bw) * 8, y = (b / cur.bw) * 8;
+  const S* a = &r0.low.data[r0.low.offset(x + m0.x, y + m0.y)];
+  const S* c = &r1.low.data[r1.low.offset(x + m1.x, y + m1.y)];
+  S avg[64];
+  for (int yy = 0; yy < 8; ++yy)
+    for (int xx = 0; xx < 8; ++xx)
+      avg[yy * 8 + xx] = (S)(((int)a[yy * r0.low.stride + xx] + c[yy * r1.low.stride + xx] + 1) >> 1);
+  return satd_scalar<S>(&cur.low.data[cur.low.offset(x, y)], cur.low.stride, avg, 8, 8, 8);
+}
+
 template <class S>
 LowRes lowres_of(const rme_picture_desc* d, const void* luma) {
   return lowres_new<S>((const S*)luma, d->width, d->height, d->stride, d->bit_depth);
 }
 LowRes lowres_any(const rme_picture_desc* d, const void* luma) {
   return d->bit_depth == 8 ? lowres_of<uint8_t>(d, luma) : lowres_of<uint16_t>(d, luma);
+}
+
+template <class S>
+LowResS<S> lowres_h264_of(const rme_picture_desc* d, const void* luma) {
+  return lowres_h264<S>((const S*)luma, d->width, d->height, d->stride);
 }
 
 }  // namespace
@@ -938,6 +1120,20 @@ int orc_chroma_predict(const rme_picture_desc* d, const void* cb, const void* cr
 int orc_lowres(const rme_picture_desc* d, const void* luma, uint8_t* plane, int32_t* stride, int32_t* rows,
                uint32_t* intra, int32_t* nblocks) {
   if (!valid_desc(d) || !luma) return RME_EINVAL;
+  if (d->codec == RME_CODEC_H264) {
+    auto run = [&](auto tag) {
+      using S = decltype(tag);
+      LowResS<S> L = lowres_h264_of<S>(d, luma);
+      if (stride) *stride = L.low.stride;
+      if (rows) *rows = L.low.rows();
+      if (nblocks) *nblocks = L.bw * L.bh;
+      if (plane) std::memcpy(plane, L.low.data.data(), L.low.data.size() * sizeof(S));
+      if (intra) std::memcpy(intra, L.intra.data(), L.intra.size() * sizeof(uint32_t));
+    };
+    if (d->bit_depth == 8) run(uint8_t{});
+    else run(uint16_t{});
+    return 0;
+  }
   LowRes L = lowres_any(d, luma);
   if (stride) *stride = L.stride;
   if (rows) *rows = L.h + 2 * LA_PAD;
@@ -953,6 +1149,15 @@ int orc_lowres(const rme_picture_desc* d, const void* luma, uint8_t* plane, int3
 int orc_lowres_search(const rme_picture_desc* d, const void* cur, const void* ref, uint32_t* cost, rme_mv* mv,
                       uint32_t* nsad) {
   if (!valid_desc(d) || !cur || !ref) return RME_EINVAL;
+  if (d->codec == RME_CODEC_H264) {
+    auto run = [&](auto tag) {
+      using S = decltype(tag);
+      lowres_search_h264<S>(lowres_h264_of<S>(d, cur), lowres_h264_of<S>(d, ref), cost, mv, nsad);
+    };
+    if (d->bit_depth == 8) run(uint8_t{});
+    else run(uint16_t{});
+    return 0;
+  }
   LowRes C = lowres_any(d, cur), R = lowres_any(d, ref);
   lowres_search(C, R, cost, mv, nsad);
   return 0;
@@ -961,6 +1166,16 @@ int orc_lowres_search(const rme_picture_desc* d, const void* cur, const void* re
 int orc_lowres_bi_cost(const rme_picture_desc* d, const void* cur, const void* r0, const rme_mv* mv0, const void* r1,
                        const rme_mv* mv1, uint32_t* cost) {
   if (!valid_desc(d) || !cur || !r0 || !r1) return RME_EINVAL;
+  if (d->codec == RME_CODEC_H264) {
+    auto run = [&](auto tag) {
+      using S = decltype(tag);
+      auto C = lowres_h264_of<S>(d, cur), A = lowres_h264_of<S>(d, r0), B = lowres_h264_of<S>(d, r1);
+      for (int b = 0; b < C.bw * C.bh; ++b) cost[b] = lowres_bi_h264<S>(C, A, mv0[b], B, mv1[b], b);
+    };
+    if (d->bit_depth == 8) run(uint8_t{});
+    else run(uint16_t{});
+    return 0;
+  }
   LowRes C = lowres_any(d, cur), A = lowres_any(d, r0), B = lowres_any(d, r1);
   for (int b = 0; b < C.bw * C.bh; ++b) cost[b] = lowres_bi_cost(C, A, mv0[b], B, mv1[b], b);
   return 0;

@@ -206,19 +206,21 @@ def chroma_predict(codec, bit_depth, luma_w, luma_h, cb, cr, blocks: np.ndarray,
     return out
 
 
-def lowres(pic: np.ndarray, bit_depth: int):
-    """The lookahead's half-resolution plane (padded) and intra costs."""
-    d = desc(capi.RME_CODEC_HEVC, pic, bit_depth)
+def lowres(pic: np.ndarray, bit_depth: int, codec: int = capi.RME_CODEC_HEVC):
+    """The lookahead's half-resolution plane (padded) and intra costs:
+    HEVC's cutree (8-bit) or H.264's lookahead (the stream's samples)."""
+    d = desc(codec, pic, bit_depth)
     stride, rows, n = C.c_int32(), C.c_int32(), C.c_int32()
     assert lib().orc_lowres(C.byref(d), pic.ctypes.data, None, C.byref(stride), C.byref(rows), None, C.byref(n)) == 0
-    plane = np.zeros((rows.value, stride.value), np.uint8)
+    dt = np.uint16 if (codec == capi.RME_CODEC_H264 and bit_depth > 8) else np.uint8
+    plane = np.zeros((rows.value, stride.value), dt)
     intra = np.zeros(n.value, np.uint32)
     assert lib().orc_lowres(C.byref(d), pic.ctypes.data, plane.ctypes.data, None, None, intra.ctypes.data, None) == 0
     return plane, intra
 
 
-def lowres_search(cur: np.ndarray, ref: np.ndarray, bit_depth: int):
-    d = desc(capi.RME_CODEC_HEVC, cur, bit_depth)
+def lowres_search(cur: np.ndarray, ref: np.ndarray, bit_depth: int, codec: int = capi.RME_CODEC_HEVC):
+    d = desc(codec, cur, bit_depth)
     n = C.c_int32()
     assert lib().orc_lowres(C.byref(d), cur.ctypes.data, None, None, None, None, C.byref(n)) == 0
     cost, nsad = np.zeros(n.value, np.uint32), np.zeros(n.value, np.uint32)
@@ -228,8 +230,8 @@ def lowres_search(cur: np.ndarray, ref: np.ndarray, bit_depth: int):
     return cost, mv, nsad
 
 
-def lowres_bi_cost(cur, r0, mv0, r1, mv1, bit_depth):
-    d = desc(capi.RME_CODEC_HEVC, cur, bit_depth)
+def lowres_bi_cost(cur, r0, mv0, r1, mv1, bit_depth, codec: int = capi.RME_CODEC_HEVC):
+    d = desc(codec, cur, bit_depth)
     mv0 = np.ascontiguousarray(mv0, np.int16)
     mv1 = np.ascontiguousarray(mv1, np.int16)
     out = np.zeros(len(mv0), np.uint32)

@@ -1148,7 +1148,7 @@ int rme_satd_batch(const void* a, int64_t a_stride, const int64_t* a_off, const 
   return dist_batch(true, a, a_stride, a_off, b, b_stride, b_off, w, h, bit_depth, n, out, stream);
 }
 
-// ---- lookahead at half resolution (h265_cutree.rs) ---------------------------
+// ---- lookahead at half resolution (h265_cutree.rs, h264_lookahead.rs) --------
 
 int rme_lowres_build(void* ctx, int32_t pic_id, void* stream) {
   Ctx* c = (Ctx*)ctx;
@@ -1159,13 +1159,23 @@ int rme_lowres_build(void* ctx, int32_t pic_id, void* stream) {
   cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
   CK(cudaSetDevice(c->device));
   LowresDesc L{};
-  const int lw = (p->d.width + 1) / 2, lh = (p->d.height + 1) / 2;
-  L.bw = (lw + 7) / 8;
-  L.bh = (lh + 7) / 8;
+  L.h264 = p->d.codec == RME_CODEC_H264;
+  if (L.h264) {
+    // One 8x8 block per macroblock (h264_lookahead.rs:87-117).
+    L.bw = (p->d.width + 15) / 16;
+    L.bh = (p->d.height + 15) / 16;
+    L.bytes = p->d.bit_depth > 8 ? 2 : 1;
+  } else {
+    const int lw = (p->d.width + 1) / 2, lh = (p->d.height + 1) / 2;
+    L.bw = (lw + 7) / 8;
+    L.bh = (lh + 7) / 8;
+    L.bytes = 1;
+  }
   L.pw = L.bw * 8;
   L.ph = L.bh * 8;
   L.stride = L.pw + 2 * kLowresPad;
-  const size_t plane = (size_t)L.stride * (L.ph + 2 * kLowresPad), intra = sizeof(uint32_t) * L.bw * L.bh;
+  const size_t plane = (size_t)L.stride * (L.ph + 2 * kLowresPad) * L.bytes,
+               intra = sizeof(uint32_t) * L.bw * L.bh;
   if (!p->lowres) CK(cudaMalloc(&p->lowres, plane + 256 + intra));
   L.plane = (uint8_t*)p->lowres;
   L.intra = (uint32_t*)((uint8_t*)p->lowres + (plane + 255) / 256 * 256);
@@ -1194,7 +1204,8 @@ int lowres_pair(Ctx* c, int32_t a, int32_t b, Picture** pa, Picture** pb) {
   if (!rc) rc = picture_of(c, b, pb);
   if (rc) return rc;
   if (!(*pa)->lowres || !(*pb)->lowres) return fail(c, RME_EINVAL, "no half-resolution plane: call rme_lowres_build");
-  if ((*pa)->lr.bw != (*pb)->lr.bw || (*pa)->lr.bh != (*pb)->lr.bh)
+  if ((*pa)->lr.bw != (*pb)->lr.bw || (*pa)->lr.bh != (*pb)->lr.bh || (*pa)->lr.h264 != (*pb)->lr.h264 ||
+      (*pa)->lr.bytes != (*pb)->lr.bytes)
     return fail(c, RME_EINVAL, "half-resolution sizes differ");
   return 0;
 }

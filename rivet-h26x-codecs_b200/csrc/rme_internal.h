@@ -85,13 +85,16 @@ cudaError_t launch_pad_plane(const void* src, int bd, int w, int h, int sstride,
                              int pad, cudaStream_t s);
 cudaError_t launch_h264_hpel(DevPlanes p, int bd, int cw, int ch, int pad, cudaStream_t s);
 cudaError_t launch_hevc_phases(DevPlanes p, int bd, int w, int h, int pad, cudaStream_t s);
-// The lookahead's half-resolution plane of a picture (h265_cutree.rs LowRes):
-// 8-bit, whole 8x8 blocks (pw x ph), padded by kLowresPad on every side.
+// The lookahead's half-resolution plane of a picture, whole 8x8 blocks
+// (pw x ph) padded by kLowresPad on every side: HEVC's cutree plane
+// (h265_cutree.rs LowRes, 8-bit) or H.264's lookahead plane
+// (h264_lookahead.rs, the stream's sample type, one block per macroblock).
 constexpr int kLowresPad = 24, kLowresRange = 16;
 struct LowresDesc {
-  uint8_t* plane;   // (ph + 2 pad) rows of `stride` bytes
+  uint8_t* plane;   // (ph + 2 pad) rows of `stride` samples of `bytes` bytes
   uint32_t* intra;  // per block, raster
   int32_t stride, pw, ph, bw, bh;
+  int32_t h264, bytes;
 };
 cudaError_t launch_lowres_build(const DevPlanes& pic, int bd, int w, int h, const LowresDesc& L, cudaStream_t s);
 cudaError_t launch_lowres_search(const LowresDesc& cur, const LowresDesc& ref, const int32_t* order, int32_t* done,

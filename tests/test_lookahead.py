@@ -1,6 +1,7 @@
-"""The lookahead's half-resolution ME (encode/h265_cutree.rs): the oracle's
-restatement against the reference's properties on the CPU, and the device
-kernels against the oracle, block for block."""
+"""The lookahead's half-resolution ME (HEVC: encode/h265_cutree.rs; H.264:
+encode/h264_lookahead.rs): the oracle's restatement against the reference's
+properties on the CPU, and the device kernels against the oracle, block for
+block."""
 import numpy as np
 import pytest
 
@@ -9,6 +10,7 @@ import rivet_h26x_codecs_b200.capi as capi
 from _common import random_picture, shifted
 
 HEVC = capi.RME_CODEC_HEVC
+H264 = capi.RME_CODEC_H264
 
 
 def test_lowres_plane_is_the_mean_of_two_by_two_squares():
@@ -45,6 +47,50 @@ def test_lowres_search_finds_a_translation():
     assert (nsad > 0).all()
 
 
+def test_h264_lowres_plane_keeps_the_sample_type():
+    """Lookahead::add (h264_lookahead.rs:87-117): 8 samples per macroblock,
+    each the rounded 2x2 mean at the stream's depth (no shift), columns and
+    rows clamped to the picture, the 24-sample border replicated."""
+    rng = np.random.default_rng(4)
+    pic = random_picture(rng, 70, 46, 10)
+    plane, intra = oracle.lowres(pic, 10, H264)
+    bw, bh = 5, 3
+    assert plane.dtype == np.uint16
+    assert plane.shape == (bh * 8 + 48, bw * 8 + 48) and len(intra) == bw * bh
+    p = pic.astype(np.int64)
+    for yy in (0, 5, 22, 23):
+        for xx in (0, 17, 34, 39):
+            x0, x1 = min(2 * xx, 69), min(2 * xx + 1, 69)
+            y0, y1 = min(2 * yy, 45), min(2 * yy + 1, 45)
+            s = p[y0, x0] + p[y0, x1] + p[y1, x0] + p[y1, x1]
+            assert plane[yy + 24, xx + 24] == (s + 2) >> 2
+    assert (plane[:24] == plane[24]).all() and (plane[:, :24] == plane[:, 24:25]).all()
+    assert (intra >= 12).all()
+
+
+def test_h264_intra_cost_of_a_flat_picture_is_the_constant():
+    """A flat picture predicts exactly from DC (its own mean where there are
+    no neighbours): every block costs the constant 12."""
+    pic = np.full((64, 96), 77, np.uint8)
+    _, intra = oracle.lowres(pic, 8, H264)
+    assert (intra == 12).all()
+
+
+def test_h264_lowres_search_finds_a_translation():
+    """A picture moved by (12, -8) samples is found at (6, -4) half-resolution
+    samples by the hexagon and square, away from the edges, at no cost."""
+    rng = np.random.default_rng(11)
+    ref = random_picture(rng, 256, 160, 8)
+    cur = np.ascontiguousarray(np.roll(np.roll(ref, -8, axis=0), 12, axis=1))
+    cost, mv, nsad = oracle.lowres_search(cur, ref, 8, H264)
+    bw = 16
+    inner = [by * bw + bx for by in range(2, 8) for bx in range(3, 13)]
+    assert (mv[inner] == np.array([-6, 4], np.int16)).all()
+    assert (cost[inner] == 0).all()
+    # The zero vector, the hexagon's first six points and the square at least.
+    assert (nsad >= 1 + 8).all()
+    # Vectors stay in the window: 16 samples into the border, 32 at most.
+    assert (np.abs(mv) <= 32).all()
 
 
 @pytest.mark.gpu
@@ -70,3 +116,31 @@ def test_lowres_kernels_match_the_oracle(ms, bd, w, h):
     np.testing.assert_array_equal(bi, oracle.lowres_bi_cost(cur, r0, want0[1], r1, want1[1], bd))
     for i in range(3):
         ms.release(800 + i)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("bd,w,h", [(8, 1920, 1080), (10, 352, 288), (8, 200, 134), (12, 136, 72)])
+def test_h264_lowres_kernels_match_the_oracle(ms, bd, w, h):
+    """The H.264 lookahead: plane, intra costs, both lists' searches and the
+    average-of-two cost, block for block."""
+    rng = np.random.default_rng(bd * 7 + w)
+    r0 = random_picture(rng, w, h, bd)
+    r1 = shifted(r0, 9, -5, rng, 1.0)
+    cur = shifted(r0, -6, 7, rng, 2.0)
+    for i, pic in enumerate((cur, r0, r1)):
+        ms.upload(900 + i, pic, H264, bd, as_ref=False)
+        ms.lowres_build(900 + i)
+    _, want_intra = oracle.lowres(cur, bd, H264)
+    np.testing.assert_array_equal(ms.lowres_intra(900), want_intra)
+    got0 = ms.lowres_search(900, 901)
+    want0 = oracle.lowres_search(cur, r0, bd, H264)
+    for g, w_, name in zip(got0, want0, ("cost", "mv", "nsad")):
+        np.testing.assert_array_equal(g, w_, name)
+    got1 = ms.lowres_search(900, 902)
+    want1 = oracle.lowres_search(cur, r1, bd, H264)
+    for g, w_, name in zip(got1, want1, ("cost", "mv", "nsad")):
+        np.testing.assert_array_equal(g, w_, name)
+    bi = ms.lowres_bi_cost(900, 901, got0[1], 902, got1[1])
+    np.testing.assert_array_equal(bi, oracle.lowres_bi_cost(cur, r0, want0[1], r1, want1[1], bd, H264))
+    for i in range(3):
+        ms.release(900 + i)
