@@ -259,6 +259,48 @@ int rme_hevc_decide(const rme_picture_desc* d, const rme_params* p, int32_t nref
 /* Statistics of the last search call on this context. */
 int rme_last_stats(void* ctx, rme_stats* s);
 
+/* ---- B pictures: bi-prediction (HEVC) ---------------------------------- */
+
+/* A B unit's two one-list searches are GIVEN jobs of rme_frame_search whose
+ * `ref` indexes a reference list holding both lists' pictures (pick_pu_b,
+ * h265_me.rs:1768-1840, runs search_full + refine_subpel per list and
+ * reference exactly as pick_pu does). What B adds is scored here: the bi
+ * trial of a vector pair and its refinement, batched.
+ *
+ * One bi-prediction job: a block, the reference each list predicts from
+ * (indexes into the frame's ref_ids), the pair's vectors, and for
+ * rme_bi_refine the list searched again with that list's AMVP pair. */
+typedef struct {
+  int32_t x, y;        /* block position in luma samples                   */
+  int32_t w, h;        /* block size, multiples of 4, at most 64           */
+  int32_t ref[2];      /* list 0's and list 1's reference                  */
+  rme_mv  mv[2];       /* the pair's quarter-sample vectors                */
+  int32_t list;        /* rme_bi_refine: the list searched again (0, 1)    */
+  rme_mv  mvp[2];      /* rme_bi_refine: that list's AMVP predictors       */
+} rme_bi_job;
+
+/* satd_bi_at (h265_me.rs:4209-4264) under default weighting, per job: the
+ * SATD of the source block against the pair's bi-prediction. Where both
+ * vectors' blocks can be read (a whole-sample vector within the plane's
+ * border, a fractional one within HalfPlanes' reach on a phase HalfPlanes
+ * builds: all fifteen up to 2,200,000 luma samples, the three half phases
+ * above), the two one-list predictions averaged, (a + b + 1) >> 1;
+ * elsewhere the exact bi-prediction of the 14-bit intermediates at
+ * 15 - bit_depth. `f` names the source and the references (jobs unused);
+ * `p` gives hevc_pad. Host jobs and output, synchronous. */
+int rme_bi_satd(void* ctx, const rme_frame* f, const rme_params* p, const rme_bi_job* jobs, int32_t n,
+                uint32_t* satd, void* stream);
+
+/* refine_bi (h265_me.rs:3933-4014) per job: the other list's prediction
+ * held fixed, list `list` searched again against the target
+ * clip(2 * src - other's prediction) — search_full from the list's
+ * current vector, then refine_subpel — at twice the SATD Lagrangian, with
+ * the job's AMVP pair. One result per job (mv is the vector refine_bi
+ * returns; cost and satd are against the target). Host jobs and output,
+ * synchronous. */
+int rme_bi_refine(void* ctx, const rme_frame* f, const rme_params* p, const rme_bi_job* jobs, int32_t n,
+                  rme_result* out, void* stream);
+
 /* ---- chroma of chosen vectors -------------------------------------------- */
 
 /* Chroma prediction of chosen luma vectors (4:2:0): HEVC predict_block's

@@ -459,6 +459,124 @@ int run_frames(const rme_picture_desc* d, int nframes, const void* const* srcs, 
   return 0;
 }
 
+// ---- B pictures: bi-prediction (HEVC) ----------------------------------------
+
+// read_at (h265_me.rs:3630-3655): a whole-sample vector's block read from
+// the reference itself while it stays within the plane's border, a
+// fractional one's from HalfPlanes; null where neither can be read.
+template <class S>
+const S* hevc_read_at(const HevcRef<S>& r, int x, int y, int w, int h, Mv mv, ptrdiff_t* stride) {
+  const int mvx = mv.x, mvy = mv.y;
+  if ((mvx & 3) == 0 && (mvy & 3) == 0) {
+    const int xi = x + (mvx >> 2), yi = y + (mvy >> 2), lim = r.g.pad;
+    if (xi < -lim || yi < -lim || xi + w > r.g.width + lim || yi + h > r.g.height + lim) return nullptr;
+    *stride = r.g.stride;
+    return r.g.data.data() + r.g.offset(xi, yi);
+  }
+  *stride = r.hp.stride;
+  return r.hp.at(x, y, w, h, mvx, mvy);
+}
+
+// The 14-bit prediction of a block (predict14, h265_me.rs:4366-4415).
+template <class S>
+void hevc_pred14(const HevcRef<S>& r, int x, int y, int w, int h, Mv mv, int bd, int16_t* out) {
+  hevc_interp(r.g, x + (mv.x >> 2), y + (mv.y >> 2), mv.x & 3, mv.y & 3, w, h, true, bd, out);
+}
+
+// satd_bi_at (h265_me.rs:4209-4264) under default weighting: both blocks
+// readable, their samples averaged (a + b + 1) >> 1; otherwise both 14-bit
+// predictions through bi at 15 - bd (dsp/hevc.rs:1015-1031).
+template <class S>
+uint32_t hevc_satd_bi(const Dist<S>& dist, const HevcRef<S>& r0, const HevcRef<S>& r1, int bd, const S* src,
+                      ptrdiff_t ss, int x, int y, int w, int h, Mv mv0, Mv mv1) {
+  const int maxv = (1 << bd) - 1;
+  std::vector<S> pred((size_t)w * h);
+  ptrdiff_t s0 = 0, s1 = 0;
+  const S* p0 = hevc_read_at(r0, x, y, w, h, mv0, &s0);
+  const S* p1 = hevc_read_at(r1, x, y, w, h, mv1, &s1);
+  if (p0 && p1) {
+    for (int yy = 0; yy < h; ++yy)
+      for (int xx = 0; xx < w; ++xx)
+        pred[(size_t)yy * w + xx] = (S)(((int)p0[yy * s0 + xx] + p1[yy * s1 + xx] + 1) >> 1);
+  } else {
+    std::vector<int16_t> a((size_t)w * h), b((size_t)w * h);
+    hevc_pred14(r0, x, y, w, h, mv0, bd, a.data());
+    hevc_pred14(r1, x, y, w, h, mv1, bd, b.data());
+    const int shift = 15 - bd, round = 1 << (shift - 1);
+    for (size_t i = 0; i < pred.size(); ++i) pred[i] = (S)std::clamp((a[i] + b[i] + round) >> shift, 0, maxv);
+  }
+  return dist.satd(src + (ptrdiff_t)y * ss + x, ss, pred.data(), w, w, h);
+}
+
+// refine_bi (h265_me.rs:3933-4014): the other list's prediction at its
+// vector (read_at, else predict14 + uni) held fixed, the target
+// clip(2 * src - it); search_full from the list's own vector, then
+// refine_subpel, against the target at 2 * lam with the job's AMVP pair.
+template <class S>
+void hevc_refine_bi(const Dist<S>& dist, HevcRef<S>* const* refs, int bd, const S* src, ptrdiff_t ss, float lam,
+                    const rme_params* p, const rme_bi_job& j, rme_result& o) {
+  const int list = j.list, other = 1 - list, x = j.x, y = j.y, w = j.w, h = j.h, maxv = (1 << bd) - 1;
+  const HevcRef<S>& ro = *refs[j.ref[other]];
+  const Mv mo(j.mv[other].x, j.mv[other].y);
+  std::vector<S> pred((size_t)w * h), t((size_t)w * h);
+  ptrdiff_t ps = 0;
+  const S* pp = hevc_read_at(ro, x, y, w, h, mo, &ps);
+  if (!pp) {
+    std::vector<int16_t> p14((size_t)w * h);
+    hevc_pred14(ro, x, y, w, h, mo, bd, p14.data());
+    hevc_uni(pred.data(), w, p14.data(), w, h, 14 - bd, maxv);
+    pp = pred.data();
+    ps = w;
+  }
+  for (int yy = 0; yy < h; ++yy)
+    for (int xx = 0; xx < w; ++xx)
+      t[(size_t)yy * w + xx] = (S)std::clamp(2 * (int)src[(yy + y) * ss + x + xx] - (int)pp[yy * ps + xx], 0, maxv);
+  const HevcRef<S>& rl = *refs[j.ref[list]];
+  HevcSearch<S> sr{&dist, &rl.g, &rl.hp, bd, t.data(), w, x, y, w, h, 2.0f * lam, {{0, 0}, {0, 0}}};
+  sr.pq[0][0] = j.mvp[0].x;
+  sr.pq[0][1] = j.mvp[0].y;
+  sr.pq[1][0] = j.mvp[1].x;
+  sr.pq[1][1] = j.mvp[1].y;
+  sr.search_range = p->hevc_search_range;
+  sr.search_rings = p->hevc_search_rings;
+  sr.quarter_cross = p->hevc_quarter_cross != 0;
+  const Mv seed(j.mv[list].x, j.mv[list].y);
+  uint32_t fc, sat, c;
+  Mv full = sr.search_full(&seed, 1, &fc);
+  Mv m = sr.refine_subpel(full, &sat, &c);
+  o.mv = {m.x, m.y};
+  o.ref = j.ref[list];
+  o.cost = c;
+  o.satd = sat;
+  o.int_mv = {full.x, full.y};
+  o.int_cost = fc;
+  o.n_sad = sr.n_sad;
+  o.n_satd = sr.n_satd;
+}
+
+template <class S>
+int bi_frame(const rme_picture_desc* d, const void* src, int nref, const void* const* refs, const rme_params* p,
+             const rme_bi_job* jobs, int n, int refine, uint32_t* satd, rme_result* out) {
+  Dist<S> dist = dist_scalar<S>();
+  const int W = d->width, H = d->height, bd = d->bit_depth;
+  std::vector<HevcRef<S>> rr(nref);
+  std::vector<HevcRef<S>*> rp(nref);
+  for (int r = 0; r < nref; ++r) {
+    hevc_prepare_ref(rr[r], (const S*)refs[r], W, H, d->stride, p->hevc_pad, bd);
+    rp[r] = &rr[r];
+  }
+  const float lam = hevc_lambda(p->qp, bd, p->hevc_lambda_scale);
+  for (int i = 0; i < n; ++i) {
+    const rme_bi_job& j = jobs[i];
+    if (refine)
+      hevc_refine_bi<S>(dist, rp.data(), bd, (const S*)src, d->stride, lam, p, j, out[i]);
+    else
+      satd[i] = hevc_satd_bi<S>(dist, *rp[j.ref[0]], *rp[j.ref[1]], bd, (const S*)src, d->stride, j.x, j.y, j.w, j.h,
+                                Mv(j.mv[0].x, j.mv[0].y), Mv(j.mv[1].x, j.mv[1].y));
+  }
+  return 0;
+}
+
 template <class S>
 int given_frame(const rme_picture_desc* d, const void* src, int nref, const void* const* refs, const rme_params* p,
                 const rme_job* jobs, int njobs, int simd, rme_result* out) {
@@ -884,6 +1002,23 @@ int orc_frame_search(const rme_picture_desc* d, const void* src, int32_t nref, c
   return d->bit_depth == 8
              ? run_frames<uint8_t>(d, 1, &src, nref, refs, p, simd, 1, out, nullptr, nullptr, nullptr)
              : run_frames<uint16_t>(d, 1, &src, nref, refs, p, simd, 1, out, nullptr, nullptr, nullptr);
+}
+
+// HEVC bi-prediction jobs: satd_bi_at per job (refine == 0, into `satd`)
+// or refine_bi per job (refine == 1, into `out`).
+int orc_hevc_bi(const rme_picture_desc* d, const void* src, int32_t nref, const void* const* refs, const rme_params* p,
+                const rme_bi_job* jobs, int32_t n, int32_t refine, uint32_t* satd, rme_result* out) {
+  if (!valid_desc(d) || d->codec != RME_CODEC_HEVC || !p || nref < 1 || nref > RME_MAX_REFS || n < 0) return RME_EINVAL;
+  for (int i = 0; i < n; ++i) {
+    const rme_bi_job& j = jobs[i];
+    if (j.ref[0] < 0 || j.ref[0] >= nref || j.ref[1] < 0 || j.ref[1] >= nref || j.list < 0 || j.list > 1 ||
+        j.w < 4 || j.h < 4 || j.w > 64 || j.h > 64 || (j.w & 3) || (j.h & 3) || j.x < 0 || j.y < 0 ||
+        j.x + j.w > d->width || j.y + j.h > d->height)
+      return RME_EINVAL;
+  }
+  if (refine ? !out : !satd) return RME_EINVAL;
+  return d->bit_depth == 8 ? bi_frame<uint8_t>(d, src, nref, refs, p, jobs, n, refine, satd, out)
+                           : bi_frame<uint16_t>(d, src, nref, refs, p, jobs, n, refine, satd, out);
 }
 
 // Many STANDALONE frames on `threads` host threads (the timed CPU

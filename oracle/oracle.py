@@ -25,6 +25,8 @@ _SIGS = {
     "orc_frame_result_count": (C.c_int, [_PD, _PP, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
     "orc_frame_search": (C.c_int, [_PD, C.c_void_p, C.c_int32, C.POINTER(C.c_void_p), _PP, _PJ, C.c_int32,
                                    C.c_int32, _PR]),
+    "orc_hevc_bi": (C.c_int, [_PD, C.c_void_p, C.c_int32, C.POINTER(C.c_void_p), _PP, C.POINTER(capi.BiJob),
+                              C.c_int32, C.c_int32, C.POINTER(C.c_uint32), _PR]),
     "orc_frames_search_mt": (C.c_int, [_PD, C.c_int32, C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p),
                                        _PP, C.c_int32, C.c_int32, _PR, C.POINTER(C.c_int64),
                                        C.POINTER(C.c_double), C.POINTER(C.c_double)]),
@@ -119,6 +121,24 @@ def frame_search(codec: int, bit_depth: int, src: np.ndarray, refs, p, jobs: np.
     if rc != 0:
         raise RuntimeError(f"oracle frame_search rc={rc}")
     return out
+
+
+def hevc_bi(bit_depth: int, src: np.ndarray, refs, p, jobs: np.ndarray, refine: bool):
+    """satd_bi_at per job (refine False: uint32 array) or refine_bi per job
+    (refine True: results)."""
+    src = np.ascontiguousarray(src)
+    d = desc(capi.RME_CODEC_HEVC, src, bit_depth)
+    jobs = np.ascontiguousarray(jobs, capi.BI_JOB_DTYPE)
+    refs = [np.ascontiguousarray(r) for r in refs]
+    rp = (C.c_void_p * len(refs))(*[r.ctypes.data for r in refs])
+    satd = np.zeros(len(jobs), np.uint32)
+    out = np.zeros(len(jobs), capi.RESULT_DTYPE)
+    rc = lib().orc_hevc_bi(C.byref(d), src.ctypes.data, len(refs), rp, C.byref(p),
+                           C.cast(jobs.ctypes.data, C.POINTER(capi.BiJob)), len(jobs), int(refine),
+                           satd.ctypes.data_as(C.POINTER(C.c_uint32)), C.cast(out.ctypes.data, _PR))
+    if rc != 0:
+        raise RuntimeError(f"oracle hevc_bi rc={rc}")
+    return out if refine else satd
 
 
 def frames_search_mt(codec: int, bit_depth: int, srcs, refs_per_frame, p, simd: int = 1, threads: int = 1):

@@ -63,6 +63,11 @@ class Result(C.Structure):
                 ("n_satd", C.c_uint32)]
 
 
+class BiJob(C.Structure):
+    _fields_ = [("x", C.c_int32), ("y", C.c_int32), ("w", C.c_int32), ("h", C.c_int32),
+                ("ref", C.c_int32 * 2), ("mv", Mv * 2), ("list", C.c_int32), ("mvp", Mv * 2)]
+
+
 class Frame(C.Structure):
     _fields_ = [("src_id", C.c_int32), ("nref", C.c_int32), ("ref_ids", C.c_int32 * RME_MAX_REFS),
                 ("jobs", C.POINTER(Job)), ("njobs", C.c_int32)]
@@ -97,6 +102,9 @@ JOB_DTYPE = np.dtype([("x", "<i4"), ("y", "<i4"), ("w", "<i4"), ("h", "<i4"), ("
                       ("nseeds", "<i4"), ("flags", "<i4"), ("mvp", "<i2", (2, 2)),
                       ("seeds", "<i2", (RME_MAX_SEEDS, 2))])
 assert JOB_DTYPE.itemsize == C.sizeof(Job)
+BI_JOB_DTYPE = np.dtype([("x", "<i4"), ("y", "<i4"), ("w", "<i4"), ("h", "<i4"), ("ref", "<i4", (2,)),
+                         ("mv", "<i2", (2, 2)), ("list", "<i4"), ("mvp", "<i2", (2, 2))])
+assert BI_JOB_DTYPE.itemsize == C.sizeof(BiJob)
 
 # Every entry point include/rivet_me.h declares, with its ctypes signature.
 _vp, _i32, _i64, _u32p = C.c_void_p, C.c_int32, C.c_int64, C.POINTER(C.c_uint32)
@@ -122,6 +130,9 @@ SIGNATURES = {
     "rme_hevc_decide": (C.c_int, [C.POINTER(PictureDesc), C.POINTER(Params), _i32, C.POINTER(Result),
                                   C.POINTER(C.c_int32), C.POINTER(C.c_uint8)]),
     "rme_last_stats": (C.c_int, [_vp, C.POINTER(Stats)]),
+    "rme_bi_satd": (C.c_int, [_vp, C.POINTER(Frame), C.POINTER(Params), C.POINTER(BiJob), _i32, _u32p, _vp]),
+    "rme_bi_refine": (C.c_int, [_vp, C.POINTER(Frame), C.POINTER(Params), C.POINTER(BiJob), _i32,
+                                C.POINTER(Result), _vp]),
     "rme_chroma_predict": (C.c_int, [_vp, _i32, _i32, C.POINTER(C.c_int32), C.POINTER(Mv), _vp, _vp]),
     "rme_lowres_build": (C.c_int, [_vp, _i32, _vp]),
     "rme_lowres_info": (C.c_int, [_vp, _i32, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _u32p]),

@@ -187,6 +187,9 @@ struct Ctx {
   DevBuf<int32_t> d_ldone;
   DevBuf<uint32_t> d_lcost, d_lsad;
   DevBuf<rme_mv> d_lmv, d_lmv2;
+  DevBuf<rme_bi_job> d_bijobs;        // bi-prediction: jobs, SATDs, refine_bi targets
+  DevBuf<uint32_t> d_bisatd;
+  DevBuf<uint8_t> d_bitarget;
   DevBuf<int32_t> d_cblk;             // chroma: blocks, vectors, output offsets, output
   DevBuf<rme_mv> d_cmv;
   DevBuf<int64_t> d_coff;
@@ -494,8 +497,9 @@ int make_frame(Ctx* c, const rme_frame* f, const rme_params* p, FrameDesc* fd, r
 
 // Launch frames[0..n) as one persistent search; results to host `out` at
 // offsets (count-prefix order).
+// `bi_src` (HEVC refine_bi): frame 0's per-task target blocks.
 int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n, rme_result* out,
-               const int64_t* offsets, cudaStream_t s, bool use_graph) {
+               const int64_t* offsets, cudaStream_t s, bool use_graph, const void* bi_src = nullptr) {
   if (n < 1 || n > 255) return fail(c, RME_EINVAL, "1..255 frames per launch");
   std::vector<int> ntask(n);
   std::vector<int64_t> toff(n + 1, 0), jobs_off(n + 1, 0);
@@ -552,6 +556,7 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
     const unsigned long long tag = ((unsigned long long)c->epoch << 32) | ((unsigned long long)i << 24);
     if (params[i].predictor_mode == RME_PRED_GIVEN) {
       fd.jobs = c->d_jobs.p + jobs_off[i];
+      if (i == 0) fd.bi_src = bi_src;
       if (frames[i].njobs > 0)
         CK(cudaMemcpyAsync(c->d_jobs.p + jobs_off[i], frames[i].jobs, sizeof(rme_job) * frames[i].njobs,
                            cudaMemcpyHostToDevice, s));
@@ -1065,6 +1070,107 @@ int rme_last_stats(void* ctx, rme_stats* s) {
   if (!c || !s) return RME_EINVAL;
   *s = c->last;
   return 0;
+}
+
+// ---- B pictures: bi-prediction (h265_me.rs satd_bi_at, refine_bi) -------------
+
+namespace {
+// The frame's source and references, checked as make_frame checks them, and
+// the jobs copied to the device.
+int bi_setup(Ctx* c, const rme_frame* f, const rme_params* p, const rme_bi_job* jobs, int32_t n, bool refine,
+             cudaStream_t s, BiDesc* B) {
+  if (!f || !p || n < 0 || (n > 0 && !jobs)) return fail(c, RME_EINVAL, "null argument");
+  Picture* src;
+  int rc = picture_of(c, f->src_id, &src);
+  if (rc) return rc;
+  if (src->d.codec != RME_CODEC_HEVC) return fail(c, RME_EINVAL, "bi-prediction jobs are HEVC's");
+  if (f->nref < 1 || f->nref > RME_MAX_REFS) return fail(c, RME_EINVAL, "nref must be 1..4");
+  if ((rc = check_params(c, p, src->d))) return rc;
+  std::memset(B, 0, sizeof(*B));
+  B->src = src->planes;
+  for (int r = 0; r < f->nref; ++r) {
+    Picture* rp;
+    if ((rc = picture_of(c, f->ref_ids[r], &rp))) return rc;
+    if (!rp->is_ref) return fail(c, RME_EINVAL, "reference picture was uploaded without as_ref");
+    if (rp->d.codec != src->d.codec || rp->d.bit_depth != src->d.bit_depth || rp->d.width != src->d.width ||
+        rp->d.height != src->d.height)
+      return fail(c, RME_EINVAL, "reference format differs from the source's");
+    B->ref[r] = rp->planes;
+  }
+  for (int i = 0; i < n; ++i) {
+    const rme_bi_job& j = jobs[i];
+    if (j.ref[0] < 0 || j.ref[0] >= f->nref || j.ref[1] < 0 || j.ref[1] >= f->nref || j.w < 4 || j.h < 4 ||
+        j.w > 64 || j.h > 64 || (j.w & 3) || (j.h & 3) || j.x < 0 || j.y < 0 || j.x + j.w > src->cw ||
+        j.y + j.h > src->ch || (refine && (j.list < 0 || j.list > 1)))
+      return fail(c, RME_EINVAL, "bi job " + std::to_string(i) + " out of range");
+  }
+  B->width = src->cw;
+  B->height = src->ch;
+  B->bd = src->d.bit_depth;
+  B->pad = p->hevc_pad;
+  // HalfPlanes builds the quarter phases up to 2,200,000 luma samples
+  // (h265_search.rs:35, 82).
+  B->quarter = (int64_t)src->d.width * src->d.height <= 2200000;
+  B->n = n;
+  CK(cudaSetDevice(c->device));
+  CK(c->d_bijobs.ensure(std::max(n, 1)));
+  if (n > 0) CK(cudaMemcpyAsync(c->d_bijobs.p, jobs, sizeof(rme_bi_job) * n, cudaMemcpyHostToDevice, s));
+  B->jobs = c->d_bijobs.p;
+  return 0;
+}
+}  // namespace
+
+int rme_bi_satd(void* ctx, const rme_frame* f, const rme_params* p, const rme_bi_job* jobs, int32_t n,
+                uint32_t* satd, void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return RME_EINVAL;
+  if (n > 0 && !satd) return fail(c, RME_EINVAL, "null argument");
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  BiDesc B;
+  int rc = bi_setup(c, f, p, jobs, n, false, s, &B);
+  if (rc || n == 0) return rc;
+  CK(c->d_bisatd.ensure(n));
+  CK(launch_bi_satd(B, c->d_bisatd.p, s));
+  CK(cudaMemcpyAsync(satd, c->d_bisatd.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+int rme_bi_refine(void* ctx, const rme_frame* f, const rme_params* p, const rme_bi_job* jobs, int32_t n,
+                  rme_result* out, void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return RME_EINVAL;
+  if (n > 0 && !out) return fail(c, RME_EINVAL, "null argument");
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  BiDesc B;
+  int rc = bi_setup(c, f, p, jobs, n, true, s, &B);
+  if (rc || n == 0) return rc;
+  const int bps = B.bd == 8 ? 1 : 2;
+  CK(c->d_bitarget.ensure((size_t)n * kBiBlock * kBiBlock * bps));
+  CK(launch_bi_target(B, c->d_bitarget.p, s));
+  // Each job is a GIVEN search of its list's reference from the list's own
+  // vector with the job's AMVP pair, whose source is the target.
+  std::vector<rme_job> gj(n);
+  for (int i = 0; i < n; ++i) {
+    const rme_bi_job& j = jobs[i];
+    rme_job& g = gj[i];
+    std::memset(&g, 0, sizeof(g));
+    g.x = j.x;
+    g.y = j.y;
+    g.w = j.w;
+    g.h = j.h;
+    g.ref = j.ref[j.list];
+    g.nseeds = 1;
+    g.mvp[0] = j.mvp[0];
+    g.mvp[1] = j.mvp[1];
+    g.seeds[0] = j.mv[j.list];
+  }
+  rme_frame gf = *f;
+  gf.jobs = gj.data();
+  gf.njobs = n;
+  rme_params gp = *p;
+  gp.predictor_mode = RME_PRED_GIVEN;
+  return run_launch(c, &gf, &gp, 1, out, nullptr, s, false, c->d_bitarget.p);
 }
 
 int rme_chroma_predict(void* ctx, int32_t ref_id, int32_t nblocks, const int32_t* blocks, const rme_mv* mvs,

@@ -58,6 +58,9 @@ struct FrameDesc {
   uint32_t ref_cost[RME_MAX_REFS];
   // GIVEN
   const rme_job* jobs;
+  // GIVEN, HEVC refine_bi: per task its source block (the bi target),
+  // kBiBlock x kBiBlock samples at t * kBiBlock^2, searched at 2 * lam.
+  const void* bi_src;
   // outputs, and per task the count of its unfinished dependencies
   rme_result* out;
   int32_t* pending;
@@ -85,6 +88,19 @@ cudaError_t launch_pad_plane(const void* src, int bd, int w, int h, int sstride,
                              int pad, cudaStream_t s);
 cudaError_t launch_h264_hpel(DevPlanes p, int bd, int cw, int ch, int pad, cudaStream_t s);
 cudaError_t launch_hevc_phases(DevPlanes p, int bd, int w, int h, int pad, cudaStream_t s);
+// HEVC bi-prediction (rme_bi.cu): the jobs of a frame's source and
+// references; refine_bi targets are kBiBlock-wide blocks.
+constexpr int kBiBlock = 64;
+struct BiDesc {
+  DevPlanes src;
+  DevPlanes ref[RME_MAX_REFS];
+  int32_t width, height, bd, pad, quarter;
+  const rme_bi_job* jobs;
+  int32_t n;
+};
+cudaError_t launch_bi_satd(const BiDesc& B, uint32_t* satd, cudaStream_t s);
+cudaError_t launch_bi_target(const BiDesc& B, void* target, cudaStream_t s);
+
 // The lookahead's half-resolution plane of a picture, whole 8x8 blocks
 // (pw x ph) padded by kLowresPad on every side: HEVC's cutree plane
 // (h265_cutree.rs LowRes, 8-bit) or H.264's lookahead plane

@@ -579,14 +579,19 @@ __device__ void hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t,
     out = &F.out[t];
   }
   const DevPlanes& R = F.ref[r];
-  if (F.mode == RME_PRED_GIVEN) stage_src<S>(sm.src, plane_at<S>(F.src, 0, x, y), F.src.stride, w, h, lane);
+  if (F.mode == RME_PRED_GIVEN) {
+    if (F.bi_src)  // refine_bi: the target block stands in for the source
+      stage_src<S>(sm.src, (const S*)F.bi_src + (int64_t)t * (kBiBlock * kBiBlock), kBiBlock, w, h, lane);
+    else
+      stage_src<S>(sm.src, plane_at<S>(F.src, 0, x, y), F.src.stride, w, h, lane);
+  }
   const S* org = plane_at<S>(R, 0, x, y);
   const int stride = R.stride;
   constexpr int SPW = 4 / sizeof(S);
   const int wr = w / SPW, tw = w >> 2, th = h >> 2;
   const int padm = F.pad - 4;  // h265_search.rs MARGIN
   const int lox = -padm - x, hix = F.width + padm - w - x, loy = -padm - y, hiy = F.height + padm - h - y;
-  const float lam = F.lam;
+  const float lam = F.bi_src ? 2.0f * F.lam : F.lam;  // refine_bi weighs the rate at 2 * lam
   uint32_t nsad = 0, nsatd = 0;
 
   // Seeds: >> 2, clamp_pos, dedupe (a seed equal to an earlier one is

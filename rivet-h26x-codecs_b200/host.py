@@ -117,6 +117,30 @@ class MotionSearch:
                                                C.cast(out.ctypes.data, C.POINTER(capi.Result)), C.c_void_p(stream)))
         return out
 
+    def bi_satd(self, src_id: int, ref_ids: Sequence[int], params: capi.Params, jobs: np.ndarray,
+                stream: int = 0) -> np.ndarray:
+        """satd_bi_at per job (capi.BI_JOB_DTYPE): the SATD of each vector
+        pair's bi-prediction."""
+        jobs = np.ascontiguousarray(jobs, capi.BI_JOB_DTYPE)
+        f = self._frame(src_id, ref_ids)
+        out = np.zeros(len(jobs), np.uint32)
+        self._check(self._lib.rme_bi_satd(self.ctx, C.byref(f), C.byref(params),
+                                          C.cast(jobs.ctypes.data, C.POINTER(capi.BiJob)), len(jobs),
+                                          out.ctypes.data_as(C.POINTER(C.c_uint32)), C.c_void_p(stream)))
+        return out
+
+    def bi_refine(self, src_id: int, ref_ids: Sequence[int], params: capi.Params, jobs: np.ndarray,
+                  stream: int = 0) -> np.ndarray:
+        """refine_bi per job: one result per job (capi.RESULT_DTYPE), mv the
+        refined vector of the job's list."""
+        jobs = np.ascontiguousarray(jobs, capi.BI_JOB_DTYPE)
+        f = self._frame(src_id, ref_ids)
+        out = np.zeros(len(jobs), capi.RESULT_DTYPE)
+        self._check(self._lib.rme_bi_refine(self.ctx, C.byref(f), C.byref(params),
+                                            C.cast(jobs.ctypes.data, C.POINTER(capi.BiJob)), len(jobs),
+                                            C.cast(out.ctypes.data, C.POINTER(capi.Result)), C.c_void_p(stream)))
+        return out
+
     def search_batch(self, frames: Sequence[tuple[int, Sequence[int]]],
                      params: capi.Params | Sequence[capi.Params], stream: int = 0, out=None) -> list:
         """Many STANDALONE frames (src_id, ref_ids) in one persistent launch.
