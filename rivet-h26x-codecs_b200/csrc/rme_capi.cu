@@ -37,7 +37,9 @@ namespace {
 constexpr int kParts = 4;
 // The launch header in device memory (u64 words): head and tail of each
 // part's queue, then the counters, the status word and the epoch.
-constexpr int kMiscCounters = 8, kMiscStatus = 13, kMiscEpoch = 14;
+// The launch header: head and tail of each part's queue (0..7), the
+// counters (8..12), status, epoch, then each part's finished-task count.
+constexpr int kMiscCounters = 8, kMiscStatus = 13, kMiscEpoch = 14, kMiscDone = 16, kMiscWords = 24;
 
 int part_of(const FrameDesc& fd) { return 2 * (fd.bd > 8) + (fd.codec == RME_CODEC_H264); }
 int part_bytes(int k) { return k >= 2 ? 2 : 1; }
@@ -530,9 +532,9 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   // (epochs start at 1).
   if (c->d_ready.p != old_ready) c->epoch = 0;
   CK(c->d_jobs.ensure(std::max<int64_t>(jobs_off[n], 1)));
-  CK(c->d_misc.ensure(16));
+  CK(c->d_misc.ensure(kMiscWords));
   if (!dev_out && !pinned_out) CK(c->h_out.ensure(std::max<int64_t>(total, 1)));
-  CK(c->h_misc.ensure(16));
+  CK(c->h_misc.ensure(kMiscWords));
   if (c->epoch == 0 || c->epoch == 0xffffffffu) {
     CK(cudaMemsetAsync(c->d_ready.p, 0, c->d_ready.n * sizeof(unsigned long long), s));
     c->epoch = 0;
@@ -585,21 +587,21 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
     std::stable_sort(init[k].begin(), init[k].end(), [](unsigned long long a, unsigned long long b) {
       return (a & 0xffffffu) < (b & 0xffffffu);
     });
-  // h_init: [head, tail of each part | counters x5, status, epoch, pad | entries]
+  // h_init: [the launch header (kMiscWords) | entries]
   size_t ninit = 0, init_off[kParts];
   for (int k = 0; k < kParts; ++k) {
     init_off[k] = ninit;
     ninit += init[k].size();
   }
-  CK(c->h_init.ensure(16 + ninit));
+  CK(c->h_init.ensure(kMiscWords + ninit));
   unsigned long long* hi = c->h_init.p;
-  std::memset(hi, 0, 16 * sizeof(unsigned long long));
+  std::memset(hi, 0, kMiscWords * sizeof(unsigned long long));
   hi[kMiscEpoch] = c->epoch;
   LaunchDesc Ls[kParts];
   int64_t slot0 = 0, slot_off[kParts];
   for (int k = 0; k < kParts; ++k) {
     hi[2 * k + 1] = init[k].size();
-    std::memcpy(hi + 16 + init_off[k], init[k].data(), init[k].size() * sizeof(unsigned long long));
+    std::memcpy(hi + kMiscWords + init_off[k], init[k].data(), init[k].size() * sizeof(unsigned long long));
     slot_off[k] = slot0;
     LaunchDesc& L = Ls[k];
     L.frames = c->d_frames.p;
@@ -610,6 +612,7 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
     L.counters = c->d_misc.p + kMiscCounters;
     L.status = reinterpret_cast<uint32_t*>(c->d_misc.p + kMiscStatus);
     L.epoch = reinterpret_cast<const uint32_t*>(c->d_misc.p + kMiscEpoch);
+    L.done = c->d_misc.p + kMiscDone + k;
     slot0 += part_tasks[k];
   }
   int nparts_used = 0;
@@ -653,10 +656,10 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
         e = cudaMemcpyAsync(c->d_pending.p + toff[pc.second], pc.first, sizeof(int32_t) * ntask[pc.second],
                             cudaMemcpyDeviceToDevice, s);
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(c->d_misc.p, hi, 16 * sizeof(unsigned long long), cudaMemcpyHostToDevice, s);
+      e = cudaMemcpyAsync(c->d_misc.p, hi, kMiscWords * sizeof(unsigned long long), cudaMemcpyHostToDevice, s);
     for (int k = 0; k < kParts; ++k)
       if (e == cudaSuccess && !init[k].empty())
-        e = cudaMemcpyAsync(c->d_ready.p + slot_off[k], hi + 16 + init_off[k],
+        e = cudaMemcpyAsync(c->d_ready.p + slot_off[k], hi + kMiscWords + init_off[k],
                             init[k].size() * sizeof(unsigned long long), cudaMemcpyHostToDevice, s);
     // Under capture the records are external ones: they become event-record
     // nodes, so the kernels' device time is measured on every replay.
@@ -678,7 +681,7 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
     if (e == cudaSuccess && !dev_out && !pinned_out)
       e = cudaMemcpyAsync(c->h_out.p, c->d_out.p, sizeof(rme_result) * total, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(c->h_misc.p, c->d_misc.p, 16 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
+      e = cudaMemcpyAsync(c->h_misc.p, c->d_misc.p, kMiscWords * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
     return e;
   };
   bool has_given = false;

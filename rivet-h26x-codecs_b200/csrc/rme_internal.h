@@ -81,6 +81,10 @@ struct LaunchDesc {
   unsigned long long* counters;  // [tasks, sad, satd, sad_samples, satd_samples]
   const uint32_t* epoch;         // this launch's epoch (device memory: a
                                  // replayed graph keeps its arguments)
+  unsigned long long* done;      // tasks finished, or null: with it a warp
+                                 // runs one task it made ready itself
+                                 // (no queue round trip) and idle warps
+                                 // leave once every task is done
 };
 
 // Launch wrappers (defined in the .cu files).

@@ -187,6 +187,7 @@ extern "C" int rme_search_given_noalloc(const rme_picture_desc* d, const rme_par
   L.counters = d_misc + 4;
   L.status = reinterpret_cast<uint32_t*>(d_misc + 9);
   L.epoch = reinterpret_cast<const uint32_t*>(d_misc + 10);
+  L.done = nullptr;  // GIVEN jobs only: no task makes another ready
   const int bytes = d->bit_depth == 8 ? 1 : 2;
   int nsm = 0;
   if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return RME_ECUDA;

@@ -299,18 +299,48 @@ __device__ __forceinline__ void push_ready(const LaunchDesc& L, int f, int t) {
     atomicOr(L.status, kStatusBadTask);
 }
 
-// One finished dependency of task `d` of frame `f` (lane 0).
-__device__ __forceinline__ void release(const LaunchDesc& L, const FrameDesc& F, int f, int d) {
-  if (dec_acq_rel(&F.pending[d]) == 1) push_ready(L, f, d);
+// A finished task's dependents, task `dtask` in each lane where `rel`
+// (all lanes call): each decrement that reaches zero makes its task ready.
+// Where the launch counts finished tasks, the warp keeps the first task made
+// ready (lowest lane) to run next itself, saving the push, the pop and the
+// hand-over to another warp, unless `cont` already holds one; the others are
+// pushed. Returns `cont`, updated.
+__device__ __forceinline__ int release_lanes(const LaunchDesc& L, const FrameDesc& F, int f, bool rel, int dtask,
+                                             int cont, int lane) {
+  const bool ready = rel && dec_acq_rel(&F.pending[dtask]) == 1;
+  const uint32_t m = __ballot_sync(kFull, ready);
+  if (m == 0u) return cont;
+  int keep = -1;
+  if (cont < 0 && L.done != nullptr) {
+    keep = __ffs(m) - 1;
+    cont = (f << 24) | __shfl_sync(kFull, dtask, keep);
+  }
+  if (ready && lane != keep) push_ready(L, f, dtask);
+  return cont;
 }
 
+__device__ __forceinline__ void red_add64(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+constexpr uint32_t kPopDone = 0xfffffffeu;  // every task of the launch is done
+
 // The entry in slot `idx` once pushed (lane 0; bounded wait with backoff),
-// or 0xffffffff when the wait runs out (status set).
+// kPopDone once every task is done (a slot that will never be filled: the
+// warps that ran tasks they made ready pushed fewer than `total`), or
+// 0xffffffff when the wait runs out (status set).
 __device__ __forceinline__ uint32_t pop_slot(const LaunchDesc& L, unsigned long long idx, uint32_t epoch) {
   uint32_t ns = 32, it = 0;
   for (;;) {
     const unsigned long long v = ld_acquire64(L.ready + idx);
     if ((uint32_t)(v >> 32) == epoch) return (uint32_t)v;
+    if (L.done != nullptr && (it & 3u) == 3u && ld_relaxed64(L.done) >= (unsigned long long)L.total) return kPopDone;
     if (++it >= kSpinLimit) {
       atomicOr(L.status, kStatusWaitTimeout);
       return 0xffffffffu;
@@ -454,8 +484,9 @@ __device__ __forceinline__ uint32_t satd_part(const uint32_t* src, int wr, int t
   return acc;
 }
 
+// Returns a task it made ready to run next (frame << 24 | task), or -1.
 template <class S>
-__device__ void hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, WarpSmem<S>& sm, int lane) {
+__device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, WarpSmem<S>& sm, int lane) {
   int r, x, y, w, h, ns;
   int p0x, p0y, p1x, p1y;
   int sx = 0, sy = 0;  // this lane's seed (lane < ns)
@@ -728,6 +759,7 @@ __device__ void hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t,
   }
   nsatd += 9;
   write_result(out, bmx, bmy, r, bc, bsatd, imx, imy, int_cost, nsad, nsatd, lane);
+  int cont = -1;
   if (F.mode != RME_PRED_GIVEN && !amp_unit) {
     // The tasks reading this result: right and lower neighbours of this
     // level, the blocks of the next evaluated size inside this one, this
@@ -743,10 +775,12 @@ __device__ void hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t,
       ncx = max(0, min((lbx + 1) * N / M, F.nbx[l + 1]) - cx0);
       ncy = max(0, min((lby + 1) * N / M, F.nby[l + 1]) - cy0);
     }
-    const int namp = l < F.amp_nlev ? 2 * F.amp_nmodes : 0, nch = ncx * ncy;
-    for (int k = lane; k < 2 + nch + namp; k += 32) {
+    const int namp = l < F.amp_nlev ? 2 * F.amp_nmodes : 0, nch = ncx * ncy, ndep = 2 + nch + namp;
+    for (int k0 = 0; k0 < ndep; k0 += 32) {
+      const int k = k0 + lane;
       int dtask = -1;
-      if (k == 0) {
+      if (k >= ndep) {
+      } else if (k == 0) {
         if (lbx + 1 < F.nbx[l]) dtask = (F.base[l] + local + 1) * F.nref + r;
       } else if (k == 1) {
         if (lby + 1 < F.nby[l]) dtask = (F.base[l] + local + F.nbx[l]) * F.nref + r;
@@ -756,10 +790,11 @@ __device__ void hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t,
       } else {
         dtask = (F.amp_base[l] + local * namp + (k - 2 - nch)) * F.nref + r;
       }
-      if (dtask >= 0) release(L, F, f, dtask);
+      cont = release_lanes(L, F, f, dtask >= 0, dtask, cont, lane);
     }
   }
   count_task(sm, lane, nsad, nsatd, w * h);
+  return cont;
 }
 
 // ---- H.264 ------------------------------------------------------------------
@@ -1047,10 +1082,12 @@ __device__ __forceinline__ void median_mvp(Nb a, Nb b, Nb c, int ref, int& ox, i
   }
 }
 
+// Returns a task it made ready to run next (frame << 24 | task), or -1.
 template <class S>
-__device__ void h264_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, WarpSmem<S>& sm, int lane) {
+__device__ int h264_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, WarpSmem<S>& sm, int lane) {
   H264Blk B;
   uint32_t nsad = 0, nsatd = 0;
+  int cont = -1;
   auto shape = [&](int x, int y, int w, int h) {  // search_bounds (h264_hpel.rs:476-488)
     B.x = x;
     B.y = y;
@@ -1212,9 +1249,10 @@ __device__ void h264_task(const LaunchDesc& L, const FrameDesc& F, int f, int t,
       rel = my + 1 < mbh && mx + 1 < mbw;
       dtask = t + mbw + 1;
     }
-    if (rel) release(L, F, f, dtask);
+    cont = release_lanes(L, F, f, rel, dtask, cont, lane);
   }
   count_task(sm, lane, nsad, nsatd, B.w * B.h);
+  return cont;
 }
 
 // One kernel per (sample width, codec, occupancy variant): a launch holds
@@ -1232,15 +1270,23 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, MINB) search_kernel(Launc
   if (lane < 5) sm.cnt[lane] = 0;
   __syncwarp();
   const uint32_t epoch = __ldg(L.epoch);
+  int cont = -1;  // a task the last one made ready, run next by this warp
   for (;;) {
-    unsigned long long idx = 0;
-    if (lane == 0) idx = atomicAdd(L.head, 1ull);
-    idx = __shfl_sync(kFull, idx, 0);
-    if (idx >= (unsigned long long)L.total) break;
-    uint32_t e = 0;
-    if (lane == 0) e = pop_slot(L, idx, epoch);
-    e = __shfl_sync(kFull, e, 0);
+    uint32_t e;
+    if (cont >= 0) {
+      e = (uint32_t)cont;
+    } else {
+      unsigned long long idx = 0;
+      if (lane == 0) idx = atomicAdd(L.head, 1ull);
+      idx = __shfl_sync(kFull, idx, 0);
+      if (idx >= (unsigned long long)L.total) break;
+      e = 0;
+      if (lane == 0) e = pop_slot(L, idx, epoch);
+      e = __shfl_sync(kFull, e, 0);
+      if (e == kPopDone) break;
+    }
     __syncwarp();
+    cont = -1;
     if (e == 0xffffffffu) continue;  // the wait ran out (status set)
     const int f = (int)(e >> 24), t = (int)(e & 0xffffffu);
     const FrameDesc& F = L.frames[f];
@@ -1250,8 +1296,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, MINB) search_kernel(Launc
       if (lane == 0) atomicOr(L.status, kStatusBadTask);
       continue;
     }
-    if constexpr (CODEC == RME_CODEC_HEVC) hevc_task<S>(L, F, f, t, sm, lane);
-    else h264_task<S>(L, F, f, t, sm, lane);
+    if constexpr (CODEC == RME_CODEC_HEVC) cont = hevc_task<S>(L, F, f, t, sm, lane);
+    else cont = h264_task<S>(L, F, f, t, sm, lane);
+    if (lane == 0 && L.done != nullptr) red_add64(L.done, 1ull);
   }
   __syncwarp();
   if (lane < 5) atomicAdd(&L.counters[lane], sm.cnt[lane]);
