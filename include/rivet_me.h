@@ -259,6 +259,36 @@ int rme_hevc_decide(const rme_picture_desc* d, const rme_params* p, int32_t nref
 /* Statistics of the last search call on this context. */
 int rme_last_stats(void* ctx, rme_stats* s);
 
+/* ---- weighted prediction (explicit weights) ----------------------------- */
+
+/* A weighted reference's search plane: resident picture `dst_id` becomes
+ * `ref_id`'s padded luma with the explicit weighting applied to every
+ * sample, border included, clipped to the sample range, and its search
+ * planes are built from it. H.264 weighted_search_plane
+ * (h264_me.rs:653-672): ((v * weight + 2^(log_wd-1)) >> log_wd) + offset,
+ * no rounding at log_wd 0 — the plane PRef::search / BRefs::search the
+ * whole-sample search and its refinement score against. HEVC
+ * weighted_search_plane (h265_me.rs:4275-4293): (((v << (14 - bd)) *
+ * weight + 2^(log_wd-1)) >> log_wd) + offset, log_wd >= 1 — the plane the
+ * whole-sample search of a weighted list scores against (the reference
+ * refines sub-sample vectors on the unweighted reference under weighted
+ * scoring, which this library does not reproduce). `offset` is at the
+ * sample depth. Use `dst_id` as any other reference. Asynchronous on
+ * `stream`. */
+int rme_picture_weighted(void* ctx, int32_t ref_id, int32_t dst_id, int32_t log_wd, int32_t weight,
+                         int32_t offset, void* stream);
+
+/* The weight fit's moments of picture `cur_id` against `ref_id` over the
+ * picture (wp_moments, dsp/distortion.rs:206-226): out[0..4] = sums of r,
+ * c, r*r, r*c and |c - r|. Synchronous. */
+int rme_wp_moments(void* ctx, int32_t cur_id, int32_t ref_id, uint64_t* out, void* stream);
+
+/* weighted_sad (dsp/distortion.rs:228-252) over the picture: the sum of
+ * |clip(((r * weight + 2^(shift-1)) >> shift) + offset) - c| (no rounding
+ * at shift 0), `offset` at the sample depth. Synchronous. */
+int rme_weighted_sad(void* ctx, int32_t cur_id, int32_t ref_id, int32_t weight, int32_t shift, int32_t offset,
+                     uint64_t* out, void* stream);
+
 /* ---- B pictures: bi-prediction (HEVC) ---------------------------------- */
 
 /* A B unit's two one-list searches are GIVEN jobs of rme_frame_search whose

@@ -950,6 +950,61 @@ LowResS<S> lowres_h264_of(const rme_picture_desc* d, const void* luma) {
   return lowres_h264<S>((const S*)luma, d->width, d->height, d->stride);
 }
 
+// ---- weighted prediction: search planes and fit moments ---------------------
+
+// wp_moments (dsp/distortion.rs:206-226) over the w x h display area: the
+// sums of r, c, r*r, r*c and |c - r| (out[0..4]).
+template <class S>
+void wp_moments(const S* cur, ptrdiff_t cs, const S* ref, ptrdiff_t rs, int w, int h, uint64_t* out) {
+  uint64_t sr = 0, sc = 0, srr = 0, src = 0, sad = 0;
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) {
+      const uint64_t r = ref[y * rs + x], c = cur[y * cs + x];
+      sr += r;
+      sc += c;
+      srr += r * r;
+      src += r * c;
+      sad += r > c ? r - c : c - r;
+    }
+  out[0] = sr;
+  out[1] = sc;
+  out[2] = srr;
+  out[3] = src;
+  out[4] = sad;
+}
+
+// weighted_sad (dsp/distortion.rs:228-252): sum of |clip(((r * weight +
+// round) >> shift) + offset) - c|, round = 2^(shift-1) (none at shift 0).
+template <class S>
+uint64_t weighted_sad(const S* cur, ptrdiff_t cs, const S* ref, ptrdiff_t rs, int w, int h, int weight, int shift,
+                      int offset, int maxv) {
+  const int round = shift >= 1 ? 1 << (shift - 1) : 0;
+  uint64_t sad = 0;
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) {
+      const int p = (((int)ref[y * rs + x] * weight + round) >> shift) + offset;
+      sad += (uint64_t)std::abs(std::clamp(p, 0, maxv) - (int)cur[y * cs + x]);
+    }
+  return sad;
+}
+
+// The weighted search plane's per-sample formula: H.264
+// weighted_search_plane (h264_me.rs:653-672), ((v * w + 2^(log_wd-1)) >>
+// log_wd) + o, no rounding at log_wd 0; HEVC weighted_search_plane
+// (h265_me.rs:4275-4293), (((v << (14 - bd)) * w + 2^(log_wd-1)) >> log_wd)
+// + o; clipped to the sample range.
+inline int weighted_sample(int codec, int bd, int v, int log_wd, int w, int o) {
+  const int maxv = (1 << bd) - 1;
+  int p;
+  if (codec == RME_CODEC_H264) {
+    const int x = v * w;
+    p = log_wd >= 1 ? ((x + (1 << (log_wd - 1))) >> log_wd) + o : x + o;
+  } else {
+    p = (((v << (14 - bd)) * w + (1 << (log_wd - 1))) >> log_wd) + o;
+  }
+  return std::clamp(p, 0, maxv);
+}
+
 }  // namespace
 
 extern "C" {
@@ -1019,6 +1074,42 @@ int orc_hevc_bi(const rme_picture_desc* d, const void* src, int32_t nref, const 
   if (refine ? !out : !satd) return RME_EINVAL;
   return d->bit_depth == 8 ? bi_frame<uint8_t>(d, src, nref, refs, p, jobs, n, refine, satd, out)
                            : bi_frame<uint16_t>(d, src, nref, refs, p, jobs, n, refine, satd, out);
+}
+
+// Weighted prediction: the fit moments of `cur` against `ref` (out[5]).
+int orc_wp_moments(const rme_picture_desc* d, const void* cur, const void* ref, uint64_t* out) {
+  if (!valid_desc(d) || !cur || !ref || !out) return RME_EINVAL;
+  if (d->bit_depth == 8)
+    wp_moments<uint8_t>((const uint8_t*)cur, d->stride, (const uint8_t*)ref, d->stride, d->width, d->height, out);
+  else
+    wp_moments<uint16_t>((const uint16_t*)cur, d->stride, (const uint16_t*)ref, d->stride, d->width, d->height, out);
+  return 0;
+}
+
+int orc_weighted_sad(const rme_picture_desc* d, const void* cur, const void* ref, int32_t weight, int32_t shift,
+                     int32_t offset, uint64_t* out) {
+  if (!valid_desc(d) || !cur || !ref || !out || shift < 0 || shift > 14) return RME_EINVAL;
+  const int maxv = (1 << d->bit_depth) - 1;
+  *out = d->bit_depth == 8 ? weighted_sad<uint8_t>((const uint8_t*)cur, d->stride, (const uint8_t*)ref, d->stride,
+                                                   d->width, d->height, weight, shift, offset, maxv)
+                           : weighted_sad<uint16_t>((const uint16_t*)cur, d->stride, (const uint16_t*)ref, d->stride,
+                                                    d->width, d->height, weight, shift, offset, maxv);
+  return 0;
+}
+
+// The weighted search plane's formula over `n` samples (any layout: the
+// weighting is per sample, so it commutes with the border replication).
+int orc_weighted_samples(int32_t codec, int32_t bit_depth, const void* in, int64_t n, int32_t log_wd, int32_t weight,
+                         int32_t offset, void* out) {
+  if (bit_depth < 8 || bit_depth > 12 || !in || !out || n < 0) return RME_EINVAL;
+  if (codec == RME_CODEC_HEVC && log_wd < 1) return RME_EINVAL;
+  for (int64_t i = 0; i < n; ++i) {
+    const int v = bit_depth == 8 ? ((const uint8_t*)in)[i] : ((const uint16_t*)in)[i];
+    const int q = weighted_sample(codec, bit_depth, v, log_wd, weight, offset);
+    if (bit_depth == 8) ((uint8_t*)out)[i] = (uint8_t)q;
+    else ((uint16_t*)out)[i] = (uint16_t)q;
+  }
+  return 0;
 }
 
 // Many STANDALONE frames on `threads` host threads (the timed CPU

@@ -27,6 +27,11 @@ _SIGS = {
                                    C.c_int32, _PR]),
     "orc_hevc_bi": (C.c_int, [_PD, C.c_void_p, C.c_int32, C.POINTER(C.c_void_p), _PP, C.POINTER(capi.BiJob),
                               C.c_int32, C.c_int32, C.POINTER(C.c_uint32), _PR]),
+    "orc_wp_moments": (C.c_int, [_PD, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint64)]),
+    "orc_weighted_sad": (C.c_int, [_PD, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32,
+                                   C.POINTER(C.c_uint64)]),
+    "orc_weighted_samples": (C.c_int, [C.c_int32, C.c_int32, C.c_void_p, C.c_int64, C.c_int32, C.c_int32,
+                                       C.c_int32, C.c_void_p]),
     "orc_frames_search_mt": (C.c_int, [_PD, C.c_int32, C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p),
                                        _PP, C.c_int32, C.c_int32, _PR, C.POINTER(C.c_int64),
                                        C.POINTER(C.c_double), C.POINTER(C.c_double)]),
@@ -139,6 +144,35 @@ def hevc_bi(bit_depth: int, src: np.ndarray, refs, p, jobs: np.ndarray, refine: 
     if rc != 0:
         raise RuntimeError(f"oracle hevc_bi rc={rc}")
     return out if refine else satd
+
+
+def wp_moments(codec: int, bit_depth: int, cur: np.ndarray, ref: np.ndarray) -> np.ndarray:
+    """(sr, sc, srr, src, sad) of `cur` against `ref` (wp_moments)."""
+    cur, ref = np.ascontiguousarray(cur), np.ascontiguousarray(ref)
+    d = desc(codec, cur, bit_depth)
+    out = np.zeros(5, np.uint64)
+    assert lib().orc_wp_moments(C.byref(d), cur.ctypes.data, ref.ctypes.data,
+                                out.ctypes.data_as(C.POINTER(C.c_uint64))) == 0
+    return out
+
+
+def weighted_sad(codec: int, bit_depth: int, cur, ref, weight: int, shift: int, offset: int) -> int:
+    cur, ref = np.ascontiguousarray(cur), np.ascontiguousarray(ref)
+    d = desc(codec, cur, bit_depth)
+    out = C.c_uint64()
+    assert lib().orc_weighted_sad(C.byref(d), cur.ctypes.data, ref.ctypes.data, weight, shift, offset,
+                                  C.byref(out)) == 0
+    return out.value
+
+
+def weighted_samples(codec: int, bit_depth: int, a: np.ndarray, log_wd: int, weight: int, offset: int):
+    """The weighted search plane's formula applied to every sample of `a`."""
+    a = np.ascontiguousarray(a)
+    out = np.empty_like(a)
+    rc = lib().orc_weighted_samples(codec, bit_depth, a.ctypes.data, a.size, log_wd, weight, offset, out.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"oracle weighted_samples rc={rc}")
+    return out
 
 
 def frames_search_mt(codec: int, bit_depth: int, srcs, refs_per_frame, p, simd: int = 1, threads: int = 1):

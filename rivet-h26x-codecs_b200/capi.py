@@ -130,6 +130,9 @@ SIGNATURES = {
     "rme_hevc_decide": (C.c_int, [C.POINTER(PictureDesc), C.POINTER(Params), _i32, C.POINTER(Result),
                                   C.POINTER(C.c_int32), C.POINTER(C.c_uint8)]),
     "rme_last_stats": (C.c_int, [_vp, C.POINTER(Stats)]),
+    "rme_picture_weighted": (C.c_int, [_vp, _i32, _i32, _i32, _i32, _i32, _vp]),
+    "rme_wp_moments": (C.c_int, [_vp, _i32, _i32, C.POINTER(C.c_uint64), _vp]),
+    "rme_weighted_sad": (C.c_int, [_vp, _i32, _i32, _i32, _i32, _i32, C.POINTER(C.c_uint64), _vp]),
     "rme_bi_satd": (C.c_int, [_vp, C.POINTER(Frame), C.POINTER(Params), C.POINTER(BiJob), _i32, _u32p, _vp]),
     "rme_bi_refine": (C.c_int, [_vp, C.POINTER(Frame), C.POINTER(Params), C.POINTER(BiJob), _i32,
                                 C.POINTER(Result), _vp]),

@@ -189,6 +189,7 @@ struct Ctx {
   DevBuf<int32_t> d_ldone;
   DevBuf<uint32_t> d_lcost, d_lsad;
   DevBuf<rme_mv> d_lmv, d_lmv2;
+  DevBuf<unsigned long long> d_wp;    // weighted prediction: moments, weighted SAD
   DevBuf<rme_bi_job> d_bijobs;        // bi-prediction: jobs, SATDs, refine_bi targets
   DevBuf<uint32_t> d_bisatd;
   DevBuf<uint8_t> d_bitarget;
@@ -818,6 +819,31 @@ void rme_ctx_destroy(void* ctx) {
 
 const char* rme_last_error(void* ctx) { return ctx ? ((Ctx*)ctx)->err.c_str() : "null context"; }
 
+namespace {
+// A picture's device layout (no memory yet): H.264 planes at the coded
+// (macroblock) size, HEVC at the picture's; rows of 128-byte multiples, the
+// visible origin 16-byte aligned (pad * bytes is a multiple of 16 for both
+// pads); a reference holds its search planes after plane 0.
+std::unique_ptr<Picture> picture_geometry(const rme_picture_desc* d, bool as_ref) {
+  auto pic = std::make_unique<Picture>();
+  pic->d = *d;
+  const bool h264 = d->codec == RME_CODEC_H264;
+  pic->cw = h264 ? (d->width + 15) / 16 * 16 : d->width;
+  pic->ch = h264 ? (d->height + 15) / 16 * 16 : d->height;
+  pic->pad = h264 ? kH264Pad : kHevcPad;
+  pic->is_ref = as_ref;
+  pic->nplanes = as_ref ? (h264 ? 4 : 16) : 1;
+  const int bps = d->bit_depth == 8 ? 1 : 2;
+  const int stride_bytes = ((pic->cw + 2 * pic->pad) * bps + 127) / 128 * 128;
+  const int stride = stride_bytes / bps, rows = pic->ch + 2 * pic->pad;
+  pic->planes.stride = stride;
+  pic->planes.plane_elems = (int64_t)stride * rows;
+  pic->planes.origin = pic->pad * stride + pic->pad;
+  pic->bytes = (size_t)pic->planes.plane_elems * bps * pic->nplanes + 256;
+  return pic;
+}
+}  // namespace
+
 int rme_picture_upload(void* ctx, int32_t pic_id, const rme_picture_desc* d, const void* luma, int32_t as_ref,
                        void* stream) {
   Ctx* c = (Ctx*)ctx;
@@ -825,23 +851,9 @@ int rme_picture_upload(void* ctx, int32_t pic_id, const rme_picture_desc* d, con
   if (!valid_desc(d) || !luma || pic_id < 0) return fail(c, RME_EINVAL, "bad picture description");
   cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
   CK(cudaSetDevice(c->device));
-  auto pic = std::make_unique<Picture>();
-  pic->d = *d;
-  bool h264 = d->codec == RME_CODEC_H264;
-  pic->cw = h264 ? (d->width + 15) / 16 * 16 : d->width;
-  pic->ch = h264 ? (d->height + 15) / 16 * 16 : d->height;
-  pic->pad = h264 ? kH264Pad : kHevcPad;
-  pic->is_ref = as_ref != 0;
-  pic->nplanes = as_ref ? (h264 ? 4 : 16) : 1;
-  int bps = d->bit_depth == 8 ? 1 : 2;
-  // Rows padded to 128 bytes; the visible origin 16-byte aligned
-  // (pad * bytes is a multiple of 16 for both pads).
-  int stride_bytes = ((pic->cw + 2 * pic->pad) * bps + 127) / 128 * 128;
-  int stride = stride_bytes / bps, rows = pic->ch + 2 * pic->pad;
-  pic->planes.stride = stride;
-  pic->planes.plane_elems = (int64_t)stride * rows;
-  pic->planes.origin = pic->pad * stride + pic->pad;
-  pic->bytes = (size_t)pic->planes.plane_elems * bps * pic->nplanes + 256;
+  auto pic = picture_geometry(d, as_ref != 0);
+  const bool h264 = d->codec == RME_CODEC_H264;
+  const int bps = d->bit_depth == 8 ? 1 : 2, stride = pic->planes.stride;
   // Re-uploading an id with the same format reuses its device buffer (a
   // stream's picture slots are refilled every frame). Work already queued
   // on the picture is ordered before the refill by the stream.
@@ -916,6 +928,96 @@ int rme_picture_build_planes(void* ctx, int32_t pic_id, void* stream) {
   CK(cudaSetDevice(c->device));
   if (p->d.codec == RME_CODEC_H264) CK(launch_h264_hpel(p->planes, p->d.bit_depth, p->cw, p->ch, p->pad, s));
   else CK(launch_hevc_phases(p->planes, p->d.bit_depth, p->cw, p->ch, p->pad, s));
+  return 0;
+}
+
+// ---- weighted prediction (h264_me.rs / h265_me.rs weighted_search_plane,
+// distortion.rs wp_moments / weighted_sad) ------------------------------------
+
+int rme_picture_weighted(void* ctx, int32_t ref_id, int32_t dst_id, int32_t log_wd, int32_t weight, int32_t offset,
+                         void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return RME_EINVAL;
+  Picture* p;
+  int rc = picture_of(c, ref_id, &p);
+  if (rc) return rc;
+  if (!p->is_ref) return fail(c, RME_EINVAL, "picture was uploaded without as_ref");
+  if (dst_id < 0 || dst_id == ref_id) return fail(c, RME_EINVAL, "the weighted plane needs an id of its own");
+  const bool h264 = p->d.codec == RME_CODEC_H264;
+  if (log_wd < (h264 ? 0 : 1) || log_wd > 14 || weight < -128 || weight > 255 || offset < -(1 << p->d.bit_depth) ||
+      offset > (1 << p->d.bit_depth))
+    return fail(c, RME_EINVAL, "weighting out of range");
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  CK(cudaSetDevice(c->device));
+  auto pic = picture_geometry(&p->d, true);
+  auto old = c->pics.find(dst_id);
+  if (old != c->pics.end() && old->second->bytes == pic->bytes && old->second->planes.stride == pic->planes.stride) {
+    pic->buf = old->second->buf;
+    old->second->buf = nullptr;
+  } else {
+    if (old != c->pics.end()) CK(cudaStreamSynchronize(s));
+    CK(cudaMalloc(&pic->buf, pic->bytes));
+  }
+  pic->planes.base = pic->buf;
+  const int bps = p->d.bit_depth == 8 ? 1 : 2;
+  CK(launch_weighted_plane(p->buf, pic->buf, pic->planes.plane_elems * bps, p->d.codec, p->d.bit_depth, log_wd, weight,
+                           offset, s));
+  if (h264) CK(launch_h264_hpel(pic->planes, p->d.bit_depth, pic->cw, pic->ch, pic->pad, s));
+  else CK(launch_hevc_phases(pic->planes, p->d.bit_depth, pic->cw, pic->ch, pic->pad, s));
+  c->pics[dst_id] = std::move(pic);
+  return 0;
+}
+
+namespace {
+int picture_pair(Ctx* c, int32_t cur_id, int32_t ref_id, Picture** pc, Picture** pr) {
+  int rc = picture_of(c, cur_id, pc);
+  if (!rc) rc = picture_of(c, ref_id, pr);
+  if (rc) return rc;
+  const rme_picture_desc &a = (*pc)->d, &b = (*pr)->d;
+  if (a.codec != b.codec || a.bit_depth != b.bit_depth || a.width != b.width || a.height != b.height ||
+      (*pc)->planes.stride != (*pr)->planes.stride)
+    return fail(c, RME_EINVAL, "the pictures' formats differ");
+  return 0;
+}
+}  // namespace
+
+int rme_wp_moments(void* ctx, int32_t cur_id, int32_t ref_id, uint64_t* out, void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !out) return c ? fail(c, RME_EINVAL, "null argument") : RME_EINVAL;
+  Picture *pc, *pr;
+  int rc = picture_pair(c, cur_id, ref_id, &pc, &pr);
+  if (rc) return rc;
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  CK(cudaSetDevice(c->device));
+  CK(c->d_wp.ensure(8));
+  CK(cudaMemsetAsync(c->d_wp.p, 0, 5 * sizeof(unsigned long long), s));
+  const int bps = pc->d.bit_depth == 8 ? 1 : 2;
+  CK(launch_wp_moments((const uint8_t*)pc->buf + (size_t)pc->planes.origin * bps,
+                       (const uint8_t*)pr->buf + (size_t)pr->planes.origin * bps, pc->planes.stride, pc->d.bit_depth,
+                       pc->d.width, pc->d.height, c->d_wp.p, s));
+  CK(cudaMemcpyAsync(out, c->d_wp.p, 5 * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+int rme_weighted_sad(void* ctx, int32_t cur_id, int32_t ref_id, int32_t weight, int32_t shift, int32_t offset,
+                     uint64_t* out, void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !out) return c ? fail(c, RME_EINVAL, "null argument") : RME_EINVAL;
+  if (shift < 0 || shift > 14 || weight < -128 || weight > 255) return fail(c, RME_EINVAL, "weighting out of range");
+  Picture *pc, *pr;
+  int rc = picture_pair(c, cur_id, ref_id, &pc, &pr);
+  if (rc) return rc;
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  CK(cudaSetDevice(c->device));
+  CK(c->d_wp.ensure(8));
+  CK(cudaMemsetAsync(c->d_wp.p + 5, 0, sizeof(unsigned long long), s));
+  const int bps = pc->d.bit_depth == 8 ? 1 : 2;
+  CK(launch_weighted_sad((const uint8_t*)pc->buf + (size_t)pc->planes.origin * bps,
+                         (const uint8_t*)pr->buf + (size_t)pr->planes.origin * bps, pc->planes.stride,
+                         pc->d.bit_depth, pc->d.width, pc->d.height, weight, shift, offset, c->d_wp.p + 5, s));
+  CK(cudaMemcpyAsync(out, c->d_wp.p + 5, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
   return 0;
 }
 

@@ -92,6 +92,15 @@ cudaError_t launch_pad_plane(const void* src, int bd, int w, int h, int sstride,
                              int pad, cudaStream_t s);
 cudaError_t launch_h264_hpel(DevPlanes p, int bd, int cw, int ch, int pad, cudaStream_t s);
 cudaError_t launch_hevc_phases(DevPlanes p, int bd, int w, int h, int pad, cudaStream_t s);
+// Weighted prediction (rme_wp.cu): the weighted copy of a padded plane
+// (`bytes`, a multiple of 16), and the fit's passes over a picture pair
+// (pointers at the visible origin, `stride` samples per row).
+cudaError_t launch_weighted_plane(const void* src, void* dst, int64_t bytes, int codec, int bd, int log_wd, int weight,
+                                  int offset, cudaStream_t s);
+cudaError_t launch_wp_moments(const void* cur, const void* ref, int stride, int bd, int w, int h,
+                              unsigned long long* out, cudaStream_t s);
+cudaError_t launch_weighted_sad(const void* cur, const void* ref, int stride, int bd, int w, int h, int weight,
+                                int shift, int offset, unsigned long long* out, cudaStream_t s);
 // HEVC bi-prediction (rme_bi.cu): the jobs of a frame's source and
 // references; refine_bi targets are kBiBlock-wide blocks.
 constexpr int kBiBlock = 64;

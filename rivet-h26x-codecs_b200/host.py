@@ -67,6 +67,26 @@ class MotionSearch:
         """Rebuild a resident reference's search planes (asynchronous)."""
         self._check(self._lib.rme_picture_build_planes(self.ctx, pic_id, C.c_void_p(stream)))
 
+    def picture_weighted(self, ref_id: int, dst_id: int, log_wd: int, weight: int, offset: int,
+                         stream: int = 0) -> None:
+        """`dst_id` := the weighted search plane of reference `ref_id` (the
+        picture's codec picks H.264's or HEVC's formula)."""
+        self._check(self._lib.rme_picture_weighted(self.ctx, ref_id, dst_id, log_wd, weight, offset,
+                                                   C.c_void_p(stream)))
+        self._desc[dst_id] = self._desc[ref_id]
+
+    def wp_moments(self, cur_id: int, ref_id: int) -> np.ndarray:
+        """(sr, sc, srr, src, sad) of `cur_id` against `ref_id`."""
+        out = np.zeros(5, np.uint64)
+        self._check(self._lib.rme_wp_moments(self.ctx, cur_id, ref_id, out.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                             None))
+        return out
+
+    def weighted_sad(self, cur_id: int, ref_id: int, weight: int, shift: int, offset: int) -> int:
+        out = C.c_uint64()
+        self._check(self._lib.rme_weighted_sad(self.ctx, cur_id, ref_id, weight, shift, offset, C.byref(out), None))
+        return out.value
+
     def release(self, pic_id: int) -> None:
         self._check(self._lib.rme_picture_release(self.ctx, pic_id))
         self._desc.pop(pic_id, None)

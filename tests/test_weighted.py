@@ -1,0 +1,109 @@
+"""Weighted prediction for the search: the weighted search planes (H.264
+h264_me.rs:653-672, HEVC h265_me.rs:4275-4293) and the weight fit's passes
+(wp_moments, weighted_sad: dsp/distortion.rs:206-252). The oracle's
+restatement against numpy on the CPU; the device kernels against the
+oracle, sample for sample and sum for sum."""
+import numpy as np
+import pytest
+
+import oracle
+import rivet_h26x_codecs_b200.capi as capi
+from _common import random_jobs, random_picture, shifted
+
+H264, HEVC = capi.RME_CODEC_H264, capi.RME_CODEC_HEVC
+
+
+def _np_weighted(codec, bd, v, log_wd, w, o):
+    v = v.astype(np.int64)
+    if codec == H264:
+        p = ((v * w + (1 << (log_wd - 1))) >> log_wd) + o if log_wd >= 1 else v * w + o
+    else:
+        p = (((v << (14 - bd)) * w + (1 << (log_wd - 1))) >> log_wd) + o
+    return np.clip(p, 0, (1 << bd) - 1)
+
+
+@pytest.mark.parametrize("codec,bd,log_wd,w,o", [(H264, 8, 5, 40, -7), (H264, 8, 0, 1, 12), (H264, 10, 6, -20, 900),
+                                                 (HEVC, 8, 12, 70, 3), (HEVC, 10, 10, 50, -40)])
+def test_weighted_plane_formula(codec, bd, log_wd, w, o):
+    rng = np.random.default_rng(bd + log_wd)
+    a = random_picture(rng, 64, 32, bd)
+    got = oracle.weighted_samples(codec, bd, a, log_wd, w, o)
+    np.testing.assert_array_equal(got.astype(np.int64), _np_weighted(codec, bd, a, log_wd, w, o))
+
+
+def test_wp_moments_and_weighted_sad_are_the_sums():
+    rng = np.random.default_rng(5)
+    cur = random_picture(rng, 70, 46, 10)
+    ref = random_picture(rng, 70, 46, 10)
+    m = oracle.wp_moments(HEVC, 10, cur, ref)
+    r, c = ref.astype(np.int64), cur.astype(np.int64)
+    assert list(m) == [r.sum(), c.sum(), (r * r).sum(), (r * c).sum(), np.abs(c - r).sum()]
+    for wt, sh, off in [(64, 6, 0), (80, 6, -12), (-5, 0, 300), (3, 1, 0)]:
+        rnd = 1 << (sh - 1) if sh >= 1 else 0
+        p = np.clip(((r * wt + rnd) >> sh) + off, 0, 1023)
+        assert oracle.weighted_sad(HEVC, 10, cur, ref, wt, sh, off) == np.abs(p - c).sum()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("codec,bd,w,h,log_wd,wt,o", [(H264, 8, 352, 288, 5, 40, -7), (H264, 10, 200, 136, 0, 1, 12),
+                                                       (HEVC, 8, 416, 240, 12, 70, 3),
+                                                       (HEVC, 10, 192, 128, 10, 50, -40)])
+def test_weighted_planes_match_the_oracle(ms, codec, bd, w, h, log_wd, wt, o):
+    """The weighted plane 0 over the whole padded area, and the search planes
+    built from it (the oracle's planes of the weighted picture)."""
+    rng = np.random.default_rng(w + bd)
+    pic = random_picture(rng, w, h, bd)
+    ms.upload(1500, pic, codec, bd, as_ref=True)
+    ms.picture_weighted(1500, 1501, log_wd, wt, o)
+    if codec == H264:
+        base = oracle.h264_planes(pic, bd)
+        want = oracle.h264_planes(oracle.weighted_samples(codec, bd, pic, log_wd, wt, o), bd)
+        rows, cols = base.shape[1:]
+        np.testing.assert_array_equal(ms.plane(1501, 0), oracle.weighted_samples(codec, bd, base[0], log_wd, wt, o))
+        for k in range(1, 4):
+            ys = slice(2, rows - 3) if k in (2, 3) else slice(0, rows)
+            xs = slice(2, cols - 3) if k in (1, 3) else slice(0, cols)
+            np.testing.assert_array_equal(ms.plane(1501, k)[ys, xs], want[k][ys, xs], err_msg=f"plane {k}")
+    else:
+        base, _ = oracle.hevc_planes(pic, bd)
+        np.testing.assert_array_equal(ms.plane(1501, 0), oracle.weighted_samples(codec, bd, base[0], log_wd, wt, o))
+        want, ext = oracle.hevc_planes(oracle.weighted_samples(codec, bd, pic, log_wd, wt, o), bd, force_quarter=True)
+        sl = (slice(80 - ext, 80 + h + ext), slice(80 - ext, 80 + w + ext))
+        for k in range(1, 16):
+            np.testing.assert_array_equal(ms.plane(1501, k)[sl], want[k][sl], err_msg=f"phase {k}")
+    ms.release(1500)
+    ms.release(1501)
+
+
+@pytest.mark.gpu
+def test_search_on_a_weighted_h264_reference(ms):
+    """GIVEN H.264 jobs against the weighted plane equal the oracle's search
+    with the weighted picture as the reference (what PRef::search scores)."""
+    rng = np.random.default_rng(17)
+    ref = random_picture(rng, 352, 288, 8)
+    src = shifted(ref, 3, -2, rng, 1.5)
+    ms.upload(1600, src, H264, 8, as_ref=False)
+    ms.upload(1601, ref, H264, 8, as_ref=True)
+    ms.picture_weighted(1601, 1602, 6, 72, -9)
+    p = oracle.params(H264, 27, predictor_mode=capi.RME_PRED_GIVEN)
+    jobs = random_jobs(rng, H264, 352, 288, 1, 150)
+    got = ms.search(1600, [1602], p, jobs)
+    want = oracle.frame_search(H264, 8, src, [oracle.weighted_samples(H264, 8, ref, 6, 72, -9)], p, jobs)
+    assert (got == want).all()
+    for i in range(3):
+        ms.release(1600 + i)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("bd,w,h", [(8, 1920, 1080), (10, 352, 288)])
+def test_wp_moments_and_weighted_sad_on_the_device(ms, bd, w, h):
+    rng = np.random.default_rng(w * bd)
+    ref = random_picture(rng, w, h, bd)
+    cur = shifted(ref, 1, 1, rng, 3.0)
+    ms.upload(1700, cur, HEVC, bd, as_ref=False)
+    ms.upload(1701, ref, HEVC, bd, as_ref=True)
+    np.testing.assert_array_equal(ms.wp_moments(1700, 1701), oracle.wp_moments(HEVC, bd, cur, ref))
+    for wt, sh, off in [(64, 6, 0), (80, 6, -12), (-5, 0, 300)]:
+        assert ms.weighted_sad(1700, 1701, wt, sh, off) == oracle.weighted_sad(HEVC, bd, cur, ref, wt, sh, off)
+    ms.release(1700)
+    ms.release(1701)
