@@ -331,6 +331,37 @@ int rme_bi_satd(void* ctx, const rme_frame* f, const rme_params* p, const rme_bi
 int rme_bi_refine(void* ctx, const rme_frame* f, const rme_params* p, const rme_bi_job* jobs, int32_t n,
                   rme_result* out, void* stream);
 
+/* ---- B macroblocks: the joint bi refinement (H.264) --------------------- */
+
+/* One pair to refine jointly: a block of a B macroblock, each list's
+ * reference (indexes into the frame's ref_ids), the pair's start vectors
+ * and each list's rate predictor, and `limit`: a pair whose start already
+ * costs more is left as it is (b_mb's bi_ratio gate; UINT32_MAX refines
+ * every pair). */
+typedef struct {
+  int32_t x, y;        /* block position in luma samples                   */
+  int32_t w, h;        /* 4, 8 or 16 each                                  */
+  int32_t ref[2];      /* list 0's and list 1's reference                  */
+  rme_mv  mv[2];       /* start vectors, quarter samples                   */
+  rme_mv  mvp[2];      /* each list's predictor (MvCostTable::of)          */
+  uint32_t limit;
+} rme_h264_bi_job;
+
+/* b_mb's bi_refine (h264_analyse.rs:2793-2900) per job, default weighting:
+ * cost = SATD of the two lists' quarter-sample predictions averaged,
+ * (p0 + p1 + 1) >> 1, plus both vectors' MvCostTable rates at the params'
+ * QP; then up to `rounds` rounds, each list in turn: the ring of 8 points
+ * (4 with `diamond`: bi_refine / bi_diamond) around that list's vector, the
+ * other held, taken in order where strictly cheaper (a point whose rate
+ * alone reaches the best is skipped), until a round moves nothing. Out:
+ * the pair (mv_out, 2 per job) and its cost. Every vector a job can reach
+ * (start +- rounds quarter samples) must lie inside search_bounds of its
+ * reference (the planes the reference scores from; RME_EINVAL otherwise).
+ * Host jobs and outputs, synchronous. */
+int rme_h264_bi_refine(void* ctx, const rme_frame* f, const rme_params* p, const rme_h264_bi_job* jobs,
+                       int32_t n, int32_t rounds, int32_t diamond, rme_mv* mv_out, uint32_t* cost_out,
+                       void* stream);
+
 /* ---- chroma of chosen vectors -------------------------------------------- */
 
 /* Chroma prediction of chosen luma vectors (4:2:0): HEVC predict_block's

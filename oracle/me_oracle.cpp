@@ -950,6 +950,91 @@ LowResS<S> lowres_h264_of(const rme_picture_desc* d, const void* luma) {
   return lowres_h264<S>((const S*)luma, d->width, d->height, d->stride);
 }
 
+// ---- H.264 B macroblocks: the joint bi refinement ----------------------------
+
+// bi_refine (h264_analyse.rs:2793-2900) under default weighting, on the
+// source `src` (coded size, stride ss) and the pair's references.
+template <class S>
+void h264_bi_refine(const Dist<S>& dist, const S* src, ptrdiff_t ss, const H264Ref<S>* const R[2],
+                    const uint16_t* tab, const rme_h264_bi_job& j, int rounds, bool diamond, rme_mv* mv_out,
+                    uint32_t* cost_out) {
+  static const int RING[8][2] = {{0, -1}, {-1, 0}, {1, 0}, {0, 1}, {-1, -1}, {1, -1}, {-1, 1}, {1, 1}};
+  const int x = j.x, y = j.y, w = j.w, h = j.h;
+  const Mv p[2] = {Mv(j.mvp[0].x, j.mvp[0].y), Mv(j.mvp[1].x, j.mvp[1].y)};
+  // satd(r, PRED_BI, ...): each list's MeRef::pred, averaged (avg_into).
+  auto satd_bi = [&](const Mv m[2]) -> uint32_t {
+    S b0[256], b1[256], avg[256];
+    int s0 = 0, s1 = 0;
+    const S* p0 = R[0]->me.pred(x, y, m[0], w, h, b0, &s0);
+    const S* p1 = R[1]->me.pred(x, y, m[1], w, h, b1, &s1);
+    for (int yy = 0; yy < h; ++yy)
+      for (int xx = 0; xx < w; ++xx)
+        avg[yy * w + xx] = (S)(((int)p0[yy * s0 + xx] + (int)p1[yy * s1 + xx] + 1) >> 1);
+    return dist.satd(src + (ptrdiff_t)y * ss + x, ss, avg, w, w, h);
+  };
+  auto rate = [&](const Mv m[2]) -> uint32_t {
+    return h264_mv_comp(tab, m[0].x - p[0].x) + h264_mv_comp(tab, m[0].y - p[0].y) +
+           h264_mv_comp(tab, m[1].x - p[1].x) + h264_mv_comp(tab, m[1].y - p[1].y);
+  };
+  Mv mbi[2] = {Mv(j.mv[0].x, j.mv[0].y), Mv(j.mv[1].x, j.mv[1].y)};
+  uint32_t bi_cost = satd_bi(mbi) + rate(mbi);
+  const int nr = bi_cost > j.limit ? 0 : rounds, npts = diamond ? 4 : 8;
+  for (int it = 0; it < nr; ++it) {
+    const Mv before[2] = {mbi[0], mbi[1]};
+    for (int l = 0; l < 2; ++l) {
+      const Mv c = mbi[l];
+      Mv ms[8][2];
+      uint32_t sc[8];
+      for (int k = 0; k < npts; ++k) {
+        ms[k][0] = mbi[0];
+        ms[k][1] = mbi[1];
+        ms[k][l] = Mv(c.x + RING[k][0], c.y + RING[k][1]);
+        sc[k] = satd_bi(ms[k]);
+      }
+      for (int k = 0; k < npts; ++k) {
+        const uint32_t rc = rate(ms[k]);
+        if (rc >= bi_cost) continue;
+        if (sc[k] + rc < bi_cost) {
+          bi_cost = sc[k] + rc;
+          mbi[0] = ms[k][0];
+          mbi[1] = ms[k][1];
+        }
+      }
+    }
+    if (mbi[0] == before[0] && mbi[1] == before[1]) break;
+  }
+  mv_out[0] = {mbi[0].x, mbi[0].y};
+  mv_out[1] = {mbi[1].x, mbi[1].y};
+  *cost_out = bi_cost;
+}
+
+template <class S>
+int h264_bi_frame(const rme_picture_desc* d, const void* src_luma, int nref, const void* const* refs,
+                  const rme_params* p, const rme_h264_bi_job* jobs, int n, int rounds, int diamond, rme_mv* mv_out,
+                  uint32_t* cost_out) {
+  const int W = d->width, H = d->height, bd = d->bit_depth, CW = (W + 15) / 16 * 16, CH = (H + 15) / 16 * 16;
+  Dist<S> dist = dist_scalar<S>();
+  std::vector<H264Ref<S>> rr(nref);
+  for (int r = 0; r < nref; ++r) h264_prepare_ref(rr[r], (const S*)refs[r], W, H, d->stride, p->h264_pad, bd);
+  auto src = coded_h264((const S*)src_luma, W, H, d->stride, CW, CH);
+  std::vector<uint16_t> tab(MV_TAB);
+  h264_cost_table(h264_lambda_satd(p->qp), tab.data());
+  for (int i = 0; i < n; ++i) {
+    const rme_h264_bi_job& j = jobs[i];
+    // Every vector the job can reach reads inside its search planes.
+    for (int l = 0; l < 2; ++l) {
+      int b[4];
+      h264_search_bounds(CW, CH, p->h264_pad, j.x, j.y, j.w, j.h, INT32_MAX, b);
+      const int lo_x = (j.mv[l].x - rounds) >> 2, hi_x = (j.mv[l].x + rounds) >> 2;
+      const int lo_y = (j.mv[l].y - rounds) >> 2, hi_y = (j.mv[l].y + rounds) >> 2;
+      if (lo_x < b[0] || hi_x >= b[1] || lo_y < b[2] || hi_y >= b[3]) return RME_EINVAL;
+    }
+    const H264Ref<S>* R[2] = {&rr[j.ref[0]], &rr[j.ref[1]]};
+    h264_bi_refine<S>(dist, src.data(), CW, R, tab.data(), j, rounds, diamond != 0, mv_out + 2 * i, cost_out + i);
+  }
+  return 0;
+}
+
 // ---- weighted prediction: search planes and fit moments ---------------------
 
 // wp_moments (dsp/distortion.rs:206-226) over the w x h display area: the
@@ -1074,6 +1159,25 @@ int orc_hevc_bi(const rme_picture_desc* d, const void* src, int32_t nref, const 
   if (refine ? !out : !satd) return RME_EINVAL;
   return d->bit_depth == 8 ? bi_frame<uint8_t>(d, src, nref, refs, p, jobs, n, refine, satd, out)
                            : bi_frame<uint16_t>(d, src, nref, refs, p, jobs, n, refine, satd, out);
+}
+
+// H.264 B pairs: bi_refine per job (mv_out 2 per job, cost_out 1).
+int orc_h264_bi_refine(const rme_picture_desc* d, const void* src, int32_t nref, const void* const* refs,
+                       const rme_params* p, const rme_h264_bi_job* jobs, int32_t n, int32_t rounds, int32_t diamond,
+                       rme_mv* mv_out, uint32_t* cost_out) {
+  if (!valid_desc(d) || d->codec != RME_CODEC_H264 || !p || nref < 1 || nref > RME_MAX_REFS || n < 0 ||
+      rounds < 0 || rounds > 16 || (n > 0 && (!jobs || !mv_out || !cost_out)))
+    return RME_EINVAL;
+  const int CW = (d->width + 15) / 16 * 16, CH = (d->height + 15) / 16 * 16;
+  for (int i = 0; i < n; ++i) {
+    const rme_h264_bi_job& j = jobs[i];
+    if (j.ref[0] < 0 || j.ref[0] >= nref || j.ref[1] < 0 || j.ref[1] >= nref || j.w < 4 || j.h < 4 || j.w > 16 ||
+        j.h > 16 || (j.w & 3) || (j.h & 3) || j.x < 0 || j.y < 0 || j.x + j.w > CW || j.y + j.h > CH)
+      return RME_EINVAL;
+  }
+  return d->bit_depth == 8
+             ? h264_bi_frame<uint8_t>(d, src, nref, refs, p, jobs, n, rounds, diamond, mv_out, cost_out)
+             : h264_bi_frame<uint16_t>(d, src, nref, refs, p, jobs, n, rounds, diamond, mv_out, cost_out);
 }
 
 // Weighted prediction: the fit moments of `cur` against `ref` (out[5]).

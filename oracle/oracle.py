@@ -32,6 +32,9 @@ _SIGS = {
                                    C.POINTER(C.c_uint64)]),
     "orc_weighted_samples": (C.c_int, [C.c_int32, C.c_int32, C.c_void_p, C.c_int64, C.c_int32, C.c_int32,
                                        C.c_int32, C.c_void_p]),
+    "orc_h264_bi_refine": (C.c_int, [_PD, C.c_void_p, C.c_int32, C.POINTER(C.c_void_p), _PP,
+                                     C.POINTER(capi.H264BiJob), C.c_int32, C.c_int32, C.c_int32, C.POINTER(capi.Mv),
+                                     C.POINTER(C.c_uint32)]),
     "orc_frames_search_mt": (C.c_int, [_PD, C.c_int32, C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p),
                                        _PP, C.c_int32, C.c_int32, _PR, C.POINTER(C.c_int64),
                                        C.POINTER(C.c_double), C.POINTER(C.c_double)]),
@@ -144,6 +147,25 @@ def hevc_bi(bit_depth: int, src: np.ndarray, refs, p, jobs: np.ndarray, refine: 
     if rc != 0:
         raise RuntimeError(f"oracle hevc_bi rc={rc}")
     return out if refine else satd
+
+
+def h264_bi_refine(bit_depth: int, src: np.ndarray, refs, p, jobs: np.ndarray, rounds: int = 2,
+                   diamond: bool = False):
+    """b_mb's bi_refine per job: (vectors n x 2 x 2, costs)."""
+    src = np.ascontiguousarray(src)
+    d = desc(capi.RME_CODEC_H264, src, bit_depth)
+    jobs = np.ascontiguousarray(jobs, capi.H264_BI_JOB_DTYPE)
+    refs = [np.ascontiguousarray(r) for r in refs]
+    rp = (C.c_void_p * len(refs))(*[r.ctypes.data for r in refs])
+    mv = np.zeros((len(jobs), 2, 2), np.int16)
+    cost = np.zeros(len(jobs), np.uint32)
+    rc = lib().orc_h264_bi_refine(C.byref(d), src.ctypes.data, len(refs), rp, C.byref(p),
+                                  C.cast(jobs.ctypes.data, C.POINTER(capi.H264BiJob)), len(jobs), rounds,
+                                  int(diamond), C.cast(mv.ctypes.data, C.POINTER(capi.Mv)),
+                                  cost.ctypes.data_as(C.POINTER(C.c_uint32)))
+    if rc != 0:
+        raise RuntimeError(f"oracle h264_bi_refine rc={rc}")
+    return mv, cost
 
 
 def wp_moments(codec: int, bit_depth: int, cur: np.ndarray, ref: np.ndarray) -> np.ndarray:

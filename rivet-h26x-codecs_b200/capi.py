@@ -68,6 +68,11 @@ class BiJob(C.Structure):
                 ("ref", C.c_int32 * 2), ("mv", Mv * 2), ("list", C.c_int32), ("mvp", Mv * 2)]
 
 
+class H264BiJob(C.Structure):
+    _fields_ = [("x", C.c_int32), ("y", C.c_int32), ("w", C.c_int32), ("h", C.c_int32),
+                ("ref", C.c_int32 * 2), ("mv", Mv * 2), ("mvp", Mv * 2), ("limit", C.c_uint32)]
+
+
 class Frame(C.Structure):
     _fields_ = [("src_id", C.c_int32), ("nref", C.c_int32), ("ref_ids", C.c_int32 * RME_MAX_REFS),
                 ("jobs", C.POINTER(Job)), ("njobs", C.c_int32)]
@@ -105,6 +110,9 @@ assert JOB_DTYPE.itemsize == C.sizeof(Job)
 BI_JOB_DTYPE = np.dtype([("x", "<i4"), ("y", "<i4"), ("w", "<i4"), ("h", "<i4"), ("ref", "<i4", (2,)),
                          ("mv", "<i2", (2, 2)), ("list", "<i4"), ("mvp", "<i2", (2, 2))])
 assert BI_JOB_DTYPE.itemsize == C.sizeof(BiJob)
+H264_BI_JOB_DTYPE = np.dtype([("x", "<i4"), ("y", "<i4"), ("w", "<i4"), ("h", "<i4"), ("ref", "<i4", (2,)),
+                              ("mv", "<i2", (2, 2)), ("mvp", "<i2", (2, 2)), ("limit", "<u4")])
+assert H264_BI_JOB_DTYPE.itemsize == C.sizeof(H264BiJob)
 
 # Every entry point include/rivet_me.h declares, with its ctypes signature.
 _vp, _i32, _i64, _u32p = C.c_void_p, C.c_int32, C.c_int64, C.POINTER(C.c_uint32)
@@ -133,6 +141,8 @@ SIGNATURES = {
     "rme_picture_weighted": (C.c_int, [_vp, _i32, _i32, _i32, _i32, _i32, _vp]),
     "rme_wp_moments": (C.c_int, [_vp, _i32, _i32, C.POINTER(C.c_uint64), _vp]),
     "rme_weighted_sad": (C.c_int, [_vp, _i32, _i32, _i32, _i32, _i32, C.POINTER(C.c_uint64), _vp]),
+    "rme_h264_bi_refine": (C.c_int, [_vp, C.POINTER(Frame), C.POINTER(Params), C.POINTER(H264BiJob), _i32, _i32,
+                                     _i32, C.POINTER(Mv), _u32p, _vp]),
     "rme_bi_satd": (C.c_int, [_vp, C.POINTER(Frame), C.POINTER(Params), C.POINTER(BiJob), _i32, _u32p, _vp]),
     "rme_bi_refine": (C.c_int, [_vp, C.POINTER(Frame), C.POINTER(Params), C.POINTER(BiJob), _i32,
                                 C.POINTER(Result), _vp]),

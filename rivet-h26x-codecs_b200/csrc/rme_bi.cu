@@ -175,6 +175,119 @@ __global__ void __launch_bounds__(256) bi_target_kernel(BiDesc B, S* target) {
   }
 }
 
+// ---- H.264 B macroblocks: bi_refine (h264_analyse.rs:2793-2900) -------------
+
+// The quarter-sample positions' plane views (h264_hpel.rs QPEL, 205-281):
+// per position, plane and offset of one view, then of the second view
+// averaged with it (plane -1: one view only). Planes: G, b, h, j.
+__constant__ int8_t c_qpel_views[16][6] = {
+    {0, 0, 0, -1, 0, 0}, {0, 0, 0, 1, 0, 0}, {1, 0, 0, -1, 0, 0}, {1, 0, 0, 0, 1, 0},
+    {0, 0, 0, 2, 0, 0},  {1, 0, 0, 2, 0, 0}, {1, 0, 0, 3, 0, 0},  {1, 0, 0, 2, 1, 0},
+    {2, 0, 0, -1, 0, 0}, {2, 0, 0, 3, 0, 0}, {3, 0, 0, -1, 0, 0}, {3, 0, 0, 2, 1, 0},
+    {2, 0, 0, 0, 0, 1},  {2, 0, 0, 1, 0, 1}, {3, 0, 0, 1, 0, 1},  {2, 1, 0, 1, 0, 1},
+};
+__constant__ int8_t c_bi_ring[8][2] = {{0, -1}, {-1, 0}, {1, 0}, {0, 1}, {-1, -1}, {1, -1}, {-1, 1}, {1, 1}};
+
+// MeRef::pred's sample (row, col) of a block at (x, y) and vector (mx, my).
+template <class S>
+__device__ __forceinline__ int qpel_sample(const DevPlanes& R, int x, int y, int mx, int my, int row, int col) {
+  const int8_t* q = c_qpel_views[(my & 3) * 4 + (mx & 3)];
+  const int xi = x + (mx >> 2) + col, yi = y + (my >> 2) + row;
+  const int a = *plane_ptr<S>(R, q[0], xi + q[1], yi + q[2]);
+  if (q[3] < 0) return a;
+  return (a + (int)*plane_ptr<S>(R, q[3], xi + q[4], yi + q[5]) + 1) >> 1;
+}
+
+struct H264BiDesc {
+  DevPlanes src;
+  DevPlanes ref[RME_MAX_REFS];
+  const uint16_t* tab;  // MvCostTable
+  const rme_h264_bi_job* jobs;
+  int32_t n, rounds, npts;
+  rme_mv* mv_out;
+  uint32_t* cost_out;
+};
+
+__device__ __forceinline__ uint32_t bi_rate(const uint16_t* tab, int m0x, int m0y, int m1x, int m1y,
+                                            const rme_h264_bi_job& j) {
+  auto comp = [&](int d) { return (uint32_t)__ldg(&tab[min(max(d, -kMvSpan), kMvSpan) + kMvSpan]); };
+  return comp(m0x - j.mvp[0].x) + comp(m0y - j.mvp[0].y) + comp(m1x - j.mvp[1].x) + comp(m1y - j.mvp[1].y);
+}
+
+// One warp per pair. A scoring pass gives each of 8 groups of 4 lanes one
+// candidate pair; a lane takes the group's 4x4 tiles sub, sub + 4, ...
+template <class S>
+__global__ void __launch_bounds__(256) h264_bi_kernel(H264BiDesc B) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, sub = lane & 3;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < B.n; i += warps) {
+    const rme_h264_bi_job& j = B.jobs[i];
+    const int x = j.x, y = j.y, w = j.w, h = j.h, tw = w >> 2, ntiles = tw * (h >> 2);
+    const DevPlanes& R0 = B.ref[j.ref[0]];
+    const DevPlanes& R1 = B.ref[j.ref[1]];
+    // The SATD of group g's pair (ok), summed over its four lanes.
+    auto score = [&](bool ok, int m0x, int m0y, int m1x, int m1y) -> uint32_t {
+      uint32_t acc = 0;
+      if (ok)
+        for (int t = sub; t < ntiles; t += 4) {
+          const int ty = t / tw, tx = t - ty * tw;
+          int d[16];
+#pragma unroll
+          for (int e = 0; e < 16; ++e) {
+            const int row = ty * 4 + (e >> 2), col = tx * 4 + (e & 3);
+            const int pr = (qpel_sample<S>(R0, x, y, m0x, m0y, row, col) +
+                            qpel_sample<S>(R1, x, y, m1x, m1y, row, col) + 1) >> 1;
+            d[e] = (int)*plane_ptr<S>(B.src, 0, x + col, y + row) - pr;
+          }
+          acc += hadamard4x4_sum(d);
+        }
+      acc += __shfl_xor_sync(kAll, acc, 1);
+      acc += __shfl_xor_sync(kAll, acc, 2);
+      return acc;
+    };
+    int bx[2] = {j.mv[0].x, j.mv[1].x}, by[2] = {j.mv[0].y, j.mv[1].y};
+    uint32_t cost = __shfl_sync(kAll, score(g == 0, bx[0], by[0], bx[1], by[1]), 0) +
+                    bi_rate(B.tab, bx[0], by[0], bx[1], by[1], j);
+    const int nr = cost > j.limit ? 0 : B.rounds;
+    for (int it = 0; it < nr; ++it) {
+      const int b0x = bx[0], b0y = by[0], b1x = bx[1], b1y = by[1];
+      for (int l = 0; l < 2; ++l) {
+        const int cx = bx[l], cy = by[l];
+        int mx[2] = {bx[0], bx[1]}, my[2] = {by[0], by[1]};
+        mx[l] = cx + c_bi_ring[g][0];
+        my[l] = cy + c_bi_ring[g][1];
+        const uint32_t sc = score(g < B.npts, mx[0], my[0], mx[1], my[1]);
+        // In order, as the reference takes them (all lanes alike).
+        for (int k = 0; k < B.npts; ++k) {
+          const uint32_t s = __shfl_sync(kAll, sc, 4 * k);
+          // The ring is around the list's vector at the ring's start; the
+          // held list's vector does not change within the ring.
+          int kx[2] = {bx[0], bx[1]}, ky[2] = {by[0], by[1]};
+          kx[l] = cx + c_bi_ring[k][0];
+          ky[l] = cy + c_bi_ring[k][1];
+          const uint32_t rc = bi_rate(B.tab, kx[0], ky[0], kx[1], ky[1], j);
+          if (rc >= cost) continue;
+          if (s + rc < cost) {
+            cost = s + rc;
+            bx[0] = kx[0];
+            by[0] = ky[0];
+            bx[1] = kx[1];
+            by[1] = ky[1];
+          }
+        }
+      }
+      if (bx[0] == b0x && by[0] == b0y && bx[1] == b1x && by[1] == b1y) break;
+    }
+    if (lane == 0) {
+      B.mv_out[2 * i].x = (int16_t)bx[0];
+      B.mv_out[2 * i].y = (int16_t)by[0];
+      B.mv_out[2 * i + 1].x = (int16_t)bx[1];
+      B.mv_out[2 * i + 1].y = (int16_t)by[1];
+      B.cost_out[i] = cost;
+    }
+  }
+}
+
 int grid_of(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 7) / 8, 148 * 16)); }
 
 }  // namespace
@@ -184,6 +297,26 @@ cudaError_t launch_bi_satd(const BiDesc& B, uint32_t* satd, cudaStream_t s) {
     bi_satd_kernel<uint8_t><<<grid_of(B.n), 256, 0, s>>>(B, satd);
   else
     bi_satd_kernel<uint16_t><<<grid_of(B.n), 256, 0, s>>>(B, satd);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_h264_bi(const DevPlanes& src, const DevPlanes* refs, int nref, int bd, const uint16_t* tab,
+                           const rme_h264_bi_job* jobs, int n, int rounds, int npts, rme_mv* mv_out,
+                           uint32_t* cost_out, cudaStream_t s) {
+  H264BiDesc B{};
+  B.src = src;
+  for (int r = 0; r < nref; ++r) B.ref[r] = refs[r];
+  B.tab = tab;
+  B.jobs = jobs;
+  B.n = n;
+  B.rounds = rounds;
+  B.npts = npts;
+  B.mv_out = mv_out;
+  B.cost_out = cost_out;
+  if (bd == 8)
+    h264_bi_kernel<uint8_t><<<grid_of(n), 256, 0, s>>>(B);
+  else
+    h264_bi_kernel<uint16_t><<<grid_of(n), 256, 0, s>>>(B);
   return cudaGetLastError();
 }
 

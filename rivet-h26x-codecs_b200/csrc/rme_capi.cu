@@ -193,6 +193,8 @@ struct Ctx {
   DevBuf<rme_bi_job> d_bijobs;        // bi-prediction: jobs, SATDs, refine_bi targets
   DevBuf<uint32_t> d_bisatd;
   DevBuf<uint8_t> d_bitarget;
+  DevBuf<rme_h264_bi_job> d_h264bi;   // H.264 B pairs: jobs, refined vectors
+  DevBuf<rme_mv> d_bimv;
   DevBuf<int32_t> d_cblk;             // chroma: blocks, vectors, output offsets, output
   DevBuf<rme_mv> d_cmv;
   DevBuf<int64_t> d_coff;
@@ -1276,6 +1278,62 @@ int rme_bi_refine(void* ctx, const rme_frame* f, const rme_params* p, const rme_
   rme_params gp = *p;
   gp.predictor_mode = RME_PRED_GIVEN;
   return run_launch(c, &gf, &gp, 1, out, nullptr, s, false, c->d_bitarget.p);
+}
+
+// ---- H.264 B pairs: b_mb's bi_refine (h264_analyse.rs:2793-2900) -------------
+
+int rme_h264_bi_refine(void* ctx, const rme_frame* f, const rme_params* p, const rme_h264_bi_job* jobs, int32_t n,
+                       int32_t rounds, int32_t diamond, rme_mv* mv_out, uint32_t* cost_out, void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return RME_EINVAL;
+  if (!f || !p || n < 0 || (n > 0 && (!jobs || !mv_out || !cost_out))) return fail(c, RME_EINVAL, "null argument");
+  if (rounds < 0 || rounds > 16) return fail(c, RME_EINVAL, "rounds must be 0..16");
+  Picture* src;
+  int rc = picture_of(c, f->src_id, &src);
+  if (rc) return rc;
+  if (src->d.codec != RME_CODEC_H264) return fail(c, RME_EINVAL, "bi refinement jobs are H.264's");
+  if (f->nref < 1 || f->nref > RME_MAX_REFS) return fail(c, RME_EINVAL, "nref must be 1..4");
+  if ((rc = check_params(c, p, src->d))) return rc;
+  DevPlanes refs[RME_MAX_REFS];
+  for (int r = 0; r < f->nref; ++r) {
+    Picture* rp;
+    if ((rc = picture_of(c, f->ref_ids[r], &rp))) return rc;
+    if (!rp->is_ref) return fail(c, RME_EINVAL, "reference picture was uploaded without as_ref");
+    if (rp->d.codec != src->d.codec || rp->d.bit_depth != src->d.bit_depth || rp->d.width != src->d.width ||
+        rp->d.height != src->d.height)
+      return fail(c, RME_EINVAL, "reference format differs from the source's");
+    refs[r] = rp->planes;
+  }
+  for (int i = 0; i < n; ++i) {
+    const rme_h264_bi_job& j = jobs[i];
+    if (j.ref[0] < 0 || j.ref[0] >= f->nref || j.ref[1] < 0 || j.ref[1] >= f->nref || j.w < 4 || j.h < 4 ||
+        j.w > 16 || j.h > 16 || (j.w & 3) || (j.h & 3) || j.x < 0 || j.y < 0 || j.x + j.w > src->cw ||
+        j.y + j.h > src->ch)
+      return fail(c, RME_EINVAL, "bi job " + std::to_string(i) + " out of range");
+    // Every vector the job can reach reads inside its search planes
+    // (search_bounds, h264_hpel.rs:476-488, no vertical limit).
+    const int lx = 4 - p->h264_pad - j.x, hx = src->cw + p->h264_pad - (j.w + 4) - j.x;
+    const int ly = 4 - p->h264_pad - j.y, hy = src->ch + p->h264_pad - (j.h + 4) - j.y;
+    for (int l = 0; l < 2; ++l)
+      if (((j.mv[l].x - rounds) >> 2) < lx || ((j.mv[l].x + rounds) >> 2) >= hx ||
+          ((j.mv[l].y - rounds) >> 2) < ly || ((j.mv[l].y + rounds) >> 2) >= hy)
+        return fail(c, RME_EINVAL, "bi job " + std::to_string(i) + " can reach outside the search planes");
+  }
+  if (n == 0) return 0;
+  const Tables* t = get_tables(c, p, src->d.bit_depth, &rc);
+  if (!t) return rc;
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  CK(cudaSetDevice(c->device));
+  CK(c->d_h264bi.ensure((size_t)n));
+  CK(c->d_bimv.ensure((size_t)2 * n));
+  CK(c->d_bisatd.ensure(n));
+  CK(cudaMemcpyAsync(c->d_h264bi.p, jobs, sizeof(rme_h264_bi_job) * n, cudaMemcpyHostToDevice, s));
+  CK(launch_h264_bi(src->planes, refs, f->nref, src->d.bit_depth, t->tab, c->d_h264bi.p, n, rounds, diamond ? 4 : 8,
+                    c->d_bimv.p, c->d_bisatd.p, s));
+  CK(cudaMemcpyAsync(mv_out, c->d_bimv.p, sizeof(rme_mv) * 2 * n, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(cost_out, c->d_bisatd.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return 0;
 }
 
 int rme_chroma_predict(void* ctx, int32_t ref_id, int32_t nblocks, const int32_t* blocks, const rme_mv* mvs,

@@ -113,6 +113,10 @@ struct BiDesc {
 };
 cudaError_t launch_bi_satd(const BiDesc& B, uint32_t* satd, cudaStream_t s);
 cudaError_t launch_bi_target(const BiDesc& B, void* target, cudaStream_t s);
+// H.264 B pairs' joint refinement (rme_bi.cu): `tab` the MvCostTable.
+cudaError_t launch_h264_bi(const DevPlanes& src, const DevPlanes* refs, int nref, int bd, const uint16_t* tab,
+                           const rme_h264_bi_job* jobs, int n, int rounds, int npts, rme_mv* mv_out,
+                           uint32_t* cost_out, cudaStream_t s);
 
 // The lookahead's half-resolution plane of a picture, whole 8x8 blocks
 // (pw x ph) padded by kLowresPad on every side: HEVC's cutree plane

@@ -161,6 +161,20 @@ class MotionSearch:
                                             C.cast(out.ctypes.data, C.POINTER(capi.Result)), C.c_void_p(stream)))
         return out
 
+    def h264_bi_refine(self, src_id: int, ref_ids: Sequence[int], params: capi.Params, jobs: np.ndarray,
+                       rounds: int = 2, diamond: bool = False, stream: int = 0):
+        """b_mb's joint refinement of B pairs (capi.H264_BI_JOB_DTYPE):
+        (vectors n x 2 x 2 int16, costs)."""
+        jobs = np.ascontiguousarray(jobs, capi.H264_BI_JOB_DTYPE)
+        f = self._frame(src_id, ref_ids)
+        mv = np.zeros((len(jobs), 2, 2), np.int16)
+        cost = np.zeros(len(jobs), np.uint32)
+        self._check(self._lib.rme_h264_bi_refine(self.ctx, C.byref(f), C.byref(params),
+                                                 C.cast(jobs.ctypes.data, C.POINTER(capi.H264BiJob)), len(jobs),
+                                                 rounds, int(diamond), C.cast(mv.ctypes.data, C.POINTER(capi.Mv)),
+                                                 cost.ctypes.data_as(C.POINTER(C.c_uint32)), C.c_void_p(stream)))
+        return mv, cost
+
     def search_batch(self, frames: Sequence[tuple[int, Sequence[int]]],
                      params: capi.Params | Sequence[capi.Params], stream: int = 0, out=None) -> list:
         """Many STANDALONE frames (src_id, ref_ids) in one persistent launch.
