@@ -39,6 +39,7 @@ constexpr int kParts = 4;
 // part's queue, then the counters, the status word and the epoch.
 // The launch header: head and tail of each part's queue (0..7), the
 // counters (8..12), status, epoch, then each part's finished-task count.
+constexpr int64_t kSpecTasks = 200000;  // about two 1080p frames of 2Nx2N PUs, 2 references
 constexpr int kMiscCounters = 8, kMiscStatus = 13, kMiscEpoch = 14, kMiscDone = 16, kMiscWords = 24;
 
 int part_of(const FrameDesc& fd) { return 2 * (fd.bd > 8) + (fd.codec == RME_CODEC_H264); }
@@ -553,8 +554,12 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   int64_t part_tasks[kParts] = {0, 0, 0, 0};
   for (int i = 0; i < n; ++i) part_tasks[part_of(c->h_frames.p[i])] += ntask[i];
   std::vector<std::pair<const int32_t*, int>> pend_copies;  // (template, frame)
+  // A launch of a frame or two is latency-bound: its 8x8 diamonds take two
+  // rounds per step (same results).
+  const bool small_launch = total <= kSpecTasks;
   for (int i = 0; i < n; ++i) {
     FrameDesc& fd = c->h_frames.p[i];
+    fd.spec = small_launch;
     const int part = part_of(fd);
     fd.out = dev_out ? out + (offsets ? offsets[i] : toff[i]) : c->d_out.p + toff[i];
     fd.pending = c->d_pending.p + toff[i];

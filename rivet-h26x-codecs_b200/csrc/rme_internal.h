@@ -46,6 +46,7 @@ struct FrameDesc {
   int32_t size[kMaxLevels], nbx[kMaxLevels], nby[kMaxLevels], base[kMaxLevels + 1];
   int32_t search_range, search_rings, quarter_cross;
   float lam;                 // SATD Lagrangian (rate = (lam * bits as f32) as u32)
+  int32_t spec;              // 8x8 diamonds two rounds per step (small launches: latency)
   // STANDALONE AMP: mode bits, their count, the levels that have AMP units
   // (the first amp_nlev: sizes of 16 or more), and per such level the block
   // index of its first AMP unit (amp_base[0] = base[nlevels]).

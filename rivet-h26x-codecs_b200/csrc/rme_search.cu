@@ -448,6 +448,21 @@ __device__ __forceinline__ uint32_t sad_part(const uint32_t* src, int w, int h, 
   return acc;
 }
 
+// An 8x8 candidate's SAD over two lanes: rows half * 4 .. half * 4 + 3.
+template <class S>
+__device__ __forceinline__ uint32_t sad8_half(const uint32_t* src, const S* rp, int stride, int half) {
+  constexpr int SPW = 4 / sizeof(S), WR = 8 / SPW;
+  uint32_t a[4][WR];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) ldwords<WR>(rp + (ptrdiff_t)(half * 4 + r) * stride, a[r]);
+  uint32_t acc = 0;
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int k = 0; k < WR; ++k) acc += vsad(src[(half * 4 + r) * WR + k], a[r][k], S());
+  return acc;
+}
+
 // SATD: lane `sub` of a group of G lanes takes the 4x4 tiles sub, sub + G,
 // ... (row-major over tw tiles per row) of the candidate whose prediction
 // starts at `pp`; each tile is the Hadamard of dsp/distortion.rs:326-381.
@@ -650,6 +665,7 @@ __device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
   uint32_t bcost = kInf;
   int state = nk > 0 ? 0 : 1, c0 = 0, it = 0, rings = 0;
   bool moved = false;
+  const bool spec = F.spec != 0 && w == 8 && h == 8;
   for (;;) {
     if (state == 1 && it >= 2 * range) {  // the diamond has settled
       if (rings >= F.search_rings) break;
@@ -659,6 +675,51 @@ __device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
       moved = false;
       cxr = bx;
       cyr = by;
+    }
+    if (spec && state == 1) {
+      // 8x8 in a small launch: two diamond rounds per step, fewer dependent
+      // steps on the frame's critical path for more loads per step (a large
+      // launch keeps one round per step: there it costs throughput).
+      // Candidates 0..3 (two lanes each)
+      // are the round around the best; 4..15 the next round's points for
+      // each way the first can move — three new ones each, the fourth being
+      // the best itself, whose cost is known and cannot win. The outcome
+      // and the count are those of the two rounds taken one after another.
+      const int q = lane >> 1, hf = lane & 1;
+      const int j0 = q < 4 ? q : (q - 4) / 3, mm = (q - 4) % 3, m = mm + (mm >= (j0 ^ 1));
+      int fx = bx + (j0 == 0 ? 1 : j0 == 1 ? -1 : 0), fy = by + (j0 == 2 ? 1 : j0 == 3 ? -1 : 0);
+      if (q >= 4) {
+        fx += m == 0 ? 1 : m == 1 ? -1 : 0;
+        fy += m == 2 ? 1 : m == 3 ? -1 : 0;
+      }
+      const bool ok = abs(fx - ox) <= range && abs(fy - oy) <= range && fx >= lox && fx <= hix && fy >= loy &&
+                      fy <= hiy;
+      uint32_t part = ok ? sad8_half<S>(sm.src, org + (ptrdiff_t)fy * stride + fx, stride, hf) : 0u;
+      part += __shfl_xor_sync(kFull, part, 1);
+      const uint32_t cost = ok ? part + hevc_rate(lam, fx * 4, fy * 4, p0x, p0y, p1x, p1y) : kInf;
+      nsad += __popc(__ballot_sync(kFull, ok && hf == 0 && q < 4));
+      const Pick pa = warp_min(q < 4 ? cost : kInf);
+      if (!(pa.cost < bcost)) {
+        it = 2 * range;
+        continue;
+      }
+      const int j = pa.lane >> 1;
+      bcost = pa.cost;
+      bx = __shfl_sync(kFull, fx, pa.lane);
+      by = __shfl_sync(kFull, fy, pa.lane);
+      if (++it >= 2 * range) continue;
+      const bool inb = q >= 4 && j0 == j;
+      nsad += 1u + __popc(__ballot_sync(kFull, inb && ok && hf == 0));
+      const Pick pb = warp_min(inb ? cost : kInf);
+      if (pb.cost < bcost) {
+        bcost = pb.cost;
+        bx = __shfl_sync(kFull, fx, pb.lane);
+        by = __shfl_sync(kFull, fy, pb.lane);
+        ++it;
+      } else {
+        it = 2 * range;
+      }
+      continue;
     }
     int fx, fy;
     bool ok;
