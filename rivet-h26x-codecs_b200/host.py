@@ -126,13 +126,20 @@ class MotionSearch:
         return n.value
 
     def search(self, src_id: int, ref_ids: Sequence[int], params: capi.Params,
-               jobs: np.ndarray | None = None, stream: int = 0) -> np.ndarray:
-        """One frame; results as a structured array (capi.RESULT_DTYPE)."""
+               jobs: np.ndarray | None = None, stream: int = 0, out: np.ndarray | None = None) -> np.ndarray:
+        """One frame; results as a structured array (capi.RESULT_DTYPE):
+        `out` when given (a caller's reused result buffer, at least the
+        result count long), else a new array."""
         if jobs is not None:
             jobs = np.ascontiguousarray(jobs, capi.JOB_DTYPE)
         f = self._frame(src_id, ref_ids, jobs)
         n = self.result_count(src_id, ref_ids, params, jobs)
-        out = np.zeros(n, capi.RESULT_DTYPE)
+        if out is None:
+            out = np.zeros(n, capi.RESULT_DTYPE)
+        elif out.dtype != capi.RESULT_DTYPE or out.size < n or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous RESULT_DTYPE array of at least the result count")
+        else:
+            out = out[:n]
         self._check(self._lib.rme_frame_search(self.ctx, C.byref(f), C.byref(params),
                                                C.cast(out.ctypes.data, C.POINTER(capi.Result)), C.c_void_p(stream)))
         return out
