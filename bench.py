@@ -377,7 +377,7 @@ def run_ours(args, world, rank, local):
     ms.close()
 
 
-def run_served(frames, capacity_fps: float, loads=(0.2, 0.5, 0.8, 1.0, 1.2), seconds: float = 2.0,
+def run_served(frames, capacity_fps: float, loads=(0.2, 0.5, 0.65, 0.8, 1.0, 1.2), seconds: float = 2.0,
                warm_s: float = 0.5, local: int = 0, max_batch: int = 64) -> dict:
     """The serving loop under Poisson load: streams of the 1080p workload at
     30 frames/s each, the total rate a fraction of the measured batched
@@ -446,10 +446,14 @@ def run_served(frames, capacity_fps: float, loads=(0.2, 0.5, 0.8, 1.0, 1.2), sec
                       "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
                       "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None})
         log(f"served load {load:.1f}: {sweep[-1]}")
-    keeps_up = [x for x in sweep if x["served_fps"] >= 0.95 * x["offered_fps"]]
+    # Keeping up: serves what is offered, and no backlog builds (a request
+    # waits at most a few launches).
+    rule = "served >= 0.97 x offered and p99 <= 250 ms"
+    keeps_up = [x for x in sweep if x["served_fps"] >= 0.97 * x["offered_fps"] and x["p99_ms"] is not None
+                and x["p99_ms"] <= 250.0]
     head = max(keeps_up, key=lambda x: x["served_fps"]) if keeps_up else sweep[0]
     return {"value": head["served_fps"], "unit": "frames/s", "load": head["load"], "p50_ms": head["p50_ms"],
-            "p99_ms": head["p99_ms"], "capacity_fps": capacity_fps, "sweep": sweep,
+            "p99_ms": head["p99_ms"], "capacity_fps": capacity_fps, "keeps_up": rule, "sweep": sweep,
             "latency": "submit to results on the host, request loop included"}
 
 
