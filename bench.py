@@ -457,6 +457,127 @@ def run_served(frames, capacity_fps: float, loads=(0.2, 0.5, 0.65, 0.8, 1.0, 1.2
             "latency": "submit to results on the host, request loop included"}
 
 
+def run_rows(local: int = 0):
+    """The rows built beside the headline path, measured on 1080p inputs: per
+    row the synchronous C-ABI call timed on the host (its own copies
+    included) and the oracle's single-thread time on the same input, one
+    JSON line each. The oracle's calls build their reference planes inside;
+    that share is timed on its own (an empty call) and taken out."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    import rivet_h26x_codecs_b200 as rme
+    import rivet_h26x_codecs_b200.capi as capi
+    from rivet_h26x_codecs_b200 import synth
+
+    def per_call(fn, reps):
+        fn()
+        fn()
+        a = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        return (time.perf_counter() - a) / reps
+
+    def line(row, unit, n, gpu_s, cpu_s, note):
+        print(json.dumps({"row": row, "unit": unit, "value": n / gpu_s, "cpu_value": n / cpu_s, "cpu_threads": 1,
+                          "speedup": cpu_s / gpu_s, "gpu_ms_per_call": gpu_s * 1e3, "cpu_ms_per_call": cpu_s * 1e3,
+                          "note": note}), flush=True)
+
+    rng = np.random.default_rng(7)
+    ms = rme.MotionSearch(local)
+    for codec, name in ((capi.RME_CODEC_HEVC, "hevc"), (capi.RME_CODEC_H264, "h264")):
+        seq = synth.make_sequence(codec, WIDTH, HEIGHT, 8, 3, synth.seed_for(1), 64, 160, 2.0)
+        f0, f1, f2 = seq.frames
+        base = 3000 if codec == capi.RME_CODEC_HEVC else 3100
+        for i, f in enumerate((f0, f1, f2)):
+            ms.upload(base + i, f, codec, 8, as_ref=True)
+            ms.lowres_build(base + i)
+        # The lookahead's work for one B picture: its plane, both searches,
+        # the average of two.
+        def gpu_la():
+            ms.lowres_build(base + 2)
+            _, m0, _ = ms.lowres_search(base + 2, base + 1)
+            _, m1, _ = ms.lowres_search(base + 2, base + 0)
+            ms.lowres_bi_cost(base + 2, base + 1, m0, base + 0, m1)
+
+        def cpu_la():
+            oracle.lowres(f2, 8, codec)
+            _, m0, _ = oracle.lowres_search(f2, f1, 8, codec)
+            _, m1, _ = oracle.lowres_search(f2, f0, 8, codec)
+            oracle.lowres_bi_cost(f2, f1, m0, f0, m1, 8, codec)
+
+        line(f"lookahead_{name}", "frames/s", 1, per_call(gpu_la, 20), per_call(cpu_la, 2),
+             "half-resolution plane + intra costs, two block searches, the average-of-two cost "
+             "(the oracle's searches rebuild both pictures' planes)")
+        for i in range(3):
+            ms.release(base + i)
+
+    # HEVC B: every 16x16 unit of a picture, a pair of vectors each.
+    seq = synth.make_sequence(capi.RME_CODEC_HEVC, WIDTH, HEIGHT, 8, 3, synth.seed_for(1), 64, 160, 2.0)
+    r0, r1, src = seq.frames
+    for i, f in enumerate((src, r0, r1)):
+        ms.upload(3200 + i, f, capi.RME_CODEC_HEVC, 8, as_ref=i > 0)
+    ph = hevc_params(oracle)
+    ph.predictor_mode = capi.RME_PRED_GIVEN
+    xs, ys = np.meshgrid(np.arange(0, WIDTH - 15, 16), np.arange(0, HEIGHT - 15, 16))
+    nb = xs.size
+    bj = np.zeros(nb, capi.BI_JOB_DTYPE)
+    bj["x"], bj["y"], bj["w"], bj["h"] = xs.ravel(), ys.ravel(), 16, 16
+    bj["ref"] = (0, 1)
+    bj["mv"] = rng.integers(-48, 49, size=(nb, 2, 2))
+    bj["list"] = rng.integers(2, size=nb)
+    bj["mvp"] = bj["mv"]
+    empty = bj[:0]
+    refs = [r0, r1]
+    cpu_base = per_call(lambda: oracle.hevc_bi(8, src, refs, ph, empty, refine=False), 1)
+    line("bi_satd_hevc", "units/s", nb, per_call(lambda: ms.bi_satd(3200, [3201, 3202], ph, bj), 20),
+         per_call(lambda: oracle.hevc_bi(8, src, refs, ph, bj, refine=False), 1) - cpu_base,
+         "satd_bi_at of every 16x16 unit of a 1080p picture")
+    line("bi_refine_hevc", "units/s", nb, per_call(lambda: ms.bi_refine(3200, [3201, 3202], ph, bj), 10),
+         per_call(lambda: oracle.hevc_bi(8, src, refs, ph, bj, refine=True), 1) - cpu_base,
+         "refine_bi of every 16x16 unit (target build, search_full + refine_subpel at 2 lam)")
+    for i in range(3):
+        ms.release(3200 + i)
+
+    # H.264 B: every macroblock's 16x16 pair, bi_refine's default 2 rounds.
+    seq = synth.make_sequence(capi.RME_CODEC_H264, WIDTH, HEIGHT, 8, 3, synth.seed_for(1), 64, 160, 2.0)
+    r0, r1, src = seq.frames
+    for i, f in enumerate((src, r0, r1)):
+        ms.upload(3300 + i, f, capi.RME_CODEC_H264, 8, as_ref=i > 0)
+    p4 = oracle.params(capi.RME_CODEC_H264, 28, predictor_mode=capi.RME_PRED_GIVEN)
+    xs, ys = np.meshgrid(np.arange(0, WIDTH, 16), np.arange(0, HEIGHT - 15, 16))
+    nb = xs.size
+    hj = np.zeros(nb, capi.H264_BI_JOB_DTYPE)
+    hj["x"], hj["y"], hj["w"], hj["h"] = xs.ravel(), ys.ravel(), 16, 16
+    hj["ref"] = (0, 1)
+    hj["mv"] = rng.integers(-40, 41, size=(nb, 2, 2))
+    hj["mvp"] = hj["mv"]
+    hj["limit"] = 0xFFFFFFFF
+    refs = [r0, r1]
+    cpu_base = per_call(lambda: oracle.h264_bi_refine(8, src, refs, p4, hj[:0], 2), 1)
+    line("bi_refine_h264", "macroblocks/s", nb,
+         per_call(lambda: ms.h264_bi_refine(3300, [3301, 3302], p4, hj, 2), 20),
+         per_call(lambda: oracle.h264_bi_refine(8, src, refs, p4, hj, 2), 1) - cpu_base,
+         "b_mb's joint refinement of every macroblock's 16x16 pair, 2 rounds, square ring")
+
+    # Weighted prediction: the weighted search plane (plane 0 and the
+    # half-sample planes rebuilt), the fit's two passes.
+    def cpu_plane():
+        oracle.h264_planes(oracle.weighted_samples(capi.RME_CODEC_H264, 8, r0, 6, 72, -9), 8)
+
+    import torch
+
+    line("weighted_plane_h264", "pictures/s", 1, per_call(lambda: (ms.picture_weighted(3301, 3303, 6, 72, -9),
+                                                                   torch.cuda.synchronize()), 50),
+         per_call(cpu_plane, 3), "weighted search plane and its b, h, j planes (one 1080p reference)")
+    line("wp_moments", "pictures/s", 1, per_call(lambda: ms.wp_moments(3300, 3301), 100),
+         per_call(lambda: oracle.wp_moments(capi.RME_CODEC_H264, 8, src, r0), 5), "the fit's sums over a picture pair")
+    line("weighted_sad", "pictures/s", 1, per_call(lambda: ms.weighted_sad(3300, 3301, 80, 6, -12), 100),
+         per_call(lambda: oracle.weighted_sad(capi.RME_CODEC_H264, 8, src, r0, 80, 6, -12), 5),
+         "the fit's weighted SAD over a picture pair")
+    for i in range(4):
+        ms.release(3300 + i)
+
+
 def profile_case(kind: str):
     """The cases the ncu captures of the search kernel run on: one 1080p
     frame (2 references, about 130 MB on the device) through the per-frame
@@ -489,12 +610,17 @@ def main():
     ap.add_argument("--ref-frames", type=int, default=8, help="reference arm: frames per step sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop sweep")
+    ap.add_argument("--rows", action="store_true",
+                    help="measure the rows beside the headline path (lookahead, B, weighted) instead")
     ap.add_argument("--profile-case", choices=["frame", "batch"], default=None,
                     help="small case for ncu: one frame (3 pictures) or a batch of 8 frames, searched twice")
     args = ap.parse_args()
     world, rank, local = dist_setup(args)
     if args.profile_case:
         profile_case(args.profile_case)
+        return
+    if args.rows:
+        run_rows(local)
         return
     try:
         if args.impl == "reference":
