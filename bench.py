@@ -513,6 +513,24 @@ def run_rows(local: int = 0):
         line(f"lookahead_{name}", "frames/s", 1, per_call(gpu_la, 20), per_call(cpu_la, 2),
              "half-resolution plane + intra costs, two block searches, the average-of-two cost "
              "(the oracle's searches rebuild both pictures' planes)")
+        # A lookahead's depth at once: every picture against its two
+        # predecessors, all pairs in one launch.
+        more = synth.make_sequence(codec, WIDTH, HEIGHT, 8, 10, synth.seed_for(2), 64, 160, 2.0).frames
+        for i, f in enumerate(more):
+            ms.upload(base + 10 + i, f, codec, 8, as_ref=True)
+            ms.lowres_build(base + 10 + i)
+        pairs = [(base + 10 + t, base + 10 + t - d) for t in range(2, 10) for d in (1, 2)]
+
+        def cpu_pairs():
+            for t in range(2, 10):
+                for d in (1, 2):
+                    oracle.lowres_search(more[t], more[t - d], 8, codec)
+
+        line(f"lookahead_search_batch_{name}", "pairs/s", len(pairs),
+             per_call(lambda: ms.lowres_search_batch(pairs), 20), per_call(cpu_pairs, 1),
+             "16 (picture, reference) block searches in one launch (the oracle's rebuild both planes)")
+        for i in range(10):
+            ms.release(base + 10 + i)
         for i in range(3):
             ms.release(base + i)
 

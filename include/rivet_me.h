@@ -467,6 +467,14 @@ int rme_lowres_info(void* ctx, int32_t pic_id, int32_t* bw, int32_t* bh, uint32_
 int rme_lowres_search(void* ctx, int32_t cur_id, int32_t ref_id, uint32_t* cost, rme_mv* mv, uint32_t* nsad,
                       void* stream);
 
+/* rme_lowres_search over `npairs` (cur_ids[k], ref_ids[k]) pairs in one
+ * launch — a lookahead's estimates of many pictures at once (its depth of
+ * pictures, each against the references it costs). All pictures share one
+ * format. Outputs pair after pair (npairs x blocks each). Host outputs,
+ * synchronous. */
+int rme_lowres_search_batch(void* ctx, int32_t npairs, const int32_t* cur_ids, const int32_t* ref_ids,
+                            uint32_t* cost, rme_mv* mv, uint32_t* nsad, void* stream);
+
 /* The average-of-two cost of every block (HEVC bi_cost,
  * h265_cutree.rs:222-243; H.264 estimate, h264_lookahead.rs:417-432): the
  * SATD against the rounded average of its blocks displaced by mv0 in r0 and

@@ -150,6 +150,8 @@ SIGNATURES = {
     "rme_lowres_build": (C.c_int, [_vp, _i32, _vp]),
     "rme_lowres_info": (C.c_int, [_vp, _i32, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _u32p]),
     "rme_lowres_search": (C.c_int, [_vp, _i32, _i32, _u32p, C.POINTER(Mv), _u32p, _vp]),
+    "rme_lowres_search_batch": (C.c_int, [_vp, _i32, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _u32p,
+                                          C.POINTER(Mv), _u32p, _vp]),
     "rme_lowres_bi_cost": (C.c_int, [_vp, _i32, _i32, C.POINTER(Mv), _i32, C.POINTER(Mv), _u32p, _vp]),
     "rme_sad_batch": (C.c_int, [_vp, _i64, _vp, _vp, _i64, _vp, _i32, _i32, _i32, _i32, _u32p, _vp]),
     "rme_satd_batch": (C.c_int, [_vp, _i64, _vp, _vp, _i64, _vp, _i32, _i32, _i32, _i32, _u32p, _vp]),

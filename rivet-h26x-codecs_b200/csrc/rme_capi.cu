@@ -190,6 +190,7 @@ struct Ctx {
   DevBuf<int32_t> d_ldone;
   DevBuf<uint32_t> d_lcost, d_lsad;
   DevBuf<rme_mv> d_lmv, d_lmv2;
+  DevBuf<LowresDesc> d_lpairs;
   DevBuf<unsigned long long> d_wp;    // weighted prediction: moments, weighted SAD
   DevBuf<rme_bi_job> d_bijobs;        // bi-prediction: jobs, SATDs, refine_bi targets
   DevBuf<uint32_t> d_bisatd;
@@ -1485,16 +1486,26 @@ int lowres_pair(Ctx* c, int32_t a, int32_t b, Picture** pa, Picture** pb) {
 }
 }  // namespace
 
-int rme_lowres_search(void* ctx, int32_t cur_id, int32_t ref_id, uint32_t* cost, rme_mv* mv, uint32_t* nsad,
-                      void* stream) {
+int rme_lowres_search_batch(void* ctx, int32_t npairs, const int32_t* cur_ids, const int32_t* ref_ids, uint32_t* cost,
+                            rme_mv* mv, uint32_t* nsad, void* stream) {
   Ctx* c = (Ctx*)ctx;
-  if (!c || !cost || !mv) return RME_EINVAL;
-  Picture *pc, *pr;
-  int rc = lowres_pair(c, cur_id, ref_id, &pc, &pr);
-  if (rc) return rc;
+  if (!c) return RME_EINVAL;
+  if (npairs < 1 || !cur_ids || !ref_ids || !cost || !mv) return fail(c, RME_EINVAL, "null argument");
+  std::vector<LowresDesc> pairs(2 * (size_t)npairs);
+  for (int k = 0; k < npairs; ++k) {
+    Picture *pc, *pr;
+    int rc = lowres_pair(c, cur_ids[k], ref_ids[k], &pc, &pr);
+    if (rc) return rc;
+    pairs[2 * k] = pc->lr;
+    pairs[2 * k + 1] = pr->lr;
+    const LowresDesc &a = pairs[0], &b = pc->lr;
+    if (b.bw != a.bw || b.bh != a.bh || b.h264 != a.h264 || b.bytes != a.bytes)
+      return fail(c, RME_EINVAL, "the pairs' half-resolution formats differ");
+  }
   cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
   CK(cudaSetDevice(c->device));
-  const int bw = pc->lr.bw, bh = pc->lr.bh, n = bw * bh;
+  const int bw = pairs[0].bw, bh = pairs[0].bh, n = bw * bh;
+  const int64_t total = (int64_t)n * npairs;
   // Claim order: anti-diagonals, each block after its left and above ones.
   if (c->lorder_shape != std::make_pair(bw, bh)) {
     std::vector<int32_t> order;
@@ -1505,26 +1516,33 @@ int rme_lowres_search(void* ctx, int32_t cur_id, int32_t ref_id, uint32_t* cost,
     CK(cudaMemcpy(c->d_lorder.p, order.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice));
     c->lorder_shape = {bw, bh};
   }
-  CK(c->d_ldone.ensure(n + 8));
-  CK(c->d_lcost.ensure(n));
-  CK(c->d_lsad.ensure(n));
-  CK(c->d_lmv.ensure(n));
+  CK(c->d_ldone.ensure(total + 8));
+  CK(c->d_lcost.ensure(total));
+  CK(c->d_lsad.ensure(total));
+  CK(c->d_lmv.ensure(total));
+  CK(c->d_lpairs.ensure(2 * (int64_t)npairs));
+  CK(cudaMemcpyAsync(c->d_lpairs.p, pairs.data(), sizeof(LowresDesc) * pairs.size(), cudaMemcpyHostToDevice, s));
   // done flags, then the claim counter and the status word (one memset).
-  CK(cudaMemsetAsync(c->d_ldone.p, 0, sizeof(int32_t) * (n + 8), s));
-  const int ci = (n + 3) & ~1;  // an 8-byte aligned word after the flags
+  CK(cudaMemsetAsync(c->d_ldone.p, 0, sizeof(int32_t) * (total + 8), s));
+  const int64_t ci = (total + 3) & ~int64_t(1);  // an 8-byte aligned word after the flags
   unsigned long long* counter = reinterpret_cast<unsigned long long*>(c->d_ldone.p + ci);
   uint32_t* status = reinterpret_cast<uint32_t*>(c->d_ldone.p + ci + 2);
-  const int grid = std::max(1, std::min(c->nsm * 4, (n + 7) / 8));
-  CK(launch_lowres_search(pc->lr, pr->lr, c->d_lorder.p, c->d_ldone.p, counter, status, c->d_lcost.p, c->d_lmv.p,
-                          c->d_lsad.p, grid, s));
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(c->nsm * 4, (total + 7) / 8));
+  CK(launch_lowres_search(c->d_lpairs.p, npairs, pairs[0], c->d_lorder.p, c->d_ldone.p, counter, status, c->d_lcost.p,
+                          c->d_lmv.p, c->d_lsad.p, grid, s));
   uint32_t st = 0;
-  CK(cudaMemcpyAsync(cost, c->d_lcost.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(mv, c->d_lmv.p, sizeof(rme_mv) * n, cudaMemcpyDeviceToHost, s));
-  if (nsad) CK(cudaMemcpyAsync(nsad, c->d_lsad.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(cost, c->d_lcost.p, sizeof(uint32_t) * total, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(mv, c->d_lmv.p, sizeof(rme_mv) * total, cudaMemcpyDeviceToHost, s));
+  if (nsad) CK(cudaMemcpyAsync(nsad, c->d_lsad.p, sizeof(uint32_t) * total, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(&st, status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   if (st) return fail(c, RME_EDEVICE, "device status " + std::to_string(st));
   return 0;
+}
+
+int rme_lowres_search(void* ctx, int32_t cur_id, int32_t ref_id, uint32_t* cost, rme_mv* mv, uint32_t* nsad,
+                      void* stream) {
+  return rme_lowres_search_batch(ctx, 1, &cur_id, &ref_id, cost, mv, nsad, stream);
 }
 
 int rme_lowres_bi_cost(void* ctx, int32_t cur_id, int32_t r0_id, const rme_mv* mv0, int32_t r1_id, const rme_mv* mv1,

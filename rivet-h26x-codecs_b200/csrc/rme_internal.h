@@ -131,9 +131,11 @@ struct LowresDesc {
   int32_t h264, bytes;
 };
 cudaError_t launch_lowres_build(const DevPlanes& pic, int bd, int w, int h, const LowresDesc& L, cudaStream_t s);
-cudaError_t launch_lowres_search(const LowresDesc& cur, const LowresDesc& ref, const int32_t* order, int32_t* done,
-                                 unsigned long long* counter, uint32_t* status, uint32_t* cost, rme_mv* mv,
-                                 uint32_t* nsad, int grid, cudaStream_t s);
+// `pairs`: device array of (cur, ref) descriptors of npairs pairs that share
+// the block grid of `first`; per-pair outputs and done flags npairs x blocks.
+cudaError_t launch_lowres_search(const LowresDesc* pairs, int npairs, const LowresDesc& first, const int32_t* order,
+                                 int32_t* done, unsigned long long* counter, uint32_t* status, uint32_t* cost,
+                                 rme_mv* mv, uint32_t* nsad, int grid, cudaStream_t s);
 cudaError_t launch_lowres_bi(const LowresDesc& cur, const LowresDesc& r0, const LowresDesc& r1, const rme_mv* m0,
                              const rme_mv* m1, uint32_t* cost, cudaStream_t s);
 

@@ -140,18 +140,26 @@ __device__ __forceinline__ Pick2 argmin(uint32_t c) {
 // search (h265_cutree.rs:152-216), one warp per block: four candidates per
 // step (group g = lane / 8, lane sub = row), the first least cost taken when
 // strictly below the best, as the reference's in-order scoring.
-__global__ void __launch_bounds__(256) lowres_search_kernel(LowresDesc cur, LowresDesc ref, const int32_t* order,
-                                                            int32_t* done, unsigned long long* counter,
-                                                            uint32_t* status, uint32_t* cost, rme_mv* mv,
-                                                            uint32_t* nsad_out) {
+__global__ void __launch_bounds__(256) lowres_search_kernel(const LowresDesc* pairs, int npairs, const int32_t* order,
+                                                            int32_t* done_all, unsigned long long* counter,
+                                                            uint32_t* status, uint32_t* cost_all, rme_mv* mv_all,
+                                                            uint32_t* nsad_all) {
   const int lane = threadIdx.x & 31, g = lane >> 3, sub = lane & 7;
-  const int n = cur.bw * cur.bh, lim = kLowresPad - 1;
+  const int n = pairs[0].bw * pairs[0].bh, lim = kLowresPad - 1;
   for (;;) {
     unsigned long long i = 0;
     if (lane == 0) i = atomicAdd(counter, 1ull);
     i = __shfl_sync(kAll, i, 0);
-    if (i >= (unsigned long long)n) break;
-    const int packed = __ldg(order + i), bx = packed & 0xffff, by = packed >> 16, b = by * cur.bw + bx;
+    if (i >= (unsigned long long)n * npairs) break;
+    // Claims interleave the pairs in wavefront order: entry e of pair pi is
+    // claim e * npairs + pi, after every block it reads.
+    const int pi = (int)(i % npairs), e = (int)(i / npairs);
+    const LowresDesc cur = pairs[2 * pi], ref = pairs[2 * pi + 1];
+    int32_t* done = done_all + (size_t)pi * n;
+    uint32_t* cost = cost_all + (size_t)pi * n;
+    rme_mv* mv = mv_all + (size_t)pi * n;
+    uint32_t* nsad_out = nsad_all ? nsad_all + (size_t)pi * n : nullptr;
+    const int packed = __ldg(order + e), bx = packed & 0xffff, by = packed >> 16, b = by * cur.bw + bx;
     if (lane == 0) {
       if (bx > 0) wait_done(done, b - 1, status);
       if (by > 0) wait_done(done, b - cur.bw, status);
@@ -355,20 +363,27 @@ struct Row8<uint16_t> {
 // the first least cost taken when strictly below the best (the reference's
 // in-order scoring), the winner's SATD.
 template <class S>
-__global__ void __launch_bounds__(256) lowres_search_h264_kernel(LowresDesc cur, LowresDesc ref, const int32_t* order,
-                                                                 int32_t* done, unsigned long long* counter,
-                                                                 uint32_t* status, uint32_t* cost, rme_mv* mv,
-                                                                 uint32_t* nsad_out) {
+__global__ void __launch_bounds__(256) lowres_search_h264_kernel(const LowresDesc* pairs, int npairs,
+                                                                 const int32_t* order, int32_t* done_all,
+                                                                 unsigned long long* counter, uint32_t* status,
+                                                                 uint32_t* cost_all, rme_mv* mv_all,
+                                                                 uint32_t* nsad_all) {
   const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
-  const int n = cur.bw * cur.bh, lim = kLowresPad - 8;
-  const S* cplane = reinterpret_cast<const S*>(cur.plane);
-  const S* rplane = reinterpret_cast<const S*>(ref.plane);
+  const int n = pairs[0].bw * pairs[0].bh, lim = kLowresPad - 8;
   for (;;) {
     unsigned long long i = 0;
     if (lane == 0) i = atomicAdd(counter, 1ull);
     i = __shfl_sync(kAll, i, 0);
-    if (i >= (unsigned long long)n) break;
-    const int packed = __ldg(order + i), bx = packed & 0xffff, by = packed >> 16, b = by * cur.bw + bx;
+    if (i >= (unsigned long long)n * npairs) break;
+    const int pi = (int)(i % npairs), e = (int)(i / npairs);  // as lowres_search_kernel's claims
+    const LowresDesc cur = pairs[2 * pi], ref = pairs[2 * pi + 1];
+    const S* cplane = reinterpret_cast<const S*>(cur.plane);
+    const S* rplane = reinterpret_cast<const S*>(ref.plane);
+    int32_t* done = done_all + (size_t)pi * n;
+    uint32_t* cost = cost_all + (size_t)pi * n;
+    rme_mv* mv = mv_all + (size_t)pi * n;
+    uint32_t* nsad_out = nsad_all ? nsad_all + (size_t)pi * n : nullptr;
+    const int packed = __ldg(order + e), bx = packed & 0xffff, by = packed >> 16, b = by * cur.bw + bx;
     if (lane == 0) {
       if (bx > 0) wait_done(done, b - 1, status);
       if (by > 0) wait_done(done, b - cur.bw, status);
@@ -527,15 +542,17 @@ cudaError_t launch_lowres_build(const DevPlanes& pic, int bd, int w, int h, cons
   return cudaGetLastError();
 }
 
-cudaError_t launch_lowres_search(const LowresDesc& cur, const LowresDesc& ref, const int32_t* order, int32_t* done,
-                                 unsigned long long* counter, uint32_t* status, uint32_t* cost, rme_mv* mv,
-                                 uint32_t* nsad, int grid, cudaStream_t s) {
-  if (!cur.h264)
-    lowres_search_kernel<<<grid, 256, 0, s>>>(cur, ref, order, done, counter, status, cost, mv, nsad);
-  else if (cur.bytes == 1)
-    lowres_search_h264_kernel<uint8_t><<<grid, 256, 0, s>>>(cur, ref, order, done, counter, status, cost, mv, nsad);
+cudaError_t launch_lowres_search(const LowresDesc* pairs, int npairs, const LowresDesc& first, const int32_t* order,
+                                 int32_t* done, unsigned long long* counter, uint32_t* status, uint32_t* cost,
+                                 rme_mv* mv, uint32_t* nsad, int grid, cudaStream_t s) {
+  if (!first.h264)
+    lowres_search_kernel<<<grid, 256, 0, s>>>(pairs, npairs, order, done, counter, status, cost, mv, nsad);
+  else if (first.bytes == 1)
+    lowres_search_h264_kernel<uint8_t>
+        <<<grid, 256, 0, s>>>(pairs, npairs, order, done, counter, status, cost, mv, nsad);
   else
-    lowres_search_h264_kernel<uint16_t><<<grid, 256, 0, s>>>(cur, ref, order, done, counter, status, cost, mv, nsad);
+    lowres_search_h264_kernel<uint16_t>
+        <<<grid, 256, 0, s>>>(pairs, npairs, order, done, counter, status, cost, mv, nsad);
   return cudaGetLastError();
 }
 

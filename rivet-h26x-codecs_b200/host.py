@@ -253,6 +253,22 @@ class MotionSearch:
                                                 nsad.ctypes.data_as(C.POINTER(C.c_uint32)), None))
         return cost, mv, nsad
 
+    def lowres_search_batch(self, pairs: Sequence[tuple[int, int]]):
+        """lowres_search over many (cur, ref) pairs in one launch: per pair
+        (cost, mv, nsad), as lowres_search returns them."""
+        bw, bh = C.c_int32(), C.c_int32()
+        self._check(self._lib.rme_lowres_info(self.ctx, pairs[0][0], C.byref(bw), C.byref(bh), None))
+        n, k = bw.value * bh.value, len(pairs)
+        cur = np.array([a for a, _ in pairs], np.int32)
+        ref = np.array([b for _, b in pairs], np.int32)
+        cost, nsad = np.zeros((k, n), np.uint32), np.zeros((k, n), np.uint32)
+        mv = np.zeros((k, n, 2), np.int16)
+        self._check(self._lib.rme_lowres_search_batch(
+            self.ctx, k, cur.ctypes.data_as(C.POINTER(C.c_int32)), ref.ctypes.data_as(C.POINTER(C.c_int32)),
+            cost.ctypes.data_as(C.POINTER(C.c_uint32)), C.cast(mv.ctypes.data, C.POINTER(capi.Mv)),
+            nsad.ctypes.data_as(C.POINTER(C.c_uint32)), None))
+        return [(cost[i], mv[i], nsad[i]) for i in range(k)]
+
     def lowres_bi_cost(self, cur_id: int, r0_id: int, mv0: np.ndarray, r1_id: int, mv1: np.ndarray) -> np.ndarray:
         mv0 = np.ascontiguousarray(mv0, np.int16)
         mv1 = np.ascontiguousarray(mv1, np.int16)

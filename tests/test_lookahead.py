@@ -144,3 +144,28 @@ def test_h264_lowres_kernels_match_the_oracle(ms, bd, w, h):
     np.testing.assert_array_equal(bi, oracle.lowres_bi_cost(cur, r0, want0[1], r1, want1[1], bd, H264))
     for i in range(3):
         ms.release(900 + i)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("codec,bd", [(HEVC, 8), (H264, 10)])
+def test_lowres_search_batch_equals_pair_by_pair(ms, codec, bd):
+    """Many (cur, ref) pairs in one launch: each pair's blocks as its own
+    search gives them, and as the oracle's."""
+    rng = np.random.default_rng(31 + bd)
+    pics = [random_picture(rng, 352, 288, bd)]
+    for k in range(4):
+        pics.append(shifted(pics[-1], 3 - k, k - 2, rng, 1.5))
+    for i, pic in enumerate(pics):
+        ms.upload(950 + i, pic, codec, bd, as_ref=False)
+        ms.lowres_build(950 + i)
+    pairs = [(954, 953), (954, 952), (953, 952), (953, 951), (952, 950), (951, 950)]
+    got = ms.lowres_search_batch(pairs)
+    for (c, r), g in zip(pairs, got):
+        single = ms.lowres_search(c, r)
+        for a, b, name in zip(g, single, ("cost", "mv", "nsad")):
+            np.testing.assert_array_equal(a, b, name)
+    want = oracle.lowres_search(pics[4], pics[3], bd, codec)
+    for a, b, name in zip(got[0], want, ("cost", "mv", "nsad")):
+        np.testing.assert_array_equal(a, b, name)
+    for i in range(len(pics)):
+        ms.release(950 + i)
