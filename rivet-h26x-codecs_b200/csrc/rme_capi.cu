@@ -157,7 +157,7 @@ struct Graph {
 
 struct Ctx {
   int device = 0, nsm = 0;
-  int bps[kParts][kSearchVariants] = {};  // resident search blocks per SM, per part and variant
+  int bps[kParts][kSearchVariants][2] = {};  // resident search blocks per SM, per part, variant, form
   // The tuner: per (part, log2 of its task count), each occupancy variant
   // is timed on one real launch of that class, then the fastest is kept.
   struct Tune {
@@ -555,12 +555,8 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   int64_t part_tasks[kParts] = {0, 0, 0, 0};
   for (int i = 0; i < n; ++i) part_tasks[part_of(c->h_frames.p[i])] += ntask[i];
   std::vector<std::pair<const int32_t*, int>> pend_copies;  // (template, frame)
-  // A launch of a frame or two is latency-bound: its 8x8 diamonds take two
-  // rounds per step (same results).
-  const bool small_launch = total <= kSpecTasks;
   for (int i = 0; i < n; ++i) {
     FrameDesc& fd = c->h_frames.p[i];
-    fd.spec = small_launch;
     const int part = part_of(fd);
     fd.out = dev_out ? out + (offsets ? offsets[i] : toff[i]) : c->d_out.p + toff[i];
     fd.pending = c->d_pending.p + toff[i];
@@ -626,6 +622,9 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   }
   int nparts_used = 0;
   for (int k = 0; k < kParts; ++k) nparts_used += part_tasks[k] > 0;
+  // A launch of a frame or two is latency-bound: it runs the latency form
+  // of the search kernel (same results).
+  const bool spec = total <= kSpecTasks;
   int variant[kParts];
   Ctx::Tune* tuning = nullptr;  // the class this launch times, if any
   for (int k = 0; k < kParts; ++k) {
@@ -641,7 +640,7 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
         tuning = &T;
       }
     }
-    if (!c->bps[k][variant[k]]) c->bps[k][variant[k]] = search_blocks_per_sm(part_bytes(k), part_codec(k), variant[k]);
+    if (!c->bps[k][variant[k]][spec]) c->bps[k][variant[k]][spec] = search_blocks_per_sm(part_bytes(k), part_codec(k), variant[k], spec);
     sig.push_back(variant[k]);
   }
   int nparts = 0, order[kParts];
@@ -681,8 +680,8 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
       cudaStream_t sk = j == 0 ? s : c->aux[j];
       if (j > 0) e = cudaStreamWaitEvent(sk, c->ev_fork, 0);
       if (e == cudaSuccess)
-        e = launch_search(Ls[k], part_bytes(k), part_codec(k), variant[k], grid_for(part_tasks[k], c->bps[k][variant[k]]),
-                          sk);
+        e = launch_search(Ls[k], part_bytes(k), part_codec(k), variant[k],
+                          grid_for(part_tasks[k], c->bps[k][variant[k]][spec]), sk, spec);
       if (e == cudaSuccess && j > 0) e = cudaEventRecord(c->ev_join[j], sk);
     }
     for (int j = 1; j < nparts && e == cudaSuccess; ++j) e = cudaStreamWaitEvent(s, c->ev_join[j], 0);

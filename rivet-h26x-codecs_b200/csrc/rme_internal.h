@@ -46,7 +46,6 @@ struct FrameDesc {
   int32_t size[kMaxLevels], nbx[kMaxLevels], nby[kMaxLevels], base[kMaxLevels + 1];
   int32_t search_range, search_rings, quarter_cross;
   float lam;                 // SATD Lagrangian (rate = (lam * bits as f32) as u32)
-  int32_t spec;              // 8x8 diamonds two rounds per step (small launches: latency)
   // STANDALONE AMP: mode bits, their count, the levels that have AMP units
   // (the first amp_nlev: sizes of 16 or more), and per such level the block
   // index of its first AMP unit (amp_base[0] = base[nlevels]).
@@ -143,9 +142,11 @@ cudaError_t launch_lowres_bi(const LowresDesc& cur, const LowresDesc& r0, const 
 // blocks pulling from L's queue. `variant` picks the kernel's occupancy
 // bound: 0, 1, 2 for 2, 3, 4 resident blocks per SM (1 is the default).
 constexpr int kSearchVariants = 3, kDefaultVariant = 1;
+// `spec` picks the latency form (HEVC: 8x8 diamonds two rounds per step)
+// for launches of a frame or two; results are the same.
 cudaError_t launch_search(const LaunchDesc& L, int bytes_per_sample, int codec, int variant, int grid,
-                          cudaStream_t s);
-int search_blocks_per_sm(int bytes_per_sample, int codec, int variant);
+                          cudaStream_t s, bool spec = false);
+int search_blocks_per_sm(int bytes_per_sample, int codec, int variant, bool spec = false);
 cudaError_t launch_chroma(const void* cb, const void* cr, int bd, int codec, int cw, int ch, int cstride,
                           int nblocks, const int32_t* blocks, const rme_mv* mvs, const int64_t* out_off, void* out,
                           cudaStream_t s);

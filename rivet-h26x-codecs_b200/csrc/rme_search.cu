@@ -500,7 +500,8 @@ __device__ __forceinline__ uint32_t satd_part(const uint32_t* src, int wr, int t
 }
 
 // Returns a task it made ready to run next (frame << 24 | task), or -1.
-template <class S>
+// SPEC: the latency kernels' two-rounds-per-step 8x8 diamond.
+template <class S, bool SPEC>
 __device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, WarpSmem<S>& sm, int lane) {
   int r, x, y, w, h, ns;
   int p0x, p0y, p1x, p1y;
@@ -665,7 +666,7 @@ __device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
   uint32_t bcost = kInf;
   int state = nk > 0 ? 0 : 1, c0 = 0, it = 0, rings = 0;
   bool moved = false;
-  const bool spec = F.spec != 0 && w == 8 && h == 8;
+  const bool spec = SPEC && w == 8 && h == 8;
   for (;;) {
     if (state == 1 && it >= 2 * range) {  // the diamond has settled
       if (rings >= F.search_rings) break;
@@ -677,9 +678,10 @@ __device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
       cyr = by;
     }
     if (spec && state == 1) {
-      // 8x8 in a small launch: two diamond rounds per step, fewer dependent
-      // steps on the frame's critical path for more loads per step (a large
-      // launch keeps one round per step: there it costs throughput).
+      // 8x8 in a latency kernel: two diamond rounds per step, fewer
+      // dependent steps on the frame's critical path for more loads per step
+      // (the throughput kernels keep one round per step, and leave this code
+      // out of their text).
       // Candidates 0..3 (two lanes each)
       // are the round around the best; 4..15 the next round's points for
       // each way the first can move — three new ones each, the fourth being
@@ -1323,7 +1325,7 @@ __device__ int h264_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
 // leaves more registers per thread (a single frame's dependency chain runs
 // faster), 4 keeps more warps resident (large batches hide more latency);
 // the host's tuner picks per kind and launch size.
-template <class S, int CODEC, int MINB>
+template <class S, int CODEC, int MINB, bool SPEC>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, MINB) search_kernel(LaunchDesc L) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1357,7 +1359,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, MINB) search_kernel(Launc
       if (lane == 0) atomicOr(L.status, kStatusBadTask);
       continue;
     }
-    if constexpr (CODEC == RME_CODEC_HEVC) cont = hevc_task<S>(L, F, f, t, sm, lane);
+    if constexpr (CODEC == RME_CODEC_HEVC) cont = hevc_task<S, SPEC>(L, F, f, t, sm, lane);
     else cont = h264_task<S>(L, F, f, t, sm, lane);
     if (lane == 0 && L.done != nullptr) red_add64(L.done, 1ull);
   }
@@ -1370,53 +1372,63 @@ size_t smem_bytes() {
   return sizeof(WarpSmem<S>) * kWarpsPerBlock;
 }
 
-template <class S, int CODEC, int MINB>
+template <class S, int CODEC, int MINB, bool SPEC>
 int blocks_per_sm() {
   int n = 0;
-  cudaError_t e = cudaFuncSetAttribute(search_kernel<S, CODEC, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem_bytes<S>());
+  cudaError_t e = cudaFuncSetAttribute(search_kernel<S, CODEC, MINB, SPEC>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<S>());
   if (e == cudaSuccess)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, search_kernel<S, CODEC, MINB>, kWarpsPerBlock * 32,
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, search_kernel<S, CODEC, MINB, SPEC>, kWarpsPerBlock * 32,
                                                       smem_bytes<S>());
   return e == cudaSuccess && n > 0 ? n : 1;
 }
 
-template <class S, int CODEC, int MINB>
+template <class S, int CODEC, int MINB, bool SPEC>
 cudaError_t launch(const LaunchDesc& L, int grid, cudaStream_t s) {
-  cudaError_t e = cudaFuncSetAttribute(search_kernel<S, CODEC, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem_bytes<S>());
+  cudaError_t e = cudaFuncSetAttribute(search_kernel<S, CODEC, MINB, SPEC>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<S>());
   if (e != cudaSuccess) return e;
-  search_kernel<S, CODEC, MINB><<<grid, kWarpsPerBlock * 32, smem_bytes<S>(), s>>>(L);
+  search_kernel<S, CODEC, MINB, SPEC><<<grid, kWarpsPerBlock * 32, smem_bytes<S>(), s>>>(L);
   return cudaGetLastError();
 }
 
-template <class S, int CODEC>
+// The latency kernels (SPEC) exist for HEVC only; H.264 runs its one form.
+template <class S, int CODEC, bool SPEC>
 int bps_variant(int v) {
-  return v == 0 ? blocks_per_sm<S, CODEC, 2>() : v == 2 ? blocks_per_sm<S, CODEC, 4>() : blocks_per_sm<S, CODEC, 3>();
+  return v == 0 ? blocks_per_sm<S, CODEC, 2, SPEC>() : v == 2 ? blocks_per_sm<S, CODEC, 4, SPEC>()
+                                                              : blocks_per_sm<S, CODEC, 3, SPEC>();
 }
-template <class S, int CODEC>
+template <class S, int CODEC, bool SPEC>
 cudaError_t launch_variant(const LaunchDesc& L, int v, int grid, cudaStream_t s) {
-  return v == 0 ? launch<S, CODEC, 2>(L, grid, s) : v == 2 ? launch<S, CODEC, 4>(L, grid, s)
-                                                           : launch<S, CODEC, 3>(L, grid, s);
+  return v == 0 ? launch<S, CODEC, 2, SPEC>(L, grid, s) : v == 2 ? launch<S, CODEC, 4, SPEC>(L, grid, s)
+                                                                 : launch<S, CODEC, 3, SPEC>(L, grid, s);
 }
 
 }  // namespace
 
-int search_blocks_per_sm(int bytes_per_sample, int codec, int variant) {
-  if (codec == RME_CODEC_HEVC)
-    return bytes_per_sample == 1 ? bps_variant<uint8_t, RME_CODEC_HEVC>(variant)
-                                 : bps_variant<uint16_t, RME_CODEC_HEVC>(variant);
-  return bytes_per_sample == 1 ? bps_variant<uint8_t, RME_CODEC_H264>(variant)
-                               : bps_variant<uint16_t, RME_CODEC_H264>(variant);
+int search_blocks_per_sm(int bytes_per_sample, int codec, int variant, bool spec) {
+  if (codec == RME_CODEC_HEVC) {
+    if (spec)
+      return bytes_per_sample == 1 ? bps_variant<uint8_t, RME_CODEC_HEVC, true>(variant)
+                                   : bps_variant<uint16_t, RME_CODEC_HEVC, true>(variant);
+    return bytes_per_sample == 1 ? bps_variant<uint8_t, RME_CODEC_HEVC, false>(variant)
+                                 : bps_variant<uint16_t, RME_CODEC_HEVC, false>(variant);
+  }
+  return bytes_per_sample == 1 ? bps_variant<uint8_t, RME_CODEC_H264, false>(variant)
+                               : bps_variant<uint16_t, RME_CODEC_H264, false>(variant);
 }
 
-cudaError_t launch_search(const LaunchDesc& L, int bytes_per_sample, int codec, int variant, int grid,
-                          cudaStream_t s) {
-  if (codec == RME_CODEC_HEVC)
-    return bytes_per_sample == 1 ? launch_variant<uint8_t, RME_CODEC_HEVC>(L, variant, grid, s)
-                                 : launch_variant<uint16_t, RME_CODEC_HEVC>(L, variant, grid, s);
-  return bytes_per_sample == 1 ? launch_variant<uint8_t, RME_CODEC_H264>(L, variant, grid, s)
-                               : launch_variant<uint16_t, RME_CODEC_H264>(L, variant, grid, s);
+cudaError_t launch_search(const LaunchDesc& L, int bytes_per_sample, int codec, int variant, int grid, cudaStream_t s,
+                          bool spec) {
+  if (codec == RME_CODEC_HEVC) {
+    if (spec)
+      return bytes_per_sample == 1 ? launch_variant<uint8_t, RME_CODEC_HEVC, true>(L, variant, grid, s)
+                                   : launch_variant<uint16_t, RME_CODEC_HEVC, true>(L, variant, grid, s);
+    return bytes_per_sample == 1 ? launch_variant<uint8_t, RME_CODEC_HEVC, false>(L, variant, grid, s)
+                                 : launch_variant<uint16_t, RME_CODEC_HEVC, false>(L, variant, grid, s);
+  }
+  return bytes_per_sample == 1 ? launch_variant<uint8_t, RME_CODEC_H264, false>(L, variant, grid, s)
+                               : launch_variant<uint16_t, RME_CODEC_H264, false>(L, variant, grid, s);
 }
 
 }  // namespace rme
