@@ -601,6 +601,83 @@ def run_rows(local: int = 0):
         ms.release(3300 + i)
 
 
+def run_configs(local: int = 0):
+    """The other workloads of the path, measured as the headline is (one JSON
+    line each): the 2160p 10-bit four-reference stream (±128, AMP units) and
+    the 64-stream mixed batch (one frame of every stream per launch). Each:
+    the batched launch (device-resident, device time of its search) against
+    the plain per-frame path (one synchronous call per frame, host clock),
+    and whether the two agree bit for bit."""
+    import torch
+    import rivet_h26x_codecs_b200 as rme
+    import rivet_h26x_codecs_b200.capi as capi
+    from rivet_h26x_codecs_b200 import synth
+
+    ms = rme.MotionSearch(local)
+
+    def measure(name, frames, params, note):
+        total = ms.batch_result_count(frames, params)
+        dev = torch.empty(total * capi.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=f"cuda:{local}")
+        for _ in range(5):  # the tuner's three trials, the graph's capture, one more
+            outs = ms.search_batch(frames, params, 0, out=dev)
+        torch.cuda.synchronize()
+        ks = []
+        for _ in range(5):
+            ms.search_batch(frames, params, 0, out=dev)
+            ks.append(ms.stats().kernel_ms)
+        batched = [v.cpu().numpy().view(capi.RESULT_DTYPE) for v in outs]
+        plain, lat = [], []
+        for k, (src, refs) in enumerate(frames):
+            ms.search(src, refs, params[k])  # warm each shape
+        for k, (src, refs) in enumerate(frames):
+            a = time.perf_counter()
+            plain.append(ms.search(src, refs, params[k]))
+            lat.append(time.perf_counter() - a)
+        exact = all((b == q).all() for b, q in zip(batched, plain))
+        kms = float(np.median(ks))
+        print(json.dumps({"config": name, "frames_per_launch": len(frames), "batched_fps": len(frames) / kms * 1e3,
+                          "batched_search_ms": kms, "plain_fps": len(frames) / sum(lat),
+                          "plain_p50_ms": float(np.median(lat)) * 1e3, "batched_vs_plain": sum(lat) / kms * 1e3,
+                          "bit_exact_batched_vs_plain": bool(exact), "note": note}), flush=True)
+
+    # 2160p HEVC 10-bit, 4 references, ±128, AMP 2NxnU / nLx2N.
+    seq = synth.config2(nframes=8)
+    p2 = capi.default_params(capi.RME_CODEC_HEVC, QP)
+    p2.hevc_search_range = 128
+    p2.hevc_amp = 0b0101
+    for i, f in enumerate(seq.frames):
+        ms.upload(4000 + i, f, capi.RME_CODEC_HEVC, 10, as_ref=True)
+    frames = [(4000 + t, [4000 + t - 1 - r for r in range(4)]) for t in range(4, 8)]
+    measure("2160p HEVC 10-bit, 4 refs, range 128, PUs 8..64 + AMP 2NxnU/nLx2N", frames, [p2] * len(frames),
+            "4 frames per launch (each against its 4 predecessors)")
+    for i in range(len(seq.frames)):
+        ms.release(4000 + i)
+    del seq
+
+    # The mixed batch: 64 streams, 2 references each, one frame of each.
+    kinds = [(capi.RME_CODEC_H264, 640, 360, 8, 32, 16), (capi.RME_CODEC_HEVC, 1280, 720, 8, 64, 24),
+             (capi.RME_CODEC_HEVC, 1920, 1080, 10, 64, 16), (capi.RME_CODEC_HEVC, 3840, 2160, 8, 128, 8)]
+    frames, params, pid, stream = [], [], 5000, 0
+    for codec, w, h, bd, rng_, count in kinds:
+        for _ in range(count):
+            seq = synth.stream_sequence(codec, w, h, bd, 3, stream, config=3)
+            ids = []
+            for f in seq.frames:
+                ms.upload(pid, f, codec, bd, as_ref=True)
+                ids.append(pid)
+                pid += 1
+            q = capi.default_params(codec, 28 if codec == capi.RME_CODEC_H264 else QP)
+            if codec == capi.RME_CODEC_H264:
+                q.h264_range = rng_
+            else:
+                q.hevc_search_range = rng_
+            frames.append((ids[2], [ids[1], ids[0]]))
+            params.append(q)
+            stream += 1
+    measure("64-stream mix: 16x360p H.264 8-bit, 24x720p HEVC 8-bit, 16x1080p HEVC 10-bit, 8x2160p HEVC 8-bit",
+            frames, params, "one frame of every stream per launch, 2 references each; four kinds on forked streams")
+
+
 def profile_case(kind: str):
     """The cases the ncu captures of the search kernel run on: one 1080p
     frame (2 references, about 130 MB on the device) through the per-frame
@@ -633,6 +710,8 @@ def main():
     ap.add_argument("--ref-frames", type=int, default=8, help="reference arm: frames per step sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop sweep")
+    ap.add_argument("--configs", action="store_true",
+                    help="measure the 2160p 10-bit stream and the 64-stream mixed batch instead")
     ap.add_argument("--rows", action="store_true",
                     help="measure the rows beside the headline path (lookahead, B, weighted) instead")
     ap.add_argument("--profile-case", choices=["frame", "batch"], default=None,
@@ -644,6 +723,9 @@ def main():
         return
     if args.rows:
         run_rows(local)
+        return
+    if args.configs:
+        run_configs(local)
         return
     try:
         if args.impl == "reference":
