@@ -462,6 +462,125 @@ def run_served(frames, capacity_fps: float, loads=(0.2, 0.5, 0.65, 0.8, 1.0, 1.2
             "latency": "submit to results on the host, request loop included"}
 
 
+def run_served_mix(local: int = 0, nstreams: int = 200, loads=(0.2, 0.5, 0.8, 1.0, 1.2), seconds: float = 3.0,
+                   warm_s: float = 1.0, max_batch: int = 64):
+    """The serving loop over a mixed population: `nstreams` streams, each of a
+    size from {360p, 720p, 1080p, 2160p}, a depth from {8, 10} and a codec
+    from {H.264, HEVC} drawn uniformly (seeded), admitted against a 120 GB
+    HBM budget; Poisson arrivals over the admitted streams at a total rate of
+    a fraction of the mix's batched capacity (a 64-frame launch drawn from
+    the same population). One JSON line: admission, capacity, the sweep."""
+    import torch
+    import rivet_h26x_codecs_b200 as rme
+    import rivet_h26x_codecs_b200.capi as capi
+    from rivet_h26x_codecs_b200 import synth
+
+    sizes = [(640, 360, 32), (1280, 720, 64), (1920, 1080, 64), (3840, 2160, 128)]
+    kinds = [(c, w, h, bd, r) for (w, h, r) in sizes for bd in (8, 10) for c in (capi.RME_CODEC_H264,
+                                                                                 capi.RME_CODEC_HEVC)]
+    rng = np.random.default_rng(4)
+    skind = rng.integers(len(kinds), size=nstreams)
+    pools = {}
+    for k in sorted(set(skind.tolist())):
+        c, w, h, bd, _ = kinds[k]
+        pools[k] = synth.stream_sequence(c, w, h, bd, 6, k, config=4).frames
+
+    def params_of(k):
+        c, w, h, bd, r = kinds[k]
+        q = capi.default_params(c, 28 if c == capi.RME_CODEC_H264 else QP)
+        if c == capi.RME_CODEC_H264:
+            q.h264_range = min(r, 32)
+        else:
+            q.hevc_search_range = r
+        return q
+
+    # The mix's batched capacity: one launch of 64 frames drawn from the
+    # population (device search time).
+    with rme.MotionSearch(local) as ms:
+        frames, params, pid = [], [], 9000
+        for k in rng.choice(skind, size=max_batch):
+            c, w, h, bd, _ = kinds[k]
+            ids = []
+            for f in pools[k][:3]:
+                ms.upload(pid, f, c, bd, as_ref=True)
+                ids.append(pid)
+                pid += 1
+            frames.append((ids[2], [ids[1], ids[0]]))
+            params.append(params_of(k))
+        total = ms.batch_result_count(frames, params)
+        dev = torch.empty(total * capi.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=f"cuda:{local}")
+        ks = []
+        for i in range(8):
+            ms.search_batch(frames, params, 0, out=dev)
+            if i >= 5:
+                ks.append(ms.stats().kernel_ms)
+        capacity = max_batch / float(np.median(ks)) * 1e3
+    del dev
+    torch.cuda.empty_cache()
+    per_stream = 4
+    sweep, admitted = [], 0
+    for load in loads:
+        with rme.MotionSearch(local) as ms:
+            srv = rme.Server(ms, hbm_budget_bytes=120 << 30, max_frames_per_launch=max_batch, max_streams=1024)
+            try:
+                live = []
+                for sid in range(nstreams):
+                    c, w, h, bd, _ = kinds[skind[sid]]
+                    if srv.open_stream(sid, c, bd, w, h, params_of(skind[sid]), NREF) == 0:
+                        live.append(sid)
+                admitted = len(live)
+                bufs = {}
+                nxt = {}
+                for sid in live:
+                    pool = pools[skind[sid]]
+                    for t in range(NREF + per_stream):
+                        srv.submit(sid, pool[t % len(pool)])
+                    nxt[sid] = NREF + per_stream
+                    n = srv.result_count(sid)
+                    bufs[sid] = [np.zeros(n, capi.RESULT_DTYPE) for _ in range(4)]
+                pending = len(live) * (NREF + per_stream)
+                deadline = time.perf_counter() + 300
+                while pending and time.perf_counter() < deadline:
+                    pending -= len(srv.poll())
+                    time.sleep(0.001)
+                rate = load * capacity / len(live)
+                events = []
+                for sid in live:
+                    t = rng.exponential(1 / rate)
+                    while t < warm_s + seconds:
+                        events.append((t, sid))
+                        t += rng.exponential(1 / rate)
+                events.sort()
+                measured, done = set(), []
+                t0 = time.perf_counter()
+                for at, sid in events:
+                    while time.perf_counter() - t0 < at:
+                        done += srv.poll()
+                        time.sleep(0.0002)
+                    pool = pools[skind[sid]]
+                    rid = srv.submit(sid, pool[nxt[sid] % len(pool)], out=bufs[sid][nxt[sid] % 4])
+                    nxt[sid] += 1
+                    if at >= warm_s:
+                        measured.add(rid)
+                deadline = time.perf_counter() + 120
+                while len(done) < len(events) and time.perf_counter() < deadline:
+                    done += srv.poll()
+                    time.sleep(0.0005)
+            finally:
+                srv.stop()
+        ok = [d for d in done if d["status"] == 0 and d["id"] in measured]
+        lat = np.array([d["done_s"] - d["submit_s"] for d in ok]) * 1e3
+        span = max(d["done_s"] for d in ok) - min(d["submit_s"] for d in ok) if ok else 1.0
+        sweep.append({"load": load, "offered_fps": len(measured) / seconds, "served_fps": len(ok) / span,
+                      "completed": len(ok), "submitted": len(measured),
+                      "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
+                      "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None})
+        log(f"served mix load {load:.1f}: {sweep[-1]}")
+    print(json.dumps({"workload": "serving mix: sizes 360p..2160p, 8/10-bit, H.264/HEVC, 2 refs",
+                      "streams": nstreams, "admitted": admitted, "hbm_budget_gb": 120,
+                      "capacity_fps": capacity, "sweep": sweep}), flush=True)
+
+
 def run_rows(local: int = 0):
     """The rows built beside the headline path, measured on 1080p inputs: per
     row the synchronous C-ABI call timed on the host (its own copies
@@ -710,6 +829,8 @@ def main():
     ap.add_argument("--ref-frames", type=int, default=8, help="reference arm: frames per step sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop sweep")
+    ap.add_argument("--served-mix", action="store_true",
+                    help="the serving loop over the mixed 200-stream population instead")
     ap.add_argument("--configs", action="store_true",
                     help="measure the 2160p 10-bit stream and the 64-stream mixed batch instead")
     ap.add_argument("--rows", action="store_true",
@@ -726,6 +847,9 @@ def main():
         return
     if args.configs:
         run_configs(local)
+        return
+    if args.served_mix:
+        run_served_mix(local)
         return
     try:
         if args.impl == "reference":
