@@ -765,15 +765,15 @@ def run_configs(local: int = 0):
                           "bit_exact_batched_vs_plain": bool(exact), "note": note}), flush=True)
 
     # 2160p HEVC 10-bit, 4 references, ±128, AMP 2NxnU / nLx2N.
-    seq = synth.config2(nframes=8)
+    seq = synth.config2(nframes=12)
     p2 = capi.default_params(capi.RME_CODEC_HEVC, QP)
     p2.hevc_search_range = 128
     p2.hevc_amp = 0b0101
     for i, f in enumerate(seq.frames):
         ms.upload(4000 + i, f, capi.RME_CODEC_HEVC, 10, as_ref=True)
-    frames = [(4000 + t, [4000 + t - 1 - r for r in range(4)]) for t in range(4, 8)]
+    frames = [(4000 + t, [4000 + t - 1 - r for r in range(4)]) for t in range(4, 12)]
     measure("2160p HEVC 10-bit, 4 refs, range 128, PUs 8..64 + AMP 2NxnU/nLx2N", frames, [p2] * len(frames),
-            "4 frames per launch (each against its 4 predecessors)")
+            "8 frames of the stream per launch (each against its 4 predecessors: source pictures, all known)")
     for i in range(len(seq.frames)):
         ms.release(4000 + i)
     del seq
