@@ -115,6 +115,17 @@ def hevc_params(oracle_mod=None):
     return p
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (/proc/cpuinfo), for the baseline's row."""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_baseline(frames, threads: int, simd: int = 1):
     """The oracle (C++ restatement, AVX2 rungs) over `threads` frames on as
     many host threads: frames/s including their reference plane builds."""
@@ -189,7 +200,7 @@ def run_reference(args, world, rank):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
         "config": {"workload": "hevc-1080p-8bit-2ref-pu8to64-range64-qp32", "frames_per_step": done // args.steps,
                    "note": "bounded sample: one 1080p frame per host thread per step"},
-        "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": threads, "kind": "port",
+        "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": threads, "kind": "port", "cpu_model": cpu_model(),
                          "sample": f"{done // args.steps} frames of the 1080p workload per step, one per thread, "
                                    "reference plane builds included"},
         "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -361,7 +372,7 @@ def run_ours(args, world, rank, local):
         cpu = {"value": fps_all, "unit": "frames/s", "cores": threads, "kind": "port",
                "sample": f"{n_all} frames of the workload, one per host thread, AVX2 rungs, "
                          "reference plane builds included",
-               "value_1_thread": fps_1}
+               "value_1_thread": fps_1, "cpu_model": cpu_model()}
 
     if rank == 0:
         lat_ms = np.array(lat) * 1e3
