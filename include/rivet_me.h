@@ -522,6 +522,14 @@ int rme_search_given_noalloc(const rme_picture_desc* d, const rme_params* p, con
  * search kernel, which is integer work with no tensor-core content. */
 int rme_probe_int_peak(int32_t device, double* ops_per_s);
 
+/* The failure path of the library's bounded device waits (no counterpart
+ * in the reference, whose ME does not wait on a device): one wait of the
+ * lookahead's wavefront on a flag that nothing sets, limited to `polls`
+ * polls (1..2^22, with back-off up to 256 ns each). It gives up, `status`
+ * gets the timeout bit the searches report as RME_EDEVICE (1), and the
+ * device stays usable; `seconds` (may be NULL) is how long the wait took. */
+int rme_probe_wait_timeout(int32_t device, uint32_t polls, uint32_t* status, double* seconds);
+
 #ifdef __cplusplus
 }
 #endif

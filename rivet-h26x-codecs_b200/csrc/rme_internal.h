@@ -101,6 +101,9 @@ cudaError_t launch_wp_moments(const void* cur, const void* ref, int stride, int 
                               unsigned long long* out, cudaStream_t s);
 cudaError_t launch_weighted_sad(const void* cur, const void* ref, int stride, int bd, int w, int h, int weight,
                                 int shift, int offset, unsigned long long* out, cudaStream_t s);
+// A bounded dependency wait that runs out (rme_lookahead.cu's wait on a flag
+// nothing sets, `limit` polls): sets kStatusWaitTimeout in *status.
+cudaError_t launch_probe_wait(const int32_t* flag, uint32_t limit, uint32_t* status, cudaStream_t s);
 // HEVC bi-prediction (rme_bi.cu): the jobs of a frame's source and
 // references; refine_bi targets are kBiBlock-wide blocks.
 constexpr int kBiBlock = 64;

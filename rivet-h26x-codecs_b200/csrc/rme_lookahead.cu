@@ -106,10 +106,11 @@ __device__ __forceinline__ void st_release32(int32_t* p, int32_t v) {
   asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// A bounded wait (lane 0) for block b to be done.
-__device__ __forceinline__ bool wait_done(const int32_t* done, int b, uint32_t* status) {
+// A bounded wait (lane 0) for block b to be done: at most `limit` polls,
+// then the status word records the timeout and the wait gives up.
+__device__ __forceinline__ bool wait_done(const int32_t* done, int b, uint32_t* status, uint32_t limit = kSpinLimit) {
   uint32_t ns = 32;
-  for (uint32_t it = 0; it < kSpinLimit; ++it) {
+  for (uint32_t it = 0; it < limit; ++it) {
     if (ld_acquire32(done + b)) return true;
     __nanosleep(ns);
     if (ns < 256) ns <<= 1;
@@ -517,7 +518,18 @@ __global__ void lowres_bi_h264_kernel(LowresDesc cur, LowresDesc r0, LowresDesc 
   cost[b] = satd8x8<S>(src, cur.stride, pred, 8);
 }
 
+// The wavefront's wait on a flag nothing sets, with a short poll limit:
+// the failure path of a dependency that never completes, taken on purpose.
+__global__ void probe_wait_kernel(const int32_t* flag, uint32_t limit, uint32_t* status) {
+  if ((threadIdx.x & 31) == 0) wait_done(flag, 0, status, limit);
+}
+
 }  // namespace
+
+cudaError_t launch_probe_wait(const int32_t* flag, uint32_t limit, uint32_t* status, cudaStream_t s) {
+  probe_wait_kernel<<<1, 32, 0, s>>>(flag, limit, status);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_lowres_build(const DevPlanes& pic, int bd, int w, int h, const LowresDesc& L, cudaStream_t s) {
   dim3 blk(32, 8), grd((L.stride + 31) / 32, (L.ph + 2 * kLowresPad + 7) / 8);

@@ -52,3 +52,32 @@ extern "C" int rme_probe_int_peak(int32_t device, double* ops_per_s) {
   *ops_per_s = (double)blocks * threads * 8.0 * iters * 3.0 / (ms * 1e-3);
   return 0;
 }
+
+// The failure path of the library's bounded waits, taken on purpose: a wait
+// on a flag that nothing sets gives up after `polls` polls and reports it in
+// the status word, and the device stays usable.
+extern "C" int rme_probe_wait_timeout(int32_t device, uint32_t polls, uint32_t* status, double* seconds) {
+  if (!status || polls == 0 || polls > (1u << 22)) return RME_EINVAL;
+  if (cudaSetDevice(device) != cudaSuccess) return RME_ECUDA;
+  int32_t* flag = nullptr;
+  uint32_t* st = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = RME_ECUDA;
+  if (cudaMalloc(&flag, 64) == cudaSuccess && cudaMemset(flag, 0, 64) == cudaSuccess) {
+    st = reinterpret_cast<uint32_t*>(flag + 8);
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0);
+    if (rme::launch_probe_wait(flag, polls, st, nullptr) == cudaSuccess && cudaEventRecord(e1) == cudaSuccess &&
+        cudaMemcpy(status, st, sizeof(uint32_t), cudaMemcpyDeviceToHost) == cudaSuccess) {
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (seconds) *seconds = ms * 1e-3;
+      rc = RME_OK;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  if (flag) cudaFree(flag);
+  return rc;
+}
