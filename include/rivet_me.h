@@ -331,6 +331,18 @@ int rme_bi_satd(void* ctx, const rme_frame* f, const rme_params* p, const rme_bi
 int rme_bi_refine(void* ctx, const rme_frame* f, const rme_params* p, const rme_bi_job* jobs, int32_t n,
                   rme_result* out, void* stream);
 
+/* A weighted list's sub-sample refinement (HEVC): refine_subpel
+ * (h265_me.rs:3868-3922) with every candidate scored by satd_at_weighted's
+ * explicit arm (4057-4073) — the reference's 14-bit prediction through
+ * weighted_uni (dsp/hevc.rs:1036-1062) at log2_wd, weight and offset (the
+ * list's luma weighting, offset at the sample depth) — on the unweighted
+ * reference, as pick_pu does for a weighted list after its whole-sample
+ * search on the weighted plane (rme_picture_weighted). `f` holds GIVEN jobs:
+ * each job's seeds[0] is the whole-sample start, mvp its AMVP pair. One
+ * result per job (int_mv the start). Host jobs and output, synchronous. */
+int rme_hevc_weighted_refine(void* ctx, const rme_frame* f, const rme_params* p, int32_t log2_wd,
+                             int32_t weight, int32_t offset, rme_result* out, void* stream);
+
 /* ---- B macroblocks: the joint bi refinement (H.264) --------------------- */
 
 /* One pair to refine jointly: a block of a B macroblock, each list's

@@ -1144,6 +1144,59 @@ int orc_frame_search(const rme_picture_desc* d, const void* src, int32_t nref, c
              : run_frames<uint16_t>(d, 1, &src, nref, refs, p, simd, 1, out, nullptr, nullptr, nullptr);
 }
 
+// A weighted list's sub-sample refinement (refine_subpel under Explicit
+// weighting, h265_me.rs:3868-3922 with satd_at_weighted): per GIVEN job,
+// from its first seed (a whole-sample vector) with its AMVP pair.
+int orc_hevc_weighted_refine(const rme_picture_desc* d, const void* src, int32_t nref, const void* const* refs,
+                             const rme_params* p, const rme_job* jobs, int32_t n, int32_t log2_wd, int32_t weight,
+                             int32_t offset, rme_result* out) {
+  if (!valid_desc(d) || d->codec != RME_CODEC_HEVC || !p || nref < 1 || nref > RME_MAX_REFS || n < 0 ||
+      (n > 0 && (!jobs || !out)))
+    return RME_EINVAL;
+  auto run = [&](auto tag) {
+    using S = decltype(tag);
+    const int W = d->width, H = d->height, bd = d->bit_depth;
+    Dist<S> dist = dist_scalar<S>();
+    std::vector<HevcRef<S>> rr(nref);
+    for (int r = 0; r < nref; ++r) hevc_prepare_ref(rr[r], (const S*)refs[r], W, H, d->stride, p->hevc_pad, bd);
+    const float lam = hevc_lambda(p->qp, bd, p->hevc_lambda_scale);
+    for (int i = 0; i < n; ++i) {
+      const rme_job& j = jobs[i];
+      HevcSearch<S> sr{&dist, &rr[j.ref].g, nullptr, bd, (const S*)src + (ptrdiff_t)j.y * d->stride + j.x,
+                       d->stride, j.x, j.y, j.w, j.h, lam, {{0, 0}, {0, 0}}};
+      sr.pq[0][0] = j.mvp[0].x;
+      sr.pq[0][1] = j.mvp[0].y;
+      sr.pq[1][0] = j.mvp[1].x;
+      sr.pq[1][1] = j.mvp[1].y;
+      sr.quarter_cross = p->hevc_quarter_cross != 0;
+      sr.wp = true;
+      sr.wp_log2 = log2_wd;
+      sr.wp_w = weight;
+      sr.wp_o = offset;
+      const Mv start(j.seeds[0].x, j.seeds[0].y);
+      uint32_t sat = 0, c = 0;
+      const Mv m = sr.refine_subpel(start, &sat, &c);
+      rme_result& o = out[i];
+      o.mv = {m.x, m.y};
+      o.ref = j.ref;
+      o.cost = c;
+      o.satd = sat;
+      o.int_mv = {start.x, start.y};
+      o.int_cost = 0;
+      o.n_sad = 0;
+      o.n_satd = sr.n_satd;
+    }
+  };
+  for (int i = 0; i < n; ++i)
+    if (jobs[i].ref < 0 || jobs[i].ref >= nref || jobs[i].w < 4 || jobs[i].h < 4 || jobs[i].w > 64 || jobs[i].h > 64 ||
+        (jobs[i].w & 3) || (jobs[i].h & 3) || jobs[i].x < 0 || jobs[i].y < 0 || jobs[i].x + jobs[i].w > d->width ||
+        jobs[i].y + jobs[i].h > d->height || jobs[i].nseeds < 1)
+      return RME_EINVAL;
+  if (d->bit_depth == 8) run(uint8_t{});
+  else run(uint16_t{});
+  return 0;
+}
+
 // HEVC bi-prediction jobs: satd_bi_at per job (refine == 0, into `satd`)
 // or refine_bi per job (refine == 1, into `out`).
 int orc_hevc_bi(const rme_picture_desc* d, const void* src, int32_t nref, const void* const* refs, const rme_params* p,

@@ -743,7 +743,14 @@ struct HevcSearch {
 
   // read_at + satd_at_weighted under default weighting
   // (h265_me.rs:3630-3655, 4039-4074).
+  // Explicit weighting of a weighted list (satd_at_weighted's Explicit arm,
+  // h265_me.rs:4057-4073): every candidate, whole samples included, is the
+  // 14-bit prediction through weighted_uni (dsp/hevc.rs:1036-1062).
+  bool wp = false;
+  int wp_log2 = 0, wp_w = 1, wp_o = 0;
+
   uint32_t satd_at(Mv mv) {
+    if (wp) return satd_weighted(mv);
     ++n_satd;
     int mvx = mv.x, mvy = mv.y;
     if ((mvx & 3) == 0 && (mvy & 3) == 0) {
@@ -759,6 +766,20 @@ struct HevcSearch {
     std::vector<S> pred((size_t)w * h);
     hevc_interp(*refp, x + (mvx >> 2), y + (mvy >> 2), mvx & 3, mvy & 3, w, h, true, bd, p14.data());
     hevc_uni(pred.data(), w, p14.data(), w, h, 14 - bd, (1 << bd) - 1);
+    return dist->satd(src, src_stride, pred.data(), w, w, h);
+  }
+
+  uint32_t satd_weighted(Mv mv) {
+    ++n_satd;
+    const int maxv = (1 << bd) - 1;
+    std::vector<int16_t> p14((size_t)w * h);
+    std::vector<S> pred((size_t)w * h);
+    hevc_interp(*refp, x + (mv.x >> 2), y + (mv.y >> 2), mv.x & 3, mv.y & 3, w, h, true, bd, p14.data());
+    for (size_t i = 0; i < pred.size(); ++i) {
+      const int v = wp_log2 >= 1 ? (((int)p14[i] * wp_w + (1 << (wp_log2 - 1))) >> wp_log2) + wp_o
+                                 : (int)p14[i] * wp_w + wp_o;
+      pred[i] = (S)std::clamp(v, 0, maxv);
+    }
     return dist->satd(src, src_stride, pred.data(), w, w, h);
   }
 

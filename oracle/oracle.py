@@ -35,6 +35,8 @@ _SIGS = {
     "orc_h264_bi_refine": (C.c_int, [_PD, C.c_void_p, C.c_int32, C.POINTER(C.c_void_p), _PP,
                                      C.POINTER(capi.H264BiJob), C.c_int32, C.c_int32, C.c_int32, C.POINTER(capi.Mv),
                                      C.POINTER(C.c_uint32)]),
+    "orc_hevc_weighted_refine": (C.c_int, [_PD, C.c_void_p, C.c_int32, C.POINTER(C.c_void_p), _PP, _PJ,
+                                           C.c_int32, C.c_int32, C.c_int32, C.c_int32, _PR]),
     "orc_frames_search_mt": (C.c_int, [_PD, C.c_int32, C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p),
                                        _PP, C.c_int32, C.c_int32, _PR, C.POINTER(C.c_int64),
                                        C.POINTER(C.c_double), C.POINTER(C.c_double)]),
@@ -166,6 +168,23 @@ def h264_bi_refine(bit_depth: int, src: np.ndarray, refs, p, jobs: np.ndarray, r
     if rc != 0:
         raise RuntimeError(f"oracle h264_bi_refine rc={rc}")
     return mv, cost
+
+
+def hevc_weighted_refine(bit_depth: int, src: np.ndarray, refs, p, jobs: np.ndarray, log2_wd: int, weight: int,
+                         offset: int) -> np.ndarray:
+    """A weighted list's refine_subpel per GIVEN job (seeds[0] the start)."""
+    src = np.ascontiguousarray(src)
+    d = desc(capi.RME_CODEC_HEVC, src, bit_depth)
+    jobs = np.ascontiguousarray(jobs, capi.JOB_DTYPE)
+    refs = [np.ascontiguousarray(r) for r in refs]
+    rp = (C.c_void_p * len(refs))(*[r.ctypes.data for r in refs])
+    out = np.zeros(len(jobs), capi.RESULT_DTYPE)
+    rc = lib().orc_hevc_weighted_refine(C.byref(d), src.ctypes.data, len(refs), rp, C.byref(p),
+                                        C.cast(jobs.ctypes.data, _PJ), len(jobs), log2_wd, weight, offset,
+                                        C.cast(out.ctypes.data, _PR))
+    if rc != 0:
+        raise RuntimeError(f"oracle hevc_weighted_refine rc={rc}")
+    return out
 
 
 def wp_moments(codec: int, bit_depth: int, cur: np.ndarray, ref: np.ndarray) -> np.ndarray:

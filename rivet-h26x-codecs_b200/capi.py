@@ -144,6 +144,8 @@ SIGNATURES = {
     "rme_h264_bi_refine": (C.c_int, [_vp, C.POINTER(Frame), C.POINTER(Params), C.POINTER(H264BiJob), _i32, _i32,
                                      _i32, C.POINTER(Mv), _u32p, _vp]),
     "rme_probe_wait_timeout": (C.c_int, [_i32, C.c_uint32, _u32p, C.POINTER(C.c_double)]),
+    "rme_hevc_weighted_refine": (C.c_int, [_vp, C.POINTER(Frame), C.POINTER(Params), _i32, _i32, _i32,
+                                           C.POINTER(Result), _vp]),
     "rme_bi_satd": (C.c_int, [_vp, C.POINTER(Frame), C.POINTER(Params), C.POINTER(BiJob), _i32, _u32p, _vp]),
     "rme_bi_refine": (C.c_int, [_vp, C.POINTER(Frame), C.POINTER(Params), C.POINTER(BiJob), _i32,
                                 C.POINTER(Result), _vp]),

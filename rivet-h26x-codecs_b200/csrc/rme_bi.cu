@@ -288,6 +288,98 @@ __global__ void __launch_bounds__(256) h264_bi_kernel(H264BiDesc B) {
   }
 }
 
+// ---- HEVC weighted lists: refine_subpel under explicit weighting -------------
+
+// mv_bits and the rate (h265_search.rs:212-255, h265_me.rs:3890).
+__device__ __forceinline__ uint32_t wr_cbits(int d) {
+  const uint32_t a = (uint32_t)abs(d);
+  return a == 0 ? 1u : 3u + 2u * (31u - __clz(a));
+}
+__device__ __forceinline__ uint32_t wr_rate(float lam, int mx, int my, const rme_job& j) {
+  const uint32_t b0 = wr_cbits(mx - j.mvp[0].x) + wr_cbits(my - j.mvp[0].y);
+  const uint32_t b1 = wr_cbits(mx - j.mvp[1].x) + wr_cbits(my - j.mvp[1].y);
+  return __float2uint_rz(__fmul_rn(lam, __uint2float_rn(min(b0, b1) + 1u)));
+}
+
+struct WeightedRefine {
+  BiDesc B;                 // source, references, sizes
+  const rme_job* jobs;      // start = seeds[0], AMVP pair mvp
+  int32_t log2_wd, weight, offset, quarter_cross;
+  float lam;
+  rme_result* out;
+};
+
+// One warp per job: refine_subpel (h265_me.rs:3868-3922) with every
+// candidate scored by satd_at_weighted's explicit arm (4057-4073): the
+// 14-bit prediction (interpolated here from the integer plane), then
+// weighted_uni (dsp/hevc.rs:1036-1062), then SATD. Lanes take 4x4 tiles.
+template <class S>
+__global__ void __launch_bounds__(256) weighted_refine_kernel(WeightedRefine P) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const BiDesc& B = P.B;
+  const int maxv = (1 << B.bd) - 1;
+  for (int64_t i = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < B.n; i += warps) {
+    const rme_job& j = P.jobs[i];
+    const int x = j.x, y = j.y, w = j.w, h = j.h, tw = w >> 2, ntiles = tw * (h >> 2);
+    const DevPlanes& R = B.ref[j.ref];
+    auto satd_w = [&](int mx, int my) -> uint32_t {
+      uint32_t acc = 0;
+      for (int t = lane; t < ntiles; t += 32) {
+        const int ty = t / tw, tx = t - ty * tw;
+        int d[16];
+#pragma unroll 4
+        for (int e = 0; e < 16; ++e) {
+          const int row = ty * 4 + (e >> 2), col = tx * 4 + (e & 3);
+          const int p14 =
+              pred14<S>(R, B.width, B.height, B.bd, x + (mx >> 2) + col, y + (my >> 2) + row, mx & 3, my & 3);
+          const int v = P.log2_wd >= 1 ? ((p14 * P.weight + (1 << (P.log2_wd - 1))) >> P.log2_wd) + P.offset
+                                       : p14 * P.weight + P.offset;
+          d[e] = (int)*plane_ptr<S>(B.src, 0, x + col, y + row) - min(max(v, 0), maxv);
+        }
+        acc += hadamard4x4_sum(d);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(kAll, acc, o);
+      return acc;
+    };
+    const int sx = j.seeds[0].x, sy = j.seeds[0].y;
+    int bx = sx, by = sy;
+    uint32_t bsatd = satd_w(bx, by), bcost = bsatd + wr_rate(P.lam, bx, by, j), nsatd = 1;
+    for (int step = 2; step >= 1; --step) {
+      const int cx = bx, cy = by;
+      const bool cross = step == 1 && P.quarter_cross != 0;
+      for (int qy = -1; qy <= 1; ++qy)
+        for (int qx = -1; qx <= 1; ++qx) {
+          if ((qx == 0 && qy == 0) || (cross && qx != 0 && qy != 0)) continue;
+          const int mx = (int)(int16_t)(cx + qx * step), my = (int)(int16_t)(cy + qy * step);
+          const uint32_t sat = satd_w(mx, my), c = sat + wr_rate(P.lam, mx, my, j);
+          ++nsatd;
+          if (c < bcost) {
+            bcost = c;
+            bsatd = sat;
+            bx = mx;
+            by = my;
+          }
+        }
+    }
+    if (lane == 0) {
+      rme_result r;
+      r.mv.x = (int16_t)bx;
+      r.mv.y = (int16_t)by;
+      r.ref = j.ref;
+      r.cost = bcost;
+      r.satd = bsatd;
+      r.int_mv.x = (int16_t)sx;
+      r.int_mv.y = (int16_t)sy;
+      r.int_cost = 0;
+      r.n_sad = 0;
+      r.n_satd = nsatd;
+      P.out[i] = r;
+    }
+  }
+}
+
 int grid_of(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 7) / 8, 148 * 16)); }
 
 }  // namespace
@@ -317,6 +409,24 @@ cudaError_t launch_h264_bi(const DevPlanes& src, const DevPlanes* refs, int nref
     h264_bi_kernel<uint8_t><<<grid_of(n), 256, 0, s>>>(B);
   else
     h264_bi_kernel<uint16_t><<<grid_of(n), 256, 0, s>>>(B);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_weighted_refine(const BiDesc& B, const rme_job* jobs, int log2_wd, int weight, int offset,
+                                   int quarter_cross, float lam, rme_result* out, cudaStream_t s) {
+  WeightedRefine P{};
+  P.B = B;
+  P.jobs = jobs;
+  P.log2_wd = log2_wd;
+  P.weight = weight;
+  P.offset = offset;
+  P.quarter_cross = quarter_cross;
+  P.lam = lam;
+  P.out = out;
+  if (B.bd == 8)
+    weighted_refine_kernel<uint8_t><<<grid_of(B.n), 256, 0, s>>>(P);
+  else
+    weighted_refine_kernel<uint16_t><<<grid_of(B.n), 256, 0, s>>>(P);
   return cudaGetLastError();
 }
 

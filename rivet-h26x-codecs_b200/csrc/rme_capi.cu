@@ -195,6 +195,8 @@ struct Ctx {
   DevBuf<rme_bi_job> d_bijobs;        // bi-prediction: jobs, SATDs, refine_bi targets
   DevBuf<uint32_t> d_bisatd;
   DevBuf<uint8_t> d_bitarget;
+  DevBuf<rme_job> d_wjobs;            // HEVC weighted refinement: jobs, results
+  DevBuf<rme_result> d_wout;
   DevBuf<rme_h264_bi_job> d_h264bi;   // H.264 B pairs: jobs, refined vectors
   DevBuf<rme_mv> d_bimv;
   DevBuf<int32_t> d_cblk;             // chroma: blocks, vectors, output offsets, output
@@ -1244,6 +1246,39 @@ int rme_bi_satd(void* ctx, const rme_frame* f, const rme_params* p, const rme_bi
   CK(c->d_bisatd.ensure(n));
   CK(launch_bi_satd(B, c->d_bisatd.p, s));
   CK(cudaMemcpyAsync(satd, c->d_bisatd.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+int rme_hevc_weighted_refine(void* ctx, const rme_frame* f, const rme_params* p, int32_t log2_wd, int32_t weight,
+                             int32_t offset, rme_result* out, void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return RME_EINVAL;
+  if (!f || (f->njobs > 0 && (!f->jobs || !out)) || f->njobs < 0) return fail(c, RME_EINVAL, "null argument");
+  if (log2_wd < 0 || log2_wd > 14 || weight < -128 || weight > 255 || offset < -(1 << 12) || offset > (1 << 12))
+    return fail(c, RME_EINVAL, "weighting out of range");
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  BiDesc B;
+  int rc = bi_setup(c, f, p, nullptr, 0, false, s, &B);
+  if (rc) return rc;
+  const int n = f->njobs;
+  for (int i = 0; i < n; ++i) {
+    const rme_job& j = f->jobs[i];
+    if (j.ref < 0 || j.ref >= f->nref || j.nseeds < 1 || j.w < 4 || j.h < 4 || j.w > 64 || j.h > 64 || (j.w & 3) ||
+        (j.h & 3) || j.x < 0 || j.y < 0 || j.x + j.w > B.width || j.y + j.h > B.height)
+      return fail(c, RME_EINVAL, "job " + std::to_string(i) + " out of range");
+  }
+  if (n == 0) return 0;
+  Picture* src;
+  if ((rc = picture_of(c, f->src_id, &src))) return rc;
+  const Tables* t = get_tables(c, p, src->d.bit_depth, &rc);
+  if (!t) return rc;
+  B.n = n;
+  CK(c->d_wjobs.ensure(n));
+  CK(c->d_wout.ensure(n));
+  CK(cudaMemcpyAsync(c->d_wjobs.p, f->jobs, sizeof(rme_job) * n, cudaMemcpyHostToDevice, s));
+  CK(launch_weighted_refine(B, c->d_wjobs.p, log2_wd, weight, offset, p->hevc_quarter_cross, t->lam, c->d_wout.p, s));
+  CK(cudaMemcpyAsync(out, c->d_wout.p, sizeof(rme_result) * n, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   return 0;
 }

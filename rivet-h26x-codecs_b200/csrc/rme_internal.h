@@ -116,6 +116,10 @@ struct BiDesc {
 };
 cudaError_t launch_bi_satd(const BiDesc& B, uint32_t* satd, cudaStream_t s);
 cudaError_t launch_bi_target(const BiDesc& B, void* target, cudaStream_t s);
+// HEVC weighted lists' refine_subpel (rme_bi.cu): B's jobs unused, `jobs`
+// GIVEN jobs (start = seeds[0]), one result per job into `out`.
+cudaError_t launch_weighted_refine(const BiDesc& B, const rme_job* jobs, int log2_wd, int weight, int offset,
+                                   int quarter_cross, float lam, rme_result* out, cudaStream_t s);
 // H.264 B pairs' joint refinement (rme_bi.cu): `tab` the MvCostTable.
 cudaError_t launch_h264_bi(const DevPlanes& src, const DevPlanes* refs, int nref, int bd, const uint16_t* tab,
                            const rme_h264_bi_job* jobs, int n, int rounds, int npts, rme_mv* mv_out,

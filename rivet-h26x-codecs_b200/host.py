@@ -144,6 +144,17 @@ class MotionSearch:
                                                C.cast(out.ctypes.data, C.POINTER(capi.Result)), C.c_void_p(stream)))
         return out
 
+    def hevc_weighted_refine(self, src_id: int, ref_ids: Sequence[int], params: capi.Params, jobs: np.ndarray,
+                             log2_wd: int, weight: int, offset: int) -> np.ndarray:
+        """A weighted list's refine_subpel per GIVEN job (seeds[0] the
+        whole-sample start): results as capi.RESULT_DTYPE."""
+        jobs = np.ascontiguousarray(jobs, capi.JOB_DTYPE)
+        f = self._frame(src_id, ref_ids, jobs)
+        out = np.zeros(len(jobs), capi.RESULT_DTYPE)
+        self._check(self._lib.rme_hevc_weighted_refine(self.ctx, C.byref(f), C.byref(params), log2_wd, weight, offset,
+                                                       C.cast(out.ctypes.data, C.POINTER(capi.Result)), None))
+        return out
+
     def bi_satd(self, src_id: int, ref_ids: Sequence[int], params: capi.Params, jobs: np.ndarray,
                 stream: int = 0) -> np.ndarray:
         """satd_bi_at per job (capi.BI_JOB_DTYPE): the SATD of each vector

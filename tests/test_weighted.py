@@ -107,3 +107,55 @@ def test_wp_moments_and_weighted_sad_on_the_device(ms, bd, w, h):
         assert ms.weighted_sad(1700, 1701, wt, sh, off) == oracle.weighted_sad(HEVC, bd, cur, ref, wt, sh, off)
     ms.release(1700)
     ms.release(1701)
+
+
+def _weighted_jobs(rng, w, h, n, given):
+    """GIVEN jobs whose first seed is a whole-sample start (from `given`,
+    the results of a GIVEN search of the same jobs)."""
+    jobs = random_jobs(rng, HEVC, w, h, 2, n)
+    if given is not None:
+        jobs["seeds"][:, 0, 0] = given["int_mvx"]
+        jobs["seeds"][:, 0, 1] = given["int_mvy"]
+    jobs["nseeds"] = np.maximum(jobs["nseeds"], 1)
+    return jobs
+
+
+def test_identity_weighting_refines_as_the_default():
+    """With log2_wd = denom + 14 - bd, weight = 2^denom, offset 0, the
+    weighted prediction is the default one: refining from a GIVEN search's
+    whole-sample winner reproduces that search's vector, SATD and cost."""
+    rng = np.random.default_rng(23)
+    ref = random_picture(rng, 160, 96, 8)
+    src = shifted(ref, 3, -2, rng, 1.5)
+    p = oracle.params(HEVC, 32, predictor_mode=capi.RME_PRED_GIVEN)
+    jobs = _weighted_jobs(rng, 160, 96, 40, None)
+    jobs["ref"] = 0
+    given = oracle.frame_search(HEVC, 8, src, [ref], p, jobs)
+    start = jobs.copy()
+    start["seeds"][:, 0, 0] = given["int_mvx"]
+    start["seeds"][:, 0, 1] = given["int_mvy"]
+    got = oracle.hevc_weighted_refine(8, src, [ref], p, start, 6 + 6, 1 << 6, 0)
+    for f in ("mvx", "mvy", "satd", "cost"):
+        np.testing.assert_array_equal(got[f], given[f], err_msg=f)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("bd,w,h,log2_wd,wt,o", [(8, 352, 288, 12, 70, 3), (10, 416, 240, 9, -20, 100),
+                                                  (8, 200, 136, 6, 64, 0)])
+def test_weighted_refine_matches_the_oracle(ms, bd, w, h, log2_wd, wt, o):
+    rng = np.random.default_rng(w + log2_wd)
+    r0 = random_picture(rng, w, h, bd)
+    r1 = shifted(r0, -4, 2, rng, 1.0)
+    src = shifted(r0, 3, -1, rng, 2.0)
+    ms.upload(2000, src, HEVC, bd, as_ref=False)
+    ms.upload(2001, r0, HEVC, bd, as_ref=True)
+    ms.upload(2002, r1, HEVC, bd, as_ref=True)
+    p = oracle.params(HEVC, 32, predictor_mode=capi.RME_PRED_GIVEN)
+    jobs = _weighted_jobs(rng, w, h, 150, None)
+    jobs["seeds"][:, 0] = (jobs["seeds"][:, 0] // 4) * 4  # whole-sample starts
+    got = ms.hevc_weighted_refine(2000, [2001, 2002], p, jobs, log2_wd, wt, o)
+    want = oracle.hevc_weighted_refine(bd, src, [r0, r1], p, jobs, log2_wd, wt, o)
+    from _common import assert_results_equal
+    assert_results_equal(got, want, "weighted refine_subpel")
+    for i in range(3):
+        ms.release(2000 + i)
