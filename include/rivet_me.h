@@ -321,6 +321,17 @@ typedef struct {
 int rme_bi_satd(void* ctx, const rme_frame* f, const rme_params* p, const rme_bi_job* jobs, int32_t n,
                 uint32_t* satd, void* stream);
 
+/* satd_bi_at's explicit-weighting arm (h265_me.rs:4247-4261) per job: both
+ * lists' 14-bit predictions (predict14, whatever the vectors) combined by
+ * weighted_bi (dsp/hevc.rs:1064-1086),
+ *   clip(((a * w0 + b * w1 + ((o0 + o1 + 1) << log2_wd)) >> (log2_wd + 1)),
+ * and the SATD of the source block against it. log2_wd 0..14, weights
+ * -128..255, offsets (at the sample depth) within +-4096; otherwise as
+ * rme_bi_satd. Host jobs and output, synchronous. */
+int rme_bi_satd_weighted(void* ctx, const rme_frame* f, const rme_params* p, const rme_bi_job* jobs, int32_t n,
+                         int32_t log2_wd, int32_t w0, int32_t w1, int32_t o0, int32_t o1, uint32_t* satd,
+                         void* stream);
+
 /* refine_bi (h265_me.rs:3933-4014) per job: the other list's prediction
  * held fixed, list `list` searched again against the target
  * clip(2 * src - other's prediction) — search_full from the list's

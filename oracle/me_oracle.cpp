@@ -508,6 +508,22 @@ uint32_t hevc_satd_bi(const Dist<S>& dist, const HevcRef<S>& r0, const HevcRef<S
   return dist.satd(src + (ptrdiff_t)y * ss + x, ss, pred.data(), w, w, h);
 }
 
+// satd_bi_at's explicit arm (h265_me.rs:4247-4261): both lists' 14-bit
+// predictions through weighted_bi (dsp/hevc.rs:1064-1086).
+template <class S>
+uint32_t hevc_satd_bi_weighted(const Dist<S>& dist, const HevcRef<S>& r0, const HevcRef<S>& r1, int bd, const S* src,
+                               ptrdiff_t ss, int x, int y, int w, int h, Mv mv0, Mv mv1, const int wt[5]) {
+  const int maxv = (1 << bd) - 1, log2_wd = wt[0], w0 = wt[1], w1 = wt[2], o0 = wt[3], o1 = wt[4];
+  std::vector<int16_t> a((size_t)w * h), b((size_t)w * h);
+  std::vector<S> pred((size_t)w * h);
+  hevc_pred14(r0, x, y, w, h, mv0, bd, a.data());
+  hevc_pred14(r1, x, y, w, h, mv1, bd, b.data());
+  const int round = (o0 + o1 + 1) << log2_wd;
+  for (size_t i = 0; i < pred.size(); ++i)
+    pred[i] = (S)std::clamp(((int)a[i] * w0 + (int)b[i] * w1 + round) >> (log2_wd + 1), 0, maxv);
+  return dist.satd(src + (ptrdiff_t)y * ss + x, ss, pred.data(), w, w, h);
+}
+
 // refine_bi (h265_me.rs:3933-4014): the other list's prediction at its
 // vector (read_at, else predict14 + uni) held fixed, the target
 // clip(2 * src - it); search_full from the list's own vector, then
@@ -556,7 +572,7 @@ void hevc_refine_bi(const Dist<S>& dist, HevcRef<S>* const* refs, int bd, const 
 
 template <class S>
 int bi_frame(const rme_picture_desc* d, const void* src, int nref, const void* const* refs, const rme_params* p,
-             const rme_bi_job* jobs, int n, int refine, uint32_t* satd, rme_result* out) {
+             const rme_bi_job* jobs, int n, int refine, uint32_t* satd, rme_result* out, const int* wt = nullptr) {
   Dist<S> dist = dist_scalar<S>();
   const int W = d->width, H = d->height, bd = d->bit_depth;
   std::vector<HevcRef<S>> rr(nref);
@@ -570,6 +586,9 @@ int bi_frame(const rme_picture_desc* d, const void* src, int nref, const void* c
     const rme_bi_job& j = jobs[i];
     if (refine)
       hevc_refine_bi<S>(dist, rp.data(), bd, (const S*)src, d->stride, lam, p, j, out[i]);
+    else if (wt)
+      satd[i] = hevc_satd_bi_weighted<S>(dist, *rp[j.ref[0]], *rp[j.ref[1]], bd, (const S*)src, d->stride, j.x, j.y,
+                                         j.w, j.h, Mv(j.mv[0].x, j.mv[0].y), Mv(j.mv[1].x, j.mv[1].y), wt);
     else
       satd[i] = hevc_satd_bi<S>(dist, *rp[j.ref[0]], *rp[j.ref[1]], bd, (const S*)src, d->stride, j.x, j.y, j.w, j.h,
                                 Mv(j.mv[0].x, j.mv[0].y), Mv(j.mv[1].x, j.mv[1].y));
@@ -1267,6 +1286,28 @@ int orc_weighted_samples(int32_t codec, int32_t bit_depth, const void* in, int64
     else ((uint16_t*)out)[i] = (uint16_t)q;
   }
   return 0;
+}
+
+// satd_bi_at under explicit weighting per job (weights: log2_wd, w0, w1,
+// o0, o1; offsets at the sample depth).
+int orc_hevc_bi_weighted(const rme_picture_desc* d, const void* src, int32_t nref, const void* const* refs,
+                         const rme_params* p, const rme_bi_job* jobs, int32_t n, const int32_t* weights,
+                         uint32_t* satd) {
+  if (!weights || weights[0] < 0 || weights[0] > 14 || weights[1] < -128 || weights[1] > 255 || weights[2] < -128 ||
+      weights[2] > 255 || std::abs(weights[3]) > 4096 || std::abs(weights[4]) > 4096)
+    return RME_EINVAL;
+  if (!valid_desc(d) || d->codec != RME_CODEC_HEVC || !p || nref < 1 || nref > RME_MAX_REFS || n < 0 || !satd)
+    return RME_EINVAL;
+  for (int i = 0; i < n; ++i) {
+    const rme_bi_job& j = jobs[i];
+    if (j.ref[0] < 0 || j.ref[0] >= nref || j.ref[1] < 0 || j.ref[1] >= nref || j.w < 4 || j.h < 4 || j.w > 64 ||
+        j.h > 64 || (j.w & 3) || (j.h & 3) || j.x < 0 || j.y < 0 || j.x + j.w > d->width || j.y + j.h > d->height)
+      return RME_EINVAL;
+  }
+  int wt[5];
+  for (int k = 0; k < 5; ++k) wt[k] = weights[k];
+  return d->bit_depth == 8 ? bi_frame<uint8_t>(d, src, nref, refs, p, jobs, n, 0, satd, nullptr, wt)
+                           : bi_frame<uint16_t>(d, src, nref, refs, p, jobs, n, 0, satd, nullptr, wt);
 }
 
 // Many STANDALONE frames on `threads` host threads (the timed CPU

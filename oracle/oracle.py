@@ -37,6 +37,9 @@ _SIGS = {
                                      C.POINTER(C.c_uint32)]),
     "orc_hevc_weighted_refine": (C.c_int, [_PD, C.c_void_p, C.c_int32, C.POINTER(C.c_void_p), _PP, _PJ,
                                            C.c_int32, C.c_int32, C.c_int32, C.c_int32, _PR]),
+    "orc_hevc_bi_weighted": (C.c_int, [_PD, C.c_void_p, C.c_int32, C.POINTER(C.c_void_p), _PP,
+                                       C.POINTER(capi.BiJob), C.c_int32, C.POINTER(C.c_int32),
+                                       C.POINTER(C.c_uint32)]),
     "orc_frames_search_mt": (C.c_int, [_PD, C.c_int32, C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p),
                                        _PP, C.c_int32, C.c_int32, _PR, C.POINTER(C.c_int64),
                                        C.POINTER(C.c_double), C.POINTER(C.c_double)]),
@@ -168,6 +171,23 @@ def h264_bi_refine(bit_depth: int, src: np.ndarray, refs, p, jobs: np.ndarray, r
     if rc != 0:
         raise RuntimeError(f"oracle h264_bi_refine rc={rc}")
     return mv, cost
+
+
+def hevc_bi_weighted(bit_depth: int, src: np.ndarray, refs, p, jobs: np.ndarray, weights) -> np.ndarray:
+    """satd_bi_at under explicit weighting (log2_wd, w0, w1, o0, o1)."""
+    src = np.ascontiguousarray(src)
+    d = desc(capi.RME_CODEC_HEVC, src, bit_depth)
+    jobs = np.ascontiguousarray(jobs, capi.BI_JOB_DTYPE)
+    refs = [np.ascontiguousarray(r) for r in refs]
+    rp = (C.c_void_p * len(refs))(*[r.ctypes.data for r in refs])
+    wt = np.ascontiguousarray(weights, np.int32)
+    out = np.zeros(len(jobs), np.uint32)
+    rc = lib().orc_hevc_bi_weighted(C.byref(d), src.ctypes.data, len(refs), rp, C.byref(p),
+                                    C.cast(jobs.ctypes.data, C.POINTER(capi.BiJob)), len(jobs),
+                                    wt.ctypes.data_as(C.POINTER(C.c_int32)), out.ctypes.data_as(C.POINTER(C.c_uint32)))
+    if rc != 0:
+        raise RuntimeError(f"oracle hevc_bi_weighted rc={rc}")
+    return out
 
 
 def hevc_weighted_refine(bit_depth: int, src: np.ndarray, refs, p, jobs: np.ndarray, log2_wd: int, weight: int,

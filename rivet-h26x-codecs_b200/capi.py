@@ -147,6 +147,8 @@ SIGNATURES = {
     "rme_hevc_weighted_refine": (C.c_int, [_vp, C.POINTER(Frame), C.POINTER(Params), _i32, _i32, _i32,
                                            C.POINTER(Result), _vp]),
     "rme_bi_satd": (C.c_int, [_vp, C.POINTER(Frame), C.POINTER(Params), C.POINTER(BiJob), _i32, _u32p, _vp]),
+    "rme_bi_satd_weighted": (C.c_int, [_vp, C.POINTER(Frame), C.POINTER(Params), C.POINTER(BiJob), _i32, _i32,
+                                       _i32, _i32, _i32, _i32, _u32p, _vp]),
     "rme_bi_refine": (C.c_int, [_vp, C.POINTER(Frame), C.POINTER(Params), C.POINTER(BiJob), _i32,
                                 C.POINTER(Result), _vp]),
     "rme_chroma_predict": (C.c_int, [_vp, _i32, _i32, C.POINTER(C.c_int32), C.POINTER(Mv), _vp, _vp]),

@@ -108,9 +108,11 @@ __device__ __forceinline__ uint32_t hadamard4x4_sum(int* d) {
   return (sum + 1) >> 1;
 }
 
-// satd_bi_at under default weighting: both blocks readable, the samples
-// averaged (a + b + 1) >> 1; otherwise bi of the two 14-bit predictions at
-// 15 - bd (dsp/hevc.rs:1015-1031). Lanes take 4x4 tiles in turn.
+// satd_bi_at: under default weighting with both blocks readable, the
+// samples averaged (a + b + 1) >> 1; otherwise bi of the two 14-bit
+// predictions at 15 - bd (dsp/hevc.rs:1015-1031), or under explicit
+// weighting weighted_bi of them (dsp/hevc.rs:1064-1086). Lanes take 4x4
+// tiles in turn.
 template <class S>
 __global__ void __launch_bounds__(256) bi_satd_kernel(BiDesc B, uint32_t* out) {
   const int lane = threadIdx.x & 31;
@@ -121,7 +123,7 @@ __global__ void __launch_bounds__(256) bi_satd_kernel(BiDesc B, uint32_t* out) {
     const int m0x = j.mv[0].x, m0y = j.mv[0].y, m1x = j.mv[1].x, m1y = j.mv[1].y;
     const DevPlanes& R0 = B.ref[j.ref[0]];
     const DevPlanes& R1 = B.ref[j.ref[1]];
-    const bool avg = readable(B, x, y, w, h, m0x, m0y) && readable(B, x, y, w, h, m1x, m1y);
+    const bool avg = !B.wp && readable(B, x, y, w, h, m0x, m0y) && readable(B, x, y, w, h, m1x, m1y);
     const int tw = w >> 2, ntiles = tw * (h >> 2);
     const int sh = 15 - B.bd, maxv = (1 << B.bd) - 1;
     uint32_t acc = 0;
@@ -140,7 +142,9 @@ __global__ void __launch_bounds__(256) bi_satd_kernel(BiDesc B, uint32_t* out) {
                                   m0y & 3);
           const int b = pred14<S>(R1, B.width, B.height, B.bd, x + (m1x >> 2) + col, y + (m1y >> 2) + row, m1x & 3,
                                   m1y & 3);
-          pred = min(max((a + b + (1 << (sh - 1))) >> sh, 0), maxv);
+          pred = B.wp ? (a * B.w0 + b * B.w1 + ((B.o0 + B.o1 + 1) << B.log2_wd)) >> (B.log2_wd + 1)
+                      : (a + b + (1 << (sh - 1))) >> sh;
+          pred = min(max(pred, 0), maxv);
         }
         d[e] = (int)*plane_ptr<S>(B.src, 0, x + col, y + row) - pred;
       }

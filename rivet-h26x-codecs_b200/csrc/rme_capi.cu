@@ -1250,6 +1250,33 @@ int rme_bi_satd(void* ctx, const rme_frame* f, const rme_params* p, const rme_bi
   return 0;
 }
 
+int rme_bi_satd_weighted(void* ctx, const rme_frame* f, const rme_params* p, const rme_bi_job* jobs, int32_t n,
+                         int32_t log2_wd, int32_t w0, int32_t w1, int32_t o0, int32_t o1, uint32_t* satd,
+                         void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return RME_EINVAL;
+  if (n > 0 && !satd) return fail(c, RME_EINVAL, "null argument");
+  const int lim = 1 << 12;
+  if (log2_wd < 0 || log2_wd > 14 || w0 < -128 || w0 > 255 || w1 < -128 || w1 > 255 || o0 < -lim || o0 > lim ||
+      o1 < -lim || o1 > lim)
+    return fail(c, RME_EINVAL, "weighting out of range");
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  BiDesc B;
+  int rc = bi_setup(c, f, p, jobs, n, false, s, &B);
+  if (rc || n == 0) return rc;
+  B.wp = 1;
+  B.log2_wd = log2_wd;
+  B.w0 = w0;
+  B.w1 = w1;
+  B.o0 = o0;
+  B.o1 = o1;
+  CK(c->d_bisatd.ensure(n));
+  CK(launch_bi_satd(B, c->d_bisatd.p, s));
+  CK(cudaMemcpyAsync(satd, c->d_bisatd.p, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
 int rme_hevc_weighted_refine(void* ctx, const rme_frame* f, const rme_params* p, int32_t log2_wd, int32_t weight,
                              int32_t offset, rme_result* out, void* stream) {
   Ctx* c = (Ctx*)ctx;

@@ -113,6 +113,9 @@ struct BiDesc {
   int32_t width, height, bd, pad, quarter;
   const rme_bi_job* jobs;
   int32_t n;
+  // Explicit weighting of the bi score (wp != 0): weighted_bi's log2WD,
+  // the two lists' weights and offsets.
+  int32_t wp, log2_wd, w0, w1, o0, o1;
 };
 cudaError_t launch_bi_satd(const BiDesc& B, uint32_t* satd, cudaStream_t s);
 cudaError_t launch_bi_target(const BiDesc& B, void* target, cudaStream_t s);

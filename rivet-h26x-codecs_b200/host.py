@@ -167,6 +167,19 @@ class MotionSearch:
                                           out.ctypes.data_as(C.POINTER(C.c_uint32)), C.c_void_p(stream)))
         return out
 
+    def bi_satd_weighted(self, src_id: int, ref_ids: Sequence[int], params: capi.Params, jobs: np.ndarray,
+                         log2_wd: int, w0: int, w1: int, o0: int, o1: int, stream: int = 0) -> np.ndarray:
+        """satd_bi_at under explicit weighting per job: weighted_bi of the
+        two lists' 14-bit predictions."""
+        jobs = np.ascontiguousarray(jobs, capi.BI_JOB_DTYPE)
+        f = self._frame(src_id, ref_ids)
+        out = np.zeros(len(jobs), np.uint32)
+        self._check(self._lib.rme_bi_satd_weighted(self.ctx, C.byref(f), C.byref(params),
+                                                   C.cast(jobs.ctypes.data, C.POINTER(capi.BiJob)), len(jobs),
+                                                   log2_wd, w0, w1, o0, o1,
+                                                   out.ctypes.data_as(C.POINTER(C.c_uint32)), C.c_void_p(stream)))
+        return out
+
     def bi_refine(self, src_id: int, ref_ids: Sequence[int], params: capi.Params, jobs: np.ndarray,
                   stream: int = 0) -> np.ndarray:
         """refine_bi per job: one result per job (capi.RESULT_DTYPE), mv the

@@ -156,3 +156,76 @@ def test_refine_bi_on_the_device_finds_the_translation(ms):
     assert (got["mvx"] == 24).all() and (got["mvy"] == -16).all() and (got["satd"] == 0).all()
     for i in range(3):
         ms.release(1400 + i)
+
+
+def test_weighted_bi_with_one_list_is_the_plain_block():
+    """Explicit weighting with w1 = 0, w0 = 2^(denom + 1) and log2_wd =
+    denom + 14 - bd keeps list 0's 14-bit prediction alone, rounded back to the
+    sample depth: at a whole-sample vector the reference block itself, so
+    the score is the SATD against that block, whatever list 1 holds."""
+    rng = np.random.default_rng(31)
+    for bd in (8, 10):
+        src, r0, r1 = (random_picture(rng, 96, 64, bd) for _ in range(3))
+        jobs = np.zeros(3, capi.BI_JOB_DTYPE)
+        for i, (x, y, w, h, m0, m1) in enumerate([(16, 8, 16, 16, (8, -4), (-13, 6)),
+                                                  (0, 0, 32, 32, (0, 0), (1203, -7)),
+                                                  (48, 16, 32, 32, (-16, 8), (17, -9))]):
+            jobs[i]["x"], jobs[i]["y"], jobs[i]["w"], jobs[i]["h"] = x, y, w, h
+            jobs[i]["ref"] = (0, 1)
+            jobs[i]["mv"] = (m0, m1)
+        denom = 5
+        got = oracle.hevc_bi_weighted(bd, src, [r0, r1], oracle.params(HEVC, 32), jobs,
+                                      (denom + 14 - bd, 2 << denom, 0, 0, 0))
+        for j, g in zip(jobs, got):
+            x, y, w, h = (int(j[k]) for k in ("x", "y", "w", "h"))
+            ax, ay = j["mv"][0] // 4
+            assert g == _satd(src[y:y + h, x:x + w], r0[y + ay:y + ay + h, x + ax:x + ax + w])
+
+
+def test_identity_weighting_is_the_exact_bi_prediction():
+    """w0 = w1 = 2^denom, no offsets, log2_wd = denom + 14 - bd is
+    (a + b + 2^(14 - bd)) >> (15 - bd), the default bi: equal to the
+    default score wherever that score takes the exact form (a vector out
+    of HalfPlanes' reach), and an offset pair shifts every sample."""
+    rng = np.random.default_rng(32)
+    src, r0, r1 = (random_picture(rng, 128, 96, 10) for _ in range(3))
+    p = oracle.params(HEVC, 32)
+    jobs = _jobs(rng, 128, 96, 60)
+    jobs["mv"][:, 1, 0] = rng.integers(800, 1200, size=60) * rng.choice([-1, 1], size=60)
+    want = oracle.hevc_bi(10, src, [r0, r1], p, jobs, refine=False)
+    for denom in (0, 3, 7):
+        got = oracle.hevc_bi_weighted(10, src, [r0, r1], p, jobs, (denom + 4, 1 << denom, 1 << denom, 0, 0))
+        np.testing.assert_array_equal(got, want)
+    flat = np.full_like(src, 512)
+    r = oracle.hevc_bi_weighted(10, flat, [flat, flat], p, jobs[:4], (4, 1, 1, 7, 5))
+    # Flat references and source: every sample predicts 512 + 6, the SATD of
+    # a constant difference 6 is 16 * 6 / 2 per 4x4 tile (its DC term).
+    assert list(r) == [(int(j["w"]) * int(j["h"]) // 16) * 48 for j in jobs[:4]]
+
+
+def test_weighted_bi_jobs_are_checked():
+    rng = np.random.default_rng(33)
+    pic = random_picture(rng, 64, 64, 8)
+    jobs = _jobs(rng, 64, 64, 2)
+    for wt in [(15, 1, 1, 0, 0), (6, 300, 1, 0, 0), (6, 1, -129, 0, 0), (6, 1, 1, 5000, 0)]:
+        with pytest.raises(RuntimeError):
+            oracle.hevc_bi_weighted(8, pic, [pic, pic], oracle.params(HEVC, 32), jobs, wt)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("bd,w,h,wt", [(8, 352, 288, (7, 90, 40, 3, -9)), (10, 416, 240, (5, -20, 70, 100, 4)),
+                                       (8, 1920, 1152, (6, 64, 64, 0, 0))])
+def test_weighted_bi_satd_matches_the_oracle(ms, bd, w, h, wt):
+    rng = np.random.default_rng(bd * 7 + w)
+    r0 = random_picture(rng, w, h, bd)
+    r1 = shifted(r0, -7, 5, rng, 1.0)
+    src = shifted(r0, 5, -3, rng, 2.0)
+    ids = _upload(ms, src, [r0, r1], bd, 1350)
+    p = oracle.params(HEVC, 32)
+    jobs = _jobs(rng, w, h, 300 if w < 1000 else 120, far=0.15)
+    got = ms.bi_satd_weighted(1350, ids, p, jobs, *wt)
+    want = oracle.hevc_bi_weighted(bd, src, [r0, r1], p, jobs, wt)
+    bad = np.nonzero(got != want)[0]
+    assert len(bad) == 0, f"{len(bad)} SATDs differ; first {bad[:5]}: {got[bad[:5]]} vs {want[bad[:5]]}"
+    for i in range(3):
+        ms.release(1350 + i)
