@@ -851,6 +851,32 @@ std::unique_ptr<Picture> picture_geometry(const rme_picture_desc* d, bool as_ref
   pic->bytes = (size_t)pic->planes.plane_elems * bps * pic->nplanes + 256;
   return pic;
 }
+
+// The device buffer of picture `id`'s new contents: the old entry's when
+// the geometry matches (a stream's picture slots are refilled every frame;
+// work already queued on the old contents is ordered before the refill by
+// the stream), else a fresh one. The old entry leaves the table here, so a
+// failure after this leaves the id unknown instead of naming a picture
+// without a buffer.
+cudaError_t take_buffer(Ctx* c, int32_t id, Picture* pic, cudaStream_t s) {
+  auto old = c->pics.find(id);
+  if (old != c->pics.end()) {
+    if (old->second->bytes == pic->bytes && old->second->planes.stride == pic->planes.stride) {
+      pic->buf = old->second->buf;
+      old->second->buf = nullptr;
+    } else {
+      cudaError_t e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) return e;
+    }
+    c->pics.erase(old);
+  }
+  if (!pic->buf) {
+    cudaError_t e = cudaMalloc(&pic->buf, pic->bytes);
+    if (e != cudaSuccess) return e;
+  }
+  pic->planes.base = pic->buf;
+  return cudaSuccess;
+}
 }  // namespace
 
 int rme_picture_upload(void* ctx, int32_t pic_id, const rme_picture_desc* d, const void* luma, int32_t as_ref,
@@ -863,18 +889,7 @@ int rme_picture_upload(void* ctx, int32_t pic_id, const rme_picture_desc* d, con
   auto pic = picture_geometry(d, as_ref != 0);
   const bool h264 = d->codec == RME_CODEC_H264;
   const int bps = d->bit_depth == 8 ? 1 : 2, stride = pic->planes.stride;
-  // Re-uploading an id with the same format reuses its device buffer (a
-  // stream's picture slots are refilled every frame). Work already queued
-  // on the picture is ordered before the refill by the stream.
-  auto old = c->pics.find(pic_id);
-  if (old != c->pics.end() && old->second->bytes == pic->bytes && old->second->planes.stride == stride) {
-    pic->buf = old->second->buf;
-    old->second->buf = nullptr;
-  } else {
-    if (old != c->pics.end()) CK(cudaStreamSynchronize(s));
-    CK(cudaMalloc(&pic->buf, pic->bytes));
-  }
-  pic->planes.base = pic->buf;
+  CK(take_buffer(c, pic_id, pic.get(), s));
   // The visible picture straight into plane 0, then its border in place:
   // nothing is staged, so nothing waits (a pageable source is consumed
   // before the copy call returns; a pinned one is read on the stream).
@@ -959,15 +974,7 @@ int rme_picture_weighted(void* ctx, int32_t ref_id, int32_t dst_id, int32_t log_
   cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
   CK(cudaSetDevice(c->device));
   auto pic = picture_geometry(&p->d, true);
-  auto old = c->pics.find(dst_id);
-  if (old != c->pics.end() && old->second->bytes == pic->bytes && old->second->planes.stride == pic->planes.stride) {
-    pic->buf = old->second->buf;
-    old->second->buf = nullptr;
-  } else {
-    if (old != c->pics.end()) CK(cudaStreamSynchronize(s));
-    CK(cudaMalloc(&pic->buf, pic->bytes));
-  }
-  pic->planes.base = pic->buf;
+  CK(take_buffer(c, dst_id, pic.get(), s));
   const int bps = p->d.bit_depth == 8 ? 1 : 2;
   CK(launch_weighted_plane(p->buf, pic->buf, pic->planes.plane_elems * bps, p->d.codec, p->d.bit_depth, log_wd, weight,
                            offset, s));
