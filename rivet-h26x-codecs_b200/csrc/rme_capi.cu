@@ -1616,7 +1616,8 @@ int rme_lowres_search(void* ctx, int32_t cur_id, int32_t ref_id, uint32_t* cost,
 int rme_lowres_bi_cost(void* ctx, int32_t cur_id, int32_t r0_id, const rme_mv* mv0, int32_t r1_id, const rme_mv* mv1,
                        uint32_t* cost, void* stream) {
   Ctx* c = (Ctx*)ctx;
-  if (!c || !mv0 || !mv1 || !cost) return RME_EINVAL;
+  if (!c) return RME_EINVAL;
+  if (!mv0 || !mv1 || !cost) return fail(c, RME_EINVAL, "null argument");
   Picture *pc, *p0, *p1;
   int rc = lowres_pair(c, cur_id, r0_id, &pc, &p0);
   if (!rc) rc = lowres_pair(c, cur_id, r1_id, &pc, &p1);

@@ -159,3 +159,32 @@ def test_weighted_refine_matches_the_oracle(ms, bd, w, h, log2_wd, wt, o):
     assert_results_equal(got, want, "weighted refine_subpel")
     for i in range(3):
         ms.release(2000 + i)
+
+
+@pytest.mark.gpu
+def test_reused_ids_take_new_contents(ms):
+    """An id uploaded again: with the same geometry its buffer is refilled,
+    with another one it is replaced; a weighted plane written over an id in
+    use likewise. Searches afterwards see the new contents only, and the
+    pictures' device memory goes when the ids are released."""
+    rng = np.random.default_rng(29)
+    p = oracle.params(HEVC, 32)
+    before = ms.memory_used()
+    a, b = random_picture(rng, 192, 128, 8), random_picture(rng, 320, 192, 8)
+    ms.upload(2100, a, HEVC, 8, as_ref=True)
+    for pic in (random_picture(rng, 192, 128, 8), b):
+        src = shifted(pic, 2, -3, rng, 1.0)
+        ms.upload(2100, pic, HEVC, 8, as_ref=True)
+        ms.upload(2101, src, HEVC, 8, as_ref=False)
+        assert (ms.search(2101, [2100], p) == oracle.frame_search(HEVC, 8, src, [pic], p)).all()
+    ms.upload(2102, b, HEVC, 8, as_ref=True)
+    held = []
+    for wt, o in ((70, 3), (50, -6)):
+        ms.picture_weighted(2102, 2100, 6, wt, o)
+        np.testing.assert_array_equal(ms.plane(2100, 0)[80:80 + 192, 80:80 + 320],
+                                      oracle.weighted_samples(HEVC, 8, b, 6, wt, o))
+        held.append(ms.memory_used())
+    assert held[0] == held[1]
+    for i in range(3):
+        ms.release(2100 + i)
+    assert ms.memory_used() == before
