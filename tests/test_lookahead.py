@@ -47,6 +47,25 @@ def test_lowres_search_finds_a_translation():
     assert (nsad > 0).all()
 
 
+def _lcg_picture(w, h):
+    """h265_cutree.rs:322-335's picture: s = s * 1103515245 + 12345 (32-bit),
+    each sample the top byte of s."""
+    s, out = 1, np.empty(w * h, np.uint8)
+    for i in range(w * h):
+        s = (s * 1103515245 + 12345) & 0xFFFFFFFF
+        out[i] = s >> 24
+    return out.reshape(h, w)
+
+
+@pytest.mark.parametrize("codec", [HEVC, H264])
+def test_a_picture_matches_itself_at_zero_cost(codec):
+    """h265_cutree.rs:322-347: searched against itself, every block costs 0
+    at the zero vector (both lookaheads)."""
+    y = _lcg_picture(64, 64)
+    cost, mv, _ = oracle.lowres_search(y, y, 8, codec=codec)
+    assert (cost == 0).all() and (mv == 0).all()
+
+
 def test_h264_lowres_plane_keeps_the_sample_type():
     """Lookahead::add (h264_lookahead.rs:87-117): 8 samples per macroblock,
     each the rounded 2x2 mean at the stream's depth (no shift), columns and
@@ -169,3 +188,17 @@ def test_lowres_search_batch_equals_pair_by_pair(ms, codec, bd):
         np.testing.assert_array_equal(a, b, name)
     for i in range(len(pics)):
         ms.release(950 + i)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("codec", [HEVC, H264])
+def test_a_picture_matches_itself_on_the_device(ms, codec):
+    rng = np.random.default_rng(41)
+    for k, pic in enumerate((_lcg_picture(64, 64), random_picture(rng, 640, 352, 8))):
+        ms.upload(2300 + k, pic, codec, 8, as_ref=False)
+        ms.lowres_build(2300 + k)
+        cost, mv, nsad = ms.lowres_search(2300 + k, 2300 + k)
+        assert (cost == 0).all() and (mv == 0).all()
+        want = oracle.lowres_search(pic, pic, 8, codec=codec)
+        np.testing.assert_array_equal(nsad, want[2])
+        ms.release(2300 + k)

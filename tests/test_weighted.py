@@ -44,6 +44,61 @@ def test_wp_moments_and_weighted_sad_are_the_sums():
         assert oracle.weighted_sad(HEVC, 10, cur, ref, wt, sh, off) == np.abs(p - c).sum()
 
 
+_SWEEP_WEIGHTS = (-128, -77, -1, 0, 1, 31, 32, 63, 64, 65, 127, 191, 255)
+
+
+def _sweep_pictures(bd, w, h, seed):
+    """The planes dsp/distortion.rs:394-456 sweeps: random samples (twice),
+    rails (each sample 0 or the maximum), and all at the maximum."""
+    rng = np.random.default_rng(seed)
+    top = (1 << bd) - 1
+    dt = np.uint8 if bd == 8 else np.uint16
+    for trial in range(4):
+        if trial < 2:
+            yield trial, random_picture(rng, w, h, bd), random_picture(rng, w, h, bd)
+        elif trial == 2:
+            yield trial, *(rng.choice([0, top], size=(h, w)).astype(dt) for _ in range(2))
+        else:
+            yield trial, np.full((h, w), top, dt), np.full((h, w), top, dt)
+
+
+@pytest.mark.parametrize("bd", [8, 10, 12])
+def test_weighted_sad_sweep_is_the_closed_form(bd):
+    """The reference's weighted-kernel sweep (every weight either table
+    carries, shifts 0..7, offsets at both ends, rails) restated for the
+    oracle: each sum equals the closed form clip(((r*w + rnd) >> s) + o)."""
+    scale = 4 if bd > 8 else 1
+    top = (1 << bd) - 1
+    for trial, cur, ref in _sweep_pictures(bd, 33, 17, bd):
+        r, c = ref.astype(np.int64), cur.astype(np.int64)
+        m = oracle.wp_moments(HEVC, bd, cur, ref)
+        assert list(m) == [r.sum(), c.sum(), (r * r).sum(), (r * c).sum(), np.abs(c - r).sum()], trial
+        for wt in _SWEEP_WEIGHTS:
+            for sh in range(8):
+                for off in (-128 * scale, -3, 0, 5, 127 * scale):
+                    rnd = 1 << (sh - 1) if sh >= 1 else 0
+                    want = np.abs(np.clip(((r * wt + rnd) >> sh) + off, 0, top) - c).sum()
+                    assert oracle.weighted_sad(HEVC, bd, cur, ref, wt, sh, off) == want, (trial, wt, sh, off)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("bd", [8, 10, 12])
+def test_weighted_sad_sweep_on_the_device(ms, bd):
+    """The same sweep through the device passes, sum for sum with the oracle."""
+    scale = 4 if bd > 8 else 1
+    for trial, cur, ref in _sweep_pictures(bd, 200, 24, bd + 100):
+        ms.upload(2200, cur, HEVC, bd, as_ref=False)
+        ms.upload(2201, ref, HEVC, bd, as_ref=False)
+        np.testing.assert_array_equal(ms.wp_moments(2200, 2201), oracle.wp_moments(HEVC, bd, cur, ref))
+        for wt in _SWEEP_WEIGHTS:
+            for sh in range(8):
+                for off in (-128 * scale, -3, 0, 5, 127 * scale):
+                    assert ms.weighted_sad(2200, 2201, wt, sh, off) == \
+                        oracle.weighted_sad(HEVC, bd, cur, ref, wt, sh, off), (trial, wt, sh, off)
+    ms.release(2200)
+    ms.release(2201)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("codec,bd,w,h,log_wd,wt,o", [(H264, 8, 352, 288, 5, 40, -7), (H264, 10, 200, 136, 0, 1, 12),
                                                        (HEVC, 8, 416, 240, 12, 70, 3),
