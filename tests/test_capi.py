@@ -29,6 +29,19 @@ def test_the_library_exports_every_declared_entry_point():
     assert set(names) == set(capi.SIGNATURES), set(names) ^ set(capi.SIGNATURES)
 
 
+def test_the_rust_declarations_match_the_header():
+    """The integration notes' FFI block declares every entry point with the
+    header's parameter count, and the ctypes binding agrees on it too."""
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    c_args = {n: (0 if a.strip() in ("", "void") else a.count(",") + 1)
+              for n, a in re.findall(r"\b(rme_[a-z0-9_]+)\s*\(([^;]*?)\)\s*;", text)}
+    notes = (HEADER.parents[1] / "INTEGRATION.md").read_text()
+    rust = {n: len(re.findall(r"\b\w+\s*:", a)) for n, a in re.findall(r"pub fn (rme_[a-z0-9_]+)\(([^)]*)\)", notes)}
+    assert set(c_args) == set(declared())
+    assert {n: c_args[n] for n in rust} == rust and set(rust) == set(c_args), set(c_args) ^ set(rust)
+    assert {n: len(capi.SIGNATURES[n][1]) for n in c_args} == c_args
+
+
 def test_struct_layouts_match_the_header():
     assert C.sizeof(capi.Mv) == 4
     assert C.sizeof(capi.Result) == 32
