@@ -42,6 +42,38 @@ def test_the_rust_declarations_match_the_header():
     assert {n: len(capi.SIGNATURES[n][1]) for n in c_args} == c_args
 
 
+_STRUCTS = {"rme_mv": "Mv", "rme_picture_desc": "PictureDesc", "rme_params": "Params", "rme_job": "Job",
+            "rme_result": "Result", "rme_frame": "Frame", "rme_stats": "Stats", "rme_bi_job": "BiJob",
+            "rme_h264_bi_job": "H264BiJob", "rme_serve_opts": "ServeOpts", "rme_completion": "Completion",
+            "rme_plane_set": "PlaneSet"}
+
+
+def test_every_struct_matches_the_c_compiler(tmp_path):
+    """Each struct of the header, compiled by the C compiler, has the size
+    and the field offsets of its ctypes mirror."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    assert set(re.findall(r"\}\s*(rme_[a-z0-9_]+)\s*;", text)) == set(_STRUCTS)
+    lines = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{HEADER}"', "int main(void) {"]
+    for cname, pyname in _STRUCTS.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for field, _ in getattr(capi, pyname)._fields_:
+            lines.append(f'  printf("{cname} {field} %zu\\n", offsetof({cname}, {field}));')
+    lines += ["  return 0;", "}"]
+    (tmp_path / "layout.c").write_text("\n".join(lines) + "\n")
+    subprocess.run([cc, "-std=c11", "-o", str(tmp_path / "layout"), str(tmp_path / "layout.c")], check=True)
+    out = subprocess.run([str(tmp_path / "layout")], check=True, capture_output=True, text=True).stdout
+    for line in out.splitlines():
+        cname, what, val = line.split()
+        cls = getattr(capi, _STRUCTS[cname])
+        got = C.sizeof(cls) if what == "size" else getattr(cls, what).offset
+        assert got == int(val), f"{cname}.{what}: ctypes {got}, C {val}"
+
+
 def test_struct_layouts_match_the_header():
     assert C.sizeof(capi.Mv) == 4
     assert C.sizeof(capi.Result) == 32
