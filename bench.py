@@ -305,9 +305,19 @@ def run_ours(args, world, rank, local):
     d2h = sum(int(o.nbytes) for o in outs)
     host_out = torch.empty(total * capi.RESULT_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True)
 
+    # The uploads alternate between two streams, so that one picture's copy
+    # runs while the previous one's planes are built; the search waits for
+    # both. (The previous step's search has returned, so nothing still reads
+    # the pictures being refilled.)
+    up = [torch.cuda.Stream(device=local) for _ in range(2)]
+    up_done = [torch.cuda.Event() for _ in range(2)]
+
     def e2e_step():
-        for i, t in zip(ids, pinned):
-            ms.upload(i, t.numpy(), capi.RME_CODEC_HEVC, 8, as_ref=True, stream=sh)
+        for k, (i, t) in enumerate(zip(ids, pinned)):
+            ms.upload(i, t.numpy(), capi.RME_CODEC_HEVC, 8, as_ref=True, stream=up[k & 1].cuda_stream)
+        for u, e in zip(up, up_done):
+            e.record(u)
+            stream.wait_event(e)
         return [v.numpy().view(capi.RESULT_DTYPE) for v in ms.search_batch(batch, p, sh, out=host_out)]
 
     for _ in range(2):
