@@ -303,32 +303,54 @@ def run_ours(args, world, rank, local):
         pinned.append(t)
     h2d = sum(int(f.nbytes) for f in frames)
     d2h = sum(int(o.nbytes) for o in outs)
-    host_out = torch.empty(total * capi.RESULT_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True)
+    rbytes = total * capi.RESULT_DTYPE.itemsize
+    host_out = [torch.empty(rbytes, dtype=torch.uint8, pin_memory=True) for _ in range(2)]
+    dev_out = [torch.empty(rbytes, dtype=torch.uint8, device=f"cuda:{local}") for _ in range(2)]
 
-    # The uploads alternate between two streams, so that one picture's copy
-    # runs while the previous one's planes are built; the search waits for
-    # both. (The previous step's search has returned, so nothing still reads
-    # the pictures being refilled.)
+    # A pipeline of two steps in flight. The uploads alternate between two
+    # streams, so one picture's copy runs while the previous picture's planes
+    # are built; the search waits for both. (The previous step's search has
+    # returned, so nothing still reads the pictures being refilled.) Each
+    # step's results stay in one of two device buffers and are read back to
+    # pinned memory on a copy stream while the next step's uploads run; a
+    # search waits for the read-back of the step before last, which used the
+    # same buffer. Every step's copies lie inside the timed region, which
+    # ends with a device-wide synchronize.
     up = [torch.cuda.Stream(device=local) for _ in range(2)]
     up_done = [torch.cuda.Event() for _ in range(2)]
+    cp = torch.cuda.Stream(device=local)
+    searched, copied = torch.cuda.Event(), [torch.cuda.Event() for _ in range(2)]
+    for e in copied:
+        e.record(cp)
 
-    def e2e_step():
-        for k, (i, t) in enumerate(zip(ids, pinned)):
-            ms.upload(i, t.numpy(), capi.RME_CODEC_HEVC, 8, as_ref=True, stream=up[k & 1].cuda_stream)
+    def e2e_step(k):
+        b = k & 1
+        for j, (i, t) in enumerate(zip(ids, pinned)):
+            ms.upload(i, t.numpy(), capi.RME_CODEC_HEVC, 8, as_ref=True, stream=up[j & 1].cuda_stream)
         for u, e in zip(up, up_done):
             e.record(u)
             stream.wait_event(e)
-        return [v.numpy().view(capi.RESULT_DTYPE) for v in ms.search_batch(batch, p, sh, out=host_out)]
+        stream.wait_event(copied[b])
+        views = ms.search_batch(batch, p, sh, out=dev_out[b])
+        searched.record(stream)
+        cp.wait_event(searched)
+        with torch.cuda.stream(cp):
+            host_out[b].copy_(dev_out[b], non_blocking=True)
+        copied[b].record(cp)
+        base = dev_out[b].data_ptr()
+        return [(b, v.data_ptr() - base, v.numel()) for v in views]
 
-    for _ in range(2):
-        e2e_step()
+    for k in range(2):
+        e2e_step(k)
+    torch.cuda.synchronize()
     barrier(world)
     a = time.perf_counter()
-    for _ in range(args.steps):
-        e2e_out = e2e_step()
+    for k in range(args.steps):
+        e2e_last = e2e_step(k)
     torch.cuda.synchronize()
     e2e_secs = max_over_ranks(time.perf_counter() - a, world)
     e2e_value = job_rate(world, frames_per_step, args.steps, e2e_secs)
+    e2e_out = [host_out[b][o:o + n].numpy().view(capi.RESULT_DTYPE) for b, o, n in e2e_last]
     for o, q in zip(e2e_out, plain_out):
         if not (o == q).all():
             raise SystemExit("end-to-end results differ from the per-frame path")
