@@ -190,7 +190,11 @@ void Server::run() {
         continue;
       }
       const int nr = (int)std::min<int64_t>(st->nref, st->frames);
-      ++st->frames;
+      {
+        // The worker alone writes `frames`; submits read it under the lock.
+        std::lock_guard<std::mutex> lk(m);
+        ++st->frames;
+      }
       if (nr == 0) continue;
       rme_frame f{};
       f.src_id = pic;
