@@ -418,7 +418,12 @@ int rme_satd_batch(const void* a, int64_t a_stride, const int64_t* a_off,
  * the persistent search kernel). Streams are admitted against an HBM
  * budget; each stream keeps its reference pictures resident. Requests are
  * per-frame ME calls; they are admitted into free slots of the next launch
- * as they arrive, overlapping with work already on the device. */
+ * as they arrive, overlapping with work already on the device.
+ * open_stream, submit, poll and close_stream may be called from any host
+ * threads at once; stop once, after the others have returned. While a
+ * server runs, its context takes no other calls. The first frame of a
+ * stream has no reference and is not searched (`out` may be NULL for it;
+ * its completion reports 0 results). */
 typedef struct {
   uint64_t hbm_budget_bytes;  /* admission limit for resident pictures      */
   int32_t  max_frames_per_launch;
