@@ -16,7 +16,8 @@ Lines printed (one JSON line each; rank 0 only):
   default            the batched form: value = frames/s on the device with
                      inputs resident; e2e = the same through the C ABI from
                      pinned host memory (uploads + plane builds + search +
-                     results back inside the timed region); the plain
+                     results back inside the timed region, two steps in
+                     flight); the plain
                      per-frame path (one frame per call) beside it, p50/p99.
                      `served`: the serving loop under Poisson load (30 fps
                      streams, 20..120 % of the batched capacity), p50/p99
