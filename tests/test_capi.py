@@ -74,6 +74,17 @@ def test_every_struct_matches_the_c_compiler(tmp_path):
         assert got == int(val), f"{cname}.{what}: ctypes {got}, C {val}"
 
 
+def test_a_missing_library_fails_loudly(monkeypatch, tmp_path):
+    """Without the built library there is no search at all: loading raises
+    instead of falling back to anything on the CPU."""
+    monkeypatch.setattr(capi, "_lib", None)
+    monkeypatch.setattr(capi, "LIB_PATH", tmp_path / "librivet_me.so")
+    with pytest.raises(RuntimeError, match="no CPU fallback"):
+        capi.lib()
+    with pytest.raises(RuntimeError):
+        host.MotionSearch(0)
+
+
 def test_struct_layouts_match_the_header():
     assert C.sizeof(capi.Mv) == 4
     assert C.sizeof(capi.Result) == 32
