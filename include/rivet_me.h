@@ -534,11 +534,17 @@ typedef struct {
  * `src` (plane 0 read) and `refs[nref]` (all planes read) as above, `jobs`
  * and `out` (njobs each) in device memory. The same results as
  * rme_frame_search in GIVEN mode. The search's scratch lives in a fixed
- * 576 KiB device array inside the library, held on every device it is used
- * on until the process exits: at most 65536 jobs per call (RME_EINVAL
- * beyond). The first call on a device looks the array up (do it before any
- * stream capture); calls share the array, so calls that overlap on the GPU
- * race and must be serialised. Synchronous on `stream`. */
+ * device array of 541,952 bytes (about 529 KiB) inside the library, held on
+ * every device it is used on until the process exits: at most 65536 jobs per
+ * call (RME_EINVAL beyond). Parameters are held to the same limits as every
+ * other search (RME_EINVAL). The jobs are in device memory, so the host
+ * cannot check them: the kernel checks each job (reference index, seed
+ * count, block size and position) before it reads anything the job names,
+ * skips a job that fails and the call returns RME_EDEVICE; the other jobs'
+ * results are written as usual. The first call on a device looks the array
+ * up (do it before any stream capture); calls share the array, so calls
+ * that overlap on the GPU race and must be serialised. The call returns
+ * once the search on `stream` has finished (it synchronises the stream). */
 int rme_search_given_noalloc(const rme_picture_desc* d, const rme_params* p, const rme_plane_set* src,
                              const rme_plane_set* refs, int32_t nref, const rme_job* jobs, int32_t njobs,
                              rme_result* out, void* stream);

@@ -28,23 +28,7 @@
 
 #include "rme_internal.h"
 
-using namespace rme;
-
-namespace {
-
-// A launch's tasks split into parts by kind, one search kernel each:
-// part = 2 * (deeper than 8 bits) + (H.264).
-constexpr int kParts = 4;
-// The launch header in device memory (u64 words): head and tail of each
-// part's queue, then the counters, the status word and the epoch.
-// The launch header: head and tail of each part's queue (0..7), the
-// counters (8..12), status, epoch, then each part's finished-task count.
-constexpr int64_t kSpecTasks = 200000;  // about two 1080p frames of 2Nx2N PUs, 2 references
-constexpr int kMiscCounters = 8, kMiscStatus = 13, kMiscEpoch = 14, kMiscDone = 16, kMiscWords = 24;
-
-int part_of(const FrameDesc& fd) { return 2 * (fd.bd > 8) + (fd.codec == RME_CODEC_H264); }
-int part_bytes(int k) { return k >= 2 ? 2 : 1; }
-int part_codec(int k) { return (k & 1) ? RME_CODEC_H264 : RME_CODEC_HEVC; }
+namespace rme {
 
 // ---- Lagrangian tables -------------------------------------------------------
 float h264_mvd_bits(int d) {  // h264_hpel.rs:407-429
@@ -69,6 +53,59 @@ float hevc_lambda(int qp, int bd, float scale) {
   float base = 0.85f * std::exp2((float)(qp - 12) / 3.0f) * scale;
   return std::sqrt(base) * (float)(1u << (bd - 8));
 }
+void h264_cost_table(float lam, uint16_t* tab) {  // MvCostTable::new (h264_hpel.rs:453-459)
+  for (int d = -kMvSpan; d <= kMvSpan; ++d) tab[d + kMvSpan] = (uint16_t)std::min(lam * h264_mvd_bits(d) + 0.5f, 65535.0f);
+}
+
+const char* param_error(const rme_params* p, const rme_picture_desc& d) {
+  if (!p) return "null params";
+  if (p->codec != d.codec) return "params codec differs from the picture's";
+  if (p->predictor_mode != RME_PRED_GIVEN && p->predictor_mode != RME_PRED_STANDALONE) return "bad predictor_mode";
+  if (p->qp < -12 || p->qp > 63) return "qp out of range";
+  if (d.codec == RME_CODEC_H264) {
+    if (p->h264_pad < 8 || p->h264_pad > kH264Pad) return "h264_pad must be 8..32";
+    if (p->h264_range < 0 || p->h264_range > 512 || p->h264_hpel_iters < 0 || p->h264_qpel_iters < 0 ||
+        p->h264_hpel_iters > 64 || p->h264_qpel_iters > 64)
+      return "bad H.264 MeCfg";
+    // vertical_search is range - 1 of a level's MaxVmvR >= 0: at least -1.
+    // (A window emptied by it still clamps every point inside the plane.)
+    if (p->h264_vertical_range < -1) return "h264_vertical_range below -1";
+    if (!std::isfinite(p->h264_refine_ratio)) return "h264_refine_ratio must be finite";
+  } else {
+    if (p->hevc_pad < 8 || p->hevc_pad > kHevcPad) return "hevc_pad must be 8..80";
+    if (p->hevc_search_range < 0 || p->hevc_search_range > 1024 || p->hevc_search_rings < 0 ||
+        p->hevc_search_rings > 64)
+      return "bad HEVC search settings";
+    // Tune::lambda_of's multipliers are small positive numbers; a scale
+    // outside [0, 1024] (or not a number) has no finite per-bit price.
+    if (!(p->hevc_lambda_scale >= 0.0f && p->hevc_lambda_scale <= 1024.0f)) return "hevc_lambda_scale must be 0..1024";
+    if (p->predictor_mode == RME_PRED_STANDALONE && ((p->hevc_pu_mask & 0xF) == 0 || (p->hevc_pu_mask & ~0xF)))
+      return "hevc_pu_mask must select sizes among 8..64";
+    if (p->hevc_amp & ~0xF) return "hevc_amp selects among four AMP modes";
+  }
+  return nullptr;
+}
+
+}  // namespace rme
+
+using namespace rme;
+
+namespace {
+
+// A launch's tasks split into parts by kind, one search kernel each:
+// part = 2 * (deeper than 8 bits) + (H.264).
+constexpr int kParts = 4;
+// The launch header in device memory (u64 words): head and tail of each
+// part's queue, then the counters, the status word and the epoch.
+// The launch header: head and tail of each part's queue (0..7), the
+// counters (8..12), status, epoch, then each part's finished-task count.
+constexpr int64_t kSpecTasks = 200000;  // about two 1080p frames of 2Nx2N PUs, 2 references
+constexpr int kMiscCounters = 8, kMiscStatus = 13, kMiscEpoch = 14, kMiscDone = 16, kMiscWords = 24;
+
+int part_of(const FrameDesc& fd) { return 2 * (fd.bd > 8) + (fd.codec == RME_CODEC_H264); }
+int part_bytes(int k) { return k >= 2 ? 2 : 1; }
+int part_codec(int k) { return (k & 1) ? RME_CODEC_H264 : RME_CODEC_HEVC; }
+
 uint32_t h264_ref_bits_cost(float lam1, int r, int nref) {  // h264_analyse.rs:1934-1942
   float bits = nref == 1 ? 0.0f : nref == 2 ? 1.0f : (float)(2 * (32 - __builtin_clz((unsigned)(r + 1))) - 1);
   return (uint32_t)(lam1 * bits);
@@ -311,29 +348,8 @@ int count_blocks(const rme_picture_desc* d, const rme_params* p, int32_t* blocks
 }
 
 int check_params(Ctx* c, const rme_params* p, const rme_picture_desc& d) {
-  if (!p) return fail(c, RME_EINVAL, "null params");
-  if (p->codec != d.codec) return fail(c, RME_EINVAL, "params codec differs from the picture's");
-  if (p->predictor_mode != RME_PRED_GIVEN && p->predictor_mode != RME_PRED_STANDALONE)
-    return fail(c, RME_EINVAL, "bad predictor_mode");
-  if (p->qp < -12 || p->qp > 63) return fail(c, RME_EINVAL, "qp out of range");
-  if (d.codec == RME_CODEC_H264) {
-    if (p->h264_pad < 8 || p->h264_pad > kH264Pad) return fail(c, RME_EINVAL, "h264_pad must be 8..32");
-    if (p->h264_range < 0 || p->h264_range > 512 || p->h264_hpel_iters < 0 || p->h264_qpel_iters < 0 ||
-        p->h264_hpel_iters > 64 || p->h264_qpel_iters > 64)
-      return fail(c, RME_EINVAL, "bad H.264 MeCfg");
-    // vertical_search is range - 1 of a level's MaxVmvR >= 0: at least -1.
-    // (A window emptied by it still clamps every point inside the plane.)
-    if (p->h264_vertical_range < -1) return fail(c, RME_EINVAL, "h264_vertical_range below -1");
-  } else {
-    if (p->hevc_pad < 8 || p->hevc_pad > kHevcPad) return fail(c, RME_EINVAL, "hevc_pad must be 8..80");
-    if (p->hevc_search_range < 0 || p->hevc_search_range > 1024 || p->hevc_search_rings < 0 ||
-        p->hevc_search_rings > 64)
-      return fail(c, RME_EINVAL, "bad HEVC search settings");
-    if (p->predictor_mode == RME_PRED_STANDALONE && ((p->hevc_pu_mask & 0xF) == 0 || (p->hevc_pu_mask & ~0xF)))
-      return fail(c, RME_EINVAL, "hevc_pu_mask must select sizes among 8..64");
-    if (p->hevc_amp & ~0xF) return fail(c, RME_EINVAL, "hevc_amp selects among four AMP modes");
-  }
-  return 0;
+  const char* why = param_error(p, d);
+  return why ? fail(c, RME_EINVAL, why) : 0;
 }
 
 const Tables* get_tables(Ctx* c, const rme_params* p, int bd, int* rc) {
@@ -347,7 +363,7 @@ const Tables* get_tables(Ctx* c, const rme_params* p, int bd, int* rc) {
   if (p->codec == RME_CODEC_H264) {
     std::vector<uint16_t> tab(kMvTab);
     float lam = h264_lambda_satd(p->qp);
-    for (int d = -kMvSpan; d <= kMvSpan; ++d) tab[d + kMvSpan] = (uint16_t)std::min(lam * h264_mvd_bits(d) + 0.5f, 65535.0f);
+    h264_cost_table(lam, tab.data());
     t.lam = lam;
     cudaError_t e = cudaMalloc(&t.tab, kMvTab * sizeof(uint16_t));
     if (e == cudaSuccess) e = cudaMemcpy(t.tab, tab.data(), kMvTab * sizeof(uint16_t), cudaMemcpyHostToDevice);

@@ -87,6 +87,16 @@ struct LaunchDesc {
                                  // leave once every task is done
 };
 
+// Host helpers shared by the entry points (rme_capi.cu; f32 arithmetic
+// compiled without contraction, so it rounds as the reference's Rust does).
+float h264_mvd_bits(int d);                  // h264_hpel.rs:407-429
+float h264_lambda_satd(int qp);              // h264_analyse.rs:402-404
+float hevc_lambda(int qp, int bd, float scale);  // h265_intra.rs:1141-2013
+void h264_cost_table(float lam, uint16_t* tab);  // kMvTab entries, MvCostTable::new
+// Why a parameter block cannot be searched for a picture of `d`'s format,
+// or null when it can.
+const char* param_error(const rme_params* p, const rme_picture_desc& d);
+
 // Launch wrappers (defined in the .cu files).
 cudaError_t launch_pad_plane(const void* src, int bd, int w, int h, int sstride, DevPlanes dst, int cw, int ch,
                              int pad, cudaStream_t s);

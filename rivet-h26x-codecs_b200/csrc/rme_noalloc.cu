@@ -37,9 +37,11 @@ constexpr size_t kOffSlots = 17664; // queue slots (kNoAllocMaxJobs x u64)
 constexpr size_t kScratchBytes = kOffSlots + (size_t)kNoAllocMaxJobs * 8;
 static_assert(sizeof(FrameDesc) <= kOffMisc - kOffFrame, "frame descriptor outgrew its scratch slot");
 static_assert(kOffTab + kMvTab * sizeof(uint16_t) <= kOffSlots, "rate table outgrew its scratch slot");
+static_assert(kScratchBytes == 541952, "the documented scratch size");
 
-// The scratch (576 KiB). Device code could name it directly; host code
-// must use the address cudaGetSymbolAddress returns, never the symbol.
+// The scratch: 541,952 bytes (about 529 KiB). Device code could name it
+// directly; host code must use the address cudaGetSymbolAddress returns,
+// never the symbol.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 __global__ void fill_ready(unsigned long long* slots, int n, uint32_t epoch) {
@@ -53,24 +55,6 @@ struct DeviceScratch {
 };
 std::mutex g_mu;
 DeviceScratch g_dev[64];
-
-float h264_mvd_bits(int d) {  // h264_hpel.rs:407-429, f32 as the reference
-  uint32_t a = (uint32_t)std::abs(d);
-  if (a == 0) return 1.0f;
-  float prefix = (float)std::min(a, 9u);
-  float bits = 1.0f + 0.85f * prefix;
-  if (a < 9) {
-    bits += 0.85f;
-  } else {
-    uint32_t v = a - 9, k = 3;
-    while (v >= (1u << k)) {
-      v -= 1u << k;
-      k += 1;
-    }
-    bits += (float)(k - 3 + 1 + k);
-  }
-  return bits + 1.0f;
-}
 
 bool plane_ok(const rme_plane_set& ps, int need_pad, int cw, int ch) {
   return ps.base && ps.pad >= need_pad && ps.stride >= cw + 2 * ps.pad &&
@@ -89,13 +73,13 @@ extern "C" int rme_search_given_noalloc(const rme_picture_desc* d, const rme_par
   if (d->codec != RME_CODEC_H264 && d->codec != RME_CODEC_HEVC) return RME_EINVAL;
   if (d->bit_depth < 8 || d->bit_depth > 12 || d->width < 16 || d->height < 16) return RME_EINVAL;
   if (p->codec != d->codec || p->predictor_mode != RME_PRED_GIVEN) return RME_EINVAL;
+  if (param_error(p, *d)) return RME_EINVAL;  // the limits every other search entry point applies
   if (nref < 1 || nref > RME_MAX_REFS) return RME_EINVAL;
   if (njobs < 0 || njobs > kNoAllocMaxJobs) return RME_EINVAL;  // beyond the scratch's queue
   if (njobs == 0) return RME_OK;
   const bool h264 = d->codec == RME_CODEC_H264;
   const int cw = h264 ? (d->width + 15) / 16 * 16 : d->width, ch = h264 ? (d->height + 15) / 16 * 16 : d->height;
   const int pad = h264 ? p->h264_pad : p->hevc_pad;
-  if (pad < 8 || pad > (h264 ? kH264Pad : kHevcPad)) return RME_EINVAL;
   if (!plane_ok(*src, pad, cw, ch)) return RME_EINVAL;
   for (int r = 0; r < nref; ++r)
     if (!plane_ok(refs[r], pad, cw, ch)) return RME_EINVAL;
@@ -144,8 +128,7 @@ extern "C" int rme_search_given_noalloc(const rme_picture_desc* d, const rme_par
   fd.ntasks = njobs;
   static thread_local uint16_t tab[kMvTab];
   if (h264) {
-    const float lam = std::sqrt(0.85f * std::exp2((float)(p->qp - 12) / 3.0f));
-    for (int k = -kMvSpan; k <= kMvSpan; ++k) tab[k + kMvSpan] = (uint16_t)std::min(lam * h264_mvd_bits(k) + 0.5f, 65535.0f);
+    h264_cost_table(h264_lambda_satd(p->qp), tab);
     fd.tab = reinterpret_cast<const uint16_t*>(base + kOffTab);
     fd.range = p->h264_range;
     fd.hpel_iters = p->h264_hpel_iters;
@@ -156,8 +139,7 @@ extern "C" int rme_search_given_noalloc(const rme_picture_desc* d, const rme_par
     fd.vr = p->h264_vertical_range;
     fd.refine_ratio = p->h264_refine_ratio;
   } else {
-    const float basel = 0.85f * std::exp2((float)(p->qp - 12) / 3.0f) * p->hevc_lambda_scale;
-    fd.lam = std::sqrt(basel) * (float)(1u << (d->bit_depth - 8));
+    fd.lam = hevc_lambda(p->qp, d->bit_depth, p->hevc_lambda_scale);
     fd.search_range = p->hevc_search_range;
     fd.search_rings = p->hevc_search_rings;
     fd.quarter_cross = p->hevc_quarter_cross;

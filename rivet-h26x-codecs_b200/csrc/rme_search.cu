@@ -3,8 +3,8 @@
 // from a device work queue.
 //
 // What a task computes is the reference's search, step for step:
-//   HEVC   search_full   (encode/h265_me.rs:3749-3858): seeds rounded
-//          toward zero (>> 2), clamp_pos to +-(pad - MARGIN), deduplicated
+//   HEVC   search_full   (encode/h265_me.rs:3749-3858): seeds floored to
+//          whole samples (arithmetic >> 2), clamp_pos to +-(pad - MARGIN), deduplicated
 //          through `tried`, scored SAD + (lam * mv_bits) as u32, strict <;
 //          then the small diamond (1,0),(-1,0),(0,1),(0,-1) from a fixed
 //          `from`, at most 2 * range rounds, inside +-range of the best
@@ -367,6 +367,19 @@ __device__ __forceinline__ void count_task(WarpSmem<S>& sm, int lane, uint32_t n
   }
 }
 
+// A GIVEN job as the host checks it before a launch (reference index,
+// seed count, a block of 4..64 in multiples of 4 inside the coded picture).
+// The kernel checks it again before reading anything the job points at,
+// because jobs handed over in device memory never pass the host's check: a
+// job that fails sets kStatusBadTask (the call returns RME_EDEVICE) and its
+// result is left unwritten.
+__device__ __forceinline__ bool given_job_ok(const FrameDesc& F, const rme_job* j, int max_seeds) {
+  const int ref = j->ref, ns = j->nseeds, x = j->x, y = j->y, w = j->w, h = j->h;
+  return ref >= 0 && ref < F.nref && ref < RME_MAX_REFS && ns >= 0 && ns <= max_seeds && w >= 4 && h >= 4 &&
+         w <= 64 && h <= 64 && (w & 3) == 0 && (h & 3) == 0 && x >= 0 && y >= 0 && x <= F.width - w &&
+         y <= F.height - h;
+}
+
 __device__ __forceinline__ void write_result(rme_result* o, int mvx, int mvy, int ref, uint32_t cost, uint32_t satd,
                                              int imx, int imy, uint32_t icost, uint32_t nsad, uint32_t nsatd,
                                              int lane) {
@@ -511,6 +524,10 @@ __device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
   rme_result* out;
   if (F.mode == RME_PRED_GIVEN) {
     const rme_job* j = &F.jobs[t];
+    if (!given_job_ok(F, j, RME_MAX_SEEDS)) {
+      if (lane == 0) atomicOr(L.status, kStatusBadTask);
+      return -1;
+    }
     r = j->ref;
     x = j->x;
     y = j->y;
@@ -1168,6 +1185,10 @@ __device__ int h264_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
   };
   if (F.mode == RME_PRED_GIVEN) {
     const rme_job* j = &F.jobs[t];
+    if (!given_job_ok(F, j, 8)) {  // p_mb's cands: at most 8
+      if (lane == 0) atomicOr(L.status, kStatusBadTask);
+      return -1;
+    }
     shape(j->x, j->y, j->w, j->h);
     B.px = j->mvp[0].x;
     B.py = j->mvp[0].y;

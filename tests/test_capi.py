@@ -30,16 +30,23 @@ def test_the_library_exports_every_declared_entry_point():
 
 
 def test_the_rust_declarations_match_the_header():
-    """The integration notes' FFI block declares every entry point with the
-    header's parameter count, and the ctypes binding agrees on it too."""
+    """The Rust FFI module (include/rivet_me_sys.rs) declares every entry
+    point with the header's parameter count, and the ctypes binding agrees
+    on it too."""
     text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
     c_args = {n: (0 if a.strip() in ("", "void") else a.count(",") + 1)
               for n, a in re.findall(r"\b(rme_[a-z0-9_]+)\s*\(([^;]*?)\)\s*;", text)}
-    notes = (HEADER.parents[1] / "INTEGRATION.md").read_text()
-    rust = {n: len(re.findall(r"\b\w+\s*:", a)) for n, a in re.findall(r"pub fn (rme_[a-z0-9_]+)\(([^)]*)\)", notes)}
+    sys_rs = (HEADER.parent / "rivet_me_sys.rs").read_text()
+    rust = {n: len(re.findall(r"\b\w+\s*:", a)) for n, a in re.findall(r"pub fn (rme_[a-z0-9_]+)\(([^)]*)\)", sys_rs)}
     assert set(c_args) == set(declared())
     assert {n: c_args[n] for n in rust} == rust and set(rust) == set(c_args), set(c_args) ^ set(rust)
     assert {n: len(capi.SIGNATURES[n][1]) for n in c_args} == c_args
+    # and every struct, field for field in the header's order
+    rs_structs = {n: re.findall(r"pub (?:r#)?(\w+)\s*:", body)
+                  for n, body in re.findall(r"pub struct (rme_[a-z0-9_]+)\s*\{(.*?)\}", sys_rs, flags=re.S)}
+    assert set(rs_structs) == set(_STRUCTS), set(rs_structs) ^ set(_STRUCTS)
+    for cname, pyname in _STRUCTS.items():
+        assert rs_structs[cname] == [f for f, _ in getattr(capi, pyname)._fields_], cname
 
 
 _STRUCTS = {"rme_mv": "Mv", "rme_picture_desc": "PictureDesc", "rme_params": "Params", "rme_job": "Job",
@@ -173,6 +180,30 @@ def test_invalid_arguments_are_refused_without_a_device():
     # and a misaligned plane
     mis = capi.PlaneSet(18, 224 * 224, 224, 80)
     assert lib.rme_search_given_noalloc(C.byref(d), C.byref(p), C.byref(mis), refs, 1, C.c_void_p(16), 4,
+                                        C.c_void_p(16), None) == capi.RME_EINVAL
+
+
+@pytest.mark.parametrize("codec,field,value", [
+    (1, "qp", 64), (1, "qp", -13), (1, "hevc_search_range", 1025), (1, "hevc_search_rings", 65),
+    (1, "hevc_search_range", -1), (1, "hevc_lambda_scale", float("nan")), (1, "hevc_lambda_scale", -1.0),
+    (1, "hevc_lambda_scale", float("inf")), (1, "hevc_pad", 81), (1, "hevc_pad", 7),
+    (0, "h264_hpel_iters", 65), (0, "h264_qpel_iters", -1), (0, "h264_range", 513), (0, "h264_pad", 33),
+    (0, "h264_vertical_range", -2), (0, "h264_refine_ratio", float("nan")),
+])
+def test_the_search_without_allocation_holds_parameters_to_the_common_limits(codec, field, value):
+    """Every bad parameter is refused (RME_EINVAL) before anything reaches a
+    device: a QP whose Lagrangian is not finite, an unbounded walk (range,
+    rings, refinement iterations) that would make one launch run for ever."""
+    lib = capi.lib()
+    d = capi.PictureDesc(codec, 8, 64, 64, 64)
+    p = capi.default_params(codec, 30)
+    p.predictor_mode = capi.RME_PRED_GIVEN
+    setattr(p, field, value)
+    pad = 80 if codec == 1 else 32
+    cols = 64 + 2 * pad
+    ps = capi.PlaneSet(16, cols * cols, cols, pad)
+    refs = (capi.PlaneSet * 1)(ps)
+    assert lib.rme_search_given_noalloc(C.byref(d), C.byref(p), C.byref(ps), refs, 1, C.c_void_p(16), 4,
                                         C.c_void_p(16), None) == capi.RME_EINVAL
 
 

@@ -84,3 +84,67 @@ def test_no_alloc_search_refuses_more_jobs_than_its_scratch_holds(ms):
     rc = capi.lib().rme_search_given_noalloc(C.byref(d), C.byref(p), C.byref(ps), refs, 1, C.c_void_p(16),
                                              65537, C.c_void_p(16), None)
     assert rc == capi.RME_EINVAL
+
+
+# Each malformed job the kernel must refuse before reading anything it names:
+# (field, value) pairs over a good job, per codec.
+_BAD_JOBS = [("ref", 2), ("ref", -1), ("w", 68), ("w", 6), ("h", 0), ("x", 160), ("y", -4), ("x", 152),
+             ("nseeds", -1)]
+
+
+@pytest.mark.parametrize("codec", [capi.RME_CODEC_HEVC, capi.RME_CODEC_H264])
+def test_no_alloc_search_refuses_a_malformed_job_and_keeps_the_others(ms, codec):
+    """The jobs live in device memory, where the host cannot check them: a
+    job naming a reference past the list, a block of a bad size or outside
+    the picture, or more seeds than the job holds is refused on the device
+    (the call returns RME_EDEVICE, its result slot is left as it was) and
+    every other job's result is the allocating search's. The next call,
+    with good jobs only, is exact again."""
+    import torch
+    bd = 8
+    rng = np.random.default_rng(77 + codec)
+    w, h = 160, 96
+    ref0 = random_picture(rng, w, h, bd)
+    ref1 = shifted(ref0, 2, 1, rng, 1.0)
+    src = shifted(ref0, -3, 2, rng, 1.0)
+    base = 760 + 10 * codec
+    ms.upload(base, src, codec, bd, as_ref=True)
+    ms.upload(base + 1, ref0, codec, bd, as_ref=True)
+    ms.upload(base + 2, ref1, codec, bd, as_ref=True)
+    p = capi.default_params(codec, 30)
+    p.predictor_mode = capi.RME_PRED_GIVEN
+    sizes = ((16, 16), (8, 8), (16, 8)) if codec == capi.RME_CODEC_H264 else ((8, 8), (16, 16), (32, 32))
+    jobs = random_jobs(rng, codec, w, h, 2, 64, sizes=sizes)
+    want = ms.search(base, [base + 1, base + 2], p, jobs)
+    nplanes = 4 if codec == capi.RME_CODEC_H264 else 16
+    bufs = [_caller_planes(ms, i, nplanes, w) for i in (base, base + 1, base + 2)]
+    src_ps = bufs[0][1]
+    refs = (capi.PlaneSet * 2)(bufs[1][1], bufs[2][1])
+    d = capi.PictureDesc(codec, bd, w, h, w)
+    too_many = 9 if codec == capi.RME_CODEC_H264 else capi.RME_MAX_SEEDS + 1
+    cases = _BAD_JOBS + [("nseeds", too_many)]
+    rsize = capi.RESULT_DTYPE.itemsize
+    for k, (field, value) in enumerate(cases):
+        bad = jobs.copy()
+        i = (7 * k + 3) % len(jobs)
+        bad[i][field] = value
+        if field == "x" and value == 152:  # inside the picture, but 8 + 16 past its right edge
+            bad[i]["w"] = 16
+        d_jobs = torch.from_numpy(bad.view(np.uint8).copy()).cuda()
+        d_out = torch.full((len(jobs) * rsize,), 0xAB, dtype=torch.uint8, device="cuda")
+        rc = capi.lib().rme_search_given_noalloc(C.byref(d), C.byref(p), C.byref(src_ps), refs, 2,
+                                                 C.c_void_p(d_jobs.data_ptr()), len(jobs),
+                                                 C.c_void_p(d_out.data_ptr()), None)
+        assert rc == capi.RME_EDEVICE, (field, value, rc)
+        raw = d_out.cpu().numpy()
+        assert (raw[i * rsize:(i + 1) * rsize] == 0xAB).all(), f"{field}={value}: the refused job's slot was written"
+        got = raw.view(capi.RESULT_DTYPE)
+        keep = np.arange(len(jobs)) != i
+        assert_results_equal(got[keep], want[keep], f"{field}={value}: the other jobs")
+    d_jobs = torch.from_numpy(jobs.view(np.uint8).copy()).cuda()
+    d_out = torch.zeros(len(jobs) * rsize, dtype=torch.uint8, device="cuda")
+    rc = capi.lib().rme_search_given_noalloc(C.byref(d), C.byref(p), C.byref(src_ps), refs, 2,
+                                             C.c_void_p(d_jobs.data_ptr()), len(jobs),
+                                             C.c_void_p(d_out.data_ptr()), None)
+    assert rc == capi.RME_OK, rc
+    assert_results_equal(d_out.cpu().numpy().view(capi.RESULT_DTYPE), want, "good jobs after the refused ones")
