@@ -278,10 +278,16 @@ struct HevcRef {
 };
 
 template <class S>
-void hevc_prepare_ref(HevcRef<S>& r, const S* luma, int W, int H, ptrdiff_t ss, int pad, int bd) {
+Interp<S> pick_interp(int simd);
+
+// `simd`: the phase planes through the AVX2 interpolation rung where the
+// CPU has it (the same planes).
+template <class S>
+void hevc_prepare_ref(HevcRef<S>& r, const S* luma, int W, int H, ptrdiff_t ss, int pad, int bd, int simd = 0) {
   r.g = Plane<S>(W, H, pad);
   r.g.load(luma, ss);
-  r.hp.build(r.g, bd);
+  const Interp<S> I = pick_interp<S>(simd);
+  r.hp.build(r.g, bd, false, &I);
 }
 
 template <class S>
@@ -399,6 +405,14 @@ template <>
 Dist<uint16_t> pick_dist<uint16_t>(int simd) {
   return simd && have_avx2() ? dist_avx2_u16() : dist_scalar<uint16_t>();
 }
+template <>
+Interp<uint8_t> pick_interp<uint8_t>(int simd) {
+  return simd && have_avx2() ? interp_avx2_u8() : interp_scalar<uint8_t>();
+}
+template <>
+Interp<uint16_t> pick_interp<uint16_t>(int simd) {
+  return simd && have_avx2() ? interp_avx2_u16() : interp_scalar<uint16_t>();
+}
 
 bool valid_desc(const rme_picture_desc* d) {
   return d && (d->codec == RME_CODEC_H264 || d->codec == RME_CODEC_HEVC) && d->bit_depth >= 8 &&
@@ -438,7 +452,7 @@ int run_frames(const rme_picture_desc* d, int nframes, const void* const* srcs, 
   };
   parallel((int)uniq.size(), [&](int i) {
     if (h264) h264_prepare_ref(r264[i], (const S*)uniq[i], W, H, ss, p->h264_pad, bd);
-    else hevc_prepare_ref(r265[i], (const S*)uniq[i], W, H, ss, p->hevc_pad, bd);
+    else hevc_prepare_ref(r265[i], (const S*)uniq[i], W, H, ss, p->hevc_pad, bd, simd);
   });
   auto t1 = std::chrono::steady_clock::now();
   parallel(nframes, [&](int f) {
@@ -1438,8 +1452,10 @@ int orc_h264_planes(const rme_picture_desc* d, const void* luma, int32_t pad, vo
 }
 
 // HEVC: the padded plane and its fifteen fractional phases (16 planes;
-// phases HalfPlanes left unbuilt are zero), and HalfPlanes::ext.
-int orc_hevc_planes(const rme_picture_desc* d, const void* luma, int32_t pad, int32_t force_quarter, void* out,
+// phases HalfPlanes left unbuilt are zero), and HalfPlanes::ext. `flags`:
+// bit 0 builds the quarter phases at any size, bit 1 interpolates with the
+// AVX2 rung.
+int orc_hevc_planes(const rme_picture_desc* d, const void* luma, int32_t pad, int32_t flags, void* out,
                     int32_t* ext) {
   if (!valid_desc(d)) return RME_EINVAL;
   auto run = [&](auto tag) {
@@ -1447,7 +1463,8 @@ int orc_hevc_planes(const rme_picture_desc* d, const void* luma, int32_t pad, in
     HevcRef<S> r;
     r.g = Plane<S>(d->width, d->height, pad);
     r.g.load((const S*)luma, d->stride);
-    r.hp.build(r.g, d->bit_depth, force_quarter != 0);
+    const Interp<S> I = pick_interp<S>((flags >> 1) & 1);
+    r.hp.build(r.g, d->bit_depth, (flags & 1) != 0, &I);
     size_t n = r.g.data.size();
     std::memcpy((S*)out, r.g.data.data(), n * sizeof(S));
     for (int k = 0; k < 15; ++k) {

@@ -584,6 +584,24 @@ void hevc_uni(S* dst, ptrdiff_t ds, const int16_t* src, int w, int h, int shift,
     for (int x = 0; x < w; ++x) dst[y * ds + x] = (S)std::clamp(((int)src[y * w + x] + round) >> shift, 0, maxv);
 }
 
+// The luma interpolation passes HalfPlanes::build runs, as a table: the
+// scalar forms above, or the AVX2 rungs (me_oracle_avx2.cpp, following the
+// pairwise-multiply-add design of dsp/hevc_avx2.rs / hevc_avx2_u8.rs), which
+// must give the same numbers (tests/test_oracle.py compares the planes).
+template <class S>
+struct Interp {
+  void (*h8)(int16_t*, const S*, ptrdiff_t, int, int, const int8_t*, int);
+  void (*v8)(int16_t*, const S*, ptrdiff_t, int, int, const int8_t*, int);
+  void (*v2_8)(int16_t*, const int16_t*, int, int, int, const int8_t*);
+  void (*uni)(S*, ptrdiff_t, const int16_t*, int, int, int, int);
+};
+template <class S>
+Interp<S> interp_scalar() {
+  return Interp<S>{&filt_h<S, 8>, &filt_v<S, 8>, &filt_v2<8>, &hevc_uni<S>};
+}
+Interp<uint8_t> interp_avx2_u8();
+Interp<uint16_t> interp_avx2_u16();
+
 // One component's 14-bit prediction of a w x h block at integer position
 // (xi, yi) with fractions (xf, yf): hevc/inter.rs:92-124 `source` (window
 // gathered with at_clamped when it leaves the padded plane) and 130-196
@@ -642,7 +660,8 @@ struct HalfPlanes {
 
   // HalfPlanes::new (h265_search.rs:79-170), 64x64 tiles over the plane
   // less MARGIN, REACH samples outside the picture.
-  void build(const Plane<S>& p, int bd, bool force_quarter = false) {
+  void build(const Plane<S>& p, int bd, bool force_quarter = false, const Interp<S>* rung = nullptr) {
+    const Interp<S> I = rung ? *rung : interp_scalar<S>();
     const int T = 64;
     stride = p.stride;
     int rows = p.rows();
@@ -666,13 +685,13 @@ struct HalfPlanes {
           bool any = false;
           for (int fy = 1; fy < 4; ++fy) any = any || wanted(fx, fy);
           if (fx != 0 && any)
-            filt_h<S, 8>(tmp.data(), d + at - 3 * stride - 3, stride, tw, th + 7, QPEL_FILTERS[fx], shift1);
+            I.h8(tmp.data(), d + at - 3 * stride - 3, stride, tw, th + 7, QPEL_FILTERS[fx], shift1);
           for (int fy = 0; fy < 4; ++fy) {
             if ((fx == 0 && fy == 0) || !wanted(fx, fy)) continue;
-            if (fy == 0) filt_h<S, 8>(out14.data(), d + at - 3, stride, tw, th, QPEL_FILTERS[fx], shift1);
-            else if (fx == 0) filt_v<S, 8>(out14.data(), d + at - 3 * stride, stride, tw, th, QPEL_FILTERS[fy], shift1);
-            else filt_v2<8>(out14.data(), tmp.data(), tw, tw, th, QPEL_FILTERS[fy]);
-            hevc_uni(planes[fy * 4 + fx - 1].data() + at, stride, out14.data(), tw, th, shift3, maxv);
+            if (fy == 0) I.h8(out14.data(), d + at - 3, stride, tw, th, QPEL_FILTERS[fx], shift1);
+            else if (fx == 0) I.v8(out14.data(), d + at - 3 * stride, stride, tw, th, QPEL_FILTERS[fy], shift1);
+            else I.v2_8(out14.data(), tmp.data(), tw, tw, th, QPEL_FILTERS[fy]);
+            I.uni(planes[fy * 4 + fx - 1].data() + at, stride, out14.data(), tw, th, shift3, maxv);
           }
         }
         x0 += tw;

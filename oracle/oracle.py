@@ -285,11 +285,14 @@ def h264_planes(pic: np.ndarray, bit_depth: int, pad: int = 32) -> np.ndarray:
     return out
 
 
-def hevc_planes(pic: np.ndarray, bit_depth: int, pad: int = 80, force_quarter: bool = False):
+def hevc_planes(pic: np.ndarray, bit_depth: int, pad: int = 80, force_quarter: bool = False, simd: int = 0):
+    """The padded plane and its 15 phases (HalfPlanes), interpolated by the
+    scalar passes or (simd=1) the AVX2 rung."""
     d = desc(capi.RME_CODEC_HEVC, pic, bit_depth)
     out = np.zeros((16, d.height + 2 * pad, d.width + 2 * pad), pic.dtype)
     ext = C.c_int32()
-    assert lib().orc_hevc_planes(C.byref(d), pic.ctypes.data, pad, int(force_quarter), out.ctypes.data,
+    flags = int(force_quarter) | (2 if simd else 0)
+    assert lib().orc_hevc_planes(C.byref(d), pic.ctypes.data, pad, flags, out.ctypes.data,
                                  C.byref(ext)) == 0
     return out, ext.value
 

@@ -84,14 +84,28 @@ def test_the_avx2_rungs_equal_the_scalar_kernels(bd):
     rng = np.random.default_rng(bd)
     dt = np.uint8 if bd == 8 else np.uint16
     for _ in range(60):
-        w = int(rng.choice([4, 8, 12, 16, 24, 32, 48, 64]))
-        h = int(rng.choice([4, 8, 12, 16, 32, 64]))
+        w = int(rng.choice([4, 8, 12, 16, 24, 32, 40, 48, 56, 64]))
+        h = int(rng.choice([4, 8, 12, 16, 24, 32, 48, 64]))
         a = rng.integers(0, 1 << bd, size=(70, 80)).astype(dt)
         b = rng.integers(0, 1 << bd, size=(70, 80)).astype(dt)
         x, y = int(rng.integers(0, 80 - w)), int(rng.integers(0, 70 - h))
         sa, sb = a[y:y + h, x:x + w], b[y:y + h, x:x + w]
         assert oracle.sad(bd, sa, sb, 1) == oracle.sad(bd, sa, sb, 0)
         assert oracle.satd(bd, sa, sb, 1) == oracle.satd(bd, sa, sb, 0)
+
+
+@pytest.mark.parametrize("bd", [8, 10, 12])
+@pytest.mark.parametrize("w,h,force", [(200, 120, True), (96, 64, False), (131, 77, True)])
+def test_the_avx2_interpolation_rung_builds_the_same_planes(bd, w, h, force):
+    """The timed CPU baseline builds HalfPlanes with AVX2 qpel_h / qpel_v /
+    qpel_v2 / uni passes: every phase plane must be the scalar one exactly,
+    tile edges and ragged widths included."""
+    rng = np.random.default_rng(100 + bd + w)
+    pic = rng.integers(0, 1 << bd, size=(h, w)).astype(np.uint8 if bd == 8 else np.uint16)
+    a, ea = oracle.hevc_planes(pic, bd, force_quarter=force, simd=0)
+    b, eb = oracle.hevc_planes(pic, bd, force_quarter=force, simd=1)
+    assert ea == eb
+    np.testing.assert_array_equal(a, b)
 
 
 # ---- planes -----------------------------------------------------------------------
