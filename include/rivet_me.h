@@ -248,6 +248,31 @@ int rme_batch_search(void* ctx, const rme_frame* frames, const rme_params* param
                      int32_t nframes, rme_result* out, const int64_t* offsets,
                      void* stream);
 
+/* The asynchronous forms of rme_frame_search / rme_batch_search (the
+ * `rme_search(..., stream)` + `rme_sync` pair of the batched boundary): the
+ * launch is queued on `stream` (NULL: the context's own) and the call
+ * returns at once; `out` must be device memory or pinned host memory
+ * (RME_EINVAL otherwise), and holds the results once the stream has reached
+ * the end of the launch. This is what lets an encoder overlap its mode
+ * decision for picture t (pick_pu, encode/h265_me.rs:1349,1363; p_mb,
+ * encode/h264_analyse.rs:1957-1966) with the search of picture t+1. The
+ * pictures the frames name must stay uploaded until rme_sync. At most four
+ * launches of one context are in flight: a fifth call waits for the oldest
+ * first (its error, if any, is kept for its stream's rme_sync). */
+int rme_frame_search_async(void* ctx, const rme_frame* f, const rme_params* p,
+                           rme_result* out, void* stream);
+int rme_batch_search_async(void* ctx, const rme_frame* frames, const rme_params* params,
+                           int32_t nframes, rme_result* out, const int64_t* offsets,
+                           void* stream);
+
+/* Wait for every asynchronous search of this context queued on `stream`
+ * (NULL: the context's own) and report how they went: 0 when all were
+ * complete and correct; RME_EDEVICE with `device_status` (may be NULL) set
+ * to the device status bits when a kernel reported a failure (1: a bounded
+ * wait ran out, 2: a malformed task); the first other error otherwise.
+ * rme_last_stats then describes the last launch finished. */
+int rme_sync(void* ctx, void* stream, uint32_t* device_status);
+
 /* The STANDALONE decision over a frame's HEVC results (host side, cheap):
  * per block the reference with the least cost + lambda * ref_idx bits, and
  * the quadtree of 2Nx2N sizes whose summed costs are least. `best` gets one

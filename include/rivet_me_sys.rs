@@ -61,6 +61,11 @@ extern "C" {
                             out: *mut rme_result, stream: *mut c_void) -> i32;
     pub fn rme_batch_search(ctx: *mut c_void, frames: *const rme_frame, params: *const rme_params,
                             n: i32, out: *mut rme_result, offsets: *const i64, stream: *mut c_void) -> i32;
+    pub fn rme_frame_search_async(ctx: *mut c_void, f: *const rme_frame, p: *const rme_params,
+                                  out: *mut rme_result, stream: *mut c_void) -> i32;
+    pub fn rme_batch_search_async(ctx: *mut c_void, frames: *const rme_frame, params: *const rme_params,
+                                  n: i32, out: *mut rme_result, offsets: *const i64, stream: *mut c_void) -> i32;
+    pub fn rme_sync(ctx: *mut c_void, stream: *mut c_void, device_status: *mut u32) -> i32;
     pub fn rme_picture_upload_chroma(ctx: *mut c_void, pic_id: i32, cb: *const c_void, cr: *const c_void,
                                      cstride: i32, stream: *mut c_void) -> i32;
     pub fn rme_chroma_predict(ctx: *mut c_void, ref_id: i32, nblocks: i32, blocks: *const i32,

@@ -135,6 +135,10 @@ SIGNATURES = {
     "rme_frame_search": (C.c_int, [_vp, C.POINTER(Frame), C.POINTER(Params), C.POINTER(Result), _vp]),
     "rme_batch_search": (C.c_int, [_vp, C.POINTER(Frame), C.POINTER(Params), _i32, C.POINTER(Result),
                                    C.POINTER(C.c_int64), _vp]),
+    "rme_frame_search_async": (C.c_int, [_vp, C.POINTER(Frame), C.POINTER(Params), C.POINTER(Result), _vp]),
+    "rme_batch_search_async": (C.c_int, [_vp, C.POINTER(Frame), C.POINTER(Params), _i32, C.POINTER(Result),
+                                         C.POINTER(C.c_int64), _vp]),
+    "rme_sync": (C.c_int, [_vp, _vp, C.POINTER(C.c_uint32)]),
     "rme_hevc_decide": (C.c_int, [C.POINTER(PictureDesc), C.POINTER(Params), _i32, C.POINTER(Result),
                                   C.POINTER(C.c_int32), C.POINTER(C.c_uint8)]),
     "rme_last_stats": (C.c_int, [_vp, C.POINTER(Stats)]),

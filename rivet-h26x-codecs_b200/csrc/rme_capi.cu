@@ -192,6 +192,39 @@ struct Graph {
   int seen = 0;  // launches of this shape so far: captured on the second
 };
 
+// One search launch's buffers and events. A context keeps kSlots of them and
+// takes them in turn: a synchronous search finishes its launch before it
+// returns; an asynchronous one leaves it in flight on the caller's stream
+// until rme_sync (or until its slot comes round again, which waits for it).
+constexpr int kSlots = 4;
+struct Slot {
+  DevBuf<FrameDesc> d_frames;
+  DevBuf<unsigned long long> d_ready;  // the dataflow queue's slots
+  DevBuf<rme_result> d_out;
+  DevBuf<int32_t> d_pending;
+  DevBuf<rme_job> d_jobs;
+  DevBuf<unsigned long long> d_misc;  // the launch header (kMisc*)
+  PinBuf<FrameDesc> h_frames;
+  PinBuf<rme_result> h_out;
+  PinBuf<unsigned long long> h_misc;
+  PinBuf<unsigned long long> h_init;  // [misc header | initial queue entries]
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, done = nullptr;
+  uint32_t epoch = 0;
+  // The launch in flight: its stream, its task count, the tuner class it
+  // times, and (synchronous calls into pageable memory) where its results go.
+  bool busy = false;
+  cudaStream_t stream = nullptr;
+  int64_t total = 0;
+  void* tuning = nullptr;
+  rme_result* host_out = nullptr;
+  std::vector<int64_t> host_off, host_count, dev_off;
+  ~Slot() {
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (done) cudaEventDestroy(done);
+  }
+};
+
 struct Ctx {
   int device = 0, nsm = 0;
   int bps[kParts][kSearchVariants][2] = {};  // resident search blocks per SM, per part, variant, form
@@ -208,20 +241,19 @@ struct Ctx {
   // forked from and joined back to the caller's stream.
   cudaStream_t aux[kParts] = {nullptr, nullptr, nullptr, nullptr};
   cudaEvent_t ev_fork = nullptr, ev_join[kParts] = {nullptr, nullptr, nullptr, nullptr};
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp0 = nullptr, evp1 = nullptr;
+  cudaEvent_t evp0 = nullptr, evp1 = nullptr;
   std::map<int, std::unique_ptr<Picture>> pics;
   std::map<std::tuple<int, int, int, uint32_t>, Tables> tables;
   std::map<std::vector<int64_t>, Deps> deps;
   std::string err;
-  uint32_t epoch = 0;
   rme_stats last{};
-  // launch buffers
-  DevBuf<FrameDesc> d_frames;
-  DevBuf<unsigned long long> d_ready;  // the dataflow queue's slots
-  DevBuf<rme_result> d_out;
-  DevBuf<int32_t> d_pending;
-  DevBuf<rme_job> d_jobs;
-  DevBuf<unsigned long long> d_misc;  // the launch header (kMisc*)
+  // launch buffers, taken in turn
+  Slot slots[kSlots];
+  int next_slot = 0;
+  // Errors of asynchronous launches finished before their rme_sync (their
+  // slot was needed again), per stream: the first error code, the device
+  // status bits.
+  std::map<cudaStream_t, std::pair<int, uint32_t>> async_err;
   DevBuf<int32_t> d_lorder;           // lookahead: claim order (per block shape), done flags, results
   std::pair<int, int> lorder_shape{0, 0};
   DevBuf<int32_t> d_ldone;
@@ -240,11 +272,6 @@ struct Ctx {
   DevBuf<rme_mv> d_cmv;
   DevBuf<int64_t> d_coff;
   DevBuf<uint8_t> d_cout;
-  PinBuf<FrameDesc> h_frames;
-  PinBuf<rme_result> h_out;
-  PinBuf<unsigned long long> h_misc;
-  PinBuf<unsigned long long> h_init;  // [misc header | initial queue entries]
-
   std::map<std::vector<int64_t>, Graph> graphs;
   bool planes_pending = false;  // uploads recorded between evp0 and evp1 since the last search
   ~Ctx() {
@@ -254,8 +281,6 @@ struct Ctx {
       if (d.second.pending) cudaFree(d.second.pending);
     for (auto& t : tables)
       if (t.second.tab) cudaFree(t.second.tab);
-    if (ev0) cudaEventDestroy(ev0);
-    if (ev1) cudaEventDestroy(ev1);
     if (evp0) cudaEventDestroy(evp0);
     if (evp1) cudaEventDestroy(evp1);
     if (ev_fork) cudaEventDestroy(ev_fork);
@@ -520,25 +545,80 @@ int make_frame(Ctx* c, const rme_frame* f, const rme_params* p, FrameDesc* fd, r
   return 0;
 }
 
-// Launch frames[0..n) as one persistent search; results to host `out` at
-// offsets (count-prefix order).
+// Finish the launch in flight on slot `sl`: wait for it, check the device
+// status and the task count, keep its statistics (and feed the tuner), move
+// results bound for pageable memory. Returns 0 or an error code.
+int finish_launch(Ctx* c, Slot& sl) {
+  if (!sl.busy) return 0;
+  sl.busy = false;
+  CK(cudaEventSynchronize(sl.done));
+  const uint32_t status = (uint32_t)(sl.h_misc.p[kMiscStatus] & 0xffffffffu);
+  float ms = 0.0f;
+  CK(cudaEventElapsedTime(&ms, sl.ev0, sl.ev1));
+  c->last.tasks = sl.h_misc.p[kMiscCounters];
+  c->last.sad_candidates = sl.h_misc.p[kMiscCounters + 1];
+  c->last.satd_candidates = sl.h_misc.p[kMiscCounters + 2];
+  c->last.sad_samples = sl.h_misc.p[kMiscCounters + 3];
+  c->last.satd_samples = sl.h_misc.p[kMiscCounters + 4];
+  c->last.kernel_ms = ms;
+  if (sl.tuning) {
+    auto* T = (Ctx::Tune*)sl.tuning;
+    sl.tuning = nullptr;
+    if (T->best < 0 && T->tried < kSearchVariants) {
+      T->ms[T->tried++] = ms;
+      if (T->tried == kSearchVariants) T->best = (int)(std::min_element(T->ms, T->ms + kSearchVariants) - T->ms);
+    }
+  }
+  c->last.planes_ms = 0.0f;
+  if (c->planes_pending) {
+    // Device time from the first upload since the previous search to the
+    // end of the last one (the uploads' stream precedes this search's).
+    cudaEventSynchronize(c->evp1);
+    if (cudaEventElapsedTime(&c->last.planes_ms, c->evp0, c->evp1) != cudaSuccess) c->last.planes_ms = 0.0f;
+    cudaGetLastError();
+    c->planes_pending = false;
+  }
+  if (status) return fail(c, RME_EDEVICE, "device status " + std::to_string(status));
+  if (c->last.tasks != (unsigned long long)sl.total)
+    return fail(c, RME_EDEVICE, "the launch ran " + std::to_string(c->last.tasks) + " of " + std::to_string(sl.total) +
+                                    " tasks");
+  if (sl.host_out) {
+    for (size_t i = 0; i < sl.host_off.size(); ++i)
+      std::memcpy(sl.host_out + sl.host_off[i], sl.h_out.p + sl.dev_off[i], sizeof(rme_result) * sl.host_count[i]);
+    sl.host_out = nullptr;
+  }
+  return 0;
+}
+
+// The next slot, free: a launch still in flight there is finished first,
+// and an error it reports is kept for its stream's rme_sync.
+Slot* take_slot(Ctx* c) {
+  Slot& sl = c->slots[c->next_slot];
+  c->next_slot = (c->next_slot + 1) % kSlots;
+  if (sl.busy) {
+    const cudaStream_t st = sl.stream;
+    const int rc = finish_launch(c, sl);
+    if (rc) {
+      auto& e = c->async_err[st];
+      if (!e.first) e.first = rc;
+      if (rc == RME_EDEVICE) e.second |= (uint32_t)(sl.h_misc.p[kMiscStatus] & 0xffffffffu);
+    }
+  }
+  return &sl;
+}
+
+// Launch frames[0..n) as one persistent search; results to `out` (device,
+// pinned or pageable host memory) at offsets (count-prefix order).
 // `bi_src` (HEVC refine_bi): frame 0's per-task target blocks.
+// `async`: return once the launch is queued on `s` (out must be device or
+// pinned memory); rme_sync finishes it.
 int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n, rme_result* out,
-               const int64_t* offsets, cudaStream_t s, bool use_graph, const void* bi_src = nullptr) {
+               const int64_t* offsets, cudaStream_t s, bool use_graph, const void* bi_src = nullptr,
+               bool async = false) {
   if (n < 1 || n > 255) return fail(c, RME_EINVAL, "1..255 frames per launch");
   std::vector<int> ntask(n);
   std::vector<int64_t> toff(n + 1, 0), jobs_off(n + 1, 0);
   for (int i = 0; i < n; ++i) jobs_off[i + 1] = jobs_off[i] + (params[i].predictor_mode == RME_PRED_GIVEN ? frames[i].njobs : 0);
-  // Pass 1: sizes (make_frame with null device pointers validates too).
-  CK(c->h_frames.ensure(n));
-  for (int i = 0; i < n; ++i) {
-    int rc = make_frame(c, &frames[i], &params[i], &c->h_frames.p[i], nullptr, nullptr, nullptr, &ntask[i]);
-    if (rc) return rc;
-    toff[i + 1] = toff[i] + ntask[i];
-  }
-  const int64_t total = toff[n];
-  for (int i = 0; i < n; ++i)
-    if (ntask[i] >= (1 << 24)) return fail(c, RME_EINVAL, "more than 2^24 tasks in one frame");
   // `out` may be device memory: the kernels then write it directly.
   cudaPointerAttributes pa{};
   // Pinned host memory takes the results straight from the device buffer.
@@ -546,23 +626,36 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   cudaGetLastError();  // a host pointer unknown to CUDA is not an error here
   const bool dev_out = known && pa.type == cudaMemoryTypeDevice;
   const bool pinned_out = known && pa.type == cudaMemoryTypeHost;
-  CK(c->d_frames.ensure(n));
-  if (!dev_out) CK(c->d_out.ensure(std::max<int64_t>(total, 1)));
-  CK(c->d_pending.ensure(std::max<int64_t>(total, 1)));
-  unsigned long long* old_ready = c->d_ready.p;
-  CK(c->d_ready.ensure(std::max<int64_t>(total, 1)));
+  if (async && !dev_out && !pinned_out)
+    return fail(c, RME_EINVAL, "an asynchronous search writes device or pinned host memory only");
+  Slot& sl = *take_slot(c);
+  // Pass 1: sizes (make_frame with null device pointers validates too).
+  CK(sl.h_frames.ensure(n));
+  for (int i = 0; i < n; ++i) {
+    int rc = make_frame(c, &frames[i], &params[i], &sl.h_frames.p[i], nullptr, nullptr, nullptr, &ntask[i]);
+    if (rc) return rc;
+    toff[i + 1] = toff[i] + ntask[i];
+  }
+  const int64_t total = toff[n];
+  for (int i = 0; i < n; ++i)
+    if (ntask[i] >= (1 << 24)) return fail(c, RME_EINVAL, "more than 2^24 tasks in one frame");
+  CK(sl.d_frames.ensure(n));
+  if (!dev_out) CK(sl.d_out.ensure(std::max<int64_t>(total, 1)));
+  CK(sl.d_pending.ensure(std::max<int64_t>(total, 1)));
+  unsigned long long* old_ready = sl.d_ready.p;
+  CK(sl.d_ready.ensure(std::max<int64_t>(total, 1)));
   // Fresh slot memory may hold any word, an epoch's among them: zero it
   // (epochs start at 1).
-  if (c->d_ready.p != old_ready) c->epoch = 0;
-  CK(c->d_jobs.ensure(std::max<int64_t>(jobs_off[n], 1)));
-  CK(c->d_misc.ensure(kMiscWords));
-  if (!dev_out && !pinned_out) CK(c->h_out.ensure(std::max<int64_t>(total, 1)));
-  CK(c->h_misc.ensure(kMiscWords));
-  if (c->epoch == 0 || c->epoch == 0xffffffffu) {
-    CK(cudaMemsetAsync(c->d_ready.p, 0, c->d_ready.n * sizeof(unsigned long long), s));
-    c->epoch = 0;
+  if (sl.d_ready.p != old_ready) sl.epoch = 0;
+  CK(sl.d_jobs.ensure(std::max<int64_t>(jobs_off[n], 1)));
+  CK(sl.d_misc.ensure(kMiscWords));
+  if (!dev_out && !pinned_out) CK(sl.h_out.ensure(std::max<int64_t>(total, 1)));
+  CK(sl.h_misc.ensure(kMiscWords));
+  if (sl.epoch == 0 || sl.epoch == 0xffffffffu) {
+    CK(cudaMemsetAsync(sl.d_ready.p, 0, sl.d_ready.n * sizeof(unsigned long long), s));
+    sl.epoch = 0;
   }
-  ++c->epoch;
+  ++sl.epoch;
   // Pass 2: device pointers; the queue's initial entries (8-bit frames'
   // tasks first, then deeper ones: each part is one kernel launch of its
   // own sample width, with its own part of the slots).
@@ -571,19 +664,19 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   sig.push_back(dev_out + 2 * pinned_out);
   std::vector<unsigned long long> init[kParts];
   int64_t part_tasks[kParts] = {0, 0, 0, 0};
-  for (int i = 0; i < n; ++i) part_tasks[part_of(c->h_frames.p[i])] += ntask[i];
+  for (int i = 0; i < n; ++i) part_tasks[part_of(sl.h_frames.p[i])] += ntask[i];
   std::vector<std::pair<const int32_t*, int>> pend_copies;  // (template, frame)
   for (int i = 0; i < n; ++i) {
-    FrameDesc& fd = c->h_frames.p[i];
+    FrameDesc& fd = sl.h_frames.p[i];
     const int part = part_of(fd);
-    fd.out = dev_out ? out + (offsets ? offsets[i] : toff[i]) : c->d_out.p + toff[i];
-    fd.pending = c->d_pending.p + toff[i];
-    const unsigned long long tag = ((unsigned long long)c->epoch << 32) | ((unsigned long long)i << 24);
+    fd.out = dev_out ? out + (offsets ? offsets[i] : toff[i]) : sl.d_out.p + toff[i];
+    fd.pending = sl.d_pending.p + toff[i];
+    const unsigned long long tag = ((unsigned long long)sl.epoch << 32) | ((unsigned long long)i << 24);
     if (params[i].predictor_mode == RME_PRED_GIVEN) {
-      fd.jobs = c->d_jobs.p + jobs_off[i];
+      fd.jobs = sl.d_jobs.p + jobs_off[i];
       if (i == 0) fd.bi_src = bi_src;
       if (frames[i].njobs > 0)
-        CK(cudaMemcpyAsync(c->d_jobs.p + jobs_off[i], frames[i].jobs, sizeof(rme_job) * frames[i].njobs,
+        CK(cudaMemcpyAsync(sl.d_jobs.p + jobs_off[i], frames[i].jobs, sizeof(rme_job) * frames[i].njobs,
                            cudaMemcpyHostToDevice, s));
       for (int t = 0; t < ntask[i]; ++t) init[part].push_back(tag | (uint32_t)t);
       sig.push_back(-1);
@@ -616,10 +709,10 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
     init_off[k] = ninit;
     ninit += init[k].size();
   }
-  CK(c->h_init.ensure(kMiscWords + ninit));
-  unsigned long long* hi = c->h_init.p;
+  CK(sl.h_init.ensure(kMiscWords + ninit));
+  unsigned long long* hi = sl.h_init.p;
   std::memset(hi, 0, kMiscWords * sizeof(unsigned long long));
-  hi[kMiscEpoch] = c->epoch;
+  hi[kMiscEpoch] = sl.epoch;
   LaunchDesc Ls[kParts];
   int64_t slot0 = 0, slot_off[kParts];
   for (int k = 0; k < kParts; ++k) {
@@ -627,15 +720,15 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
     std::memcpy(hi + kMiscWords + init_off[k], init[k].data(), init[k].size() * sizeof(unsigned long long));
     slot_off[k] = slot0;
     LaunchDesc& L = Ls[k];
-    L.frames = c->d_frames.p;
-    L.ready = c->d_ready.p + slot0;
+    L.frames = sl.d_frames.p;
+    L.ready = sl.d_ready.p + slot0;
     L.total = part_tasks[k];
-    L.head = c->d_misc.p + 2 * k;
-    L.tail = c->d_misc.p + 2 * k + 1;
-    L.counters = c->d_misc.p + kMiscCounters;
-    L.status = reinterpret_cast<uint32_t*>(c->d_misc.p + kMiscStatus);
-    L.epoch = reinterpret_cast<const uint32_t*>(c->d_misc.p + kMiscEpoch);
-    L.done = c->d_misc.p + kMiscDone + k;
+    L.head = sl.d_misc.p + 2 * k;
+    L.tail = sl.d_misc.p + 2 * k + 1;
+    L.counters = sl.d_misc.p + kMiscCounters;
+    L.status = reinterpret_cast<uint32_t*>(sl.d_misc.p + kMiscStatus);
+    L.epoch = reinterpret_cast<const uint32_t*>(sl.d_misc.p + kMiscEpoch);
+    L.done = sl.d_misc.p + kMiscDone + k;
     slot0 += part_tasks[k];
   }
   int nparts_used = 0;
@@ -653,7 +746,7 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
       Ctx::Tune& T = c->tune[{k, bucket}];
       if (T.best >= 0) {
         variant[k] = T.best;
-      } else if (nparts_used == 1) {  // one kind in the launch: its time is the part's
+      } else if (nparts_used == 1 && !async) {  // one kind in the launch: its time is the part's
         variant[k] = T.tried;
         tuning = &T;
       }
@@ -676,20 +769,20 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   sig.push_back(nparts);
   auto enqueue = [&](bool capturing) -> cudaError_t {
     const unsigned rec = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
-    cudaError_t e = cudaMemcpyAsync(c->d_frames.p, c->h_frames.p, sizeof(FrameDesc) * n, cudaMemcpyHostToDevice, s);
+    cudaError_t e = cudaMemcpyAsync(sl.d_frames.p, sl.h_frames.p, sizeof(FrameDesc) * n, cudaMemcpyHostToDevice, s);
     for (auto& pc : pend_copies)
       if (e == cudaSuccess)
-        e = cudaMemcpyAsync(c->d_pending.p + toff[pc.second], pc.first, sizeof(int32_t) * ntask[pc.second],
+        e = cudaMemcpyAsync(sl.d_pending.p + toff[pc.second], pc.first, sizeof(int32_t) * ntask[pc.second],
                             cudaMemcpyDeviceToDevice, s);
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(c->d_misc.p, hi, kMiscWords * sizeof(unsigned long long), cudaMemcpyHostToDevice, s);
+      e = cudaMemcpyAsync(sl.d_misc.p, hi, kMiscWords * sizeof(unsigned long long), cudaMemcpyHostToDevice, s);
     for (int k = 0; k < kParts; ++k)
       if (e == cudaSuccess && !init[k].empty())
-        e = cudaMemcpyAsync(c->d_ready.p + slot_off[k], hi + kMiscWords + init_off[k],
+        e = cudaMemcpyAsync(sl.d_ready.p + slot_off[k], hi + kMiscWords + init_off[k],
                             init[k].size() * sizeof(unsigned long long), cudaMemcpyHostToDevice, s);
     // Under capture the records are external ones: they become event-record
     // nodes, so the kernels' device time is measured on every replay.
-    if (e == cudaSuccess) e = cudaEventRecordWithFlags(c->ev0, s, rec);
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(sl.ev0, s, rec);
     // Parts after the first run concurrently on the auxiliary streams
     // (parallel branches of a captured graph).
     if (e == cudaSuccess && nparts > 1) e = cudaEventRecord(c->ev_fork, s);
@@ -703,11 +796,11 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
       if (e == cudaSuccess && j > 0) e = cudaEventRecord(c->ev_join[j], sk);
     }
     for (int j = 1; j < nparts && e == cudaSuccess; ++j) e = cudaStreamWaitEvent(s, c->ev_join[j], 0);
-    if (e == cudaSuccess) e = cudaEventRecordWithFlags(c->ev1, s, rec);
+    if (e == cudaSuccess) e = cudaEventRecordWithFlags(sl.ev1, s, rec);
     if (e == cudaSuccess && !dev_out && !pinned_out)
-      e = cudaMemcpyAsync(c->h_out.p, c->d_out.p, sizeof(rme_result) * total, cudaMemcpyDeviceToHost, s);
+      e = cudaMemcpyAsync(sl.h_out.p, sl.d_out.p, sizeof(rme_result) * total, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(c->h_misc.p, c->d_misc.p, kMiscWords * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
+      e = cudaMemcpyAsync(sl.h_misc.p, sl.d_misc.p, kMiscWords * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
     return e;
   };
   bool has_given = false;
@@ -717,6 +810,7 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
     gsig.push_back(total);
     for (int k = 0; k < kParts; ++k) gsig.push_back((int64_t)init[k].size());
     gsig.push_back((int64_t)(uintptr_t)s);
+    gsig.push_back((int64_t)(&sl - c->slots));
     gsig.push_back((int64_t)g_buffer_generation);
     Graph& g = c->graphs[gsig];
     // A shape is captured when it comes a second time (a one-off batch,
@@ -748,45 +842,29 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
       while (j < n && (!offsets || offsets[j] == offsets[i] + (toff[j] - toff[i]))) ++j;
       const int64_t off = offsets ? offsets[i] : toff[i];
       if (toff[j] > toff[i])
-        CK(cudaMemcpyAsync(out + off, c->d_out.p + toff[i], sizeof(rme_result) * (toff[j] - toff[i]),
+        CK(cudaMemcpyAsync(out + off, sl.d_out.p + toff[i], sizeof(rme_result) * (toff[j] - toff[i]),
                            cudaMemcpyDeviceToHost, s));
       i = j;
     }
   }
-  CK(cudaStreamSynchronize(s));
-  uint32_t status = (uint32_t)(c->h_misc.p[kMiscStatus] & 0xffffffffu);
-  float ms = 0.0f;
-  CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
-  c->last.tasks = c->h_misc.p[kMiscCounters];
-  c->last.sad_candidates = c->h_misc.p[kMiscCounters + 1];
-  c->last.satd_candidates = c->h_misc.p[kMiscCounters + 2];
-  c->last.sad_samples = c->h_misc.p[kMiscCounters + 3];
-  c->last.satd_samples = c->h_misc.p[kMiscCounters + 4];
-  c->last.kernel_ms = ms;
-  if (tuning && tuning->best < 0) {
-    tuning->ms[tuning->tried++] = ms;
-    if (tuning->tried == kSearchVariants)
-      tuning->best = (int)(std::min_element(tuning->ms, tuning->ms + kSearchVariants) - tuning->ms);
+  CK(cudaEventRecord(sl.done, s));
+  sl.busy = true;
+  sl.stream = s;
+  sl.total = total;
+  sl.tuning = tuning;
+  if (!dev_out && !pinned_out) {
+    sl.host_out = out;
+    sl.host_off.resize(n);
+    sl.host_count.resize(n);
+    sl.dev_off.resize(n);
+    for (int i = 0; i < n; ++i) {
+      sl.host_off[i] = offsets ? offsets[i] : toff[i];
+      sl.host_count[i] = ntask[i];
+      sl.dev_off[i] = toff[i];
+    }
   }
-  c->last.planes_ms = 0.0f;
-  if (c->planes_pending) {
-    // Device time from the first upload since the previous search to the
-    // end of the last one (the uploads' stream precedes this search's).
-    cudaEventSynchronize(c->evp1);
-    if (cudaEventElapsedTime(&c->last.planes_ms, c->evp0, c->evp1) != cudaSuccess) c->last.planes_ms = 0.0f;
-    cudaGetLastError();
-    c->planes_pending = false;
-  }
-  if (status) return fail(c, RME_EDEVICE, "device status " + std::to_string(status));
-  if (c->last.tasks != (unsigned long long)total)
-    return fail(c, RME_EDEVICE, "the launch ran " + std::to_string(c->last.tasks) + " of " + std::to_string(total) +
-                                    " tasks");
-  if (dev_out || pinned_out) return 0;
-  for (int i = 0; i < n; ++i) {
-    int64_t off = offsets ? offsets[i] : toff[i];
-    std::memcpy(out + off, c->h_out.p + toff[i], sizeof(rme_result) * ntask[i]);
-  }
-  return 0;
+  if (async) return 0;
+  return finish_launch(c, sl);
 }
 
 }  // namespace
@@ -827,9 +905,11 @@ int rme_ctx_create(void** out, int32_t device) {
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return RME_ECUDA;
   // RME_TUNE=0 keeps every launch on the default occupancy variant.
   if (const char* t = std::getenv("RME_TUNE")) c->tune_on = t[0] != '0';
-  if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
-      cudaEventCreate(&c->evp0) != cudaSuccess || cudaEventCreate(&c->evp1) != cudaSuccess)
-    return RME_ECUDA;
+  if (cudaEventCreate(&c->evp0) != cudaSuccess || cudaEventCreate(&c->evp1) != cudaSuccess) return RME_ECUDA;
+  for (Slot& sl : c->slots)
+    if (cudaEventCreate(&sl.ev0) != cudaSuccess || cudaEventCreate(&sl.ev1) != cudaSuccess ||
+        cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess)
+      return RME_ECUDA;
   *out = c.release();
   return 0;
 }
@@ -1113,6 +1193,47 @@ int rme_batch_search(void* ctx, const rme_frame* frames, const rme_params* param
   if (!c || !frames || !params || !out || nframes < 1) return c ? fail(c, RME_EINVAL, "null argument") : RME_EINVAL;
   CK(cudaSetDevice(c->device));
   return run_launch(c, frames, params, nframes, out, offsets, stream ? (cudaStream_t)stream : c->stream, true);
+}
+
+int rme_frame_search_async(void* ctx, const rme_frame* f, const rme_params* p, rme_result* out, void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !f || !p || !out) return c ? fail(c, RME_EINVAL, "null argument") : RME_EINVAL;
+  CK(cudaSetDevice(c->device));
+  return run_launch(c, f, p, 1, out, nullptr, stream ? (cudaStream_t)stream : c->stream, false, nullptr, true);
+}
+
+int rme_batch_search_async(void* ctx, const rme_frame* frames, const rme_params* params, int32_t nframes,
+                           rme_result* out, const int64_t* offsets, void* stream) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !frames || !params || !out || nframes < 1) return c ? fail(c, RME_EINVAL, "null argument") : RME_EINVAL;
+  CK(cudaSetDevice(c->device));
+  return run_launch(c, frames, params, nframes, out, offsets, stream ? (cudaStream_t)stream : c->stream, false,
+                    nullptr, true);
+}
+
+int rme_sync(void* ctx, void* stream, uint32_t* device_status) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c) return RME_EINVAL;
+  CK(cudaSetDevice(c->device));
+  const cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  int rc = 0;
+  uint32_t st = 0;
+  auto it = c->async_err.find(s);
+  if (it != c->async_err.end()) {
+    rc = it->second.first;
+    st = it->second.second;
+    c->async_err.erase(it);
+  }
+  // Oldest first: the slot after the last one taken, round the ring.
+  for (int k = 0; k < kSlots; ++k) {
+    Slot& sl = c->slots[(c->next_slot + k) % kSlots];
+    if (!sl.busy || sl.stream != s) continue;
+    const int r = finish_launch(c, sl);
+    if (r == RME_EDEVICE) st |= (uint32_t)(sl.h_misc.p[kMiscStatus] & 0xffffffffu);
+    if (r && !rc) rc = r;
+  }
+  if (device_status) *device_status = st;
+  return rc;
 }
 
 int rme_hevc_decide(const rme_picture_desc* d, const rme_params* p, int32_t nref, const rme_result* res,

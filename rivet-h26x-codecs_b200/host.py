@@ -144,6 +144,27 @@ class MotionSearch:
                                                C.cast(out.ctypes.data, C.POINTER(capi.Result)), C.c_void_p(stream)))
         return out
 
+    def search_async(self, src_id: int, ref_ids: Sequence[int], params: capi.Params, out,
+                     jobs: np.ndarray | None = None, stream: int = 0) -> None:
+        """Queue one frame's search on `stream` and return at once. `out` is
+        pinned host memory (a structured array over a pinned buffer, or a
+        pinned tensor) or a device tensor of at least the result count; it
+        holds the results after sync(stream)."""
+        if jobs is not None:
+            jobs = np.ascontiguousarray(jobs, capi.JOB_DTYPE)
+        f = self._frame(src_id, ref_ids, jobs)
+        addr = out.data_ptr() if hasattr(out, "data_ptr") else out.ctypes.data
+        self._check(self._lib.rme_frame_search_async(self.ctx, C.byref(f), C.byref(params),
+                                                     C.cast(C.c_void_p(addr), C.POINTER(capi.Result)),
+                                                     C.c_void_p(stream)))
+
+    def sync(self, stream: int = 0) -> int:
+        """Wait for the asynchronous searches queued on `stream`; raises on a
+        failed one. Returns the device status bits (0)."""
+        st = C.c_uint32()
+        self._check(self._lib.rme_sync(self.ctx, C.c_void_p(stream), C.byref(st)))
+        return st.value
+
     def hevc_weighted_refine(self, src_id: int, ref_ids: Sequence[int], params: capi.Params, jobs: np.ndarray,
                              log2_wd: int, weight: int, offset: int) -> np.ndarray:
         """A weighted list's refine_subpel per GIVEN job (seeds[0] the
