@@ -219,6 +219,48 @@ def run_reference(args, world, rank):
     }), flush=True)
 
 
+def plain_latency(ms, frames, p, stream, nframes: int = 600, warm: int = 8) -> dict:
+    """The plain per-frame path as an encoder drives it, one picture at a
+    time: each timed call uploads the new picture from pinned host memory
+    (its planes built on the device), searches it against the two pictures
+    before it, and reads its results back into a pinned buffer the caller
+    keeps. `nframes` calls over the sequence (cycled), after `warm` untimed
+    ones; p50/p99 over the timed calls (host clock around the whole call)."""
+    import torch
+    import rivet_h26x_codecs_b200.capi as capi
+    ring = 4  # picture slots: the new picture, its two references and one spare
+    pinned = []
+    for f in frames:
+        t = torch.empty(f.shape, dtype=torch.uint8, pin_memory=True)
+        t.numpy()[...] = f
+        pinned.append(t.numpy())
+    base = 5000
+    for k in range(NREF):
+        ms.upload(base + k, pinned[k], capi.RME_CODEC_HEVC, 8, as_ref=True, stream=stream)
+    n = ms.result_count(base, [base + r for r in range(NREF)], p)
+    bufs = []
+    for _ in range(2):
+        b = torch.empty(n * capi.RESULT_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True)
+        b.fill_(1)
+        bufs.append(b.numpy().view(capi.RESULT_DTYPE))
+    lat = []
+    for i in range(NREF, NREF + warm + nframes):
+        slot = base + i % ring
+        refs = [base + (i - 1 - r) % ring for r in range(NREF)]
+        a = time.perf_counter()
+        ms.upload(slot, pinned[i % len(frames)], capi.RME_CODEC_HEVC, 8, as_ref=True, stream=stream)
+        ms.search(slot, refs, p, stream=stream, out=bufs[i & 1])
+        if i >= NREF + warm:
+            lat.append(time.perf_counter() - a)
+    for k in range(ring):
+        ms.release(base + k)
+    lat_ms = np.array(lat) * 1e3
+    return {"value": len(lat) / float(np.sum(lat)), "unit": "frames/s", "frames": len(lat),
+            "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99)),
+            "max_ms": float(lat_ms.max()),
+            "call": "upload from pinned memory + plane build + search + results to pinned memory, one picture a call"}
+
+
 def workload_config(frames_per_step: int, world: int) -> dict:
     """The bench's workload, named by what it is (both arms report it)."""
     return {"workload": "hevc-1080p-8bit-2ref-pu8to64-range64-qp32", "frames_per_step": frames_per_step,

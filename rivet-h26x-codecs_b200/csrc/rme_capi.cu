@@ -184,6 +184,7 @@ struct Tables {
 struct Deps {  // the dependency structure of one frame shape
   int32_t* pending = nullptr;    // device: per task, how many tasks it reads
   std::vector<uint32_t> ready;   // tasks that read none, in order
+  uint32_t* d_ready = nullptr;   // device copy of `ready` (the resident engine publishes from it)
   size_t ntasks = 0;
 };
 
@@ -277,8 +278,10 @@ struct Ctx {
   ~Ctx() {
     for (auto& g : graphs)
       if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
-    for (auto& d : deps)
+    for (auto& d : deps) {
       if (d.second.pending) cudaFree(d.second.pending);
+      if (d.second.d_ready) cudaFree(d.second.d_ready);
+    }
     for (auto& t : tables)
       if (t.second.tab) cudaFree(t.second.tab);
     if (evp0) cudaEventDestroy(evp0);
@@ -444,8 +447,12 @@ const Deps* get_deps(Ctx* c, const rme_picture_desc& d, const rme_params* p, int
   cudaError_t e = cudaMalloc(&dp.pending, std::max<size_t>(pend.size(), 1) * sizeof(int32_t));
   if (e == cudaSuccess)
     e = cudaMemcpy(dp.pending, pend.data(), pend.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc(&dp.d_ready, std::max<size_t>(dp.ready.size(), 1) * sizeof(uint32_t));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(dp.d_ready, dp.ready.data(), dp.ready.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     if (dp.pending) cudaFree(dp.pending);
+    if (dp.d_ready) cudaFree(dp.d_ready);
     *rc = cuda_fail(c, e, "dependency template");
     return nullptr;
   }
@@ -713,7 +720,7 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   unsigned long long* hi = sl.h_init.p;
   std::memset(hi, 0, kMiscWords * sizeof(unsigned long long));
   hi[kMiscEpoch] = sl.epoch;
-  LaunchDesc Ls[kParts];
+  LaunchDesc Ls[kParts] = {};
   int64_t slot0 = 0, slot_off[kParts];
   for (int k = 0; k < kParts; ++k) {
     hi[2 * k + 1] = init[k].size();
@@ -868,6 +875,30 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
 }
 
 }  // namespace
+
+namespace rme {
+// A STANDALONE frame for the resident engine: its descriptor over the
+// context's pictures (launch buffers left null), its task count, its
+// dependency template and its root tasks (device memory, held by the
+// context).
+int ctx_standalone_frame(void* ctx, const rme_frame* f, const rme_params* p, FrameDesc* fd, int* ntasks,
+                         const int32_t** pending_tmpl, const uint32_t** roots, int* nroots) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !f || !p || !fd || !ntasks) return RME_EINVAL;
+  if (p->predictor_mode != RME_PRED_STANDALONE) return fail(c, RME_EINVAL, "the engine searches STANDALONE frames");
+  int rc = make_frame(c, f, p, fd, nullptr, nullptr, nullptr, ntasks);
+  if (rc) return rc;
+  if (*ntasks >= (1 << 24)) return fail(c, RME_EINVAL, "more than 2^24 tasks in one frame");
+  Picture* src;
+  if ((rc = picture_of(c, f->src_id, &src))) return rc;
+  const Deps* dp = get_deps(c, src->d, p, f->nref, &rc);
+  if (!dp) return rc;
+  *pending_tmpl = dp->pending;
+  *roots = dp->d_ready;
+  *nroots = (int)dp->ready.size();
+  return 0;
+}
+}  // namespace rme
 
 extern "C" {
 

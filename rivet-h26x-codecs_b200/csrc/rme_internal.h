@@ -65,6 +65,7 @@ struct FrameDesc {
   rme_result* out;
   int32_t* pending;
   int32_t ntasks;
+  uint32_t gen;  // the resident engine: this frame's generation in its slot
 };
 
 // A launch's dataflow queue: a task is pushed when its last dependency
@@ -85,7 +86,45 @@ struct LaunchDesc {
                                  // runs one task it made ready itself
                                  // (no queue round trip) and idle warps
                                  // leave once every task is done
+  int32_t ring_shift;            // nonzero: the resident engine's ring of
+                                 // 2^ring_shift slots (slot idx holds
+                                 // ((idx >> ring_shift) + 1) << 32 | entry)
 };
+
+// The resident engine (rme_engine.cu): one search kernel that stays on the
+// GPU while a serving loop feeds it frames of any kind. Frames occupy slots
+// of a device table; a frame's tasks enter the ring as its planes are built;
+// the warp that finishes a frame's last task raises the frame's flag in
+// mapped host memory.
+constexpr int kEngineFrames = 256;  // frame slots (the queue's 8-bit frame field)
+struct EngineCtl {
+  uint32_t* fdone;                 // per frame slot: its tasks finished
+  volatile uint32_t* hflags;       // mapped host memory: per slot, the generation finished
+  volatile const uint32_t* hstop;  // mapped host memory: nonzero once idle warps may leave
+  uint32_t idle_polls;             // idle polls (backing off to ~1 us) before a warp leaves
+};
+cudaError_t launch_engine(const LaunchDesc& L, const EngineCtl& E, int grid, cudaStream_t s);
+int engine_blocks_per_sm();
+cudaError_t launch_publish(const LaunchDesc& L, int frame, const uint32_t* roots, int nroots, cudaStream_t s);
+// The host side (one engine per context, driven by one thread): a frame is
+// submitted behind its uploads on `upload` and takes a slot; engine_done
+// tells when its results (engine_results, device memory) are complete;
+// engine_release frees the slot once they have been copied out.
+struct Engine;
+int engine_create(void* ctx, int device, Engine** out);
+void engine_destroy(Engine* g);
+int engine_submit(Engine* g, const rme_frame* f, const rme_params* p, cudaStream_t upload, int* slot);
+bool engine_done(Engine* g, int slot);
+int engine_keep_running(Engine* g);
+bool engine_idle(Engine* g);
+const rme_result* engine_results(Engine* g, int slot);
+int engine_slot_tasks(Engine* g, int slot);
+const uint32_t* engine_status_word(Engine* g);
+void engine_release(Engine* g, int slot);
+// rme_capi.cu: a STANDALONE frame's descriptor over a context's pictures,
+// its task count, dependency template and root tasks (device memory).
+int ctx_standalone_frame(void* ctx, const rme_frame* f, const rme_params* p, FrameDesc* fd, int* ntasks,
+                         const int32_t** pending_tmpl, const uint32_t** roots, int* nroots);
 
 // Host helpers shared by the entry points (rme_capi.cu; f32 arithmetic
 // compiled without contraction, so it rounds as the reference's Rust does).

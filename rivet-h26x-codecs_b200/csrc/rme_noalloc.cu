@@ -160,7 +160,7 @@ extern "C" int rme_search_given_noalloc(const rme_picture_desc* d, const rme_par
   fill_ready<<<(njobs + 255) / 256, 256, 0, s>>>(slots, njobs, epoch);
   if (cudaGetLastError() != cudaSuccess) return RME_ECUDA;
 
-  LaunchDesc L;
+  LaunchDesc L = {};
   L.frames = reinterpret_cast<const FrameDesc*>(base + kOffFrame);
   L.ready = slots;
   L.total = njobs;

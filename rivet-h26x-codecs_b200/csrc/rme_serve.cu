@@ -1,17 +1,19 @@
-// The serving loop: a host thread that turns per-frame ME requests from many
-// streams into batched persistent launches (continuous batching at launch
-// granularity). Requests that arrive while a launch runs on the device wait
-// in the queue and join the next launch; each stream keeps its reference
-// pictures resident on the device, and streams are admitted against an HBM
-// budget. It is a client of the library's own C ABI: uploads, the batched
-// search, releases.
+// The serving loop: per-frame ME requests from many streams fed into the
+// resident engine (rme_engine.cu) as they arrive. A frame is uploaded into
+// its stream's ring of resident pictures on the upload stream, its planes are
+// built there, and it joins the engine's running search behind them: frames
+// that arrive while others are on the GPU are admitted as soon as a frame
+// slot and ring room are free, and their tasks share the SMs with the frames
+// already in flight (continuous batching at task granularity, not launch
+// granularity). Streams are admitted against an HBM budget of their
+// resident pictures.
 //
-// Frames are searched STANDALONE against the stream's previous `nref`
-// source pictures (the reference's ME stage run as a pre-pass, without the
-// reconstruction loop), so a frame's references are ready as soon as they
-// are uploaded. A stream contributes up to kPerStream frames (in order) to
-// one launch; a copier thread moves finished results out while the next
-// launch runs.
+// One worker thread owns the context and the engine: it admits requests,
+// polls the engine's completion flags (host memory the device writes),
+// copies finished frames' results out on a copy stream and posts the
+// completions. Frames are searched STANDALONE against the stream's previous
+// `nref` source pictures (the reference's ME stage as a pre-pass, without
+// the reconstruction loop).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -23,6 +25,7 @@
 #include <deque>
 #include <map>
 #include <mutex>
+#include <set>
 #include <thread>
 #include <vector>
 
@@ -32,42 +35,44 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+// Frames of one stream in flight at once: its picture ring holds nref +
+// kPerStream pictures, and a picture is refilled only once every frame that
+// reads it is complete.
+constexpr int kPerStream = 4;
+
 struct Stream {
   rme_picture_desc d{};
   rme_params p{};
   int nref = 0;
-  int64_t frames = 0;      // frames uploaded so far
-  uint64_t bytes = 0;      // resident bytes charged against the budget
+  int64_t frames = 0;        // frames admitted so far
+  uint64_t bytes = 0;        // resident bytes charged against the budget
   bool closing = false;
-  int pending = 0;         // requests queued or in flight
-  int32_t pic_base = 0;    // picture ids pic_base .. pic_base + nref + kPerStream - 1
+  int pending = 0;           // requests queued or in flight
+  int32_t pic_base = 0;      // picture ids pic_base .. pic_base + nref + kPerStream - 1
+  std::set<int64_t> open;    // frame numbers admitted and not yet complete
 };
 
 struct Request {
   int64_t id = 0;
   int32_t stream = 0;
-  void* luma = nullptr;  // pinned copy of the frame (from the pool)
+  void* luma = nullptr;      // pinned copy of the frame (from the pool)
   size_t bytes = 0;
   rme_result* out = nullptr;
+  bool out_pinned = false;   // results go straight into `out`
   double submit_s = 0.0;
-};
-
-// Frames of one stream that can join one launch (its picture ring holds
-// nref + kPerStream pictures).
-constexpr int kPerStream = 4;
-
-// A launch handed from the worker to the copier.
-struct Launch {
-  std::vector<Request> batch;
-  std::vector<int> status;
-  std::vector<int64_t> offset, count;
-  int slot = 0;
-  size_t left = 0;
-  double t_take = 0, t_up = 0, t_search = 0;
+  // in flight
+  int64_t frame = -1;        // the stream's frame number
+  int slot = -1;             // the engine's frame slot (-1: not searched)
+  int nresults = 0;
+  rme_result* staging = nullptr;
+  size_t staging_n = 0;
+  cudaEvent_t ev = nullptr;  // the upload (first frames) or the results copy
+  int status = 0;
 };
 
 struct Server {
   void* ctx = nullptr;
+  int device = 0;
   rme_serve_opts o{};
   Clock::time_point t0 = Clock::now();
   std::mutex m;
@@ -79,19 +84,19 @@ struct Server {
   int64_t next_id = 0;
   int32_t next_pic_base = 1 << 20;
   bool stop = false;
-  int cleanups = 0;  // closed streams whose pictures the worker must release
+  int closes = 0;  // close_stream calls the worker has not yet looked at
   std::thread worker;
-  // Two pinned result buffers: the worker fills one while the copier
-  // empties the other.
-  rme_result* staging[2] = {nullptr, nullptr};
-  size_t staging_n[2] = {0, 0};
-  bool slot_busy[2] = {false, false};
-  std::deque<Launch> copies;
-  bool copier_stop = false;
-  std::condition_variable copy_cv, copied_cv;
   // Pinned frame buffers by size: a submit copies into one, the upload reads
-  // it asynchronously, the worker returns it once its launch is complete.
+  // it asynchronously, the worker returns it once its frame is complete.
   std::map<size_t, std::vector<void*>> pool;
+  // worker-only state
+  rme::Engine* eng = nullptr;
+  cudaStream_t upload = nullptr, copy = nullptr;
+  uint32_t* h_status = nullptr;  // pinned: the engine's status word, read back with each copy
+  std::vector<Request> searching, copying, submitting;
+  std::vector<cudaEvent_t> events;
+  std::map<size_t, std::vector<rme_result*>> staging_pool;
+  std::vector<std::pair<int32_t, int>> release_later;  // closed streams' pictures (id base, count)
 
   void* take_buffer(size_t bytes) {  // lock held
     auto& v = pool[bytes];
@@ -103,24 +108,35 @@ struct Server {
     void* b = nullptr;
     return cudaMallocHost(&b, bytes) == cudaSuccess ? b : nullptr;
   }
+  cudaEvent_t take_event() {
+    if (!events.empty()) {
+      cudaEvent_t e = events.back();
+      events.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    return e;
+  }
+  rme_result* take_staging(size_t n) {
+    auto& v = staging_pool[n];
+    if (!v.empty()) {
+      rme_result* b = v.back();
+      v.pop_back();
+      return b;
+    }
+    void* b = nullptr;
+    return cudaMallocHost(&b, std::max<size_t>(n, 1) * sizeof(rme_result)) == cudaSuccess ? (rme_result*)b : nullptr;
+  }
 
   double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
   void run();
-  void copy_loop();
-  // Release the pictures of closed streams with nothing queued or in flight
-  // (worker thread, lock held: only the worker touches the context).
-  void release_closed() {
-    for (auto it = streams.begin(); it != streams.end();) {
-      if (it->second.closing && it->second.pending == 0) {
-        for (int k = 0; k < it->second.nref + kPerStream; ++k) rme_picture_release(ctx, it->second.pic_base + k);
-        resident -= it->second.bytes;
-        it = streams.erase(it);
-      } else {
-        ++it;
-      }
-    }
-    cleanups = 0;
-  }
+  void admit(std::vector<Request>& taken);
+  rme_frame frame_of(const Stream& st, int64_t j) const;
+  void submit_search(Request& r, const Stream& st);
+  void start(Request& r);
+  void finish(Request& r, double t);
+  void release_closed(bool engine_idle);
 };
 
 // Device bytes of one resident picture of this format: the padded planes
@@ -134,155 +150,204 @@ uint64_t picture_bytes(const rme_picture_desc& d) {
   return stride_bytes * (uint64_t)(ch + 2 * pad) * (h264 ? 4 : 16) + 256;
 }
 
-void Server::run() {
-  // RME_SERVE_TRACE=1 prints one line per launch to stderr: frames, queue
-  // left behind, and the host-side split of the launch's time.
-  const bool trace = std::getenv("RME_SERVE_TRACE") && std::getenv("RME_SERVE_TRACE")[0] == '1';
-  std::thread copier([this] { copy_loop(); });
-  int slot = 0;
-  for (;;) {
-    Launch L;
-    {
-      std::unique_lock<std::mutex> lk(m);
-      cv.wait(lk, [&] { return stop || !queue.empty() || cleanups > 0; });
-      if (cleanups > 0) release_closed();
-      if (stop && queue.empty()) break;
-      if (queue.empty()) continue;
-      // Oldest first, at most kPerStream frames of a stream (in order) and
-      // max_frames_per_launch in all.
-      std::map<int32_t, int> taken;
-      for (auto it = queue.begin(); it != queue.end() && (int)L.batch.size() < o.max_frames_per_launch;) {
-        if (taken[it->stream] >= kPerStream) {
-          ++it;
-          continue;
-        }
-        ++taken[it->stream];
-        L.batch.push_back(std::move(*it));
-        it = queue.erase(it);
-      }
-      L.left = queue.size();
-      // The staging buffer of this slot is free once the copier has
-      // finished the launch that used it last.
-      copied_cv.wait(lk, [&] { return !slot_busy[slot]; });
-      slot_busy[slot] = true;
+// Requests that may start now, oldest first (lock held): a stream's frame
+// waits while the frame kPerStream before it is incomplete (its picture
+// slot would be refilled under a search), and a stream's frames keep their
+// order.
+void Server::admit(std::vector<Request>& taken) {
+  std::set<int32_t> blocked;
+  for (auto it = queue.begin(); it != queue.end();) {
+    Stream& st = streams[it->stream];
+    const int64_t j = st.frames;
+    const bool room = st.open.empty() || *st.open.begin() > j - kPerStream;
+    if (blocked.count(it->stream) || !room) {
+      blocked.insert(it->stream);
+      ++it;
+      continue;
     }
-    L.slot = slot;
-    L.t_take = now();
-    // Upload each frame into its stream's ring of pictures; frames with at
-    // least one earlier picture are searched against up to nref of them.
-    std::vector<rme_frame> frames;
-    std::vector<rme_params> params;
-    L.status.assign(L.batch.size(), 0);
-    L.count.assign(L.batch.size(), 0);
-    L.offset.assign(L.batch.size(), 0);
-    std::vector<size_t> searched;
-    for (size_t i = 0; i < L.batch.size(); ++i) {
-      Stream* st;
-      {
-        std::lock_guard<std::mutex> lk(m);
-        st = &streams[L.batch[i].stream];
-      }
-      const int slots = st->nref + kPerStream;
-      const int32_t pic = st->pic_base + (int32_t)(st->frames % slots);
-      int rc = rme_picture_upload(ctx, pic, &st->d, L.batch[i].luma, 1, nullptr);
-      if (rc) {
-        L.status[i] = rc;
-        continue;
-      }
-      const int nr = (int)std::min<int64_t>(st->nref, st->frames);
-      {
-        // The worker alone writes `frames`; submits read it under the lock.
-        std::lock_guard<std::mutex> lk(m);
-        ++st->frames;
-      }
-      if (nr == 0) continue;
-      rme_frame f{};
-      f.src_id = pic;
-      f.nref = nr;
-      for (int r = 0; r < nr; ++r) f.ref_ids[r] = st->pic_base + (int32_t)((st->frames - 2 - r) % slots);
-      frames.push_back(f);
-      params.push_back(st->p);
-      searched.push_back(i);
-    }
-    L.t_up = now();
-    if (!frames.empty()) {
-      std::vector<int64_t> offs(frames.size());
-      int64_t total = 0;
-      for (size_t k = 0; k < frames.size(); ++k) {
-        int32_t cnt = 0;
-        rme_frame_result_count(ctx, &frames[k], &params[k], &cnt);
-        offs[k] = total;
-        L.offset[searched[k]] = total;
-        L.count[searched[k]] = cnt;
-        total += cnt;
-      }
-      if ((int64_t)staging_n[slot] < total) {
-        if (staging[slot]) cudaFreeHost(staging[slot]);
-        staging[slot] = nullptr;
-        staging_n[slot] = 0;
-        if (cudaMallocHost(&staging[slot], sizeof(rme_result) * total) == cudaSuccess) staging_n[slot] = total;
-      }
-      // Pinned results: the search copies them there directly.
-      const int rc = staging[slot] ? rme_batch_search(ctx, frames.data(), params.data(), (int32_t)frames.size(),
-                                                      staging[slot], offs.data(), nullptr)
-                                   : RME_ENOMEM;
-      if (rc)
-        for (size_t k = 0; k < frames.size(); ++k) L.status[searched[k]] = rc;
-    } else {
-      cudaDeviceSynchronize();  // the uploads have read their buffers
-    }
-    L.t_search = now();
-    if (trace)
-      std::fprintf(stderr, "serve: %zu frames (%zu searched), %zu queued; upload %.2f ms, search %.2f ms\n",
-                   L.batch.size(), frames.size(), L.left, (L.t_up - L.t_take) * 1e3, (L.t_search - L.t_up) * 1e3);
-    {
-      std::lock_guard<std::mutex> lk(m);
-      copies.push_back(std::move(L));
-    }
-    copy_cv.notify_one();
-    slot ^= 1;
+    it->frame = j;
+    ++st.frames;
+    st.open.insert(j);
+    taken.push_back(std::move(*it));
+    it = queue.erase(it);
   }
-  {
-    std::lock_guard<std::mutex> lk(m);
-    copier_stop = true;
-  }
-  copy_cv.notify_one();
-  copier.join();
 }
 
-// The copier thread: results of finished launches into the requests'
-// buffers, then their completions, while the worker runs the next launch.
-void Server::copy_loop() {
+// Frame j of a stream: its picture slot and its references' (the previous
+// nref pictures of the ring).
+rme_frame Server::frame_of(const Stream& st, int64_t j) const {
+  const int slots = st.nref + kPerStream;
+  rme_frame f{};
+  f.src_id = st.pic_base + (int32_t)(j % slots);
+  f.nref = (int)std::min<int64_t>(st.nref, j);
+  for (int k = 0; k < f.nref; ++k) f.ref_ids[k] = st.pic_base + (int32_t)((j - 1 - k) % slots);
+  return f;
+}
+
+// Hand a frame (uploaded) to the engine; without room there, try again
+// when a frame finishes; on an error, complete it behind its upload.
+void Server::submit_search(Request& r, const Stream& st) {
+  const rme_frame f = frame_of(st, r.frame);
+  const int rc = rme::engine_submit(eng, &f, &st.p, upload, &r.slot);
+  if (rc == RME_EBUSY) {
+    r.slot = -1;
+    submitting.push_back(r);
+    return;
+  }
+  if (rc == 0) {
+    r.nresults = rme::engine_slot_tasks(eng, r.slot);
+    searching.push_back(r);
+    return;
+  }
+  r.status = rc;
+  r.slot = -1;
+  r.ev = take_event();
+  cudaEventRecord(r.ev, upload);
+  copying.push_back(r);
+}
+
+// Upload the frame into its stream's ring, then (frames with a reference)
+// submit it to the engine behind the upload.
+void Server::start(Request& r) {
+  const Stream* st;
+  {
+    std::lock_guard<std::mutex> lk(m);
+    st = &streams[r.stream];
+  }
+  const rme_frame f = frame_of(*st, r.frame);
+  r.status = rme_picture_upload(ctx, f.src_id, &st->d, r.luma, 1, upload);
+  if (r.status == 0 && f.nref > 0) {
+    submit_search(r, *st);
+    return;
+  }
+  // Not searched (a stream's first frame) or failed: complete once the
+  // upload has read the frame's buffer.
+  r.slot = -1;
+  r.ev = take_event();
+  cudaEventRecord(r.ev, upload);
+  copying.push_back(r);
+}
+
+void Server::finish(Request& r, double t) {  // lock held
+  rme_completion c{};
+  c.request_id = r.id;
+  c.stream_id = r.stream;
+  c.status = r.status;
+  c.submit_s = r.submit_s;
+  c.done_s = t;
+  c.nresults = r.status == 0 && r.slot >= 0 ? r.nresults : 0;
+  done.push_back(c);
+  pool[r.bytes].push_back(r.luma);
+  Stream& st = streams[r.stream];
+  st.open.erase(r.frame);
+  --st.pending;
+}
+
+// Drop closed streams with nothing queued or in flight (their budget is
+// free at once); their pictures are released while no engine kernel runs (a
+// device free waits for every kernel).
+void Server::release_closed(bool engine_idle) {
+  std::vector<std::pair<int32_t, int>> now;
+  {
+    std::lock_guard<std::mutex> lk(m);
+    for (auto it = streams.begin(); it != streams.end();) {
+      if (it->second.closing && it->second.pending == 0) {
+        release_later.emplace_back(it->second.pic_base, it->second.nref + kPerStream);
+        resident -= it->second.bytes;
+        it = streams.erase(it);
+      } else {
+        ++it;
+      }
+    }
+    if (engine_idle) now.swap(release_later);
+  }
+  for (auto& pr : now)
+    for (int k = 0; k < pr.second; ++k) rme_picture_release(ctx, pr.first + k);
+}
+
+void Server::run() {
   for (;;) {
-    Launch L;
+    std::vector<Request> taken;
+    bool any_close = false;
+    const bool busy = !searching.empty() || !copying.empty() || !submitting.empty();
     {
       std::unique_lock<std::mutex> lk(m);
-      copy_cv.wait(lk, [&] { return copier_stop || !copies.empty(); });
-      if (copies.empty()) return;
-      L = std::move(copies.front());
-      copies.pop_front();
+      if (busy)
+        cv.wait_for(lk, std::chrono::microseconds(20), [&] { return stop || !queue.empty() || closes > 0; });
+      else
+        cv.wait_for(lk, std::chrono::milliseconds(50),
+                    [&] { return stop || !queue.empty() || closes > 0 || !release_later.empty(); });
+      if (stop && queue.empty() && !busy) break;
+      any_close = closes > 0;
+      closes = 0;
+      admit(taken);
     }
-    for (size_t i = 0; i < L.batch.size(); ++i)
-      if (L.status[i] == 0 && L.count[i] > 0)
-        std::memcpy(L.batch[i].out, staging[L.slot] + L.offset[i], sizeof(rme_result) * L.count[i]);
-    const double t = now();
-    std::lock_guard<std::mutex> lk(m);
-    for (size_t i = 0; i < L.batch.size(); ++i) {
-      rme_completion c{};
-      c.request_id = L.batch[i].id;
-      c.stream_id = L.batch[i].stream;
-      c.status = L.status[i];
-      c.submit_s = L.batch[i].submit_s;
-      c.done_s = t;
-      c.nresults = L.status[i] == 0 ? (int32_t)L.count[i] : 0;
-      done.push_back(c);
-      pool[L.batch[i].bytes].push_back(L.batch[i].luma);
-      Stream& st = streams[L.batch[i].stream];
-      if (--st.pending == 0 && st.closing) ++cleanups;
+    for (Request& r : taken) start(r);
+    // Frames the engine had no room for: again, oldest first.
+    if (!submitting.empty()) {
+      std::vector<Request> again;
+      again.swap(submitting);
+      for (Request& r : again) {
+        const Stream* st;
+        {
+          std::lock_guard<std::mutex> lk(m);
+          st = &streams[r.stream];
+        }
+        submit_search(r, *st);
+      }
     }
-    slot_busy[L.slot] = false;
-    copied_cv.notify_all();
-    if (cleanups) cv.notify_one();
+    // Finished searches: their results out on the copy stream.
+    for (size_t i = 0; i < searching.size();) {
+      Request& r = searching[i];
+      if (!rme::engine_done(eng, r.slot)) {
+        ++i;
+        continue;
+      }
+      rme_result* dst = r.out;
+      if (!r.out_pinned) {
+        r.staging = take_staging((size_t)r.nresults);
+        r.staging_n = (size_t)r.nresults;
+        dst = r.staging;
+      }
+      cudaError_t e = dst ? cudaMemcpyAsync(dst, rme::engine_results(eng, r.slot), sizeof(rme_result) * r.nresults,
+                                            cudaMemcpyDeviceToHost, copy)
+                          : cudaErrorMemoryAllocation;
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(h_status, rme::engine_status_word(eng), sizeof(uint32_t), cudaMemcpyDeviceToHost, copy);
+      r.ev = take_event();
+      cudaEventRecord(r.ev, copy);
+      if (e != cudaSuccess) r.status = RME_ECUDA;
+      copying.push_back(r);
+      searching[i] = searching.back();
+      searching.pop_back();
+    }
+    // The engine leaves when idle: launch it again while frames are in flight.
+    if (!searching.empty()) rme::engine_keep_running(eng);
+    // Copies done: results to the caller, slots back to the engine.
+    bool any = false;
+    for (size_t i = 0; i < copying.size();) {
+      Request& r = copying[i];
+      if (cudaEventQuery(r.ev) != cudaSuccess) {
+        ++i;
+        continue;
+      }
+      if (r.slot >= 0) {
+        if (r.status == 0 && *(volatile uint32_t*)h_status != 0) r.status = RME_EDEVICE;
+        if (r.status == 0 && r.staging) std::memcpy(r.out, r.staging, sizeof(rme_result) * r.nresults);
+        rme::engine_release(eng, r.slot);
+      }
+      if (r.staging) staging_pool[r.staging_n].push_back(r.staging);
+      events.push_back(r.ev);
+      const double t = now();
+      {
+        std::lock_guard<std::mutex> lk(m);
+        finish(r, t);
+      }
+      any = true;
+      copying[i] = copying.back();
+      copying.pop_back();
+    }
+    if (!release_later.empty() || any || any_close) release_closed(rme::engine_idle(eng));
   }
 }
 
@@ -296,7 +361,20 @@ int rme_serve_start(void* ctx, const rme_serve_opts* o, void** server) {
   auto* s = new Server();
   s->ctx = ctx;
   s->o = *o;
-  s->worker = std::thread([s] { s->run(); });
+  cudaGetDevice(&s->device);
+  if (rme::engine_create(ctx, s->device, &s->eng) != 0 ||
+      cudaStreamCreateWithFlags(&s->upload, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMallocHost(&s->h_status, 64) != cudaSuccess) {
+    if (s->eng) rme::engine_destroy(s->eng);
+    delete s;
+    return RME_ECUDA;
+  }
+  *s->h_status = 0;
+  s->worker = std::thread([s] {
+    cudaSetDevice(s->device);
+    s->run();
+  });
   *server = s;
   return RME_OK;
 }
@@ -331,6 +409,11 @@ int rme_serve_submit(void* server, int32_t stream_id, const void* luma, rme_resu
   if (!s || !luma) return RME_EINVAL;
   Request r;
   r.submit_s = s->now();
+  if (out) {
+    cudaPointerAttributes pa{};
+    r.out_pinned = cudaPointerGetAttributes(&pa, out) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+  }
   std::unique_lock<std::mutex> lk(s->m);
   auto it = s->streams.find(stream_id);
   if (it == s->streams.end() || it->second.closing) return RME_ENOTFOUND;
@@ -371,9 +454,9 @@ int rme_serve_close_stream(void* server, int32_t stream_id) {
     std::lock_guard<std::mutex> lk(s->m);
     auto it = s->streams.find(stream_id);
     if (it == s->streams.end() || it->second.closing) return RME_ENOTFOUND;
-    // The worker releases its pictures once its last request completes.
+    // The worker drops it once its last request completes.
     it->second.closing = true;
-    ++s->cleanups;
+    ++s->closes;
   }
   s->cv.notify_one();
   return RME_OK;
@@ -388,13 +471,20 @@ int rme_serve_stop(void* server) {
   }
   s->cv.notify_all();
   if (s->worker.joinable()) s->worker.join();
+  rme::engine_destroy(s->eng);  // the kernel leaves (asked to), then its memory goes
   for (auto& kv : s->streams)
     for (int k = 0; k < kv.second.nref + kPerStream; ++k) rme_picture_release(s->ctx, kv.second.pic_base + k);
+  for (auto& pr : s->release_later)
+    for (int k = 0; k < pr.second; ++k) rme_picture_release(s->ctx, pr.first + k);
   for (auto& q : s->queue) cudaFreeHost(q.luma);
-  for (int k = 0; k < 2; ++k)
-    if (s->staging[k]) cudaFreeHost(s->staging[k]);
   for (auto& kv : s->pool)
     for (void* b : kv.second) cudaFreeHost(b);
+  for (auto& kv : s->staging_pool)
+    for (rme_result* b : kv.second) cudaFreeHost(b);
+  for (cudaEvent_t e : s->events) cudaEventDestroy(e);
+  cudaFreeHost(s->h_status);
+  cudaStreamDestroy(s->upload);
+  cudaStreamDestroy(s->copy);
   delete s;
   return RME_OK;
 }

@@ -114,3 +114,52 @@ def test_admission_is_bounded_by_the_budget():
             assert srv.open_stream(2, HEVC, 8, 1920, 1080, p, 2) == 0
         finally:
             srv.stop()
+
+
+def test_many_frames_recycle_the_engine_slots_and_survive_idle_periods():
+    """300 frames of one stream and 60 of another through the resident
+    engine: more frames than it has frame slots (each slot reused with a new
+    generation), submitted in bursts with pauses long enough for the engine
+    kernel to leave and be launched again. Every checked frame equals the
+    plain per-frame path."""
+    streams = [(21, HEVC, 8, 128, 64, 2, 32), (22, H264, 8, 96, 64, 1, 28)]
+    counts = {21: 300, 22: 60}
+    seqs = {sid: synth.make_sequence(codec, w, h, bd, 8, 2000 + sid, 32, 32, 2.0).frames
+            for sid, codec, bd, w, h, _, _ in streams}
+    pics = {sid: [seqs[sid][t % 8] if (t // 8) % 2 == 0 else seqs[sid][7 - t % 8] for t in range(counts[sid])]
+            for sid in counts}
+    with host.MotionSearch(0) as ms:
+        srv = host.Server(ms, hbm_budget_bytes=8 << 30, max_frames_per_launch=8)
+        got = {}
+        try:
+            for sid, codec, bd, w, h, nref, qp in streams:
+                assert srv.open_stream(sid, codec, bd, w, h, _params(codec, qp), nref) == 0
+            ids = {}
+            t = {sid: 0 for sid in counts}
+            burst = 0
+            while any(t[s] < counts[s] for s in counts):
+                for _ in range(40):
+                    for sid in counts:
+                        if t[sid] < counts[sid]:
+                            ids[srv.submit(sid, pics[sid][t[sid]])] = (sid, t[sid])
+                            t[sid] += 1
+                done = _wait(srv, len(ids) - len(got))
+                for c in done:
+                    assert c["status"] == 0, c
+                    got[ids[c["id"]]] = c["results"]
+                burst += 1
+                if burst % 3 == 0:
+                    time.sleep(0.6)  # the engine kernel leaves after a quarter second idle
+        finally:
+            srv.stop()
+        for sid, codec, bd, w, h, nref, qp in streams:
+            for k in range(1, counts[sid]):
+                if k % 7 and k > 20:  # every seventh frame, and the first twenty, against the plain path
+                    continue
+                ms.upload(100, pics[sid][k], codec, bd, as_ref=True)
+                refs = []
+                for r in range(min(nref, k)):
+                    ms.upload(101 + r, pics[sid][k - 1 - r], codec, bd, as_ref=True)
+                    refs.append(101 + r)
+                want = ms.search(100, refs, _params(codec, qp))
+                assert_results_equal(got[(sid, k)], want, f"stream {sid} frame {k}")
