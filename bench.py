@@ -495,37 +495,49 @@ def run_ours(args, world, rank, local):
     ms.close()
 
 
-def run_served(frames, capacity_fps: float, loads=(0.2, 0.5, 0.65, 0.8, 1.0, 1.2), seconds: float = 2.0,
-               warm_s: float = 0.5, local: int = 0, max_batch: int = 64) -> dict:
+P99_TARGET_MS = 8.0
+
+
+def run_served(frames, capacity_fps: float, loads=(0.2, 0.4, 0.6, 0.8, 1.0, 1.2), min_requests: int = 1000,
+               warm_s: float = 0.5, local: int = 0) -> dict:
     """The serving loop under Poisson load: streams of the 1080p workload at
     30 frames/s each, the total rate a fraction of the measured batched
-    capacity; per-frame latency is submit -> results complete (host clock,
-    request loop included), over the requests submitted in a `seconds`
-    window after `warm_s` of the same load. Returns the sweep and the
-    headline point (the highest load the loop keeps up with)."""
+    capacity; per-frame latency is submit -> results in the client's buffer
+    (host clock, request loop included), over at least `min_requests`
+    requests submitted after `warm_s` of the same load. A load is kept up
+    with when served >= 0.97 x offered and p99 <= 8 ms; the headline is the
+    highest served rate that is."""
+    import torch
     import rivet_h26x_codecs_b200 as rme
     import rivet_h26x_codecs_b200.capi as capi
     p = hevc_params()
     sweep = []
     rng = np.random.default_rng(2024)
-    per_stream = 4  # frames of a stream that can join one launch (rme_serve_open_stream)
+    per_stream = 4  # frames of a stream in flight at once (rme_serve_open_stream)
+    count = 42900 * NREF
     for load in loads:
         rate = load * capacity_fps
         nstreams = max(1, int(round(rate / 30.0)))
+        seconds = max(2.0, min_requests / (nstreams * 30.0))
         with rme.MotionSearch(local) as ms:
-            srv = rme.Server(ms, hbm_budget_bytes=120 << 30, max_frames_per_launch=max_batch, max_streams=1024)
+            srv = rme.Server(ms, hbm_budget_bytes=120 << 30, max_frames_per_launch=64, max_streams=1024)
             try:
                 for sid in range(nstreams):
                     assert srv.open_stream(sid, capi.RME_CODEC_HEVC, 8, WIDTH, HEIGHT, p, NREF) == 0
-                # Each stream's client reuses a ring of result buffers (as an
-                # encoder reuses its motion field), touched once here.
-                count = 42900 * NREF
-                bufs = {sid: [np.zeros(count, capi.RESULT_DTYPE) for _ in range(8)] for sid in range(nstreams)}
+                # Each stream's client reuses a ring of pinned result buffers
+                # (as an encoder reuses its motion field), touched once here.
+                bufs = {}
+                for sid in range(nstreams):
+                    bufs[sid] = []
+                    for _ in range(8):
+                        t = torch.empty(count * capi.RESULT_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True)
+                        t.fill_(1)
+                        bufs[sid].append(t.numpy().view(capi.RESULT_DTYPE))
                 # Fill every stream's picture ring once (allocations, not timed).
                 nxt = {}
                 for sid in range(nstreams):
                     for t in range(NREF + per_stream):
-                        srv.submit(sid, frames[(sid * 7 + t) % len(frames)])
+                        srv.submit(sid, frames[(sid * 7 + t) % len(frames)], out=bufs[sid][t % 8] if t else None)
                     nxt[sid] = NREF + per_stream
                 pending = nstreams * (NREF + per_stream)
                 while pending:
@@ -545,7 +557,7 @@ def run_served(frames, capacity_fps: float, loads=(0.2, 0.5, 0.65, 0.8, 1.0, 1.2
                 for at, sid in events:
                     while time.perf_counter() - t0 < at:
                         done += srv.poll()
-                        time.sleep(0.0002)
+                        time.sleep(0.0001)
                     rid = srv.submit(sid, frames[(sid * 7 + nxt[sid]) % len(frames)], out=bufs[sid][nxt[sid] % 8])
                     nxt[sid] += 1
                     if at >= warm_s:
@@ -553,7 +565,7 @@ def run_served(frames, capacity_fps: float, loads=(0.2, 0.5, 0.65, 0.8, 1.0, 1.2
                 deadline = time.perf_counter() + 60
                 while len(done) < len(events) and time.perf_counter() < deadline:
                     done += srv.poll()
-                    time.sleep(0.0005)
+                    time.sleep(0.0002)
             finally:
                 srv.stop()
         ok = [d for d in done if d["status"] == 0 and d["id"] in measured]
@@ -564,15 +576,16 @@ def run_served(frames, capacity_fps: float, loads=(0.2, 0.5, 0.65, 0.8, 1.0, 1.2
                       "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
                       "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None})
         log(f"served load {load:.1f}: {sweep[-1]}")
-    # Keeping up: serves what is offered, and no backlog builds (a request
-    # waits at most a few launches).
-    rule = "served >= 0.97 x offered and p99 <= 250 ms"
+    rule = f"served >= 0.97 x offered and p99 <= {P99_TARGET_MS:g} ms"
     keeps_up = [x for x in sweep if x["served_fps"] >= 0.97 * x["offered_fps"] and x["p99_ms"] is not None
-                and x["p99_ms"] <= 250.0]
-    head = max(keeps_up, key=lambda x: x["served_fps"]) if keeps_up else sweep[0]
-    return {"value": head["served_fps"], "unit": "frames/s", "load": head["load"], "p50_ms": head["p50_ms"],
-            "p99_ms": head["p99_ms"], "capacity_fps": capacity_fps, "keeps_up": rule, "sweep": sweep,
-            "latency": "submit to results on the host, request loop included"}
+                and x["p99_ms"] <= P99_TARGET_MS]
+    head = max(keeps_up, key=lambda x: x["served_fps"]) if keeps_up else None
+    return {"value": head["served_fps"] if head else 0.0, "unit": "frames/s",
+            "streams_at_30fps": head["streams"] if head else 0,
+            "load": head["load"] if head else None, "p50_ms": head["p50_ms"] if head else None,
+            "p99_ms": head["p99_ms"] if head else None, "capacity_fps": capacity_fps, "keeps_up": rule,
+            "met": head is not None, "sweep": sweep,
+            "latency": "submit to results in the client's pinned buffer, host clock, request loop included"}
 
 
 def run_served_mix(local: int = 0, nstreams: int = 200, loads=(0.2, 0.5, 0.8, 1.0, 1.2), seconds: float = 3.0,

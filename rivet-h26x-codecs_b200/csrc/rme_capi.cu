@@ -100,7 +100,7 @@ constexpr int kParts = 4;
 // The launch header: head and tail of each part's queue (0..7), the
 // counters (8..12), status, epoch, then each part's finished-task count.
 constexpr int64_t kSpecTasks = 200000;  // about two 1080p frames of 2Nx2N PUs, 2 references
-constexpr int kMiscCounters = 8, kMiscStatus = 13, kMiscEpoch = 14, kMiscDone = 16, kMiscWords = 24;
+constexpr int kMiscCounters = 8, kMiscStatus = 13, kMiscEpoch = 14, kMiscDone = 16, kMiscBig = 20, kMiscWords = 32;
 
 int part_of(const FrameDesc& fd) { return 2 * (fd.bd > 8) + (fd.codec == RME_CODEC_H264); }
 int part_bytes(int k) { return k >= 2 ? 2 : 1; }
@@ -507,6 +507,13 @@ int make_frame(Ctx* c, const rme_frame* f, const rme_params* p, FrameDesc* fd, r
       fd->nby[l] = src->d.height / sizes[l];
       fd->base[l + 1] = fd->base[l] + fd->nbx[l] * fd->nby[l];
     }
+    // Blocks of 32 or more (the first levels): the tasks a CTA runs in the
+    // latency form.
+    if (p->predictor_mode == RME_PRED_STANDALONE) {
+      int lb = 0;
+      while (lb < fd->nlevels && fd->size[lb] >= 32) ++lb;
+      fd->big_end = fd->base[lb];
+    }
     if (p->predictor_mode == RME_PRED_STANDALONE && p->hevc_amp) {
       fd->amp = p->hevc_amp;
       fd->amp_nmodes = __builtin_popcount((unsigned)p->hevc_amp);
@@ -650,7 +657,7 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   if (!dev_out) CK(sl.d_out.ensure(std::max<int64_t>(total, 1)));
   CK(sl.d_pending.ensure(std::max<int64_t>(total, 1)));
   unsigned long long* old_ready = sl.d_ready.p;
-  CK(sl.d_ready.ensure(std::max<int64_t>(total, 1)));
+  CK(sl.d_ready.ensure(2 * std::max<int64_t>(total, 1)));  // the warps' queues, then the CTAs' queues
   // Fresh slot memory may hold any word, an epoch's among them: zero it
   // (epochs start at 1).
   if (sl.d_ready.p != old_ready) sl.epoch = 0;
@@ -669,7 +676,11 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   std::vector<int64_t> sig;
   sig.push_back(n);
   sig.push_back(dev_out + 2 * pinned_out);
-  std::vector<unsigned long long> init[kParts];
+  std::vector<unsigned long long> init[kParts], init_big[kParts];
+  // A launch of a frame or two is latency-bound: it runs the latency form
+  // of the search kernel (same results), where CTAs run the 32x32 and 64x64
+  // blocks of HEVC STANDALONE frames together.
+  const bool spec = total <= kSpecTasks;
   int64_t part_tasks[kParts] = {0, 0, 0, 0};
   for (int i = 0; i < n; ++i) part_tasks[part_of(sl.h_frames.p[i])] += ntask[i];
   std::vector<std::pair<const int32_t*, int>> pend_copies;  // (template, frame)
@@ -696,7 +707,9 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
       const Deps* dp = get_deps(c, src->d, &params[i], frames[i].nref, &rc);
       if (!dp) return rc;
       pend_copies.emplace_back(dp->pending, i);
-      for (uint32_t t : dp->ready) init[part].push_back(tag | t);
+      const bool groups = spec && fd.codec == RME_CODEC_HEVC;
+      for (uint32_t t : dp->ready)
+        (groups && (int)(t / fd.nref) < fd.big_end ? init_big : init)[part].push_back(tag | t);
       sig.push_back(fd.bd);
       sig.push_back(fd.codec);
       sig.push_back(fd.width);
@@ -707,14 +720,19 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   }
   // Frames' first tasks interleaved, so every frame starts at once.
   for (int k = 0; k < kParts; ++k)
-    std::stable_sort(init[k].begin(), init[k].end(), [](unsigned long long a, unsigned long long b) {
-      return (a & 0xffffffu) < (b & 0xffffffu);
-    });
-  // h_init: [the launch header (kMiscWords) | entries]
-  size_t ninit = 0, init_off[kParts];
+    for (auto* v : {&init[k], &init_big[k]})
+      std::stable_sort(v->begin(), v->end(), [](unsigned long long a, unsigned long long b) {
+        return (a & 0xffffffu) < (b & 0xffffffu);
+      });
+  // h_init: [the launch header (kMiscWords) | entries | the CTAs' entries]
+  size_t ninit = 0, init_off[kParts], init_big_off[kParts];
   for (int k = 0; k < kParts; ++k) {
     init_off[k] = ninit;
     ninit += init[k].size();
+  }
+  for (int k = 0; k < kParts; ++k) {
+    init_big_off[k] = ninit;
+    ninit += init_big[k].size();
   }
   CK(sl.h_init.ensure(kMiscWords + ninit));
   unsigned long long* hi = sl.h_init.p;
@@ -724,7 +742,9 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   int64_t slot0 = 0, slot_off[kParts];
   for (int k = 0; k < kParts; ++k) {
     hi[2 * k + 1] = init[k].size();
+    hi[kMiscBig + 2 * k + 1] = init_big[k].size();
     std::memcpy(hi + kMiscWords + init_off[k], init[k].data(), init[k].size() * sizeof(unsigned long long));
+    std::memcpy(hi + kMiscWords + init_big_off[k], init_big[k].data(), init_big[k].size() * sizeof(unsigned long long));
     slot_off[k] = slot0;
     LaunchDesc& L = Ls[k];
     L.frames = sl.d_frames.p;
@@ -736,13 +756,14 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
     L.status = reinterpret_cast<uint32_t*>(sl.d_misc.p + kMiscStatus);
     L.epoch = reinterpret_cast<const uint32_t*>(sl.d_misc.p + kMiscEpoch);
     L.done = sl.d_misc.p + kMiscDone + k;
+    L.ready_big = sl.d_ready.p + total + slot0;
+    L.head_big = sl.d_misc.p + kMiscBig + 2 * k;
+    L.tail_big = sl.d_misc.p + kMiscBig + 2 * k + 1;
+    L.group_ctas = 0;
     slot0 += part_tasks[k];
   }
   int nparts_used = 0;
   for (int k = 0; k < kParts; ++k) nparts_used += part_tasks[k] > 0;
-  // A launch of a frame or two is latency-bound: it runs the latency form
-  // of the search kernel (same results).
-  const bool spec = total <= kSpecTasks;
   int variant[kParts];
   Ctx::Tune* tuning = nullptr;  // the class this launch times, if any
   for (int k = 0; k < kParts; ++k) {
@@ -769,11 +790,27 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
     if (!c->ev_join[j]) CK(cudaEventCreateWithFlags(&c->ev_join[j], cudaEventDisableTiming));
   }
   if (nparts > 1 && !c->ev_fork) CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
-  auto grid_for = [&](int64_t tasks, int bps) {
-    int64_t want = (tasks + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    return (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)c->nsm * bps, want));
-  };
   sig.push_back(nparts);
+  // Grids: in the latency form a part with large HEVC blocks gives them up
+  // to half the SMs' worth of CTAs (one block at a time each) and the rest to
+  // the warps; all CTAs fit on the GPU at once, so neither kind waits for
+  // the other to be scheduled.
+  int grid[kParts] = {0, 0, 0, 0};
+  for (int k = 0; k < kParts; ++k) {
+    if (part_tasks[k] == 0) continue;
+    const int cap = c->nsm * c->bps[k][variant[k]][spec];
+    int64_t big = 0;
+    if (spec && part_codec(k) == RME_CODEC_HEVC)
+      for (int i = 0; i < n; ++i)
+        if (part_of(sl.h_frames.p[i]) == k && params[i].predictor_mode == RME_PRED_STANDALONE)
+          big += (int64_t)sl.h_frames.p[i].big_end * sl.h_frames.p[i].nref;
+    const int g = big > 0 ? (int)std::min<int64_t>({(int64_t)c->nsm / 2, big, (int64_t)cap - 1}) : 0;
+    const int64_t small = part_tasks[k] - big;
+    const int solo = (int)std::max<int64_t>(1, std::min<int64_t>(cap - g, (small + kWarpsPerBlock - 1) / kWarpsPerBlock));
+    Ls[k].group_ctas = g;
+    grid[k] = g + solo;
+    sig.push_back(g);
+  }
   auto enqueue = [&](bool capturing) -> cudaError_t {
     const unsigned rec = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
     cudaError_t e = cudaMemcpyAsync(sl.d_frames.p, sl.h_frames.p, sizeof(FrameDesc) * n, cudaMemcpyHostToDevice, s);
@@ -783,10 +820,14 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
                             cudaMemcpyDeviceToDevice, s);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(sl.d_misc.p, hi, kMiscWords * sizeof(unsigned long long), cudaMemcpyHostToDevice, s);
-    for (int k = 0; k < kParts; ++k)
+    for (int k = 0; k < kParts; ++k) {
       if (e == cudaSuccess && !init[k].empty())
         e = cudaMemcpyAsync(sl.d_ready.p + slot_off[k], hi + kMiscWords + init_off[k],
                             init[k].size() * sizeof(unsigned long long), cudaMemcpyHostToDevice, s);
+      if (e == cudaSuccess && !init_big[k].empty())
+        e = cudaMemcpyAsync(sl.d_ready.p + total + slot_off[k], hi + kMiscWords + init_big_off[k],
+                            init_big[k].size() * sizeof(unsigned long long), cudaMemcpyHostToDevice, s);
+    }
     // Under capture the records are external ones: they become event-record
     // nodes, so the kernels' device time is measured on every replay.
     if (e == cudaSuccess) e = cudaEventRecordWithFlags(sl.ev0, s, rec);
@@ -798,8 +839,7 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
       cudaStream_t sk = j == 0 ? s : c->aux[j];
       if (j > 0) e = cudaStreamWaitEvent(sk, c->ev_fork, 0);
       if (e == cudaSuccess)
-        e = launch_search(Ls[k], part_bytes(k), part_codec(k), variant[k],
-                          grid_for(part_tasks[k], c->bps[k][variant[k]][spec]), sk, spec);
+        e = launch_search(Ls[k], part_bytes(k), part_codec(k), variant[k], grid[k], sk, spec);
       if (e == cudaSuccess && j > 0) e = cudaEventRecord(c->ev_join[j], sk);
     }
     for (int j = 1; j < nparts && e == cudaSuccess; ++j) e = cudaStreamWaitEvent(s, c->ev_join[j], 0);

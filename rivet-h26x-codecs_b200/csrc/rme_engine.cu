@@ -65,14 +65,17 @@ __device__ __forceinline__ void settle(const EngineCtl& E, Settle& st) {
 
 // Lane 0: the entry of the next pushed slot, kPopDone once the warp may
 // leave (the host asked, or nothing came for E.idle_polls polls), or
-// 0xffffffff when a claimed slot's write never came (status set).
-__device__ __forceinline__ uint32_t engine_pop(const LaunchDesc& L, const EngineCtl& E, Settle& st) {
+// 0xffffffff when a claimed slot's write never came (status set). `big`:
+// the ring of the tasks a CTA runs.
+__device__ __forceinline__ uint32_t engine_pop(const LaunchDesc& L, const EngineCtl& E, Settle& st, bool big) {
+  unsigned long long* const head = big ? L.head_big : L.head;
+  unsigned long long* const tail = big ? L.tail_big : L.tail;
   uint32_t idle = 0, ns = 64;
   unsigned long long idx = 0;
   for (;;) {
-    const unsigned long long t = ld_relaxed64(L.tail), h = ld_relaxed64(L.head);
+    const unsigned long long t = ld_relaxed64(tail), h = ld_relaxed64(head);
     if (h < t) {
-      if (atomicCAS(L.head, h, h + 1) == h) {
+      if (atomicCAS(head, h, h + 1) == h) {
         idx = h;
         break;
       }
@@ -86,7 +89,7 @@ __device__ __forceinline__ uint32_t engine_pop(const LaunchDesc& L, const Engine
   }
   // Pushed (the tail moved past it), perhaps not yet written.
   const unsigned long long lap = (idx >> L.ring_shift) + 1ull;
-  const unsigned long long* slot = L.ready + (idx & ((1ull << L.ring_shift) - 1ull));
+  const unsigned long long* slot = (big ? L.ready_big : L.ready) + (idx & ((1ull << L.ring_shift) - 1ull));
   for (uint32_t it = 0, ns2 = 32;; ++it) {
     const unsigned long long v = ld_acquire64(slot);
     if ((v >> 32) == lap) return (uint32_t)v;
@@ -101,9 +104,72 @@ __device__ __forceinline__ uint32_t engine_pop(const LaunchDesc& L, const Engine
 
 constexpr int kEngineMinBlocks = 3;
 
+// A CTA serving the ring of 32x32 and 64x64 HEVC blocks: all its threads
+// run each task together (hevc_group_task).
+template <class S>
+__device__ void engine_group_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, GroupSmem<S>& gs, int tid,
+                                  int& cont) {
+  const int blk = t / F.nref;
+  int l = 0;
+  while (l + 1 < F.nlevels && blk >= F.base[l + 1]) ++l;
+  if (F.size[l] == 64) cont = hevc_group_task<S, 64>(L, F, f, t, gs, tid);
+  else if (F.size[l] == 32) cont = hevc_group_task<S, 32>(L, F, f, t, gs, tid);
+  else if (tid == 0) atomicOr(L.status, kStatusBadTask);
+}
+
+__device__ void engine_group_loop(const LaunchDesc& L, const EngineCtl& E, unsigned char* smem_raw, FrameDesc& F) {
+  GroupSmem<uint16_t>& g16 = *reinterpret_cast<GroupSmem<uint16_t>*>(smem_raw);
+  GroupSmem<uint8_t>& g8 = *reinterpret_cast<GroupSmem<uint8_t>*>(smem_raw);
+  const int tid = threadIdx.x;
+  if (tid < 6) g16.cnt[tid] = 0;
+  __syncthreads();
+  Settle st;
+  int cont = -1;
+  for (;;) {
+    uint32_t e;
+    if (cont >= 0) {
+      e = (uint32_t)cont;
+    } else {
+      if (tid == 0) g16.bc[7] = engine_pop(L, E, st, true);
+      __syncthreads();
+      e = g16.bc[7];
+      if (e != kPopDone && e != 0xffffffffu) {
+        const uint32_t* from = reinterpret_cast<const uint32_t*>(&L.frames[e >> 24]);
+        uint32_t* to = reinterpret_cast<uint32_t*>(&F);
+        for (int i = tid; i < (int)(sizeof(FrameDesc) / 4); i += kGroupThreads) to[i] = __ldcg(from + i);
+      }
+      __syncthreads();
+      if (e == kPopDone) break;
+    }
+    cont = -1;
+    if (e == 0xffffffffu) continue;
+    const int f = (int)(e >> 24), t = (int)(e & 0xffffffu);
+    if (t >= F.ntasks || !group_task_of(L, F, t)) {
+      if (tid == 0) atomicOr(L.status, kStatusBadTask);
+      continue;
+    }
+    if (F.bd == 8) engine_group_task<uint8_t>(L, F, f, t, g8, tid, cont);
+    else engine_group_task<uint16_t>(L, F, f, t, g16, tid, cont);
+    if (tid == 0) {
+      settle(E, st);
+      st.old = atom_add_release(&E.fdone[f], 1u);  // thread 0 wrote the result itself
+      st.f = f;
+      st.n = (uint32_t)F.ntasks;
+      st.gen = F.gen;
+    }
+  }
+  if (tid == 0) settle(E, st);
+  __syncthreads();
+  if (tid < 5) atomicAdd(&L.counters[tid], g16.cnt[tid]);
+}
+
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kEngineMinBlocks) engine_kernel(LaunchDesc L, EngineCtl E) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ FrameDesc fdesc[kWarpsPerBlock];
+  if ((int)blockIdx.x < L.group_ctas) {
+    engine_group_loop(L, E, smem_raw, fdesc[0]);
+    return;
+  }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   WarpSmem<uint16_t>& sm16 = reinterpret_cast<WarpSmem<uint16_t>*>(smem_raw)[warp];
   WarpSmem<uint8_t>& sm8 = reinterpret_cast<WarpSmem<uint8_t>&>(sm16);
@@ -118,7 +184,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kEngineMinBlocks) engine_
       e = (uint32_t)cont;  // a task of the same frame: its descriptor is here already
     } else {
       e = 0;
-      if (lane == 0) e = engine_pop(L, E, st);
+      if (lane == 0) e = engine_pop(L, E, st, false);
       e = __shfl_sync(kFull, e, 0);
       if (e == kPopDone) break;
       if (e != 0xffffffffu) {
@@ -153,16 +219,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kEngineMinBlocks) engine_
   if (lane < 5) atomicAdd(&L.counters[lane], sm16.cnt[lane]);
 }
 
-// A frame's root tasks (those that read no other task's result) into the
-// ring, queued behind everything the frame needs.
+// A frame's root tasks (those that read no other task's result) into their
+// rings, queued behind everything the frame needs (its descriptor among it).
 __global__ void publish_kernel(LaunchDesc L, int f, const uint32_t* roots, int n) {
-  __shared__ unsigned long long base;
-  if (threadIdx.x == 0) base = atomicAdd(L.tail, (unsigned long long)n);
-  __syncthreads();
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const unsigned long long idx = base + i, lap = (idx >> L.ring_shift) + 1ull;
-    st_release64(L.ready + (idx & ((1ull << L.ring_shift) - 1ull)), (lap << 32) | ((uint32_t)f << 24) | roots[i]);
-  }
+  const FrameDesc& F = L.frames[f];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) push_ready(L, f, (int)roots[i], group_task_of(L, F, (int)roots[i]));
 }
 
 size_t engine_smem() { return sizeof(WarpSmem<uint16_t>) * kWarpsPerBlock; }
@@ -193,7 +254,8 @@ cudaError_t launch_publish(const LaunchDesc& L, int frame, const uint32_t* roots
 
 namespace {
 constexpr int kRingShift = 22;  // 4 Mi slots (32 MiB): the tasks in flight at once
-constexpr int kHdrHead = 0, kHdrTail = 1, kHdrStatus = 2, kHdrCounters = 3, kHdrEpoch = 8, kHdrWords = 16;
+constexpr int kHdrHead = 0, kHdrTail = 1, kHdrStatus = 2, kHdrCounters = 3, kHdrEpoch = 8, kHdrHeadBig = 9,
+              kHdrTailBig = 10, kHdrWords = 16;
 }  // namespace
 
 struct EngineSlot {
@@ -210,7 +272,7 @@ struct Engine {
   void* ctx = nullptr;
   int device = 0, grid = 0;
   unsigned long long* d_hdr = nullptr;
-  unsigned long long* d_ring = nullptr;
+  unsigned long long* d_ring = nullptr;  // the warps' ring, then the CTAs' ring
   FrameDesc* d_frames = nullptr;
   FrameDesc* h_frames = nullptr;  // pinned: each slot's descriptor, copied at submit
   uint32_t* d_fdone = nullptr;
@@ -262,9 +324,9 @@ int engine_create(void* ctx, int device, Engine** out) {
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
   if (e == cudaSuccess) e = cudaMalloc(&g->d_hdr, kHdrWords * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMemset(g->d_hdr, 0, kHdrWords * sizeof(unsigned long long));
-  if (e == cudaSuccess) e = cudaMalloc(&g->d_ring, sizeof(unsigned long long) << kRingShift);
+  if (e == cudaSuccess) e = cudaMalloc(&g->d_ring, 2 * (sizeof(unsigned long long) << kRingShift));
   // Slot words start at zero: lap tags start at 1.
-  if (e == cudaSuccess) e = cudaMemset(g->d_ring, 0, sizeof(unsigned long long) << kRingShift);
+  if (e == cudaSuccess) e = cudaMemset(g->d_ring, 0, 2 * (sizeof(unsigned long long) << kRingShift));
   if (e == cudaSuccess) e = cudaMalloc(&g->d_frames, sizeof(FrameDesc) * kEngineFrames);
   if (e == cudaSuccess) e = cudaMemset(g->d_frames, 0, sizeof(FrameDesc) * kEngineFrames);
   if (e == cudaSuccess) e = cudaMallocHost(&g->h_frames, sizeof(FrameDesc) * kEngineFrames);
@@ -286,6 +348,8 @@ int engine_create(void* ctx, int device, Engine** out) {
   // At most two of the kernel's blocks per SM: room is left on every SM for
   // the uploads' plane builds, which run beside it.
   g->grid = nsm * std::min(2, engine_blocks_per_sm());
+  // A quarter of them run the 32x32 and 64x64 HEVC blocks, a CTA per block.
+  const int groups = std::max(1, g->grid / 4);
   for (int k = kEngineFrames - 1; k >= 0; --k) g->free_slots.push_back(k);
   LaunchDesc& L = g->L;
   L.frames = g->d_frames;
@@ -297,6 +361,10 @@ int engine_create(void* ctx, int device, Engine** out) {
   L.counters = g->d_hdr + kHdrCounters;
   L.epoch = reinterpret_cast<const uint32_t*>(g->d_hdr + kHdrEpoch);
   L.done = nullptr;
+  L.ready_big = g->d_ring + (1ull << kRingShift);
+  L.head_big = g->d_hdr + kHdrHeadBig;
+  L.tail_big = g->d_hdr + kHdrTailBig;
+  L.group_ctas = groups;
   L.ring_shift = kRingShift;
   EngineCtl& E = g->E;
   E.fdone = g->d_fdone;

@@ -66,6 +66,7 @@ struct FrameDesc {
   int32_t* pending;
   int32_t ntasks;
   uint32_t gen;  // the resident engine: this frame's generation in its slot
+  int32_t big_end;  // HEVC STANDALONE: tasks below big_end * nref are blocks of 32 or more
 };
 
 // A launch's dataflow queue: a task is pushed when its last dependency
@@ -86,6 +87,12 @@ struct LaunchDesc {
                                  // runs one task it made ready itself
                                  // (no queue round trip) and idle warps
                                  // leave once every task is done
+  // The queue of the tasks a whole CTA runs (32x32 and 64x64 blocks in the
+  // latency form), served by the first `group_ctas` CTAs; 0: none.
+  unsigned long long* ready_big;
+  unsigned long long* head_big;
+  unsigned long long* tail_big;
+  int32_t group_ctas;
   int32_t ring_shift;            // nonzero: the resident engine's ring of
                                  // 2^ring_shift slots (slot idx holds
                                  // ((idx >> ring_shift) + 1) << 32 | entry)

@@ -57,9 +57,59 @@ namespace {
 // leaves more registers per thread (a single frame's dependency chain runs
 // faster), 4 keeps more warps resident (large batches hide more latency);
 // the host's tuner picks per kind and launch size.
+// A CTA of the latency form serving the queue of 32x32 and 64x64 blocks:
+// all its threads run each task together (hevc_group_task).
+template <class S>
+__device__ void group_loop(const LaunchDesc& L, unsigned char* smem_raw) {
+  GroupSmem<S>& gs = *reinterpret_cast<GroupSmem<S>*>(smem_raw);
+  const int tid = threadIdx.x;
+  if (tid < 6) gs.cnt[tid] = 0;
+  const uint32_t epoch = __ldg(L.epoch);
+  int cont = -1;
+  __syncthreads();
+  for (;;) {
+    uint32_t e;
+    if (cont >= 0) {
+      e = (uint32_t)cont;
+    } else {
+      if (tid == 0) {
+        const unsigned long long idx = atomicAdd(L.head_big, 1ull);
+        gs.bc[7] = idx >= (unsigned long long)L.total ? kPopDone : pop_slot(L, idx, epoch, true);
+      }
+      __syncthreads();
+      e = gs.bc[7];
+      __syncthreads();
+      if (e == kPopDone) break;
+    }
+    cont = -1;
+    if (e == 0xffffffffu) continue;  // the wait ran out (status set)
+    const int f = (int)(e >> 24), t = (int)(e & 0xffffffu);
+    const FrameDesc& F = L.frames[f];
+    if (t >= F.ntasks || (sizeof(S) == 1) != (F.bd == 8) || !group_task_of(L, F, t)) {
+      if (tid == 0) atomicOr(L.status, kStatusBadTask);
+      continue;
+    }
+    const int blk = t / F.nref;
+    int l = 0;
+    while (l + 1 < F.nlevels && blk >= F.base[l + 1]) ++l;
+    if (F.size[l] == 64) cont = hevc_group_task<S, 64>(L, F, f, t, gs, tid);
+    else if (F.size[l] == 32) cont = hevc_group_task<S, 32>(L, F, f, t, gs, tid);
+    else if (tid == 0) atomicOr(L.status, kStatusBadTask);
+    if (tid == 0 && L.done != nullptr) red_add64(L.done, 1ull);
+  }
+  __syncthreads();
+  if (tid < 5) atomicAdd(&L.counters[tid], gs.cnt[tid]);
+}
+
 template <class S, int CODEC, int MINB, bool SPEC>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, MINB) search_kernel(LaunchDesc L) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  if constexpr (SPEC && CODEC == RME_CODEC_HEVC) {
+    if ((int)blockIdx.x < L.group_ctas) {
+      group_loop<S>(L, smem_raw);
+      return;
+    }
+  }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   WarpSmem<S>& sm = reinterpret_cast<WarpSmem<S>*>(smem_raw)[warp];
   if (lane < 5) sm.cnt[lane] = 0;

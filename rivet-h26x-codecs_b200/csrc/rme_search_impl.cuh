@@ -265,17 +265,21 @@ __device__ __forceinline__ const S* plane_at(const DevPlanes& p, int plane, int 
 
 // ---- dataflow queue ---------------------------------------------------------
 
-// Push task `t` of frame `f` (lane 0): its last dependency just finished.
-__device__ __forceinline__ void push_ready(const LaunchDesc& L, int f, int t) {
-  const unsigned long long idx = atomicAdd(L.tail, 1ull);
+// Push task `t` of frame `f` (one thread): its last dependency just
+// finished. `big`: into the queue of the tasks a CTA runs.
+__device__ __forceinline__ void push_ready(const LaunchDesc& L, int f, int t, bool big = false) {
+  unsigned long long* const ready = big ? L.ready_big : L.ready;
+  const unsigned long long idx = atomicAdd(big ? L.tail_big : L.tail, 1ull);
   if (L.ring_shift) {  // the engine's ring: the host keeps fewer tasks in flight than it has slots
     const unsigned long long lap = (idx >> L.ring_shift) + 1ull;
-    st_release64(L.ready + (idx & ((1ull << L.ring_shift) - 1ull)), (lap << 32) | ((uint32_t)f << 24) | (uint32_t)t);
+    st_release64(ready + (idx & ((1ull << L.ring_shift) - 1ull)), (lap << 32) | ((uint32_t)f << 24) | (uint32_t)t);
   } else if (idx < (unsigned long long)L.total)
-    st_release64(L.ready + idx, ((unsigned long long)__ldg(L.epoch) << 32) | ((uint32_t)f << 24) | (uint32_t)t);
+    st_release64(ready + idx, ((unsigned long long)__ldg(L.epoch) << 32) | ((uint32_t)f << 24) | (uint32_t)t);
   else
     atomicOr(L.status, kStatusBadTask);
 }
+
+__device__ __forceinline__ bool group_task_of(const LaunchDesc& L, const FrameDesc& F, int t);
 
 // A finished task's dependents, task `dtask` in each lane where `rel`
 // (all lanes call): each decrement that reaches zero makes its task ready.
@@ -283,17 +287,20 @@ __device__ __forceinline__ void push_ready(const LaunchDesc& L, int f, int t) {
 // ready (lowest lane) to run next itself, saving the push, the pop and the
 // hand-over to another warp, unless `cont` already holds one; the others are
 // pushed. Returns `cont`, updated.
+// Tasks a CTA runs go to their own queue; a warp keeps only a task of its
+// own kind (`group`: the caller is a CTA).
 __device__ __forceinline__ int release_lanes(const LaunchDesc& L, const FrameDesc& F, int f, bool rel, int dtask,
-                                             int cont, int lane) {
+                                             int cont, int lane, bool group = false) {
   const bool ready = rel && dec_acq_rel(&F.pending[dtask]) == 1;
-  const uint32_t m = __ballot_sync(kFull, ready);
-  if (m == 0u) return cont;
+  const bool big = ready && group_task_of(L, F, dtask);
+  const uint32_t m = __ballot_sync(kFull, ready && big == group);
+  if (__ballot_sync(kFull, ready) == 0u) return cont;
   int keep = -1;
-  if (cont < 0 && (L.done != nullptr || L.ring_shift)) {
+  if (m != 0u && cont < 0 && (L.done != nullptr || L.ring_shift)) {
     keep = __ffs(m) - 1;
     cont = (f << 24) | __shfl_sync(kFull, dtask, keep);
   }
-  if (ready && lane != keep) push_ready(L, f, dtask);
+  if (ready && lane != keep) push_ready(L, f, dtask, big);
   return cont;
 }
 
@@ -313,10 +320,11 @@ constexpr uint32_t kPopDone = 0xfffffffeu;  // every task of the launch is done
 // kPopDone once every task is done (a slot that will never be filled: the
 // warps that ran tasks they made ready pushed fewer than `total`), or
 // 0xffffffff when the wait runs out (status set).
-__device__ __forceinline__ uint32_t pop_slot(const LaunchDesc& L, unsigned long long idx, uint32_t epoch) {
+__device__ __forceinline__ uint32_t pop_slot(const LaunchDesc& L, unsigned long long idx, uint32_t epoch,
+                                             bool big = false) {
   uint32_t ns = 32, it = 0;
   for (;;) {
-    const unsigned long long v = ld_acquire64(L.ready + idx);
+    const unsigned long long v = ld_acquire64((big ? L.ready_big : L.ready) + idx);
     if ((uint32_t)(v >> 32) == epoch) return (uint32_t)v;
     if (L.done != nullptr && (it & 3u) == 3u && ld_relaxed64(L.done) >= (unsigned long long)L.total) return kPopDone;
     if (++it >= kSpinLimit) {
@@ -1007,6 +1015,408 @@ __device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
   }
   count_task(sm, lane, nsad, nsatd, w * h);
   return cont;
+}
+
+// ---- HEVC, large blocks: one CTA per task (latency form) ----------------------
+//
+// A 32x32 or 64x64 block's search is the longest dependent chain of a
+// frame (its level's wavefront has few blocks in flight, each of 1-4 K
+// samples per candidate), so in the latency form a whole CTA runs one: the
+// 256 threads split every step's candidate rows (SAD) or 4x4 tiles (SATD),
+// each warp's partial sum goes to shared memory, and after one barrier every
+// thread reads the step's costs and takes the same decision. The steps are
+// the single-warp search's, with more candidates per step where that saves
+// dependent steps: the seeds together, the small diamond two rounds at a
+// time (the second round's three new points for each way the first can
+// move), the 24 ring points together, and the start with the half ring
+// together. Each decision is the reference's in-order strict-< walk over the
+// step's candidates, so the results and the candidate counts are the
+// single-warp search's.
+constexpr int kGroupThreads = kWarpsPerBlock * 32;
+
+template <class S>
+struct alignas(16) GroupSmem {
+  unsigned long long cnt[6];
+  uint32_t part[2][96];  // per step, per 32-job chunk: a warp's partial sum (two steps alternate)
+  uint32_t bc[8];        // broadcasts: predictor words, the popped entry
+  uint32_t src[kMaxBlk * kMaxBlk * sizeof(S) / 4];
+};
+
+// True for the tasks a CTA runs (32x32 and 64x64 STANDALONE blocks) when
+// the launch has CTAs for them.
+__device__ __forceinline__ bool group_task_of(const LaunchDesc& L, const FrameDesc& F, int t) {
+  return L.group_ctas > 0 && F.mode == RME_PRED_STANDALONE && F.codec == RME_CODEC_HEVC && t / F.nref < F.big_end;
+}
+
+// One row of the candidate's SAD (N samples).
+template <class S, int N>
+__device__ __forceinline__ uint32_t row_sad(const uint32_t* srow, const S* rp) {
+  constexpr int WR = N * (int)sizeof(S) / 4, CW = WR < 16 ? WR : 16;
+  uint32_t acc = 0;
+#pragma unroll
+  for (int c = 0; c < WR; c += CW) {
+    uint32_t a[CW];
+    ldwords<CW>(rp + c * (4 / (int)sizeof(S)), a);
+#pragma unroll
+    for (int j = 0; j < CW; ++j) acc += vsad(srow[c + j], a[j], S());
+  }
+  return acc;
+}
+
+// The SADs of `nc` candidates of an N x N block (rows split over the CTA):
+// pos(c, fx, fy) gives candidate c's whole-sample offset and whether it is
+// scored. Sums per 32-row chunk into part[buf].
+template <class S, int N, class Pos>
+__device__ __forceinline__ void cta_sad(GroupSmem<S>& gs, int buf, const S* org, int stride, int nc, Pos pos,
+                                          int tid) {
+  constexpr int SPW = 4 / sizeof(S), WR = N / SPW;
+  const int jobs = nc * N;
+#pragma unroll 2
+  for (int j0 = 0; j0 < jobs; j0 += kGroupThreads) {
+    const int j = j0 + tid;
+    uint32_t acc = 0;
+    if (j < jobs) {
+      const int c = j / N, row = j - c * N;
+      int fx, fy;
+      if (pos(c, fx, fy)) acc = row_sad<S, N>(gs.src + row * WR, org + (ptrdiff_t)(fy + row) * stride + fx);
+    }
+    acc = __reduce_add_sync(kFull, acc);
+    if ((tid & 31) == 0 && j < jobs) gs.part[buf][j >> 5] = acc;
+  }
+  __syncthreads();
+}
+
+// The SATDs of `nc` candidates (quarter-sample vectors from pos), 4x4 tiles
+// split over the CTA; sums per 32-tile chunk into part[buf].
+template <class S, int N, class Pos>
+__device__ __forceinline__ void cta_satd(GroupSmem<S>& gs, int buf, const DevPlanes& R, int x, int y, int nc,
+                                           Pos pos, int tid) {
+  constexpr int SPW = 4 / sizeof(S), WPT = 4 / SPW, TW = N / 4, NT = TW * TW, WR = N / SPW;
+  const int jobs = nc * NT;
+#pragma unroll 3
+  for (int j0 = 0; j0 < jobs; j0 += kGroupThreads) {
+    const int j = j0 + tid;
+    uint32_t acc = 0;
+    if (j < jobs) {
+      const int c = j / NT, i = j - c * NT, ty = i / TW, tx = i - ty * TW;
+      int mx, my;
+      if (pos(c, mx, my)) {
+        const S* pp = plane_at<S>(R, (my & 3) * 4 + (mx & 3), x + (mx >> 2) + tx * 4, y + (my >> 2) + ty * 4);
+        uint32_t pw[4][WPT];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) ldwords<WPT>(pp + (ptrdiff_t)r * R.stride, pw[r]);
+        int d[16];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const uint32_t* srow = &gs.src[(ty * 4 + r) * WR + tx * WPT];
+#pragma unroll
+          for (int k = 0; k < WPT; ++k) {
+            const uint32_t sw = srow[k], qw = pw[r][k];
+#pragma unroll
+            for (int e = 0; e < SPW; ++e) {
+              const int shf = e * (32 / SPW);
+              const uint32_t m = SPW == 4 ? 0xffu : 0xffffu;
+              d[r * 4 + k * SPW + e] = (int)((sw >> shf) & m) - (int)((qw >> shf) & m);
+            }
+          }
+        }
+        acc = satd4x4(d);
+      }
+    }
+    acc = __reduce_add_sync(kFull, acc);
+    if ((tid & 31) == 0 && j < jobs) gs.part[buf][j >> 5] = acc;
+  }
+  __syncthreads();
+}
+
+// Candidate c's distortion after a step: the sum of its chunks.
+template <class S>
+__device__ __forceinline__ uint32_t cta_cost(const GroupSmem<S>& gs, int buf, int c, int chunks) {
+  uint32_t v = 0;
+  for (int k = 0; k < chunks; ++k) v += gs.part[buf][c * chunks + k];
+  return v;
+}
+
+// search_full + refine_subpel of one STANDALONE square block of N in {32, 64}
+// by the whole CTA (all threads call). Returns a task it made ready to run
+// next (frame << 24 | task; another group task) or -1.
+template <class S, int N>
+__device__ int hevc_group_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, GroupSmem<S>& gs, int tid) {
+  constexpr int SPW = 4 / sizeof(S), WR = N / SPW;
+  const int lane = tid & 31;
+  const int r = t % F.nref, blk = t / F.nref;
+  int l = 0;
+  while (l + 1 < F.nlevels && blk >= F.base[l + 1]) ++l;
+  const int local = blk - F.base[l], nbx = F.nbx[l], lby = local / nbx, lbx = local - lby * nbx;
+  const int x = lbx * N, y = lby * N;
+  // The left, upper and parent results (threads 0..2), while all threads
+  // stage the source block.
+  if (tid < 3) {
+    int didx = -1;
+    if (tid == 0 && lbx > 0) didx = (F.base[l] + local - 1) * F.nref + r;
+    if (tid == 1 && lby > 0) didx = (F.base[l] + local - nbx) * F.nref + r;
+    if (tid == 2 && l > 0) {
+      const int Np = F.size[l - 1], px = x / Np, py = y / Np;
+      if (px < F.nbx[l - 1] && py < F.nby[l - 1]) didx = (F.base[l - 1] + py * F.nbx[l - 1] + px) * F.nref + r;
+    }
+    gs.bc[tid] = didx >= 0 ? ldcg_u32(&F.out[didx].mv) : 0u;
+    gs.bc[3 + tid] = didx >= 0 ? 1u : 0u;
+  }
+  {
+    const S* so = plane_at<S>(F.src, 0, x, y);
+    for (int i = tid; i < WR * N; i += kGroupThreads) {
+      const int row = i / WR, wd = i - row * WR;
+      gs.src[i] = ldw(so + (ptrdiff_t)row * F.src.stride + wd * SPW);
+    }
+  }
+  __syncthreads();
+  int p0x = 0, p0y = 0, p1x = 0, p1y = 0, na = 0;
+  if (gs.bc[3]) {
+    p0x = mvx_of(gs.bc[0]);
+    p0y = mvy_of(gs.bc[0]);
+    na = 1;
+  }
+  if (gs.bc[4]) {
+    const int qx = mvx_of(gs.bc[1]), qy = mvy_of(gs.bc[1]);
+    if (na == 0) {
+      p0x = qx;
+      p0y = qy;
+      na = 1;
+    } else if (qx != p0x || qy != p0y) {
+      p1x = qx;
+      p1y = qy;
+      na = 2;
+    }
+  }
+  const int ns = gs.bc[5] ? 4 : 3;
+  const int sdx[4] = {0, p0x, p1x, mvx_of(gs.bc[2])}, sdy[4] = {0, p0y, p1y, mvy_of(gs.bc[2])};
+  const DevPlanes& R = F.ref[r];
+  const S* org = plane_at<S>(R, 0, x, y);
+  const int stride = R.stride;
+  const int padm = F.pad - 4;  // h265_search.rs MARGIN
+  const int lox = -padm - x, hix = F.width + padm - N - x, loy = -padm - y, hiy = F.height + padm - N - y;
+  const float lam = F.lam;
+  const int range = F.search_range;
+  uint32_t nsad = 0, nsatd = 0;
+  int buf = 0;
+  // Seeds: >> 2 (floor), clamp_pos, dedupe through `tried`, in order
+  // (seed i is scored unless an earlier one landed on the same point).
+  int kx[4], ky[4];
+  bool kept[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    kx[i] = min(max(sdx[i] >> 2, lox), hix);
+    ky[i] = min(max(sdy[i] >> 2, loy), hiy);
+    bool dup = i >= ns;
+#pragma unroll
+    for (int j = 0; j < i; ++j) dup |= kx[j] == kx[i] && ky[j] == ky[i];
+    kept[i] = !dup;
+  }
+  auto spos = [&](int c, int& fx, int& fy) {
+    fx = c == 0 ? kx[0] : c == 1 ? kx[1] : c == 2 ? kx[2] : kx[3];
+    fy = c == 0 ? ky[0] : c == 1 ? ky[1] : c == 2 ? ky[2] : ky[3];
+    return c == 0 ? kept[0] : c == 1 ? kept[1] : c == 2 ? kept[2] : kept[3];
+  };
+  int bx = 0, by = 0;
+  uint32_t bcost = kInf;
+  cta_sad<S, N>(gs, buf, org, stride, 4, spos, tid);
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    int fx, fy;
+    if (!spos(c, fx, fy)) continue;
+    ++nsad;
+    const uint32_t cost = cta_cost(gs, buf, c, N / 32) + hevc_rate(lam, fx * 4, fy * 4, p0x, p0y, p1x, p1y);
+    if (cost < bcost) {
+      bcost = cost;
+      bx = fx;
+      by = fy;
+    }
+  }
+  buf ^= 1;
+  const int ox = bx, oy = by;  // the descent stays within +-range of the best seed
+  auto inside = [&](int fx, int fy) {
+    return abs(fx - ox) <= range && abs(fy - oy) <= range && fx >= lox && fx <= hix && fy >= loy && fy <= hiy;
+  };
+  int rings = 0;
+  for (;;) {
+    // The small diamond, two rounds a step: candidates 0..3 around the
+    // best, 4..15 the next round's three new points for each way the first
+    // can move (the fourth point being the best, which cannot win).
+    for (int it = 0; it < 2 * range;) {
+      const int cbx = bx, cby = by;
+      auto pos = [&](int q, int& fx, int& fy) {
+        const int j0 = q < 4 ? q : (q - 4) / 3, mm = (q - 4) % 3, m = mm + (mm >= (j0 ^ 1));
+        fx = cbx + (j0 == 0 ? 1 : j0 == 1 ? -1 : 0);
+        fy = cby + (j0 == 2 ? 1 : j0 == 3 ? -1 : 0);
+        if (q >= 4) {
+          fx += m == 0 ? 1 : m == 1 ? -1 : 0;
+          fy += m == 2 ? 1 : m == 3 ? -1 : 0;
+        }
+        return inside(fx, fy);
+      };
+      cta_sad<S, N>(gs, buf, org, stride, 16, pos, tid);
+      int j = -1;
+      uint32_t best1 = bcost;
+      for (int q = 0; q < 4; ++q) {
+        int fx, fy;
+        if (!pos(q, fx, fy)) continue;
+        ++nsad;
+        const uint32_t cost = cta_cost(gs, buf, q, N / 32) + hevc_rate(lam, fx * 4, fy * 4, p0x, p0y, p1x, p1y);
+        if (cost < best1) {
+          best1 = cost;
+          j = q;
+        }
+      }
+      if (j < 0) {  // the first round moved nothing: settled
+        buf ^= 1;
+        break;
+      }
+      bcost = best1;
+      pos(j, bx, by);
+      if (++it >= 2 * range) {
+        buf ^= 1;
+        break;
+      }
+      int j2 = -1, nbx2 = bx, nby2 = by;
+      ++nsad;  // the old best, scored again by the reference
+      for (int q = 4 + 3 * j; q < 7 + 3 * j; ++q) {
+        int fx, fy;
+        if (!pos(q, fx, fy)) continue;
+        ++nsad;
+        const uint32_t cost = cta_cost(gs, buf, q, N / 32) + hevc_rate(lam, fx * 4, fy * 4, p0x, p0y, p1x, p1y);
+        if (cost < bcost) {
+          bcost = cost;
+          j2 = q;
+          nbx2 = fx;
+          nby2 = fy;
+        }
+      }
+      buf ^= 1;
+      if (j2 < 0) break;
+      bx = nbx2;
+      by = nby2;
+      ++it;
+    }
+    if (rings >= F.search_rings) break;
+    ++rings;
+    // The 24 ring points at 4, 8, 16 around the settled point, together.
+    const int cxr = bx, cyr = by;
+    auto rpos = [&](int c, int& fx, int& fy) {
+      const int rr = c < 8 ? 4 : c < 16 ? 8 : 16, k8 = c & 7;
+      fx = cxr + ((k8 == 0 || k8 == 4 || k8 == 6) ? rr : (k8 == 1 || k8 == 5 || k8 == 7) ? -rr : 0);
+      fy = cyr + ((k8 == 2 || k8 == 4 || k8 == 5) ? rr : (k8 == 3 || k8 == 6 || k8 == 7) ? -rr : 0);
+      return inside(fx, fy);
+    };
+    cta_sad<S, N>(gs, buf, org, stride, 24, rpos, tid);
+    bool moved = false;
+    for (int c = 0; c < 24; ++c) {
+      int fx, fy;
+      if (!rpos(c, fx, fy)) continue;
+      ++nsad;
+      const uint32_t cost = cta_cost(gs, buf, c, N / 32) + hevc_rate(lam, fx * 4, fy * 4, p0x, p0y, p1x, p1y);
+      if (cost < bcost) {
+        bcost = cost;
+        bx = fx;
+        by = fy;
+        moved = true;
+      }
+    }
+    buf ^= 1;
+    if (!moved) break;
+  }
+  const uint32_t int_cost = bcost;
+  const int imx = bx * 4, imy = by * 4;
+  // refine_subpel: the start and the half ring (dy outer, dx inner) in one
+  // step, then the quarter ring around the winner.
+  constexpr int TC = (N / 4) * (N / 4) / 32;  // 32-tile chunks per candidate
+  auto hpos = [&](int c, int& mx, int& my) {
+    const int q = c == 0 ? 4 : (c <= 4 ? c - 1 : c);
+    mx = imx + (q % 3 - 1) * 2;
+    my = imy + (q / 3 - 1) * 2;
+    return true;
+  };
+  cta_satd<S, N>(gs, buf, R, x, y, 9, hpos, tid);
+  int bmx = imx, bmy = imy;
+  uint32_t bc = kInf, bsatd = 0;
+  for (int c = 0; c < 9; ++c) {
+    int mx, my;
+    hpos(c, mx, my);
+    const uint32_t sv = cta_cost(gs, buf, c, TC), cost = sv + hevc_rate(lam, mx, my, p0x, p0y, p1x, p1y);
+    if (cost < bc) {
+      bc = cost;
+      bsatd = sv;
+      bmx = mx;
+      bmy = my;
+    }
+  }
+  buf ^= 1;
+  const int hmx = bmx, hmy = bmy, cross = F.quarter_cross;
+  auto qpos = [&](int c, int& mx, int& my) {
+    const int q = c < 4 ? c : c + 1, dx = q % 3 - 1, dy = q / 3 - 1;
+    mx = (int)(int16_t)(hmx + dx);
+    my = (int)(int16_t)(hmy + dy);
+    return !(cross != 0 && dx != 0 && dy != 0);
+  };
+  cta_satd<S, N>(gs, buf, R, x, y, 8, qpos, tid);
+  for (int c = 0; c < 8; ++c) {
+    int mx, my;
+    if (!qpos(c, mx, my)) continue;
+    ++nsatd;
+    const uint32_t sv = cta_cost(gs, buf, c, TC), cost = sv + hevc_rate(lam, mx, my, p0x, p0y, p1x, p1y);
+    if (cost < bc) {
+      bc = cost;
+      bsatd = sv;
+      bmx = mx;
+      bmy = my;
+    }
+  }
+  nsatd += 9;
+  rme_result* out = &F.out[t];
+  if (tid == 0) {
+    write_result(out, bmx, bmy, r, bc, bsatd, imx, imy, int_cost, nsad, nsatd, 0);
+    __threadfence();
+    gs.cnt[0] += 1;
+    gs.cnt[1] += nsad;
+    gs.cnt[2] += nsatd;
+    gs.cnt[3] += (unsigned long long)nsad * N * N;
+    gs.cnt[4] += (unsigned long long)nsatd * N * N;
+  }
+  __syncthreads();
+  // The tasks reading this result (warp 0 releases them, one per lane):
+  // right and lower neighbours, the next size's blocks inside this one,
+  // this CU's AMP units. A group task made ready is kept, if this CTA has
+  // none yet; the rest are pushed to their queues.
+  int cont = -1;
+  if (tid < 32) {
+    int ncx = 0, ncy = 0, cx0 = 0, cy0 = 0;
+    if (l + 1 < F.nlevels) {
+      const int M = F.size[l + 1];
+      cx0 = lbx * N / M;
+      cy0 = lby * N / M;
+      ncx = max(0, min((lbx + 1) * N / M, F.nbx[l + 1]) - cx0);
+      ncy = max(0, min((lby + 1) * N / M, F.nby[l + 1]) - cy0);
+    }
+    const int namp = l < F.amp_nlev ? 2 * F.amp_nmodes : 0, nch = ncx * ncy, ndep = 2 + nch + namp;
+    for (int k0 = 0; k0 < ndep; k0 += 32) {
+      const int k = k0 + lane;
+      int dtask = -1;
+      if (k >= ndep) {
+      } else if (k == 0) {
+        if (lbx + 1 < F.nbx[l]) dtask = (F.base[l] + local + 1) * F.nref + r;
+      } else if (k == 1) {
+        if (lby + 1 < F.nby[l]) dtask = (F.base[l] + local + F.nbx[l]) * F.nref + r;
+      } else if (k < 2 + nch) {
+        const int c = k - 2, cy = cy0 + c / ncx, cx = cx0 + c % ncx;
+        dtask = (F.base[l + 1] + cy * F.nbx[l + 1] + cx) * F.nref + r;
+      } else {
+        dtask = (F.amp_base[l] + local * namp + (k - 2 - nch)) * F.nref + r;
+      }
+      cont = release_lanes(L, F, f, dtask >= 0, dtask, cont, lane, true);
+    }
+    if (tid == 0) gs.bc[6] = (uint32_t)cont;
+  }
+  __syncthreads();
+  return (int)gs.bc[6];
 }
 
 // ---- H.264 ------------------------------------------------------------------
