@@ -307,10 +307,10 @@ def run_ours(args, world, rank, local):
     # Each frame's results go to a buffer the caller keeps (as an encoder
     # keeps its motion field) in pinned memory, which the results' copy
     # fills directly; touched before the timing.
-    # The occupancy tuner times its three variants on the first three
-    # launches of this size: one frame three times, so that they are compared
-    # on the same content.
-    for _ in range(4):
+    # The tuner times its launch shapes (six for one HEVC frame) on the first
+    # launches of this size: one frame several times, so that they are
+    # compared on the same content.
+    for _ in range(8):
         ms.search(batch[0][0], batch[0][1], p, stream=sh)
     per_frame = ms.result_count(batch[0][0], batch[0][1], p)
     plain_bufs = []
@@ -451,13 +451,18 @@ def run_ours(args, world, rank, local):
         try:
             tr = json.loads(traffic_file.read_text())
             roof["traffic"] = tr.get("bytes_per_launch_1080p")
+            roof["traffic_source"] = ("scaled from profiles/search_kernel_traffic.json (ncu DRAM bytes of an "
+                                      "8-frame launch, times 60/8), not measured in this run")
         except ValueError:
             pass
 
-    # ---- serving loop under load --------------------------------------------------
+    # ---- plain per-frame path, one picture a call (upload inside) -------------------
+    plain_stream = plain_latency(ms, frames, p, sh)
+
+    # ---- serving loop under load (every rank serves its own streams) ---------------
     served = None
-    if rank == 0 and world == 1 and not args.no_serve:
-        served = run_served(frames, value, local=local)
+    if not args.no_serve:
+        served = run_served(frames, value / world, local=local)
 
     # ---- CPU baseline (bounded sample) ---------------------------------------------
     cpu = None
@@ -471,21 +476,50 @@ def run_ours(args, world, rank, local):
                "plane_build_share": ps_all / secs_all,
                "value_1_thread": fps_1, "cpu_model": cpu_model()}
 
+    # The headline: the served rate at the highest load kept up with (served
+    # >= 0.97 x offered and p99 <= 8 ms), over all ranks; where no load met
+    # the rule on every rank, the batched device-resident rate, and the line
+    # says which.
+    met = served is not None and served["met"]
+    if world > 1:
+        met = max_over_ranks(0.0 if met else 1.0, world) == 0.0
+    served_total = (served["value"] if served else 0.0) * 1.0
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        tt = torch.tensor([served_total], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt)
+        served_total = float(tt.item())
+    frame_in = WIDTH * HEIGHT
+    frame_out = 42900 * NREF * capi.RESULT_DTYPE.itemsize
     if rank == 0:
         lat_ms = np.array(lat) * 1e3
+        batched = {"value": value, "unit": "frames/s", "ms_per_step": elapsed / args.steps * 1e3,
+                   "frames_per_step": frames_per_step, "timing": "CUDA events over the steps, max over ranks",
+                   "e2e": {"value": e2e_value, "unit": "frames/s", "h2d_bytes_per_step": h2d,
+                           "d2h_bytes_per_step": d2h}}
+        e2e = ({"value": served_total, "unit": "frames/s", "h2d_bytes_per_step": frame_in,
+                "d2h_bytes_per_step": frame_out, "step": "one served frame request, through rme_serve_*"}
+               if met else batched["e2e"])
         print(json.dumps({
-            "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+            "metric": METRIC, "value": served_total if met else value, "unit": "frames/s", "n_gpus": world,
+            "steps": args.steps,
+            "value_is": ("served frames/s at the highest Poisson load with served >= 0.97 x offered and p99 <= 8 ms"
+                         if met else "batched device-resident frames/s: no served load met p99 <= 8 ms"),
             "warmup": warm, "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
             "config": {"workload": "hevc-1080p-8bit-2ref-pu8to64-range64-qp32", "frames_per_step": frames_per_step,
                        "width": WIDTH, "height": HEIGHT, "refs": NREF, "pus_per_ref": int(stats.tasks // frames_per_step // NREF),
                        "predictors": "standalone", "parallelism": f"replicas{world}",
                        "l2": "inputs larger than L2 (2.6 GB of planes)"},
-            "plain_per_frame": {"value": plain_fps, "unit": "frames/s", "p50_ms": float(np.percentile(lat_ms, 50)),
-                                "p99_ms": float(np.percentile(lat_ms, 99))},
-            "batched_latency_ms": elapsed / args.steps * 1e3,
+            "plain_per_frame": plain_stream,
+            "plain_per_frame_resident": {"value": plain_fps, "unit": "frames/s", "frames": len(lat),
+                                         "p50_ms": float(np.percentile(lat_ms, 50)),
+                                         "p99_ms": float(np.percentile(lat_ms, 99)),
+                                         "call": "search only, pictures already resident"},
+            "batched": batched,
             "pu_cost_evals_per_s": (st.sad_candidates + st.satd_candidates) / kms * world,
-            "e2e": {"value": e2e_value, "unit": "frames/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "e2e": e2e,
             "served": served,
             "roofline": roof,
             "cpu_baseline": cpu,

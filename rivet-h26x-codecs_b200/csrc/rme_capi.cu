@@ -193,6 +193,19 @@ struct Graph {
   int seen = 0;  // launches of this shape so far: captured on the second
 };
 
+// A launch shape the tuner chooses among: the search kernel's occupancy
+// variant (registers per thread against resident warps), in the latency form
+// the share of CTAs that search 32x32 and 64x64 HEVC blocks a CTA per block
+// (0, a quarter or half of the SMs), and whether 8x8 blocks refine from
+// staged phase patches (the search window's neighbourhood in shared memory)
+// or straight from the caches.
+struct Shape {
+  int variant, groups, patch;
+};
+constexpr Shape kThroughputShapes[] = {{1, 0, 0}, {0, 0, 0}, {2, 0, 0}};
+constexpr Shape kLatencyHevcShapes[] = {{1, 2, 1}, {0, 2, 1}, {1, 0, 1}, {1, 1, 1}, {1, 2, 0}, {2, 2, 1}};
+constexpr Shape kLatencyShapes[] = {{1, 0, 0}, {0, 0, 0}, {2, 0, 0}};
+
 // One search launch's buffers and events. A context keeps kSlots of them and
 // takes them in turn: a synchronous search finishes its launch before it
 // returns; an asynchronous one leaves it in flight on the caller's stream
@@ -217,6 +230,7 @@ struct Slot {
   cudaStream_t stream = nullptr;
   int64_t total = 0;
   void* tuning = nullptr;
+  int tune_shapes = 0;
   rme_result* host_out = nullptr;
   std::vector<int64_t> host_off, host_count, dev_off;
   ~Slot() {
@@ -229,11 +243,12 @@ struct Slot {
 struct Ctx {
   int device = 0, nsm = 0;
   int bps[kParts][kSearchVariants][2] = {};  // resident search blocks per SM, per part, variant, form
-  // The tuner: per (part, log2 of its task count), each occupancy variant
-  // is timed on one real launch of that class, then the fastest is kept.
+  // The tuner: per (part, form, log2 of its task count), each launch shape
+  // of that class (kShapes) is timed on one real launch, then the fastest is
+  // kept. Results do not depend on the shape.
   struct Tune {
     int best = -1, tried = 0;
-    float ms[kSearchVariants] = {};
+    float ms[8] = {};
   };
   std::map<std::pair<int, int>, Tune> tune;
   bool tune_on = true;
@@ -578,9 +593,9 @@ int finish_launch(Ctx* c, Slot& sl) {
   if (sl.tuning) {
     auto* T = (Ctx::Tune*)sl.tuning;
     sl.tuning = nullptr;
-    if (T->best < 0 && T->tried < kSearchVariants) {
+    if (T->best < 0 && T->tried < sl.tune_shapes) {
       T->ms[T->tried++] = ms;
-      if (T->tried == kSearchVariants) T->best = (int)(std::min_element(T->ms, T->ms + kSearchVariants) - T->ms);
+      if (T->tried == sl.tune_shapes) T->best = (int)(std::min_element(T->ms, T->ms + sl.tune_shapes) - T->ms);
     }
   }
   c->last.planes_ms = 0.0f;
@@ -683,6 +698,33 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   const bool spec = total <= kSpecTasks;
   int64_t part_tasks[kParts] = {0, 0, 0, 0};
   for (int i = 0; i < n; ++i) part_tasks[part_of(sl.h_frames.p[i])] += ntask[i];
+  // Each part's launch shape: the tuned one for its class, or the next one
+  // to time (a launch of one kind only, so that its time is the part's).
+  int nparts_used = 0;
+  for (int k = 0; k < kParts; ++k) nparts_used += part_tasks[k] > 0;
+  Shape shape[kParts];
+  int variant[kParts];
+  Ctx::Tune* tuning = nullptr;  // the class this launch times, if any
+  int tune_shapes = 0;
+  for (int k = 0; k < kParts; ++k) {
+    const Shape* shapes = !spec ? kThroughputShapes : part_codec(k) == RME_CODEC_HEVC ? kLatencyHevcShapes : kLatencyShapes;
+    const int nsh = !spec ? 3 : part_codec(k) == RME_CODEC_HEVC ? 6 : 3;
+    shape[k] = shapes[0];
+    if (part_tasks[k] > 0 && c->tune_on) {
+      const int bucket = 63 - __builtin_clzll((unsigned long long)part_tasks[k]);
+      Ctx::Tune& T = c->tune[{k * 2 + spec, bucket}];
+      if (T.best >= 0) {
+        shape[k] = shapes[T.best];
+      } else if (nparts_used == 1 && !async) {
+        shape[k] = shapes[T.tried];
+        tuning = &T;
+        tune_shapes = nsh;
+      }
+    }
+    variant[k] = shape[k].variant;
+    if (part_tasks[k] > 0 && !c->bps[k][variant[k]][spec])
+      c->bps[k][variant[k]][spec] = search_blocks_per_sm(part_bytes(k), part_codec(k), variant[k], spec);
+  }
   std::vector<std::pair<const int32_t*, int>> pend_copies;  // (template, frame)
   for (int i = 0; i < n; ++i) {
     FrameDesc& fd = sl.h_frames.p[i];
@@ -707,7 +749,7 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
       const Deps* dp = get_deps(c, src->d, &params[i], frames[i].nref, &rc);
       if (!dp) return rc;
       pend_copies.emplace_back(dp->pending, i);
-      const bool groups = spec && fd.codec == RME_CODEC_HEVC;
+      const bool groups = spec && fd.codec == RME_CODEC_HEVC && shape[part].groups > 0;
       for (uint32_t t : dp->ready)
         (groups && (int)(t / fd.nref) < fd.big_end ? init_big : init)[part].push_back(tag | t);
       sig.push_back(fd.bd);
@@ -762,25 +804,10 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
     L.group_ctas = 0;
     slot0 += part_tasks[k];
   }
-  int nparts_used = 0;
-  for (int k = 0; k < kParts; ++k) nparts_used += part_tasks[k] > 0;
-  int variant[kParts];
-  Ctx::Tune* tuning = nullptr;  // the class this launch times, if any
   for (int k = 0; k < kParts; ++k) {
-    variant[k] = kDefaultVariant;
-    if (part_tasks[k] == 0) continue;
-    if (c->tune_on) {
-      const int bucket = 63 - __builtin_clzll((unsigned long long)part_tasks[k]);
-      Ctx::Tune& T = c->tune[{k, bucket}];
-      if (T.best >= 0) {
-        variant[k] = T.best;
-      } else if (nparts_used == 1 && !async) {  // one kind in the launch: its time is the part's
-        variant[k] = T.tried;
-        tuning = &T;
-      }
-    }
-    if (!c->bps[k][variant[k]][spec]) c->bps[k][variant[k]][spec] = search_blocks_per_sm(part_bytes(k), part_codec(k), variant[k], spec);
     sig.push_back(variant[k]);
+    sig.push_back(shape[k].patch);
+    Ls[k].patch8 = shape[k].patch;
   }
   int nparts = 0, order[kParts];
   for (int k = 0; k < kParts; ++k)
@@ -804,7 +831,8 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
       for (int i = 0; i < n; ++i)
         if (part_of(sl.h_frames.p[i]) == k && params[i].predictor_mode == RME_PRED_STANDALONE)
           big += (int64_t)sl.h_frames.p[i].big_end * sl.h_frames.p[i].nref;
-    const int g = big > 0 ? (int)std::min<int64_t>({(int64_t)c->nsm / 2, big, (int64_t)cap - 1}) : 0;
+    const int share = shape[k].groups == 2 ? c->nsm / 2 : shape[k].groups == 1 ? c->nsm / 4 : 0;
+    const int g = big > 0 && share > 0 ? (int)std::min<int64_t>({(int64_t)share, big, (int64_t)cap - 1}) : 0;
     const int64_t small = part_tasks[k] - big;
     const int solo = (int)std::max<int64_t>(1, std::min<int64_t>(cap - g, (small + kWarpsPerBlock - 1) / kWarpsPerBlock));
     Ls[k].group_ctas = g;
@@ -899,6 +927,7 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   sl.stream = s;
   sl.total = total;
   sl.tuning = tuning;
+  sl.tune_shapes = tune_shapes;
   if (!dev_out && !pinned_out) {
     sl.host_out = out;
     sl.host_off.resize(n);

@@ -365,6 +365,7 @@ int engine_create(void* ctx, int device, Engine** out) {
   L.head_big = g->d_hdr + kHdrHeadBig;
   L.tail_big = g->d_hdr + kHdrTailBig;
   L.group_ctas = groups;
+  L.patch8 = 1;
   L.ring_shift = kRingShift;
   EngineCtl& E = g->E;
   E.fdone = g->d_fdone;

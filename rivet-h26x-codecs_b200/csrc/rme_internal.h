@@ -93,6 +93,7 @@ struct LaunchDesc {
   unsigned long long* head_big;
   unsigned long long* tail_big;
   int32_t group_ctas;
+  int32_t patch8;                // the latency form: 8x8 blocks refine from staged phase patches
   int32_t ring_shift;            // nonzero: the resident engine's ring of
                                  // 2^ring_shift slots (slot idx holds
                                  // ((idx >> ring_shift) + 1) << 32 | entry)

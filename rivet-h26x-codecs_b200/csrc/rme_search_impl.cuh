@@ -944,11 +944,44 @@ __device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
   const int ntiles = tw * th;
   // Patches need every plane and row a whole number of words apart (true
   // of the library's pictures: 128-byte strides).
-  if (spec && ((R.stride * (int)sizeof(S)) & 3) == 0 && ((R.plane_elems * (int64_t)sizeof(S)) & 3) == 0) {
+  if (spec && L.patch8 && ((R.stride * (int)sizeof(S)) & 3) == 0 &&
+      ((R.plane_elems * (int64_t)sizeof(S)) & 3) == 0) {
     refine8_patched<S>(sm, R, x, y, bx, by, lam, p0x, p0y, p1x, p1y, F.quarter_cross, lane, bmx, bmy, bc, bsatd,
                        nsatd);
   } else {
-  for (int pass = 0; pass < 3; ++pass) {
+  // The latency form scores a 16x16 block's start and half ring in one
+  // pass: 9 candidates x 16 tiles, two candidates of 16 lanes at a time.
+  const bool merge16 = SPEC && w == 16 && h == 16;
+  for (int pass = merge16 ? 1 : 0; pass < 3; ++pass) {
+    if (merge16 && pass == 1) {
+      uint32_t sv = 0;
+#pragma unroll
+      for (int it = 0; it < 5; ++it) {
+        const int c = 2 * it + (lane >> 4);
+        uint32_t v = 0;
+        if (c < 9) {
+          const int q = c == 0 ? 4 : (c <= 4 ? c - 1 : c);
+          const int mx = imx + (q % 3 - 1) * 2, my = imy + (q / 3 - 1) * 2;
+          const S* pp = plane_at<S>(R, (my & 3) * 4 + (mx & 3), x + (mx >> 2), y + (my >> 2));
+          v = satd_part<S>(sm.src, wr, tw, ntiles, pp, stride, lane & 15, 16);
+        }
+        v += __shfl_xor_sync(kFull, v, 1);
+        v += __shfl_xor_sync(kFull, v, 2);
+        v += __shfl_xor_sync(kFull, v, 4);
+        v += __shfl_xor_sync(kFull, v, 8);
+        const uint32_t got = __shfl_sync(kFull, v, (lane & 1) * 16);
+        if (lane < 9 && (lane >> 1) == it) sv = got;
+      }
+      const int q = lane == 0 ? 4 : (lane <= 4 ? lane - 1 : lane);
+      const int mx = imx + (q % 3 - 1) * 2, my = imy + (q / 3 - 1) * 2;
+      const uint32_t cost = lane < 9 ? sv + hevc_rate(lam, mx, my, p0x, p0y, p1x, p1y) : kInf;
+      const Pick p = warp_min(cost);
+      bc = p.cost;
+      bsatd = __shfl_sync(kFull, sv, p.lane);
+      bmx = __shfl_sync(kFull, mx, p.lane);
+      bmy = __shfl_sync(kFull, my, p.lane);
+      continue;
+    }
     const int G = pass == 1 ? 32 : 4, c = pass == 1 ? 8 : lane >> 2, gsub = pass == 1 ? lane : lane & 3;
     int mx, my;
     bool ok;
