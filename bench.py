@@ -466,6 +466,9 @@ def run_ours(args, world, rank, local):
 
     # ---- CPU baseline (bounded sample) ---------------------------------------------
     cpu = None
+    others = None
+    if rank == 0 and world == 1 and not args.no_serve:
+        others = other_configs(local)
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
         fps_all, n_all, secs_all, ps_all = cpu_baseline(frames, threads)
@@ -521,6 +524,7 @@ def run_ours(args, world, rank, local):
             "pu_cost_evals_per_s": (st.sad_candidates + st.satd_candidates) / kms * world,
             "e2e": e2e,
             "served": served,
+            "other_configs": others,
             "roofline": roof,
             "cpu_baseline": cpu,
             "clocks": clocks,
@@ -955,6 +959,174 @@ def run_configs(local: int = 0):
             stream += 1
     measure("64-stream mix: 16x360p H.264 8-bit, 24x720p HEVC 8-bit, 16x1080p HEVC 10-bit, 8x2160p HEVC 8-bit",
             frames, params, "one frame of every stream per launch, 2 references each; four kinds on forked streams")
+
+
+def other_configs(local: int = 0) -> dict:
+    """The path's other workloads, reported inside the headline line (a few
+    seconds each): the H.264 CIF frame (frames/s of the plain path and parity
+    with the oracle), the 2160p 10-bit four-reference stream (batched against
+    plain, bit-exact between them) and the mixed serving population (how many
+    30 frames/s streams drawn from it are served at p99 <= 8 ms)."""
+    import torch
+    import rivet_h26x_codecs_b200 as rme
+    import rivet_h26x_codecs_b200.capi as capi
+    from rivet_h26x_codecs_b200 import synth
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    out = {}
+    with rme.MotionSearch(local) as ms:
+        # H.264 CIF, one reference, QP 28, the medium MeCfg.
+        seq = synth.config0()
+        ms.upload(1, seq.frames[0], capi.RME_CODEC_H264, 8, as_ref=True)
+        ms.upload(2, seq.frames[1], capi.RME_CODEC_H264, 8, as_ref=True)
+        p4 = capi.default_params(capi.RME_CODEC_H264, 28)
+        for _ in range(5):
+            got = ms.search(2, [1], p4)
+        lat = []
+        for _ in range(200):
+            a = time.perf_counter()
+            ms.search(2, [1], p4)
+            lat.append(time.perf_counter() - a)
+        want = oracle.frame_search(capi.RME_CODEC_H264, 8, seq.frames[1], [seq.frames[0]], oracle.params(capi.RME_CODEC_H264, 28))
+        lat_ms = np.array(lat) * 1e3
+        out["h264_cif"] = {"value": len(lat) / float(np.sum(lat)), "unit": "frames/s", "p50_ms": float(np.median(lat_ms)),
+                           "p99_ms": float(np.percentile(lat_ms, 99)), "macroblocks": int(len(got)),
+                           "bit_exact_vs_oracle": bool((got == want).all()),
+                           "call": "plain per-frame search, pictures resident, results to host"}
+        # 2160p HEVC 10-bit, 4 references, +-128, PUs 8..64 + AMP 2NxnU / nLx2N.
+        seq = synth.config2(nframes=12)
+        p2 = capi.default_params(capi.RME_CODEC_HEVC, QP)
+        p2.hevc_search_range = 128
+        p2.hevc_amp = 0b0101
+        for i, f in enumerate(seq.frames):
+            ms.upload(100 + i, f, capi.RME_CODEC_HEVC, 10, as_ref=True)
+        frames = [(100 + t, [100 + t - 1 - r for r in range(4)]) for t in range(4, 12)]
+        total = ms.batch_result_count(frames, p2)
+        dev = torch.empty(total * capi.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=f"cuda:{local}")
+        for _ in range(5):
+            outs = ms.search_batch(frames, p2, 0, out=dev)
+        ks = []
+        for _ in range(3):
+            ms.search_batch(frames, p2, 0, out=dev)
+            ks.append(ms.stats().kernel_ms)
+        batched = [v.cpu().numpy().view(capi.RESULT_DTYPE) for v in outs]
+        for _ in range(8):
+            ms.search(*frames[0], p2)
+        plain, lat = [], []
+        for src, refs in frames:
+            a = time.perf_counter()
+            plain.append(ms.search(src, refs, p2))
+            lat.append(time.perf_counter() - a)
+        kms = float(np.median(ks))
+        out["hevc_2160p10"] = {"batched_fps": len(frames) / kms * 1e3, "plain_fps": len(frames) / float(np.sum(lat)),
+                               "plain_p50_ms": float(np.median(lat)) * 1e3, "plain_max_ms": float(np.max(lat)) * 1e3,
+                               "bit_exact_batched_vs_plain": bool(all((b == q).all() for b, q in zip(batched, plain))),
+                               "note": "8 frames a launch, each against its 4 predecessors; range 128; AMP 2NxnU/nLx2N"}
+        del dev, seq
+        for i in range(12):
+            ms.release(100 + i)
+    torch.cuda.empty_cache()
+    out["served_mix"] = served_mix_streams(local)
+    return out
+
+
+def served_mix_streams(local: int = 0, counts=(8, 24, 48), seconds: float = 2.0) -> dict:
+    """Streams drawn from the mixed population (sizes 360p..2160p, 8/10-bit,
+    H.264/HEVC, 2 references each), each at 30 frames/s (Poisson), served by
+    the resident engine: per stream count, p50/p99 over all frames and by
+    size; the largest count with served >= 0.97 x offered and p99 <= 8 ms."""
+    import torch
+    import rivet_h26x_codecs_b200 as rme
+    import rivet_h26x_codecs_b200.capi as capi
+    from rivet_h26x_codecs_b200 import synth
+    sizes = [(640, 360, 32), (1280, 720, 64), (1920, 1080, 64), (3840, 2160, 128)]
+    kinds = [(c, w, h, bd, r) for (w, h, r) in sizes for bd in (8, 10) for c in (capi.RME_CODEC_H264, capi.RME_CODEC_HEVC)]
+    rng = np.random.default_rng(4)
+    skind = rng.integers(len(kinds), size=200)
+    pools = {}
+
+    def params_of(k):
+        c, w, h, bd, r = kinds[k]
+        q = capi.default_params(c, 28 if c == capi.RME_CODEC_H264 else QP)
+        if c == capi.RME_CODEC_H264:
+            q.h264_range = min(r, 32)
+        else:
+            q.hevc_search_range = r
+        return q
+
+    sweep = []
+    for n in counts:
+        for k in sorted(set(skind[:n].tolist())):
+            if k not in pools:
+                c, w, h, bd, _ = kinds[k]
+                pools[k] = synth.stream_sequence(c, w, h, bd, 6, k, config=4).frames
+        with rme.MotionSearch(local) as ms:
+            srv = rme.Server(ms, hbm_budget_bytes=120 << 30, max_frames_per_launch=64, max_streams=1024)
+            try:
+                bufs, nxt = {}, {}
+                for sid in range(n):
+                    c, w, h, bd, _ = kinds[skind[sid]]
+                    assert srv.open_stream(sid, c, bd, w, h, params_of(skind[sid]), NREF) == 0
+                for sid in range(n):
+                    pool = pools[skind[sid]]
+                    codec, nb = srv._streams[sid][0], srv._streams[sid][1]
+                    cnt = nb if codec == capi.RME_CODEC_H264 else nb * NREF
+                    bufs[sid] = []
+                    for _ in range(4):
+                        tt = torch.empty(cnt * capi.RESULT_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True)
+                        bufs[sid].append(tt.numpy().view(capi.RESULT_DTYPE))
+                    srv.submit(sid, pool[0])
+                    for t in range(1, NREF + 4):
+                        srv.submit(sid, pool[t % len(pool)], out=bufs[sid][t % 4])
+                    nxt[sid] = NREF + 4
+                pending = n * (NREF + 4)
+                deadline = time.perf_counter() + 120
+                while pending and time.perf_counter() < deadline:
+                    pending -= len(srv.poll())
+                    time.sleep(0.0005)
+                events = []
+                for sid in range(n):
+                    t = rng.exponential(1 / 30.0)
+                    while t < 0.5 + seconds:
+                        events.append((t, sid))
+                        t += rng.exponential(1 / 30.0)
+                events.sort()
+                measured, done, size_of = set(), [], {}
+                t0 = time.perf_counter()
+                for at, sid in events:
+                    while time.perf_counter() - t0 < at:
+                        done += srv.poll()
+                        time.sleep(0.0001)
+                    pool = pools[skind[sid]]
+                    rid = srv.submit(sid, pool[nxt[sid] % len(pool)], out=bufs[sid][nxt[sid] % 4])
+                    nxt[sid] += 1
+                    if at >= 0.5:
+                        measured.add(rid)
+                        size_of[rid] = kinds[skind[sid]][2]
+                deadline = time.perf_counter() + 60
+                while len(done) < len(events) and time.perf_counter() < deadline:
+                    done += srv.poll()
+                    time.sleep(0.0002)
+            finally:
+                srv.stop()
+        ok = [d for d in done if d["status"] == 0 and d["id"] in measured]
+        lat = np.array([d["done_s"] - d["submit_s"] for d in ok]) * 1e3
+        span = max(d["done_s"] for d in ok) - min(d["submit_s"] for d in ok) if ok else 1.0
+        by_size = {}
+        for hgt in sorted(set(size_of.values())):
+            ls = np.array([d["done_s"] - d["submit_s"] for d in ok if size_of[d["id"]] == hgt]) * 1e3
+            if len(ls):
+                by_size[f"{hgt}p"] = {"frames": int(len(ls)), "p50_ms": float(np.median(ls)),
+                                      "p99_ms": float(np.percentile(ls, 99))}
+        sweep.append({"streams": n, "offered_fps": len(measured) / seconds, "served_fps": len(ok) / span,
+                      "p50_ms": float(np.median(lat)) if len(lat) else None,
+                      "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None, "by_size": by_size})
+        log(f"served mix {n} streams: {sweep[-1]}")
+    good = [x for x in sweep if x["p99_ms"] is not None and x["p99_ms"] <= P99_TARGET_MS
+            and x["served_fps"] >= 0.97 * x["offered_fps"]]
+    return {"streams_at_30fps_p99_8ms": max((x["streams"] for x in good), default=0), "sweep": sweep,
+            "population": "200 streams drawn uniformly over {360p, 720p, 1080p, 2160p} x {8, 10 bit} x {H.264, HEVC}; "
+                          "the first n of them, 30 frames/s each"}
 
 
 def profile_case(kind: str):

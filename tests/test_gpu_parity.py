@@ -343,3 +343,22 @@ def test_the_gpu_reproduces_the_golden_fixtures(ms, name):
         ms.upload(901 + i, r, codec, bd, as_ref=True)
     got = ms.search(900, [901 + i for i in range(len(refs))], p)
     assert_results_equal(got, z["results"].view(capi.RESULT_DTYPE), name)
+
+
+@pytest.mark.parametrize("bd", [8, 10])
+def test_every_launch_shape_gives_the_oracles_results(bd):
+    """A fresh context times each launch shape of a class on its first
+    launches (occupancy variant, CTAs for the 32x32 and 64x64 blocks or
+    none, staged 8x8 patches or cache reads): the same frame searched once
+    per shape, and once more on the chosen one, equals the oracle every
+    time."""
+    import rivet_h26x_codecs_b200 as rme
+    seq = synth.make_sequence(HEVC, 320, 192, bd, 3, 77 + bd, 64, 96, 2.0)
+    p = oracle.params(HEVC, 30, hevc_search_range=40, hevc_search_rings=1, hevc_amp=0b1001)
+    want = oracle.frame_search(HEVC, bd, seq.frames[2], [seq.frames[1], seq.frames[0]], p)
+    with rme.MotionSearch(0) as ms2:
+        for i, f in enumerate(seq.frames):
+            ms2.upload(i, f, HEVC, bd, as_ref=True)
+        for k in range(7):
+            got = ms2.search(2, [1, 0], p)
+            assert_results_equal(got, want, f"launch {k}")
