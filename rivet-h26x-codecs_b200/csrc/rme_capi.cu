@@ -203,7 +203,7 @@ struct Shape {
   int variant, groups, patch;
 };
 constexpr Shape kThroughputShapes[] = {{1, 0, 0}, {0, 0, 0}, {2, 0, 0}};
-constexpr Shape kLatencyHevcShapes[] = {{1, 2, 1}, {0, 2, 1}, {1, 0, 1}, {1, 1, 1}, {1, 2, 0}, {2, 2, 1}};
+constexpr Shape kLatencyHevcShapes[] = {{1, 2, 1}, {1, 2, 0}, {1, 1, 1}, {1, 0, 0}, {1, 0, 1}, {0, 2, 1}};
 constexpr Shape kLatencyShapes[] = {{1, 0, 0}, {0, 0, 0}, {2, 0, 0}};
 
 // One search launch's buffers and events. A context keeps kSlots of them and

@@ -63,43 +63,37 @@ __device__ __forceinline__ void settle(const EngineCtl& E, Settle& st) {
   st.f = -1;
 }
 
-// Lane 0: the entry of the next pushed slot, kPopDone once the warp may
-// leave (the host asked, or nothing came for E.idle_polls polls), or
-// 0xffffffff when a claimed slot's write never came (status set). `big`:
-// the ring of the tasks a CTA runs.
+// Lane 0: the entry of the next slot of a ring (`big`: the CTAs' ring). The
+// warp takes a ticket (the head's next index) and waits for that slot to be
+// pushed, backing off to a microsecond between polls: a ticket per pop, so
+// thousands of idle warps never contend on the head. Returns kPopDone when
+// the host asks the kernel to leave (it does so only with nothing in flight,
+// and resets the heads before launching it again), or 0xffffffff when the
+// wait runs out (kSpinLimit polls: the status word's timeout bit).
 __device__ __forceinline__ uint32_t engine_pop(const LaunchDesc& L, const EngineCtl& E, Settle& st, bool big) {
-  unsigned long long* const head = big ? L.head_big : L.head;
-  unsigned long long* const tail = big ? L.tail_big : L.tail;
-  uint32_t idle = 0, ns = 64;
-  unsigned long long idx = 0;
-  for (;;) {
-    const unsigned long long t = ld_relaxed64(tail), h = ld_relaxed64(head);
-    if (h < t) {
-      if (atomicCAS(head, h, h + 1) == h) {
-        idx = h;
-        break;
-      }
-      continue;
-    }
-    settle(E, st);
-    if ((idle & 7u) == 0u && ld_relaxed_sys(E.hstop) != 0u) return kPopDone;
-    if (++idle >= E.idle_polls) return kPopDone;
-    __nanosleep(ns);
-    if (ns < 1024) ns <<= 1;
-  }
-  // Pushed (the tail moved past it), perhaps not yet written.
+  const unsigned long long idx = atomicAdd(big ? L.head_big : L.head, 1ull);
   const unsigned long long lap = (idx >> L.ring_shift) + 1ull;
   const unsigned long long* slot = (big ? L.ready_big : L.ready) + (idx & ((1ull << L.ring_shift) - 1ull));
-  for (uint32_t it = 0, ns2 = 32;; ++it) {
+  uint32_t ns = 32;
+  for (uint32_t it = 0;; ++it) {
     const unsigned long long v = ld_acquire64(slot);
     if ((v >> 32) == lap) return (uint32_t)v;
+    settle(E, st);
+    if ((it & 7u) == 7u && ld_relaxed_sys(E.hstop) != 0u) return kPopDone;
     if (it >= kSpinLimit) {
       atomicOr(L.status, kStatusWaitTimeout);
       return 0xffffffffu;
     }
-    __nanosleep(ns2);
-    if (ns2 < 256) ns2 <<= 1;
+    __nanosleep(ns);
+    if (ns < 1024) ns <<= 1;
   }
+}
+
+// After the kernel has left: the next pop of each ring is the next push
+// (tickets taken by warps that left unserved are dropped).
+__global__ void reset_heads_kernel(LaunchDesc L) {
+  *L.head = *L.tail;
+  *L.head_big = *L.tail_big;
 }
 
 constexpr int kEngineMinBlocks = 3;
@@ -226,6 +220,16 @@ __global__ void publish_kernel(LaunchDesc L, int f, const uint32_t* roots, int n
   for (int i = threadIdx.x; i < n; i += blockDim.x) push_ready(L, f, (int)roots[i], group_task_of(L, F, (int)roots[i]));
 }
 
+// A frame's dependency counts from its shape's template into its slot, and
+// its finished-task count cleared: a kernel (beside the resident one)
+// rather than a device copy and a memset, which the driver may run as
+// kernels of its own that would wait for the resident kernel to leave.
+__global__ void prepare_kernel(int32_t* pending, const int32_t* tmpl, int n, uint32_t* fdone) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int k = i; k < n; k += gridDim.x * blockDim.x) pending[k] = tmpl[k];
+  if (i == 0) *fdone = 0u;
+}
+
 size_t engine_smem() { return sizeof(WarpSmem<uint16_t>) * kWarpsPerBlock; }
 
 }  // namespace
@@ -241,11 +245,19 @@ int engine_blocks_per_sm() {
 cudaError_t launch_engine(const LaunchDesc& L, const EngineCtl& E, int grid, cudaStream_t s) {
   cudaError_t e = cudaFuncSetAttribute(engine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)engine_smem());
   if (e != cudaSuccess) return e;
+  prefer_max_shared(engine_kernel);
   engine_kernel<<<grid, kWarpsPerBlock * 32, engine_smem(), s>>>(L, E);
   return cudaGetLastError();
 }
 
+static cudaError_t launch_prepare(int32_t* pending, const int32_t* tmpl, int n, uint32_t* fdone, cudaStream_t s) {
+  prefer_max_shared(prepare_kernel);
+  prepare_kernel<<<std::min(64, (n + 255) / 256 + 1), 256, 0, s>>>(pending, tmpl, n, fdone);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_publish(const LaunchDesc& L, int frame, const uint32_t* roots, int nroots, cudaStream_t s) {
+  prefer_max_shared(publish_kernel);
   publish_kernel<<<1, 256, 0, s>>>(L, frame, roots, nroots);
   return cudaGetLastError();
 }
@@ -283,6 +295,7 @@ struct Engine {
   cudaStream_t kstream = nullptr;
   cudaEvent_t ended = nullptr;
   bool launched = false;
+  int64_t launches = 0;  // kernel launches (it leaves when idle)
   EngineSlot slots[kEngineFrames];
   std::vector<int> free_slots;
   int64_t inflight_tasks = 0;
@@ -295,7 +308,7 @@ void engine_destroy(Engine* g) {
   if (!g) return;
   cudaSetDevice(g->device);
   if (g->h_stop) {
-    *(volatile uint32_t*)g->h_stop = 1u;
+    *(volatile uint32_t*)g->h_stop = 1u;  // the warps leave (waiting ones within microseconds)
     if (g->launched) cudaEventSynchronize(g->ended);
   }
   cudaDeviceSynchronize();
@@ -371,7 +384,7 @@ int engine_create(void* ctx, int device, Engine** out) {
   E.fdone = g->d_fdone;
   E.hflags = g->dh_flags;
   E.hstop = g->dh_stop;
-  E.idle_polls = 1u << 18;  // about a quarter of a second at the longest back-off
+  E.idle_polls = 0u;  // unused: the host stops the kernel when it has been idle
   *out = g;
   return 0;
 }
@@ -389,6 +402,7 @@ static int engine_run(Engine* g) {
   if (launch_engine(g->L, g->E, g->grid, g->kstream) != cudaSuccess) return RME_ECUDA;
   if (cudaEventRecord(g->ended, g->kstream) != cudaSuccess) return RME_ECUDA;
   g->launched = true;
+  ++g->launches;
   return 0;
 }
 
@@ -421,8 +435,7 @@ int engine_submit(Engine* g, const rme_frame* f, const rme_params* p, cudaStream
   fd.pending = s.d_pending;
   fd.gen = s.gen;
   g->h_frames[k] = fd;
-  if (cudaMemcpyAsync(s.d_pending, tmpl, sizeof(int32_t) * ntasks, cudaMemcpyDeviceToDevice, upload) != cudaSuccess ||
-      cudaMemsetAsync(g->d_fdone + k, 0, sizeof(uint32_t), upload) != cudaSuccess ||
+  if (launch_prepare(s.d_pending, tmpl, ntasks, g->d_fdone + k, upload) != cudaSuccess ||
       cudaMemcpyAsync(g->d_frames + k, g->h_frames + k, sizeof(FrameDesc), cudaMemcpyHostToDevice, upload) !=
           cudaSuccess ||
       launch_publish(g->L, k, roots, nroots, upload) != cudaSuccess)
@@ -433,6 +446,23 @@ int engine_submit(Engine* g, const rme_frame* f, const rme_params* p, cudaStream
   g->inflight_tasks += ntasks;
   *slot_out = k;
   return engine_run(g);
+}
+
+// Stop the kernel (nothing in flight): ask its warps to leave, wait, reset
+// the heads. The next submit launches it again.
+int engine_stop(Engine* g) {
+  if (!g->launched || engine_idle(g)) return 0;
+  if (g->inflight_tasks > 0) return RME_EBUSY;
+  *(volatile uint32_t*)g->h_stop = 1u;
+  cudaError_t e = cudaEventSynchronize(g->ended);
+  if (e == cudaSuccess) {
+    prefer_max_shared(reset_heads_kernel);
+    reset_heads_kernel<<<1, 1, 0, g->kstream>>>(g->L);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->kstream);
+  *(volatile uint32_t*)g->h_stop = 0u;
+  return e == cudaSuccess ? 0 : RME_ECUDA;
 }
 
 bool engine_done(Engine* g, int slot) {

@@ -109,7 +109,7 @@ struct EngineCtl {
   uint32_t* fdone;                 // per frame slot: its tasks finished
   volatile uint32_t* hflags;       // mapped host memory: per slot, the generation finished
   volatile const uint32_t* hstop;  // mapped host memory: nonzero once idle warps may leave
-  uint32_t idle_polls;             // idle polls (backing off to ~1 us) before a warp leaves
+  uint32_t idle_polls;             // reserved
 };
 cudaError_t launch_engine(const LaunchDesc& L, const EngineCtl& E, int grid, cudaStream_t s);
 int engine_blocks_per_sm();
@@ -125,6 +125,7 @@ int engine_submit(Engine* g, const rme_frame* f, const rme_params* p, cudaStream
 bool engine_done(Engine* g, int slot);
 int engine_keep_running(Engine* g);
 bool engine_idle(Engine* g);
+int engine_stop(Engine* g);
 const rme_result* engine_results(Engine* g, int slot);
 int engine_slot_tasks(Engine* g, int slot);
 const uint32_t* engine_status_word(Engine* g);
@@ -143,6 +144,17 @@ void h264_cost_table(float lam, uint16_t* tab);  // kMvTab entries, MvCostTable:
 // Why a parameter block cannot be searched for a picture of `d`'s format,
 // or null when it can.
 const char* param_error(const rme_params* p, const rme_picture_desc& d);
+
+// The kernels that run beside a resident search (the uploads' plane builds,
+// the engine's publish) and the search kernels ask for one shared-memory
+// carveout, the most shared memory: an SM's carveout is fixed while blocks
+// run on it, so a kernel preferring another one waits for the SM to empty,
+// which a resident search never does.
+template <class K>
+inline cudaError_t prefer_max_shared(K* kernel) {
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                              (int)cudaSharedmemCarveoutMaxShared);
+}
 
 // Launch wrappers (defined in the .cu files).
 cudaError_t launch_pad_plane(const void* src, int bd, int w, int h, int sstride, DevPlanes dst, int cw, int ch,

@@ -134,6 +134,8 @@ cudaError_t launch_pad_plane(const void* src, int bd, int w, int h, int sstride,
                              int pad, cudaStream_t s) {
   int prow = ch + 2 * pad, pcol = cw + 2 * pad;
   dim3 blk(32, 8), grd((pcol + 31) / 32, (prow + 7) / 8);
+  prefer_max_shared(pad_plane_kernel<uint8_t>);
+  prefer_max_shared(pad_plane_kernel<uint16_t>);
   if (bd == 8)
     pad_plane_kernel<uint8_t><<<grd, blk, 0, s>>>((const uint8_t*)src, w, h, sstride, (uint8_t*)dst.base, dst.stride,
                                                   prow, pcol, pad);
@@ -146,6 +148,8 @@ cudaError_t launch_pad_plane(const void* src, int bd, int w, int h, int sstride,
 cudaError_t launch_h264_hpel(DevPlanes p, int bd, int cw, int ch, int pad, cudaStream_t s) {
   int prow = ch + 2 * pad, pcol = cw + 2 * pad;
   dim3 blk(32, 8), grd((pcol + 31) / 32, (prow + 7) / 8);
+  prefer_max_shared(h264_hpel_kernel<uint8_t>);
+  prefer_max_shared(h264_hpel_kernel<uint16_t>);
   if (bd == 8) {
     auto b = (uint8_t*)p.base;
     h264_hpel_kernel<uint8_t><<<grd, blk, 0, s>>>(b, b + p.plane_elems, b + 2 * p.plane_elems, b + 3 * p.plane_elems,
@@ -161,6 +165,8 @@ cudaError_t launch_h264_hpel(DevPlanes p, int bd, int cw, int ch, int pad, cudaS
 cudaError_t launch_hevc_phases(DevPlanes p, int bd, int w, int h, int pad, cudaStream_t s) {
   int prow = h + 2 * pad, pcol = w + 2 * pad;
   dim3 blk(32, 8), grd((pcol + 31) / 32, (prow + 7) / 8);
+  prefer_max_shared(hevc_phase_kernel<uint8_t>);
+  prefer_max_shared(hevc_phase_kernel<uint16_t>);
   if (bd == 8)
     hevc_phase_kernel<uint8_t><<<grd, blk, 0, s>>>((const uint8_t*)p.base, (uint8_t*)p.base, p.plane_elems, p.stride,
                                                    prow, pcol, bd);

@@ -170,6 +170,7 @@ cudaError_t launch(const LaunchDesc& L, int grid, cudaStream_t s) {
   cudaError_t e = cudaFuncSetAttribute(search_kernel<S, CODEC, MINB, SPEC>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<S>());
   if (e != cudaSuccess) return e;
+  prefer_max_shared(search_kernel<S, CODEC, MINB, SPEC>);
   search_kernel<S, CODEC, MINB, SPEC><<<grid, kWarpsPerBlock * 32, smem_bytes<S>(), s>>>(L);
   return cudaGetLastError();
 }

@@ -506,19 +506,19 @@ __device__ __forceinline__ uint32_t satd_part(const uint32_t* src, int wr, int t
 // ((qy & 3) * 4 + (qx & 3)) at whole-sample offset (floor(qx / 4),
 // floor(qy / 4)), so every candidate's 8x8 prediction sits inside the 9x9
 // block at B - (1, 1) of one of the 16 planes. Those 16 patches are staged
-// in shared memory with one round of loads, all 49 positions are scored
-// from there, and the reference's in-order walk (start, half ring, quarter
-// ring; strict <) runs on the 49 costs: three dependent passes over the
-// caches become one.
+// in shared memory with one round of loads, and the reference's walk
+// (start and half ring, then the quarter ring around the winner; strict <)
+// scores its candidates from there: three dependent passes over the caches
+// become one round of loads.
 constexpr int kPatch = 9;        // patch rows and samples per row
 constexpr int kPatchOff = 64;    // words of WarpSmem::src before the patches
 template <class S>
 struct PatchGeo {
   static constexpr int WR = sizeof(S) == 1 ? 3 : 5;  // words per staged row (any sample offset)
   static constexpr int PW = kPatch * WR;             // words per plane
-  static constexpr int SATD = kPatchOff + 16 * PW;   // 49 SATDs after the patches
+  static constexpr int N = 16 * PW, PER = (N + 31) / 32;  // words staged, per lane
 };
-static_assert(PatchGeo<uint16_t>::SATD + 49 <= kMaxBlk * kMaxBlk / 2, "patches outgrew the source buffer");
+static_assert(kPatchOff + 16 * PatchGeo<uint16_t>::PW + 1 <= kMaxBlk * kMaxBlk / 2, "patches outgrew the source buffer");
 
 // Stage the 16 planes' 9x9 patches at plane position (px, py) of R: word
 // loads from the aligned word holding each row's first sample (all loads of
@@ -526,27 +526,37 @@ static_assert(PatchGeo<uint16_t>::SATD + 49 <= kMaxBlk * kMaxBlk / 2, "patches o
 // sample within its word (the same in every plane and row: planes and rows
 // are whole words apart, which the caller checks).
 template <class S>
-__device__ __forceinline__ uint32_t stage_patches(uint32_t* dst, const DevPlanes& R, int px, int py, int lane) {
+__device__ __forceinline__ uint32_t load_patches(uint32_t (&v)[PatchGeo<S>::PER], const DevPlanes& R, int px, int py,
+                                                 int lane) {
   using G = PatchGeo<S>;
   const S* p0 = (const S*)R.base + R.origin + (int64_t)py * R.stride + px;
   const uintptr_t a0 = reinterpret_cast<uintptr_t>(p0);
   const uint32_t* w0 = reinterpret_cast<const uint32_t*>(a0 & ~uintptr_t(3));
   const int64_t pstep = R.plane_elems * (int64_t)sizeof(S) / 4, rstep = (int64_t)R.stride * sizeof(S) / 4;
-  constexpr int N = 16 * G::PW, PER = (N + 31) / 32;
-  uint32_t v[PER];
 #pragma unroll
-  for (int k = 0; k < PER; ++k) {
+  for (int k = 0; k < G::PER; ++k) {
     const int i = lane + 32 * k;
     v[k] = 0u;
-    if (i < N) {
+    if (i < G::N) {
       const int pl = i / G::PW, rem = i - pl * G::PW, row = rem / G::WR, wd = rem - row * G::WR;
       v[k] = RME_LD32(w0 + pl * pstep + row * rstep + wd);
     }
   }
-#pragma unroll
-  for (int k = 0; k < PER; ++k)
-    if (lane + 32 * k < N) dst[lane + 32 * k] = v[k];
   return (uint32_t)(a0 & 3);
+}
+template <class S>
+__device__ __forceinline__ void store_patches(uint32_t* dst, const uint32_t (&v)[PatchGeo<S>::PER], int lane) {
+  using G = PatchGeo<S>;
+#pragma unroll
+  for (int k = 0; k < G::PER; ++k)
+    if (lane + 32 * k < G::N) dst[lane + 32 * k] = v[k];
+}
+template <class S>
+__device__ __forceinline__ uint32_t stage_patches(uint32_t* dst, const DevPlanes& R, int px, int py, int lane) {
+  uint32_t v[PatchGeo<S>::PER];
+  const uint32_t off = load_patches<S>(v, R, px, py, lane);
+  store_patches<S>(dst, v, lane);
+  return off;
 }
 
 // One 4x4 tile's SATD against the patch: tile (tx, ty) of the candidate
@@ -578,44 +588,48 @@ __device__ __forceinline__ uint32_t patch_tile_satd(const uint32_t* src, const u
 }
 
 // refine_subpel of an 8x8 block around whole-sample (bx, by) from staged
-// patches: the vector, its cost and SATD. Lanes score the 49 positions
-// (196 tiles, four lanes per position), then the in-order walk runs on the
-// costs.
+// patches: the vector, its cost and SATD. The half step and then the
+// quarter ring around its winner, both read from shared memory: one round
+// of loads for the whole refinement.
 template <class S>
 __device__ __forceinline__ void refine8_patched(WarpSmem<S>& sm, const DevPlanes& R, int x, int y, int bx, int by,
                                                 float lam, int p0x, int p0y, int p1x, int p1y, int quarter_cross,
                                                 int lane, int& bmx, int& bmy, uint32_t& bc, uint32_t& bsatd,
-                                                uint32_t& nsatd) {
+                                                uint32_t& nsatd, bool staged, uint32_t staged_off) {
   using G = PatchGeo<S>;
   uint32_t* patch = sm.src + kPatchOff;
-  uint32_t* satd = sm.src + G::SATD;
-  const uint32_t off = stage_patches<S>(patch, R, x + bx - 1, y + by - 1, lane);
+  // `staged`: the diamond's last step loaded these patches already.
+  const uint32_t off = staged ? staged_off : stage_patches<S>(patch, R, x + bx - 1, y + by - 1, lane);
   __syncwarp();
+  const int imx = bx * 4, imy = by * 4;
+  // The start and the half ring (lane 0 the start, lanes 1..8 the ring in
+  // the reference's order: dy outer, dx inner, centre skipped), four lanes
+  // per position (one 4x4 tile each), from the patches.
+  auto score = [&](int c, int qx, int qy, int t) -> uint32_t {
+    const int pl = (qy & 3) * 4 + (qx & 3);
+    (void)c;
+    return patch_tile_satd<S>(sm.src, patch + pl * G::PW, off, qx < 0 ? 0 : 1, qy < 0 ? 0 : 1, t & 1, t >> 1);
+  };
+  uint32_t sv = 0;
 #pragma unroll
-  for (int it = 0; it < 7; ++it) {
-    const int c = it * 8 + (lane >> 2), t = lane & 3;
+  for (int it = 0; it < 2; ++it) {
+    const int c = it * 8 + (lane >> 2);
     uint32_t v = 0;
-    if (c < 49) {
-      const int qx = c % 7 - 3, qy = c / 7 - 3;
-      const int pl = (qy & 3) * 4 + (qx & 3);
-      v = patch_tile_satd<S>(sm.src, patch + pl * G::PW, off, qx < 0 ? 0 : 1, qy < 0 ? 0 : 1, t & 1, t >> 1);
+    if (c < 9) {
+      const int q = c == 0 ? 4 : (c <= 4 ? c - 1 : c);
+      v = score(c, (q % 3 - 1) * 2, (q / 3 - 1) * 2, lane & 3);
     }
     v += __shfl_xor_sync(kFull, v, 1);
     v += __shfl_xor_sync(kFull, v, 2);
-    if (c < 49 && t == 0) satd[c] = v;
+    const uint32_t got = __shfl_sync(kFull, v, ((lane - it * 8) & 7) * 4);
+    if (lane >= it * 8 && lane < it * 8 + 8 && lane < 9) sv = got;
   }
-  __syncwarp();
-  const int imx = bx * 4, imy = by * 4;
-  // The start and the half ring: lane 0 the start, lanes 1..8 the ring in
-  // the reference's order (dy outer, dx inner, centre skipped).
   int mx = imx, my = imy;
-  uint32_t cost = kInf, sv = 0;
+  uint32_t cost = kInf;
   if (lane < 9) {
     const int q = lane == 0 ? 4 : (lane <= 4 ? lane - 1 : lane);
-    const int dx = (q % 3 - 1) * 2, dy = (q / 3 - 1) * 2;
-    mx = imx + dx;
-    my = imy + dy;
-    sv = satd[(dy + 3) * 7 + dx + 3];
+    mx = imx + (q % 3 - 1) * 2;
+    my = imy + (q / 3 - 1) * 2;
     cost = sv + hevc_rate(lam, mx, my, p0x, p0y, p1x, p1y);
   }
   Pick p = warp_min(cost);
@@ -623,23 +637,22 @@ __device__ __forceinline__ void refine8_patched(WarpSmem<S>& sm, const DevPlanes
   bsatd = __shfl_sync(kFull, sv, p.lane);
   bmx = __shfl_sync(kFull, mx, p.lane);
   bmy = __shfl_sync(kFull, my, p.lane);
-  // The quarter ring around the winner (the cross only when asked).
+  // The quarter ring around the winner (the cross only when asked), from
+  // the same patches: eight positions, four lanes each.
   const int hx = bmx - imx, hy = bmy - imy;
-  cost = kInf;
-  bool ok = false;
-  if (lane < 8) {
-    const int q = lane < 4 ? lane : lane + 1, dx = q % 3 - 1, dy = q / 3 - 1;
-    ok = !(quarter_cross != 0 && dx != 0 && dy != 0);
-    mx = (int)(int16_t)(bmx + dx);
-    my = (int)(int16_t)(bmy + dy);
-    sv = satd[(hy + dy + 3) * 7 + hx + dx + 3];
-    if (ok) cost = sv + hevc_rate(lam, mx, my, p0x, p0y, p1x, p1y);
-  }
-  nsatd += 9 + __popc(__ballot_sync(kFull, ok));
+  const int c = lane >> 2, q = c < 4 ? c : c + 1, dx = q % 3 - 1, dy = q / 3 - 1;
+  const bool ok = !(quarter_cross != 0 && dx != 0 && dy != 0);
+  uint32_t v = ok ? score(c, hx + dx, hy + dy, lane & 3) : 0u;
+  v += __shfl_xor_sync(kFull, v, 1);
+  v += __shfl_xor_sync(kFull, v, 2);
+  mx = (int)(int16_t)(bmx + dx);
+  my = (int)(int16_t)(bmy + dy);
+  cost = ok ? v + hevc_rate(lam, mx, my, p0x, p0y, p1x, p1y) : kInf;
+  nsatd += 9 + __popc(__ballot_sync(kFull, ok && (lane & 3) == 0));
   p = warp_min(cost);
   if (p.cost < bc) {
     bc = p.cost;
-    bsatd = __shfl_sync(kFull, sv, p.lane);
+    bsatd = __shfl_sync(kFull, v, p.lane);
     bmx = __shfl_sync(kFull, mx, p.lane);
     bmy = __shfl_sync(kFull, my, p.lane);
   }
@@ -817,6 +830,12 @@ __device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
   int state = nk > 0 ? 0 : 1, c0 = 0, it = 0, rings = 0;
   bool moved = false;
   const bool spec = SPEC && w == 8 && h == 8;
+  // The 8x8 refinement's patches, loaded during the diamond's step: a step
+  // that moves nothing leaves the best where the patches are centred.
+  const bool patched = spec && L.patch8 && ((R.stride * (int)sizeof(S)) & 3) == 0 &&
+                       ((R.plane_elems * (int64_t)sizeof(S)) & 3) == 0;
+  bool pre_staged = false;
+  uint32_t pre_off = 0;
   for (;;) {
     if (state == 1 && it >= 2 * range) {  // the diamond has settled
       if (rings >= F.search_rings) break;
@@ -846,12 +865,20 @@ __device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
       }
       const bool ok = abs(fx - ox) <= range && abs(fy - oy) <= range && fx >= lox && fx <= hix && fy >= loy &&
                       fy <= hiy;
+      uint32_t pv[PatchGeo<S>::PER];
+      uint32_t poff = 0;
+      if (patched) poff = load_patches<S>(pv, R, x + bx - 1, y + by - 1, lane);
       uint32_t part = ok ? sad8_half<S>(sm.src, org + (ptrdiff_t)fy * stride + fx, stride, hf) : 0u;
       part += __shfl_xor_sync(kFull, part, 1);
       const uint32_t cost = ok ? part + hevc_rate(lam, fx * 4, fy * 4, p0x, p0y, p1x, p1y) : kInf;
       nsad += __popc(__ballot_sync(kFull, ok && hf == 0 && q < 4));
       const Pick pa = warp_min(q < 4 ? cost : kInf);
       if (!(pa.cost < bcost)) {
+        if (patched) {
+          store_patches<S>(sm.src + kPatchOff, pv, lane);
+          pre_staged = true;
+          pre_off = poff;
+        }
         it = 2 * range;
         continue;
       }
@@ -947,44 +974,28 @@ __device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
   if (spec && L.patch8 && ((R.stride * (int)sizeof(S)) & 3) == 0 &&
       ((R.plane_elems * (int64_t)sizeof(S)) & 3) == 0) {
     refine8_patched<S>(sm, R, x, y, bx, by, lam, p0x, p0y, p1x, p1y, F.quarter_cross, lane, bmx, bmy, bc, bsatd,
-                       nsatd);
+                       nsatd, pre_staged, pre_off);
   } else {
-  // The latency form scores a 16x16 block's start and half ring in one
-  // pass: 9 candidates x 16 tiles, two candidates of 16 lanes at a time.
-  const bool merge16 = SPEC && w == 16 && h == 16;
-  for (int pass = merge16 ? 1 : 0; pass < 3; ++pass) {
-    if (merge16 && pass == 1) {
-      uint32_t sv = 0;
-#pragma unroll
-      for (int it = 0; it < 5; ++it) {
-        const int c = 2 * it + (lane >> 4);
-        uint32_t v = 0;
-        if (c < 9) {
-          const int q = c == 0 ? 4 : (c <= 4 ? c - 1 : c);
-          const int mx = imx + (q % 3 - 1) * 2, my = imy + (q / 3 - 1) * 2;
-          const S* pp = plane_at<S>(R, (my & 3) * 4 + (mx & 3), x + (mx >> 2), y + (my >> 2));
-          v = satd_part<S>(sm.src, wr, tw, ntiles, pp, stride, lane & 15, 16);
-        }
-        v += __shfl_xor_sync(kFull, v, 1);
-        v += __shfl_xor_sync(kFull, v, 2);
-        v += __shfl_xor_sync(kFull, v, 4);
-        v += __shfl_xor_sync(kFull, v, 8);
-        const uint32_t got = __shfl_sync(kFull, v, (lane & 1) * 16);
-        if (lane < 9 && (lane >> 1) == it) sv = got;
-      }
-      const int q = lane == 0 ? 4 : (lane <= 4 ? lane - 1 : lane);
-      const int mx = imx + (q % 3 - 1) * 2, my = imy + (q / 3 - 1) * 2;
-      const uint32_t cost = lane < 9 ? sv + hevc_rate(lam, mx, my, p0x, p0y, p1x, p1y) : kInf;
-      const Pick p = warp_min(cost);
-      bc = p.cost;
-      bsatd = __shfl_sync(kFull, sv, p.lane);
-      bmx = __shfl_sync(kFull, mx, p.lane);
-      bmy = __shfl_sync(kFull, my, p.lane);
-      continue;
-    }
+  // The latency form folds pass 1 (the half ring's last point) into pass 0
+  // where the block has at most 32 tiles: lane t also scores its tile t, so
+  // both passes' loads are in flight together; the in-order walk is kept
+  // (pass 0's winner, then the last point only when strictly cheaper).
+  const bool fold = SPEC && ntiles <= 32;
+  for (int pass = 0; pass < 3; ++pass) {
+    if (fold && pass == 1) continue;
     const int G = pass == 1 ? 32 : 4, c = pass == 1 ? 8 : lane >> 2, gsub = pass == 1 ? lane : lane & 3;
     int mx, my;
     bool ok;
+    uint32_t part8 = 0;  // folded: this lane's tile of the last half point
+    int mx8 = 0, my8 = 0;
+    if (fold && pass == 0) {
+      mx8 = imx + 2;
+      my8 = imy + 2;
+      if (lane < ntiles) {
+        const S* pp8 = plane_at<S>(R, (my8 & 3) * 4 + (mx8 & 3), x + (mx8 >> 2), y + (my8 >> 2));
+        part8 = satd_part<S>(sm.src, wr, tw, ntiles, pp8, stride, lane, 32);
+      }
+    }
     if (pass < 2) {
       const int q = c == 0 ? 4 : (c <= 4 ? c - 1 : c);
       mx = imx + (q % 3 - 1) * 2;
@@ -1008,6 +1019,16 @@ __device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
       bmx = __shfl_sync(kFull, mx, p.lane);
       bmy = __shfl_sync(kFull, my, p.lane);
     }
+    if (fold && pass == 0) {
+      for (int o = 16; o > 0; o >>= 1) part8 += __shfl_xor_sync(kFull, part8, o);
+      const uint32_t cost8 = part8 + hevc_rate(lam, mx8, my8, p0x, p0y, p1x, p1y);
+      if (cost8 < bc) {
+        bc = cost8;
+        bsatd = part8;
+        bmx = mx8;
+        bmy = my8;
+      }
+    }
   }
   nsatd += 9;
   }
@@ -1016,9 +1037,10 @@ __device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
   if (F.mode != RME_PRED_GIVEN && !amp_unit) {
     // The tasks reading this result: right and lower neighbours of this
     // level, the blocks of the next evaluated size inside this one, this
-    // CU's AMP units. Lane 0's result is fenced, then each lane releases one
-    // of them.
-    if (lane == 0) __threadfence();
+    // CU's AMP units; each lane releases one of them. Lane 0's result is
+    // ordered before the other lanes' accesses by the warp barrier, and each
+    // release is an acquire-release atomic, cumulative over it: no separate
+    // fence.
     __syncwarp();
     int ncx = 0, ncy = 0, cx0 = 0, cy0 = 0;
     if (l + 1 < F.nlevels) {
@@ -1055,22 +1077,26 @@ __device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
 // A 32x32 or 64x64 block's search is the longest dependent chain of a
 // frame (its level's wavefront has few blocks in flight, each of 1-4 K
 // samples per candidate), so in the latency form a whole CTA runs one: the
-// 256 threads split every step's candidate rows (SAD) or 4x4 tiles (SATD),
-// each warp's partial sum goes to shared memory, and after one barrier every
-// thread reads the step's costs and takes the same decision. The steps are
-// the single-warp search's, with more candidates per step where that saves
-// dependent steps: the seeds together, the small diamond two rounds at a
-// time (the second round's three new points for each way the first can
-// move), the 24 ring points together, and the start with the half ring
-// together. Each decision is the reference's in-order strict-< walk over the
-// step's candidates, so the results and the candidate counts are the
-// single-warp search's.
+// 256 threads split every step's candidate rows (SAD, a lane per word of a
+// row: coalesced) or 4x4 tiles (SATD), each warp's sum is added into the
+// candidate's cost in shared memory, and after one barrier every thread
+// reads the step's costs and takes the same decision. The steps are the
+// single-warp search's (a diamond round a step: at these sizes the
+// candidates' samples, not the dependent round trips, bound a step), with
+// the 24 ring points together and the start with the half ring together.
+// Each decision is the reference's in-order strict-< walk over the step's
+// candidates, so the results and the candidate counts are the single-warp
+// search's.
 constexpr int kGroupThreads = kWarpsPerBlock * 32;
 
 template <class S>
 struct alignas(16) GroupSmem {
   unsigned long long cnt[6];
-  uint32_t part[2][96];  // per step, per 32-job chunk: a warp's partial sum (two steps alternate)
+  // Per step, each candidate's distortion, summed by the warps' atomic adds.
+  // Three buffers in turn: a step adds into one, clears the next (read two
+  // steps ago, before the last barrier) and its decision reads the one it
+  // filled after its barrier.
+  uint32_t cost[3][32];
   uint32_t bc[8];        // broadcasts: predictor words, the popped entry
   uint32_t src[kMaxBlk * kMaxBlk * sizeof(S) / 4];
 };
@@ -1081,59 +1107,142 @@ __device__ __forceinline__ bool group_task_of(const LaunchDesc& L, const FrameDe
   return L.group_ctas > 0 && F.mode == RME_PRED_STANDALONE && F.codec == RME_CODEC_HEVC && t / F.nref < F.big_end;
 }
 
-// One row of the candidate's SAD (N samples).
-template <class S, int N>
-__device__ __forceinline__ uint32_t row_sad(const uint32_t* srow, const S* rp) {
-  constexpr int WR = N * (int)sizeof(S) / 4, CW = WR < 16 ? WR : 16;
-  uint32_t acc = 0;
+// The SADs of `nc` candidates of an N x N block: pos(c, fx, fy) gives
+// candidate c's whole-sample offset and whether it is scored. A warp takes
+// 32 / WR rows of one candidate at a time, a lane a word of a row (loads
+// coalesced along the row; the word after a lane's comes from its neighbour,
+// the row's last lane loads it), four such passes' loads in flight; each
+// warp's sum is added into cost[b][c].
+template <class S, int N, class Pos>
+__device__ __forceinline__ void cta_sad(GroupSmem<S>& gs, int b, const S* org, int stride, int nc, Pos pos, int tid) {
+  constexpr int SPW = 4 / sizeof(S), WR = N / SPW, RPW = 32 / WR, K = 4, STEP = kWarpsPerBlock * RPW;
+  const int lane = tid & 31, warp = tid >> 5, wd = lane % WR, rsub = lane / WR;
+  if (tid < 32) gs.cost[(b + 1) % 3][tid] = 0u;
+  const int rows = nc * N;
+  for (int r0 = warp * RPW; r0 < rows; r0 += K * STEP) {
+    uint32_t lo[K], hi[K], sh[K];
+    int cc[K], rw[K];
+    bool ok[K];
 #pragma unroll
-  for (int c = 0; c < WR; c += CW) {
-    uint32_t a[CW];
-    ldwords<CW>(rp + c * (4 / (int)sizeof(S)), a);
+    for (int k = 0; k < K; ++k) {
+      const int rr = r0 + k * STEP + rsub;
+      ok[k] = false;
+      cc[k] = 0;
+      rw[k] = 0;
+      lo[k] = hi[k] = sh[k] = 0u;
+      if (rr < rows) {  // uniform over the warp, as is the candidate
+        const int c = rr / N;
+        int fx, fy;
+        cc[k] = c;
+        rw[k] = rr - c * N;
+        ok[k] = pos(c, fx, fy);
+        if (ok[k]) {
+          const uintptr_t a = reinterpret_cast<uintptr_t>(org + (ptrdiff_t)(fy + rw[k]) * stride + fx);
+          const uint32_t* q = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
+          sh[k] = (uint32_t)(a & 3) * 8u;
+          lo[k] = RME_LD32(q + wd);
+          if (wd == WR - 1) hi[k] = RME_LD32(q + WR);
+        }
+      }
+    }
 #pragma unroll
-    for (int j = 0; j < CW; ++j) acc += vsad(srow[c + j], a[j], S());
+    for (int k = 0; k < K; ++k) {
+      const uint32_t nx = __shfl_down_sync(kFull, lo[k], 1);
+      if (wd != WR - 1) hi[k] = nx;
+      uint32_t acc = ok[k] ? vsad(gs.src[rw[k] * WR + wd], __funnelshift_r(lo[k], hi[k], sh[k]), S()) : 0u;
+      acc = __reduce_add_sync(kFull, acc);
+      if (lane == 0 && ok[k]) atomicAdd(&gs.cost[b][cc[k]], acc);
+    }
   }
-  return acc;
+  __syncthreads();
 }
 
-// The SADs of `nc` candidates of an N x N block (rows split over the CTA):
-// pos(c, fx, fy) gives candidate c's whole-sample offset and whether it is
-// scored. Sums per 32-row chunk into part[buf].
+// The diamond's window: the reference's integer plane around a staging
+// centre (scx, scy) (whole-sample offsets from the block), kWinR samples
+// beyond the block on every side, staged in shared memory behind the
+// GroupSmem with coalesced word loads. A diamond round from any best within
+// kWinR - 1 of the centre reads only the window, so a walk restages every
+// few rounds instead of reading four candidates' rows through the caches
+// every round.
+constexpr int kWinR = 4;
+template <class S, int N>
+struct WinGeo {
+  static constexpr int ROWS = N + 2 * kWinR;
+  static constexpr int WRW = (N + 2 * kWinR) * (int)sizeof(S) / 4 + 1;  // words per staged row (any sample offset)
+};
+static_assert(sizeof(GroupSmem<uint8_t>) + WinGeo<uint8_t, 64>::ROWS * WinGeo<uint8_t, 64>::WRW * 4 <=
+                  kWarpsPerBlock * sizeof(WarpSmem<uint8_t>),
+              "the window outgrew the CTA's shared memory");
+static_assert(sizeof(GroupSmem<uint16_t>) + WinGeo<uint16_t, 64>::ROWS * WinGeo<uint16_t, 64>::WRW * 4 <=
+                  kWarpsPerBlock * sizeof(WarpSmem<uint16_t>),
+              "the window outgrew the CTA's shared memory");
+
+// Stage the window around (scx, scy); returns the byte offset of its first
+// sample within the first word (the same on every row: rows are whole words
+// apart). All threads call; ends with a barrier.
+template <class S, int N>
+__device__ __forceinline__ uint32_t stage_window(uint32_t* win, const S* org, int stride, int scx, int scy, int tid) {
+  using W = WinGeo<S, N>;
+  const uintptr_t a0 = reinterpret_cast<uintptr_t>(org + (ptrdiff_t)(scy - kWinR) * stride + (scx - kWinR));
+  const uint32_t* w0 = reinterpret_cast<const uint32_t*>(a0 & ~uintptr_t(3));
+  const int rstep = stride * (int)sizeof(S) / 4;
+  for (int i = tid; i < W::ROWS * W::WRW; i += kGroupThreads) {
+    const int row = i / W::WRW, wd = i - row * W::WRW;
+    win[i] = RME_LD32(w0 + (ptrdiff_t)row * rstep + wd);
+  }
+  __syncthreads();
+  return (uint32_t)(a0 & 3);
+}
+
+// The SADs of `nc` candidates, all within kWinR of the window's centre, from
+// the window (a lane per word of a candidate row, each thread's words of a
+// candidate summed, each warp's sum added into cost[b][c]).
 template <class S, int N, class Pos>
-__device__ __forceinline__ void cta_sad(GroupSmem<S>& gs, int buf, const S* org, int stride, int nc, Pos pos,
-                                          int tid) {
-  constexpr int SPW = 4 / sizeof(S), WR = N / SPW;
-  const int jobs = nc * N;
-#pragma unroll 2
-  for (int j0 = 0; j0 < jobs; j0 += kGroupThreads) {
-    const int j = j0 + tid;
+__device__ __forceinline__ void cta_sad_win(GroupSmem<S>& gs, int b, const uint32_t* win, uint32_t off0, int scx,
+                                            int scy, int nc, Pos pos, int tid) {
+  using W = WinGeo<S, N>;
+  constexpr int SPW = 4 / sizeof(S), WR = N / SPW, JOBS = N * WR, PER = JOBS / kGroupThreads;
+  if (tid < 32) gs.cost[(b + 1) % 3][tid] = 0u;
+  for (int c = 0; c < nc; ++c) {
+    int fx, fy;
+    if (!pos(c, fx, fy)) continue;
+    const uint32_t b0 = off0 + (uint32_t)((fx - scx + kWinR) * (int)sizeof(S));
+    const int r0 = fy - scy + kWinR;
     uint32_t acc = 0;
-    if (j < jobs) {
-      const int c = j / N, row = j - c * N;
-      int fx, fy;
-      if (pos(c, fx, fy)) acc = row_sad<S, N>(gs.src + row * WR, org + (ptrdiff_t)(fy + row) * stride + fx);
+#pragma unroll
+    for (int m = 0; m < PER; ++m) {
+      const int j = tid + m * kGroupThreads, row = j / WR, k = j - row * WR;
+      const uint32_t bb = b0 + 4u * k, wi = bb >> 2, sh = (bb & 3u) * 8u;
+      const uint32_t* wr = win + (r0 + row) * W::WRW;
+      acc += vsad(gs.src[row * WR + k], __funnelshift_r(wr[wi], wr[wi + 1], sh), S());
     }
     acc = __reduce_add_sync(kFull, acc);
-    if ((tid & 31) == 0 && j < jobs) gs.part[buf][j >> 5] = acc;
+    if ((tid & 31) == 0) atomicAdd(&gs.cost[b][c], acc);
   }
   __syncthreads();
 }
 
 // The SATDs of `nc` candidates (quarter-sample vectors from pos), 4x4 tiles
-// split over the CTA; sums per 32-tile chunk into part[buf].
+// split over the CTA (a warp's lanes on adjacent tiles of a tile row:
+// coalesced), each warp's sum added into cost[b][c].
 template <class S, int N, class Pos>
-__device__ __forceinline__ void cta_satd(GroupSmem<S>& gs, int buf, const DevPlanes& R, int x, int y, int nc,
-                                           Pos pos, int tid) {
+__device__ __forceinline__ void cta_satd(GroupSmem<S>& gs, int b, const DevPlanes& R, int x, int y, int nc, Pos pos,
+                                         int tid) {
   constexpr int SPW = 4 / sizeof(S), WPT = 4 / SPW, TW = N / 4, NT = TW * TW, WR = N / SPW;
+  if (tid < 32) gs.cost[(b + 1) % 3][tid] = 0u;
   const int jobs = nc * NT;
 #pragma unroll 3
   for (int j0 = 0; j0 < jobs; j0 += kGroupThreads) {
     const int j = j0 + tid;
     uint32_t acc = 0;
+    int c = 0;
+    bool ok = false;
     if (j < jobs) {
-      const int c = j / NT, i = j - c * NT, ty = i / TW, tx = i - ty * TW;
+      c = j / NT;
+      const int i = j - c * NT, ty = i / TW, tx = i - ty * TW;
       int mx, my;
-      if (pos(c, mx, my)) {
+      ok = pos(c, mx, my);
+      if (ok) {
         const S* pp = plane_at<S>(R, (my & 3) * 4 + (mx & 3), x + (mx >> 2) + tx * 4, y + (my >> 2) + ty * 4);
         uint32_t pw[4][WPT];
 #pragma unroll
@@ -1156,18 +1265,10 @@ __device__ __forceinline__ void cta_satd(GroupSmem<S>& gs, int buf, const DevPla
         acc = satd4x4(d);
       }
     }
-    acc = __reduce_add_sync(kFull, acc);
-    if ((tid & 31) == 0 && j < jobs) gs.part[buf][j >> 5] = acc;
+    acc = __reduce_add_sync(kFull, acc);  // a warp's 32 jobs are tiles of one candidate (NT >= 64)
+    if ((tid & 31) == 0 && ok) atomicAdd(&gs.cost[b][c], acc);
   }
   __syncthreads();
-}
-
-// Candidate c's distortion after a step: the sum of its chunks.
-template <class S>
-__device__ __forceinline__ uint32_t cta_cost(const GroupSmem<S>& gs, int buf, int c, int chunks) {
-  uint32_t v = 0;
-  for (int k = 0; k < chunks; ++k) v += gs.part[buf][c * chunks + k];
-  return v;
 }
 
 // search_full + refine_subpel of one STANDALONE square block of N in {32, 64}
@@ -1195,6 +1296,7 @@ __device__ int hevc_group_task(const LaunchDesc& L, const FrameDesc& F, int f, i
     gs.bc[tid] = didx >= 0 ? ldcg_u32(&F.out[didx].mv) : 0u;
     gs.bc[3 + tid] = didx >= 0 ? 1u : 0u;
   }
+  if (tid < 64) gs.cost[tid >> 5][tid & 31] = 0u;  // the first step's buffer (and the next)
   {
     const S* so = plane_at<S>(F.src, 0, x, y);
     for (int i = tid; i < WR * N; i += kGroupThreads) {
@@ -1231,7 +1333,8 @@ __device__ int hevc_group_task(const LaunchDesc& L, const FrameDesc& F, int f, i
   const float lam = F.lam;
   const int range = F.search_range;
   uint32_t nsad = 0, nsatd = 0;
-  int buf = 0;
+  int buf = 0;  // the cost buffer of the next step (cta_sad / cta_satd)
+  auto next = [&] { buf = buf == 2 ? 0 : buf + 1; };
   // Seeds: >> 2 (floor), clamp_pos, dedupe through `tried`, in order
   // (seed i is scored unless an earlier one landed on the same point).
   int kx[4], ky[4];
@@ -1258,77 +1361,57 @@ __device__ int hevc_group_task(const LaunchDesc& L, const FrameDesc& F, int f, i
     int fx, fy;
     if (!spos(c, fx, fy)) continue;
     ++nsad;
-    const uint32_t cost = cta_cost(gs, buf, c, N / 32) + hevc_rate(lam, fx * 4, fy * 4, p0x, p0y, p1x, p1y);
+    const uint32_t cost = gs.cost[buf][c] + hevc_rate(lam, fx * 4, fy * 4, p0x, p0y, p1x, p1y);
     if (cost < bcost) {
       bcost = cost;
       bx = fx;
       by = fy;
     }
   }
-  buf ^= 1;
+  next();
   const int ox = bx, oy = by;  // the descent stays within +-range of the best seed
   auto inside = [&](int fx, int fy) {
     return abs(fx - ox) <= range && abs(fy - oy) <= range && fx >= lox && fx <= hix && fy >= loy && fy <= hiy;
   };
   int rings = 0;
+  uint32_t* const win = reinterpret_cast<uint32_t*>(&gs + 1);
+  int scx = 0, scy = 0;
+  uint32_t woff = 0;
+  bool staged = false;
   for (;;) {
-    // The small diamond, two rounds a step: candidates 0..3 around the
-    // best, 4..15 the next round's three new points for each way the first
-    // can move (the fourth point being the best, which cannot win).
-    for (int it = 0; it < 2 * range;) {
+    // The small diamond, a round a step: (1,0), (-1,0), (0,1), (0,-1)
+    // around the best, taken in order when strictly cheaper; scored from
+    // the window, restaged around the best when the round would leave it.
+    for (int it = 0; it < 2 * range; ++it) {
       const int cbx = bx, cby = by;
       auto pos = [&](int q, int& fx, int& fy) {
-        const int j0 = q < 4 ? q : (q - 4) / 3, mm = (q - 4) % 3, m = mm + (mm >= (j0 ^ 1));
-        fx = cbx + (j0 == 0 ? 1 : j0 == 1 ? -1 : 0);
-        fy = cby + (j0 == 2 ? 1 : j0 == 3 ? -1 : 0);
-        if (q >= 4) {
-          fx += m == 0 ? 1 : m == 1 ? -1 : 0;
-          fy += m == 2 ? 1 : m == 3 ? -1 : 0;
-        }
+        fx = cbx + (q == 0 ? 1 : q == 1 ? -1 : 0);
+        fy = cby + (q == 2 ? 1 : q == 3 ? -1 : 0);
         return inside(fx, fy);
       };
-      cta_sad<S, N>(gs, buf, org, stride, 16, pos, tid);
-      int j = -1;
-      uint32_t best1 = bcost;
+      if (!staged || abs(cbx - scx) > kWinR - 1 || abs(cby - scy) > kWinR - 1) {
+        scx = cbx;
+        scy = cby;
+        woff = stage_window<S, N>(win, org, stride, scx, scy, tid);
+        staged = true;
+      }
+      cta_sad_win<S, N>(gs, buf, win, woff, scx, scy, 4, pos, tid);
+      bool improved = false;
+#pragma unroll
       for (int q = 0; q < 4; ++q) {
         int fx, fy;
         if (!pos(q, fx, fy)) continue;
         ++nsad;
-        const uint32_t cost = cta_cost(gs, buf, q, N / 32) + hevc_rate(lam, fx * 4, fy * 4, p0x, p0y, p1x, p1y);
-        if (cost < best1) {
-          best1 = cost;
-          j = q;
-        }
-      }
-      if (j < 0) {  // the first round moved nothing: settled
-        buf ^= 1;
-        break;
-      }
-      bcost = best1;
-      pos(j, bx, by);
-      if (++it >= 2 * range) {
-        buf ^= 1;
-        break;
-      }
-      int j2 = -1, nbx2 = bx, nby2 = by;
-      ++nsad;  // the old best, scored again by the reference
-      for (int q = 4 + 3 * j; q < 7 + 3 * j; ++q) {
-        int fx, fy;
-        if (!pos(q, fx, fy)) continue;
-        ++nsad;
-        const uint32_t cost = cta_cost(gs, buf, q, N / 32) + hevc_rate(lam, fx * 4, fy * 4, p0x, p0y, p1x, p1y);
+        const uint32_t cost = gs.cost[buf][q] + hevc_rate(lam, fx * 4, fy * 4, p0x, p0y, p1x, p1y);
         if (cost < bcost) {
           bcost = cost;
-          j2 = q;
-          nbx2 = fx;
-          nby2 = fy;
+          bx = fx;
+          by = fy;
+          improved = true;
         }
       }
-      buf ^= 1;
-      if (j2 < 0) break;
-      bx = nbx2;
-      by = nby2;
-      ++it;
+      next();
+      if (!improved) break;
     }
     if (rings >= F.search_rings) break;
     ++rings;
@@ -1346,7 +1429,7 @@ __device__ int hevc_group_task(const LaunchDesc& L, const FrameDesc& F, int f, i
       int fx, fy;
       if (!rpos(c, fx, fy)) continue;
       ++nsad;
-      const uint32_t cost = cta_cost(gs, buf, c, N / 32) + hevc_rate(lam, fx * 4, fy * 4, p0x, p0y, p1x, p1y);
+      const uint32_t cost = gs.cost[buf][c] + hevc_rate(lam, fx * 4, fy * 4, p0x, p0y, p1x, p1y);
       if (cost < bcost) {
         bcost = cost;
         bx = fx;
@@ -1354,14 +1437,13 @@ __device__ int hevc_group_task(const LaunchDesc& L, const FrameDesc& F, int f, i
         moved = true;
       }
     }
-    buf ^= 1;
+    next();
     if (!moved) break;
   }
   const uint32_t int_cost = bcost;
   const int imx = bx * 4, imy = by * 4;
   // refine_subpel: the start and the half ring (dy outer, dx inner) in one
   // step, then the quarter ring around the winner.
-  constexpr int TC = (N / 4) * (N / 4) / 32;  // 32-tile chunks per candidate
   auto hpos = [&](int c, int& mx, int& my) {
     const int q = c == 0 ? 4 : (c <= 4 ? c - 1 : c);
     mx = imx + (q % 3 - 1) * 2;
@@ -1374,7 +1456,7 @@ __device__ int hevc_group_task(const LaunchDesc& L, const FrameDesc& F, int f, i
   for (int c = 0; c < 9; ++c) {
     int mx, my;
     hpos(c, mx, my);
-    const uint32_t sv = cta_cost(gs, buf, c, TC), cost = sv + hevc_rate(lam, mx, my, p0x, p0y, p1x, p1y);
+    const uint32_t sv = gs.cost[buf][c], cost = sv + hevc_rate(lam, mx, my, p0x, p0y, p1x, p1y);
     if (cost < bc) {
       bc = cost;
       bsatd = sv;
@@ -1382,7 +1464,7 @@ __device__ int hevc_group_task(const LaunchDesc& L, const FrameDesc& F, int f, i
       bmy = my;
     }
   }
-  buf ^= 1;
+  next();
   const int hmx = bmx, hmy = bmy, cross = F.quarter_cross;
   auto qpos = [&](int c, int& mx, int& my) {
     const int q = c < 4 ? c : c + 1, dx = q % 3 - 1, dy = q / 3 - 1;
@@ -1395,7 +1477,7 @@ __device__ int hevc_group_task(const LaunchDesc& L, const FrameDesc& F, int f, i
     int mx, my;
     if (!qpos(c, mx, my)) continue;
     ++nsatd;
-    const uint32_t sv = cta_cost(gs, buf, c, TC), cost = sv + hevc_rate(lam, mx, my, p0x, p0y, p1x, p1y);
+    const uint32_t sv = gs.cost[buf][c], cost = sv + hevc_rate(lam, mx, my, p0x, p0y, p1x, p1y);
     if (cost < bc) {
       bc = cost;
       bsatd = sv;
@@ -1407,7 +1489,6 @@ __device__ int hevc_group_task(const LaunchDesc& L, const FrameDesc& F, int f, i
   rme_result* out = &F.out[t];
   if (tid == 0) {
     write_result(out, bmx, bmy, r, bc, bsatd, imx, imy, int_cost, nsad, nsatd, 0);
-    __threadfence();
     gs.cnt[0] += 1;
     gs.cnt[1] += nsad;
     gs.cnt[2] += nsatd;
@@ -1889,9 +1970,9 @@ __device__ int h264_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
       }
     }
     write_result(&F.out[t], mv16x, mv16y, r16, c16, s16, mi16x, mi16y, ci16, nsad, nsatd, lane);
-    // The macroblocks whose A, B, C or D this one is, one per lane.
+    // The macroblocks whose A, B, C or D this one is, one per lane (the
+    // warp barrier orders lane 0's result before the releasing atomics).
     const int mbh = F.height / 16;
-    if (lane == 0) __threadfence();
     __syncwarp();
     bool rel = false;
     int dtask = 0;

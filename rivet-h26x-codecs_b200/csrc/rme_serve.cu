@@ -68,6 +68,7 @@ struct Request {
   size_t staging_n = 0;
   cudaEvent_t ev = nullptr;  // the upload (first frames) or the results copy
   int status = 0;
+  double t_start = 0.0, t_flag = 0.0;  // host clock: handed to the engine, its flag seen
 };
 
 struct Server {
@@ -97,6 +98,8 @@ struct Server {
   std::vector<cudaEvent_t> events;
   std::map<size_t, std::vector<rme_result*>> staging_pool;
   std::vector<std::pair<int32_t, int>> release_later;  // closed streams' pictures (id base, count)
+  bool trace = false;  // RME_SERVE_TRACE=1: one line per frame on stderr
+  double idle_since = 0.0;  // nothing in flight since
 
   void* take_buffer(size_t bytes) {  // lock held
     auto& v = pool[bytes];
@@ -209,6 +212,7 @@ void Server::submit_search(Request& r, const Stream& st) {
 // Upload the frame into its stream's ring, then (frames with a reference)
 // submit it to the engine behind the upload.
 void Server::start(Request& r) {
+  r.t_start = now();
   const Stream* st;
   {
     std::lock_guard<std::mutex> lk(m);
@@ -303,6 +307,7 @@ void Server::run() {
         ++i;
         continue;
       }
+      r.t_flag = now();
       rme_result* dst = r.out;
       if (!r.out_pinned) {
         r.staging = take_staging((size_t)r.nresults);
@@ -339,6 +344,10 @@ void Server::run() {
       if (r.staging) staging_pool[r.staging_n].push_back(r.staging);
       events.push_back(r.ev);
       const double t = now();
+      if (trace)
+        std::fprintf(stderr, "serve: stream %d frame %lld slot %d: queued %.3f ms, engine %.3f ms, copy %.3f ms\n",
+                     r.stream, (long long)r.frame, r.slot, (r.t_start - r.submit_s) * 1e3,
+                     r.slot >= 0 ? (r.t_flag - r.t_start) * 1e3 : 0.0, r.slot >= 0 ? (t - r.t_flag) * 1e3 : 0.0);
       {
         std::lock_guard<std::mutex> lk(m);
         finish(r, t);
@@ -346,6 +355,15 @@ void Server::run() {
       any = true;
       copying[i] = copying.back();
       copying.pop_back();
+    }
+    // Nothing in flight for a while: stop the engine kernel (the waiting
+    // warps leave), so that it holds no SM while the server is idle; the
+    // next frame launches it again.
+    if (searching.empty() && submitting.empty()) {
+      if (any || !taken.empty()) idle_since = now();
+      else if (now() - idle_since > 0.02) rme::engine_stop(eng);
+    } else {
+      idle_since = now();
     }
     if (!release_later.empty() || any || any_close) release_closed(rme::engine_idle(eng));
   }
@@ -371,6 +389,7 @@ int rme_serve_start(void* ctx, const rme_serve_opts* o, void** server) {
     return RME_ECUDA;
   }
   *s->h_status = 0;
+  s->trace = std::getenv("RME_SERVE_TRACE") && std::getenv("RME_SERVE_TRACE")[0] == '1';
   s->worker = std::thread([s] {
     cudaSetDevice(s->device);
     s->run();
