@@ -186,6 +186,12 @@ struct Deps {  // the dependency structure of one frame shape
   std::vector<uint32_t> ready;   // tasks that read none, in order
   uint32_t* d_ready = nullptr;   // device copy of `ready` (the resident engine publishes from it)
   size_t ntasks = 0;
+  // The row form (HEVC without AMP): the rows a warp runs (16x16 and 8x8)
+  // and the rows a CTA runs (64x64 and 32x32), as row_entry words, each
+  // list ordered by the row's first sample row, larger blocks first: every
+  // row comes after the rows it reads (its upper row, its parents' rows).
+  std::vector<uint32_t> rows, rows_big;
+  uint32_t* d_rows = nullptr;    // device: rows, then rows_big
 };
 
 struct Graph {
@@ -198,13 +204,19 @@ struct Graph {
 // the share of CTAs that search 32x32 and 64x64 HEVC blocks a CTA per block
 // (0, a quarter or half of the SMs), and whether 8x8 blocks refine from
 // staged phase patches (the search window's neighbourhood in shared memory)
-// or straight from the caches.
+// or straight from the caches; and whether HEVC STANDALONE frames without
+// AMP run in the row form (a warp or a CTA per row of blocks; `groups` 3:
+// a CTA for every row of large blocks, up to half the grid).
 struct Shape {
-  int variant, groups, patch;
+  int variant, groups, patch, rows;
 };
-constexpr Shape kThroughputShapes[] = {{1, 0, 0}, {0, 0, 0}, {2, 0, 0}};
-constexpr Shape kLatencyHevcShapes[] = {{1, 2, 1}, {1, 2, 0}, {1, 1, 1}, {1, 0, 0}, {1, 0, 1}, {0, 2, 1}};
-constexpr Shape kLatencyShapes[] = {{1, 0, 0}, {0, 0, 0}, {2, 0, 0}};
+constexpr Shape kThroughputShapes[] = {{1, 0, 0, 0}, {0, 0, 0, 0}, {2, 0, 0, 0}};
+constexpr Shape kLatencyHevcShapes[] = {{0, 3, 1, 1}, {1, 3, 1, 1}, {0, 3, 0, 1}, {1, 2, 1, 0},
+                                        {1, 2, 0, 0}, {1, 1, 1, 0}, {1, 0, 0, 0}, {0, 2, 1, 0}};
+constexpr Shape kLatencyShapes[] = {{1, 0, 0, 0}, {0, 0, 0, 0}, {2, 0, 0, 0}};
+constexpr int kNumShapes[3] = {(int)(sizeof(kThroughputShapes) / sizeof(Shape)),
+                               (int)(sizeof(kLatencyHevcShapes) / sizeof(Shape)),
+                               (int)(sizeof(kLatencyShapes) / sizeof(Shape))};
 
 // One search launch's buffers and events. A context keeps kSlots of them and
 // takes them in turn: a synchronous search finishes its launch before it
@@ -218,6 +230,7 @@ struct Slot {
   DevBuf<int32_t> d_pending;
   DevBuf<rme_job> d_jobs;
   DevBuf<unsigned long long> d_misc;  // the launch header (kMisc*)
+  DevBuf<unsigned long long> d_mvf;   // the row form's published vectors (tagged with the epoch)
   PinBuf<FrameDesc> h_frames;
   PinBuf<rme_result> h_out;
   PinBuf<unsigned long long> h_misc;
@@ -296,6 +309,7 @@ struct Ctx {
     for (auto& d : deps) {
       if (d.second.pending) cudaFree(d.second.pending);
       if (d.second.d_ready) cudaFree(d.second.d_ready);
+      if (d.second.d_rows) cudaFree(d.second.d_rows);
     }
     for (auto& t : tables)
       if (t.second.tab) cudaFree(t.second.tab);
@@ -459,15 +473,41 @@ const Deps* get_deps(Ctx* c, const rme_picture_desc& d, const rme_params* p, int
   for (size_t t = 0; t < pend.size(); ++t)
     if (pend[t] == 0) dp.ready.push_back((uint32_t)t);
   dp.ntasks = pend.size();
+  if (d.codec == RME_CODEC_HEVC && p->hevc_amp == 0) {
+    struct Row {
+      int y, size;
+      uint32_t entry;
+    };
+    std::vector<Row> all;
+    int sizes[4];
+    const int nl = level_sizes(p, sizes);
+    for (int l = 0; l < nl; ++l) {
+      const int N = sizes[l];
+      if (d.width / N == 0) continue;
+      for (int row = 0; row < d.height / N; ++row)
+        for (int r = 0; r < nref; ++r) all.push_back({row * N, N, row_entry(l, r, row)});
+    }
+    std::stable_sort(all.begin(), all.end(),
+                     [](const Row& a, const Row& b) { return a.y != b.y ? a.y < b.y : a.size > b.size; });
+    for (const Row& w : all) (w.size >= 32 ? dp.rows_big : dp.rows).push_back(w.entry);
+  }
   cudaError_t e = cudaMalloc(&dp.pending, std::max<size_t>(pend.size(), 1) * sizeof(int32_t));
   if (e == cudaSuccess)
     e = cudaMemcpy(dp.pending, pend.data(), pend.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMalloc(&dp.d_ready, std::max<size_t>(dp.ready.size(), 1) * sizeof(uint32_t));
   if (e == cudaSuccess)
     e = cudaMemcpy(dp.d_ready, dp.ready.data(), dp.ready.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
+  const size_t nrows = dp.rows.size() + dp.rows_big.size();
+  if (e == cudaSuccess && nrows > 0) e = cudaMalloc(&dp.d_rows, nrows * sizeof(uint32_t));
+  if (e == cudaSuccess && !dp.rows.empty())
+    e = cudaMemcpy(dp.d_rows, dp.rows.data(), dp.rows.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !dp.rows_big.empty())
+    e = cudaMemcpy(dp.d_rows + dp.rows.size(), dp.rows_big.data(), dp.rows_big.size() * sizeof(uint32_t),
+                   cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     if (dp.pending) cudaFree(dp.pending);
     if (dp.d_ready) cudaFree(dp.d_ready);
+    if (dp.d_rows) cudaFree(dp.d_rows);
     *rc = cuda_fail(c, e, "dependency template");
     return nullptr;
   }
@@ -672,16 +712,19 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   if (!dev_out) CK(sl.d_out.ensure(std::max<int64_t>(total, 1)));
   CK(sl.d_pending.ensure(std::max<int64_t>(total, 1)));
   unsigned long long* old_ready = sl.d_ready.p;
+  unsigned long long* old_mvf = sl.d_mvf.p;
   CK(sl.d_ready.ensure(2 * std::max<int64_t>(total, 1)));  // the warps' queues, then the CTAs' queues
+  CK(sl.d_mvf.ensure(std::max<int64_t>(total, 1)));
   // Fresh slot memory may hold any word, an epoch's among them: zero it
   // (epochs start at 1).
-  if (sl.d_ready.p != old_ready) sl.epoch = 0;
+  if (sl.d_ready.p != old_ready || sl.d_mvf.p != old_mvf) sl.epoch = 0;
   CK(sl.d_jobs.ensure(std::max<int64_t>(jobs_off[n], 1)));
   CK(sl.d_misc.ensure(kMiscWords));
   if (!dev_out && !pinned_out) CK(sl.h_out.ensure(std::max<int64_t>(total, 1)));
   CK(sl.h_misc.ensure(kMiscWords));
   if (sl.epoch == 0 || sl.epoch == 0xffffffffu) {
     CK(cudaMemsetAsync(sl.d_ready.p, 0, sl.d_ready.n * sizeof(unsigned long long), s));
+    CK(cudaMemsetAsync(sl.d_mvf.p, 0, sl.d_mvf.n * sizeof(unsigned long long), s));
     sl.epoch = 0;
   }
   ++sl.epoch;
@@ -708,7 +751,7 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   int tune_shapes = 0;
   for (int k = 0; k < kParts; ++k) {
     const Shape* shapes = !spec ? kThroughputShapes : part_codec(k) == RME_CODEC_HEVC ? kLatencyHevcShapes : kLatencyShapes;
-    const int nsh = !spec ? 3 : part_codec(k) == RME_CODEC_HEVC ? 6 : 3;
+    const int nsh = kNumShapes[!spec ? 0 : part_codec(k) == RME_CODEC_HEVC ? 1 : 2];
     shape[k] = shapes[0];
     if (part_tasks[k] > 0 && c->tune_on) {
       const int bucket = 63 - __builtin_clzll((unsigned long long)part_tasks[k]);
@@ -725,6 +768,24 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
     if (part_tasks[k] > 0 && !c->bps[k][variant[k]][spec])
       c->bps[k][variant[k]][spec] = search_blocks_per_sm(part_bytes(k), part_codec(k), variant[k], spec);
   }
+  // The row form, for a part of the latency form whose frames are all HEVC
+  // STANDALONE without AMP when its shape asks for it.
+  bool rows[kParts] = {false, false, false, false};
+  std::vector<const Deps*> fdeps(n, nullptr);
+  for (int k = 0; k < kParts; ++k) rows[k] = spec && part_tasks[k] > 0 && shape[k].rows;
+  for (int i = 0; i < n; ++i) {
+    const FrameDesc& fd = sl.h_frames.p[i];
+    if (params[i].predictor_mode == RME_PRED_STANDALONE) {
+      Picture* src;
+      picture_of(c, frames[i].src_id, &src);
+      int rc = 0;
+      fdeps[i] = get_deps(c, src->d, &params[i], frames[i].nref, &rc);
+      if (!fdeps[i]) return rc;
+    }
+    if (fd.codec != RME_CODEC_HEVC || params[i].predictor_mode != RME_PRED_STANDALONE || fd.amp != 0)
+      rows[part_of(fd)] = false;
+  }
+  int64_t rows_small[kParts] = {0, 0, 0, 0}, rows_large[kParts] = {0, 0, 0, 0};
   std::vector<std::pair<const int32_t*, int>> pend_copies;  // (template, frame)
   for (int i = 0; i < n; ++i) {
     FrameDesc& fd = sl.h_frames.p[i];
@@ -742,12 +803,23 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
       sig.push_back(-1);
       sig.push_back(frames[i].njobs);
       sig.push_back(fd.bd);
+    } else if (rows[part]) {
+      // Every row of the frame is pushed now (interleaved with the other
+      // frames' rows below); a search of this buffer tags its words anew.
+      const Deps* dp = fdeps[i];
+      fd.mvf = sl.d_mvf.p + toff[i];
+      fd.tag = sl.epoch;
+      fd.nrows = (int32_t)(dp->rows.size() + dp->rows_big.size());
+      rows_small[part] += (int64_t)dp->rows.size();
+      rows_large[part] += (int64_t)dp->rows_big.size();
+      sig.push_back(fd.bd);
+      sig.push_back(fd.codec);
+      sig.push_back(fd.width);
+      sig.push_back(fd.height);
+      sig.push_back(fd.nref);
+      sig.push_back(params[i].hevc_pu_mask);
     } else {
-      Picture* src;
-      picture_of(c, frames[i].src_id, &src);
-      int rc = 0;
-      const Deps* dp = get_deps(c, src->d, &params[i], frames[i].nref, &rc);
-      if (!dp) return rc;
+      const Deps* dp = fdeps[i];
       pend_copies.emplace_back(dp->pending, i);
       const bool groups = spec && fd.codec == RME_CODEC_HEVC && shape[part].groups > 0;
       for (uint32_t t : dp->ready)
@@ -766,6 +838,24 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
       std::stable_sort(v->begin(), v->end(), [](unsigned long long a, unsigned long long b) {
         return (a & 0xffffffu) < (b & 0xffffffu);
       });
+  // Row-form parts: the frames' rows interleaved row for row (each frame's
+  // own order kept).
+  for (int k = 0; k < kParts; ++k) {
+    if (!rows[k]) continue;
+    for (int big = 0; big < 2; ++big) {
+      size_t most = 0;
+      for (int i = 0; i < n; ++i)
+        if (part_of(sl.h_frames.p[i]) == k) most = std::max(most, (big ? fdeps[i]->rows_big : fdeps[i]->rows).size());
+      for (size_t j = 0; j < most; ++j)
+        for (int i = 0; i < n; ++i) {
+          if (part_of(sl.h_frames.p[i]) != k) continue;
+          const std::vector<uint32_t>& v = big ? fdeps[i]->rows_big : fdeps[i]->rows;
+          if (j < v.size())
+            (big ? init_big : init)[k].push_back(((unsigned long long)sl.epoch << 32) |
+                                                 ((unsigned long long)i << 24) | v[j]);
+        }
+    }
+  }
   // h_init: [the launch header (kMiscWords) | entries | the CTAs' entries]
   size_t ninit = 0, init_off[kParts], init_big_off[kParts];
   for (int k = 0; k < kParts; ++k) {
@@ -802,11 +892,18 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
     L.head_big = sl.d_misc.p + kMiscBig + 2 * k;
     L.tail_big = sl.d_misc.p + kMiscBig + 2 * k + 1;
     L.group_ctas = 0;
+    if (rows[k]) {
+      L.rows = 1;
+      L.total = rows_small[k];
+      L.total_big = rows_large[k];
+      L.done = nullptr;
+    }
     slot0 += part_tasks[k];
   }
   for (int k = 0; k < kParts; ++k) {
     sig.push_back(variant[k]);
     sig.push_back(shape[k].patch);
+    sig.push_back(rows[k]);
     Ls[k].patch8 = shape[k].patch;
   }
   int nparts = 0, order[kParts];
@@ -831,9 +928,20 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
       for (int i = 0; i < n; ++i)
         if (part_of(sl.h_frames.p[i]) == k && params[i].predictor_mode == RME_PRED_STANDALONE)
           big += (int64_t)sl.h_frames.p[i].big_end * sl.h_frames.p[i].nref;
-    const int share = shape[k].groups == 2 ? c->nsm / 2 : shape[k].groups == 1 ? c->nsm / 4 : 0;
-    const int g = big > 0 && share > 0 ? (int)std::min<int64_t>({(int64_t)share, big, (int64_t)cap - 1}) : 0;
-    const int64_t small = part_tasks[k] - big;
+    const int share = shape[k].groups == 3 ? cap / 2
+                      : shape[k].groups == 2 ? c->nsm / 2
+                      : shape[k].groups == 1 ? c->nsm / 4
+                                             : 0;
+    int g = big > 0 && share > 0 ? (int)std::min<int64_t>({(int64_t)share, big, (int64_t)cap - 1}) : 0;
+    int64_t small = part_tasks[k] - big;
+    if (rows[k]) {
+      // A CTA per row of large blocks (at least one when there are any), a
+      // warp per row of small ones.
+      g = rows_large[k] > 0
+              ? (int)std::max<int64_t>(1, std::min<int64_t>({(int64_t)std::max(share, 1), rows_large[k], (int64_t)cap - 1}))
+              : 0;
+      small = rows_small[k];
+    }
     const int solo = (int)std::max<int64_t>(1, std::min<int64_t>(cap - g, (small + kWarpsPerBlock - 1) / kWarpsPerBlock));
     Ls[k].group_ctas = g;
     grid[k] = g + solo;
@@ -967,6 +1075,22 @@ int ctx_standalone_frame(void* ctx, const rme_frame* f, const rme_params* p, Fra
   *nroots = (int)dp->ready.size();
   return 0;
 }
+
+bool ctx_frame_rows(void* ctx, const rme_frame* f, const rme_params* p, const uint32_t** rows, int* nrows,
+                    const uint32_t** rows_big, int* nrows_big) {
+  Ctx* c = (Ctx*)ctx;
+  if (!c || !f || !p || p->predictor_mode != RME_PRED_STANDALONE || p->hevc_amp != 0) return false;
+  auto it = c->pics.find(f->src_id);
+  if (it == c->pics.end() || it->second->d.codec != RME_CODEC_HEVC) return false;
+  int rc = 0;
+  const Deps* dp = get_deps(c, it->second->d, p, f->nref, &rc);
+  if (!dp || !dp->d_rows) return false;
+  *rows = dp->d_rows;
+  *nrows = (int)dp->rows.size();
+  *rows_big = dp->d_rows + dp->rows.size();
+  *nrows_big = (int)dp->rows_big.size();
+  return true;
+}
 }  // namespace rme
 
 extern "C" {
@@ -1077,6 +1201,14 @@ cudaError_t take_buffer(Ctx* c, int32_t id, Picture* pic, cudaStream_t s) {
 
 int rme_picture_upload(void* ctx, int32_t pic_id, const rme_picture_desc* d, const void* luma, int32_t as_ref,
                        void* stream) {
+  return rme::ctx_picture_upload(ctx, pic_id, d, luma, as_ref, as_ref != 0, stream);
+}
+
+}  // extern "C"
+
+namespace rme {
+int ctx_picture_upload(void* ctx, int32_t pic_id, const rme_picture_desc* d, const void* luma, int32_t as_ref,
+                       bool build_planes, void* stream) {
   Ctx* c = (Ctx*)ctx;
   if (!c) return RME_EINVAL;
   if (!valid_desc(d) || !luma || pic_id < 0) return fail(c, RME_EINVAL, "bad picture description");
@@ -1094,7 +1226,7 @@ int rme_picture_upload(void* ctx, int32_t pic_id, const rme_picture_desc* d, con
   CK(cudaMemcpy2DAsync(origin, (size_t)stride * bps, luma, (size_t)d->stride * bps, (size_t)d->width * bps, d->height,
                        cudaMemcpyHostToDevice, s));
   CK(launch_pad_plane(origin, d->bit_depth, d->width, d->height, stride, pic->planes, pic->cw, pic->ch, pic->pad, s));
-  if (as_ref) {
+  if (as_ref && build_planes) {
     if (h264) CK(launch_h264_hpel(pic->planes, d->bit_depth, pic->cw, pic->ch, pic->pad, s));
     else CK(launch_hevc_phases(pic->planes, d->bit_depth, pic->cw, pic->ch, pic->pad, s));
   }
@@ -1103,6 +1235,9 @@ int rme_picture_upload(void* ctx, int32_t pic_id, const rme_picture_desc* d, con
   c->pics[pic_id] = std::move(pic);
   return 0;
 }
+}  // namespace rme
+
+extern "C" {
 
 int rme_picture_upload_chroma(void* ctx, int32_t pic_id, const void* cb, const void* cr, int32_t cstride,
                               void* stream) {

@@ -67,7 +67,19 @@ struct FrameDesc {
   int32_t ntasks;
   uint32_t gen;  // the resident engine: this frame's generation in its slot
   int32_t big_end;  // HEVC STANDALONE: tasks below big_end * nref are blocks of 32 or more
+  // The row form (HEVC STANDALONE without AMP, latency kernels and the
+  // engine): a warp or a CTA owns a row of one level and reference and
+  // searches its blocks left to right; per task its motion vector is
+  // published as one word, (tag << 32) | mv, which the rows below and the
+  // next size's rows wait for. Null: the dataflow form.
+  unsigned long long* mvf;
+  uint32_t tag;     // nonzero, new for every search of the buffer (the launch's epoch, the slot's generation)
+  int32_t nrows;    // rows of the frame, both kinds (the engine counts them to completion)
 };
+
+// A row-form queue entry's low 24 bits: level (bits 22-23), reference
+// (20-21), row (0-19).
+constexpr uint32_t row_entry(int l, int r, int row) { return (uint32_t)l << 22 | (uint32_t)r << 20 | (uint32_t)row; }
 
 // A launch's dataflow queue: a task is pushed when its last dependency
 // finishes (the frames' dependency-free tasks are pushed by the host), and
@@ -95,8 +107,9 @@ struct LaunchDesc {
   int32_t group_ctas;
   int32_t patch8;                // the latency form: 8x8 blocks refine from staged phase patches
   int32_t ring_shift;            // nonzero: the resident engine's ring of
-                                 // 2^ring_shift slots (slot idx holds
-                                 // ((idx >> ring_shift) + 1) << 32 | entry)
+                                 // 2^ring_shift slots (ring_entry)
+  int32_t rows;                  // the row form: the queues hold rows, all pushed by the host
+  int64_t total_big;             // the row form: rows in the CTAs' queue
 };
 
 // The resident engine (rme_engine.cu): one search kernel that stays on the
@@ -108,7 +121,7 @@ constexpr int kEngineFrames = 256;  // frame slots (the queue's 8-bit frame fiel
 struct EngineCtl {
   uint32_t* fdone;                 // per frame slot: its tasks finished
   volatile uint32_t* hflags;       // mapped host memory: per slot, the generation finished
-  volatile const uint32_t* hstop;  // mapped host memory: nonzero once idle warps may leave
+  const uint32_t* stop;            // device memory: nonzero once waiting warps are to leave
   uint32_t idle_polls;             // reserved
 };
 cudaError_t launch_engine(const LaunchDesc& L, const EngineCtl& E, int grid, cudaStream_t s);
@@ -134,6 +147,17 @@ void engine_release(Engine* g, int slot);
 // its task count, dependency template and root tasks (device memory).
 int ctx_standalone_frame(void* ctx, const rme_frame* f, const rme_params* p, FrameDesc* fd, int* ntasks,
                          const int32_t** pending_tmpl, const uint32_t** roots, int* nroots);
+// rme_picture_upload with the choice to leave a reference picture's
+// interpolated planes for a later rme_picture_build_planes on the same
+// stream (the serving loop publishes the picture's own search first: it
+// reads only the integer plane).
+int ctx_picture_upload(void* ctx, int32_t pic_id, const rme_picture_desc* d, const void* luma, int32_t as_ref,
+                       bool build_planes, void* stream);
+// The same frame's rows (row_entry; device memory) when it can run in the
+// row form: rows a warp runs, then rows a CTA runs, each in the order every
+// row comes after the rows it reads. False for other frames.
+bool ctx_frame_rows(void* ctx, const rme_frame* f, const rme_params* p, const uint32_t** rows, int* nrows,
+                    const uint32_t** rows_big, int* nrows_big);
 
 // Host helpers shared by the entry points (rme_capi.cu; f32 arithmetic
 // compiled without contraction, so it rounds as the reference's Rust does).

@@ -101,10 +101,80 @@ __device__ void group_loop(const LaunchDesc& L, unsigned char* smem_raw) {
   if (tid < 5) atomicAdd(&L.counters[tid], gs.cnt[tid]);
 }
 
+// The row form: a CTA takes rows of 32x32 or 64x64 blocks (hevc_group_row)
+// from the CTAs' queue, a warp rows of 16x16 or 8x8 blocks (hevc_row) from
+// the warps' queue, until each queue is empty. The host pushed every row, in
+// an order where each comes after the rows it reads, so a row's owner only
+// waits for rows that are owned already.
+template <class S>
+__device__ void group_row_loop(const LaunchDesc& L, unsigned char* smem_raw) {
+  GroupSmem<S>& gs = *reinterpret_cast<GroupSmem<S>*>(smem_raw);
+  const int tid = threadIdx.x;
+  if (tid < 6) gs.cnt[tid] = 0;
+  const uint32_t epoch = __ldg(L.epoch);
+  __syncthreads();
+  for (;;) {
+    if (tid == 0) {
+      const unsigned long long idx = atomicAdd(L.head_big, 1ull);
+      gs.bc[7] = idx >= (unsigned long long)L.total_big ? kPopDone : pop_slot(L, idx, epoch, true);
+    }
+    __syncthreads();
+    const uint32_t e = gs.bc[7];
+    __syncthreads();
+    if (e == kPopDone) break;
+    if (e == 0xffffffffu) continue;
+    const int f = (int)(e >> 24);
+    const FrameDesc& F = L.frames[f];
+    if ((sizeof(S) == 1) != (F.bd == 8)) {
+      if (tid == 0) atomicOr(L.status, kStatusBadTask);
+      continue;
+    }
+    hevc_group_row<S>(L, F, f, e & 0xffffffu, gs, tid);
+  }
+  __syncthreads();
+  if (tid < 5) atomicAdd(&L.counters[tid], gs.cnt[tid]);
+}
+
+template <class S>
+__device__ void row_loop(const LaunchDesc& L, WarpSmem<S>& sm, int lane) {
+  const uint32_t epoch = __ldg(L.epoch);
+  for (;;) {
+    unsigned long long idx = 0;
+    if (lane == 0) idx = atomicAdd(L.head, 1ull);
+    idx = __shfl_sync(kFull, idx, 0);
+    if (idx >= (unsigned long long)L.total) break;
+    uint32_t e = 0;
+    if (lane == 0) e = pop_slot(L, idx, epoch);
+    e = __shfl_sync(kFull, e, 0);
+    if (e == 0xffffffffu) continue;
+    const int f = (int)(e >> 24);
+    const FrameDesc& F = L.frames[f];
+    if ((sizeof(S) == 1) != (F.bd == 8)) {
+      if (lane == 0) atomicOr(L.status, kStatusBadTask);
+      continue;
+    }
+    hevc_row<S, true>(L, F, f, e & 0xffffffu, sm, lane);
+  }
+}
+
 template <class S, int CODEC, int MINB, bool SPEC>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, MINB) search_kernel(LaunchDesc L) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   if constexpr (SPEC && CODEC == RME_CODEC_HEVC) {
+    if (L.rows) {
+      if ((int)blockIdx.x < L.group_ctas) {
+        group_row_loop<S>(L, smem_raw);
+      } else {
+        const int lane = threadIdx.x & 31;
+        WarpSmem<S>& sm = reinterpret_cast<WarpSmem<S>*>(smem_raw)[threadIdx.x >> 5];
+        if (lane < 5) sm.cnt[lane] = 0;
+        __syncwarp();
+        row_loop<S>(L, sm, lane);
+        __syncwarp();
+        if (lane < 5) atomicAdd(&L.counters[lane], sm.cnt[lane]);
+      }
+      return;
+    }
     if ((int)blockIdx.x < L.group_ctas) {
       group_loop<S>(L, smem_raw);
       return;

@@ -3,8 +3,12 @@
 // distortion and interpolation-plane reads, the dataflow queue. Each file
 // includes it into its own anonymous namespace. Reads of pictures go
 // through RME_LD32: the read-only cache path in the batched kernels (a
-// launch's pictures do not change while it runs), L2 only in the engine
-// (pictures are refilled while it runs, so no stale L1 line may be read).
+// launch's pictures do not change while it runs); in the engine, where
+// picture slots are refilled while the kernel runs, ordinary cached loads,
+// which the memory model keeps fresh: a frame's pictures are written before
+// its entries are released into the ring, the warp or CTA that takes an
+// entry acquires it (then synchronises its threads) before any read, and a
+// slot is refilled only after every frame reading it has completed.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -13,7 +17,7 @@
 #include "rme_internal.h"
 
 #ifdef RME_PICTURES_CHANGE_IN_FLIGHT
-#define RME_LD32(p) __ldcg(p)
+#define RME_LD32(p) __ldca(p)
 #else
 #define RME_LD32(p) __ldg(p)
 #endif
@@ -265,14 +269,26 @@ __device__ __forceinline__ const S* plane_at(const DevPlanes& p, int plane, int 
 
 // ---- dataflow queue ---------------------------------------------------------
 
+// A ring slot of the resident engine holds the lap tag of its index (1 to
+// 65535, so that consecutive laps differ and a zeroed slot matches none),
+// the frame's generation in its slot (low 16 bits), frame and task.
+__device__ __forceinline__ uint32_t ring_lap(int ring_shift, unsigned long long idx) {
+  return (uint32_t)((idx >> ring_shift) % 65535ull) + 1u;
+}
+__device__ __forceinline__ unsigned long long ring_entry(int ring_shift, unsigned long long idx, uint32_t gen, int f,
+                                                         int t) {
+  return (unsigned long long)ring_lap(ring_shift, idx) << 48 | (unsigned long long)(gen & 0xffffu) << 32 |
+         ((uint32_t)f << 24) | (uint32_t)t;
+}
+
 // Push task `t` of frame `f` (one thread): its last dependency just
-// finished. `big`: into the queue of the tasks a CTA runs.
-__device__ __forceinline__ void push_ready(const LaunchDesc& L, int f, int t, bool big = false) {
+// finished. `big`: into the queue of the tasks a CTA runs; `gen`: the
+// frame's generation (the engine's rings).
+__device__ __forceinline__ void push_ready(const LaunchDesc& L, int f, int t, bool big = false, uint32_t gen = 0) {
   unsigned long long* const ready = big ? L.ready_big : L.ready;
   const unsigned long long idx = atomicAdd(big ? L.tail_big : L.tail, 1ull);
   if (L.ring_shift) {  // the engine's ring: the host keeps fewer tasks in flight than it has slots
-    const unsigned long long lap = (idx >> L.ring_shift) + 1ull;
-    st_release64(ready + (idx & ((1ull << L.ring_shift) - 1ull)), (lap << 32) | ((uint32_t)f << 24) | (uint32_t)t);
+    st_release64(ready + (idx & ((1ull << L.ring_shift) - 1ull)), ring_entry(L.ring_shift, idx, gen, f, t));
   } else if (idx < (unsigned long long)L.total)
     st_release64(ready + idx, ((unsigned long long)__ldg(L.epoch) << 32) | ((uint32_t)f << 24) | (uint32_t)t);
   else
@@ -300,7 +316,7 @@ __device__ __forceinline__ int release_lanes(const LaunchDesc& L, const FrameDes
     keep = __ffs(m) - 1;
     cont = (f << 24) | __shfl_sync(kFull, dtask, keep);
   }
-  if (ready && lane != keep) push_ready(L, f, dtask, big);
+  if (ready && lane != keep) push_ready(L, f, dtask, big, F.gen);
   return cont;
 }
 
@@ -312,6 +328,33 @@ __device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long l
   unsigned long long v;
   asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
+}
+
+__device__ __forceinline__ void st_relaxed64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// The row form: the published word of a task another row owns, waited for
+// until it carries this search's tag (bounded: kSpinLimit polls with
+// backoff, then the status word's timeout bit and a zero vector, so that a
+// lost dependency ends the search with an error instead of hanging it). The
+// caller has loaded the word once already (`w`), while it staged its source.
+__device__ __noinline__ unsigned long long wait_word(const LaunchDesc& L, const unsigned long long* p, uint32_t tag,
+                                                     unsigned long long w) {
+  uint32_t ns = 32;
+  for (uint32_t it = 0; (uint32_t)(w >> 32) != tag; ++it) {
+    if (it >= kSpinLimit) {
+      atomicOr(L.status, kStatusWaitTimeout);
+      return (unsigned long long)tag << 32;
+    }
+    __nanosleep(ns);
+    if (ns < 256) ns <<= 1;
+    w = ld_relaxed64(p);
+  }
+  return w;
+}
+__device__ __forceinline__ unsigned long long mv_word(uint32_t tag, int mvx, int mvy) {
+  return (unsigned long long)tag << 32 | (uint32_t)(uint16_t)(int16_t)mvx | (uint32_t)(uint16_t)(int16_t)mvy << 16;
 }
 
 constexpr uint32_t kPopDone = 0xfffffffeu;  // every task of the launch is done
@@ -444,6 +487,25 @@ __device__ __forceinline__ uint32_t sad_part(const uint32_t* src, int w, int h, 
   uint32_t acc = 0;
   for (int row = sub; row < h; row += 8)
     for (int k = 0; k < wr; ++k) acc += vsad(src[row * wr + k], ldw(rp + (ptrdiff_t)row * stride + k * SPW), S());
+  return acc;
+}
+
+// A 16x16 candidate's SAD over two lanes: rows half * 8 .. half * 8 + 7,
+// loaded four rows at a time.
+template <class S>
+__device__ __forceinline__ uint32_t sad16_half(const uint32_t* src, const S* rp, int stride, int half) {
+  constexpr int SPW = 4 / sizeof(S), WR = 16 / SPW;
+  uint32_t acc = 0;
+#pragma unroll
+  for (int r0 = 0; r0 < 8; r0 += 4) {
+    uint32_t a[4][WR];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) ldwords<WR>(rp + (ptrdiff_t)(half * 8 + r0 + r) * stride, a[r]);
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int k = 0; k < WR; ++k) acc += vsad(src[(half * 8 + r0 + r) * WR + k], a[r][k], S());
+  }
   return acc;
 }
 
@@ -595,11 +657,10 @@ template <class S>
 __device__ __forceinline__ void refine8_patched(WarpSmem<S>& sm, const DevPlanes& R, int x, int y, int bx, int by,
                                                 float lam, int p0x, int p0y, int p1x, int p1y, int quarter_cross,
                                                 int lane, int& bmx, int& bmy, uint32_t& bc, uint32_t& bsatd,
-                                                uint32_t& nsatd, bool staged, uint32_t staged_off) {
+                                                uint32_t& nsatd) {
   using G = PatchGeo<S>;
   uint32_t* patch = sm.src + kPatchOff;
-  // `staged`: the diamond's last step loaded these patches already.
-  const uint32_t off = staged ? staged_off : stage_patches<S>(patch, R, x + bx - 1, y + by - 1, lane);
+  const uint32_t off = stage_patches<S>(patch, R, x + bx - 1, y + by - 1, lane);
   __syncwarp();
   const int imx = bx * 4, imy = by * 4;
   // The start and the half ring (lane 0 the start, lanes 1..8 the ring in
@@ -659,8 +720,10 @@ __device__ __forceinline__ void refine8_patched(WarpSmem<S>& sm, const DevPlanes
 }
 
 // Returns a task it made ready to run next (frame << 24 | task), or -1.
-// SPEC: the latency kernels' two-rounds-per-step 8x8 diamond.
-template <class S, bool SPEC>
+// SPEC: the latency kernels' two-rounds-per-step 8x8 and 16x16 diamond.
+// ROW: the row form (the neighbours' vectors from their published words,
+// this task's published in turn; nothing released).
+template <class S, bool SPEC, bool ROW = false>
 __device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, WarpSmem<S>& sm, int lane) {
   int r, x, y, w, h, ns;
   int p0x, p0y, p1x, p1y;
@@ -754,9 +817,16 @@ __device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
       const int Np = F.size[l - 1], px = x / Np, py = y / Np;
       if (px < F.nbx[l - 1] && py < F.nby[l - 1]) didx = (F.base[l - 1] + py * F.nbx[l - 1] + px) * F.nref + r;
     }
-    const uint32_t dv = didx >= 0 ? ldcg_u32(&F.out[didx].mv) : 0u;
+    uint32_t dv = 0u;
+    unsigned long long dw = 0ull;
+    if (ROW) {
+      if (didx >= 0) dw = ld_relaxed64(F.mvf + didx);
+    } else {
+      dv = didx >= 0 ? ldcg_u32(&F.out[didx].mv) : 0u;
+    }
     // The source block is staged while those loads are in flight.
     stage_src<S>(sm.src, plane_at<S>(F.src, 0, x, y), F.src.stride, w, h, lane);
+    if (ROW && didx >= 0) dv = (uint32_t)wait_word(L, F.mvf + didx, F.tag, dw);
     const uint32_t have = __ballot_sync(kFull, didx >= 0);
     const uint32_t va = __shfl_sync(kFull, dv, 0), vb = __shfl_sync(kFull, dv, 1), vp = __shfl_sync(kFull, dv, 2);
     int na = 0, ax = 0, ay = 0, cx = 0, cy = 0;
@@ -829,13 +899,7 @@ __device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
   uint32_t bcost = kInf;
   int state = nk > 0 ? 0 : 1, c0 = 0, it = 0, rings = 0;
   bool moved = false;
-  const bool spec = SPEC && w == 8 && h == 8;
-  // The 8x8 refinement's patches, loaded during the diamond's step: a step
-  // that moves nothing leaves the best where the patches are centred.
-  const bool patched = spec && L.patch8 && ((R.stride * (int)sizeof(S)) & 3) == 0 &&
-                       ((R.plane_elems * (int64_t)sizeof(S)) & 3) == 0;
-  bool pre_staged = false;
-  uint32_t pre_off = 0;
+  const bool spec = SPEC && w == h && (w == 8 || w == 16);
   for (;;) {
     if (state == 1 && it >= 2 * range) {  // the diamond has settled
       if (rings >= F.search_rings) break;
@@ -847,7 +911,7 @@ __device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
       cyr = by;
     }
     if (spec && state == 1) {
-      // 8x8 in a latency kernel: two diamond rounds per step, fewer
+      // 8x8 and 16x16 in a latency kernel: two diamond rounds per step, fewer
       // dependent steps on the frame's critical path for more loads per step
       // (the throughput kernels keep one round per step, and leave this code
       // out of their text).
@@ -865,20 +929,15 @@ __device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
       }
       const bool ok = abs(fx - ox) <= range && abs(fy - oy) <= range && fx >= lox && fx <= hix && fy >= loy &&
                       fy <= hiy;
-      uint32_t pv[PatchGeo<S>::PER];
-      uint32_t poff = 0;
-      if (patched) poff = load_patches<S>(pv, R, x + bx - 1, y + by - 1, lane);
-      uint32_t part = ok ? sad8_half<S>(sm.src, org + (ptrdiff_t)fy * stride + fx, stride, hf) : 0u;
+      uint32_t part = 0u;
+      if (ok)
+        part = w == 8 ? sad8_half<S>(sm.src, org + (ptrdiff_t)fy * stride + fx, stride, hf)
+                      : sad16_half<S>(sm.src, org + (ptrdiff_t)fy * stride + fx, stride, hf);
       part += __shfl_xor_sync(kFull, part, 1);
       const uint32_t cost = ok ? part + hevc_rate(lam, fx * 4, fy * 4, p0x, p0y, p1x, p1y) : kInf;
       nsad += __popc(__ballot_sync(kFull, ok && hf == 0 && q < 4));
       const Pick pa = warp_min(q < 4 ? cost : kInf);
       if (!(pa.cost < bcost)) {
-        if (patched) {
-          store_patches<S>(sm.src + kPatchOff, pv, lane);
-          pre_staged = true;
-          pre_off = poff;
-        }
         it = 2 * range;
         continue;
       }
@@ -971,31 +1030,15 @@ __device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
   const int ntiles = tw * th;
   // Patches need every plane and row a whole number of words apart (true
   // of the library's pictures: 128-byte strides).
-  if (spec && L.patch8 && ((R.stride * (int)sizeof(S)) & 3) == 0 &&
+  if (spec && w == 8 && L.patch8 && ((R.stride * (int)sizeof(S)) & 3) == 0 &&
       ((R.plane_elems * (int64_t)sizeof(S)) & 3) == 0) {
     refine8_patched<S>(sm, R, x, y, bx, by, lam, p0x, p0y, p1x, p1y, F.quarter_cross, lane, bmx, bmy, bc, bsatd,
-                       nsatd, pre_staged, pre_off);
+                       nsatd);
   } else {
-  // The latency form folds pass 1 (the half ring's last point) into pass 0
-  // where the block has at most 32 tiles: lane t also scores its tile t, so
-  // both passes' loads are in flight together; the in-order walk is kept
-  // (pass 0's winner, then the last point only when strictly cheaper).
-  const bool fold = SPEC && ntiles <= 32;
   for (int pass = 0; pass < 3; ++pass) {
-    if (fold && pass == 1) continue;
     const int G = pass == 1 ? 32 : 4, c = pass == 1 ? 8 : lane >> 2, gsub = pass == 1 ? lane : lane & 3;
     int mx, my;
     bool ok;
-    uint32_t part8 = 0;  // folded: this lane's tile of the last half point
-    int mx8 = 0, my8 = 0;
-    if (fold && pass == 0) {
-      mx8 = imx + 2;
-      my8 = imy + 2;
-      if (lane < ntiles) {
-        const S* pp8 = plane_at<S>(R, (my8 & 3) * 4 + (mx8 & 3), x + (mx8 >> 2), y + (my8 >> 2));
-        part8 = satd_part<S>(sm.src, wr, tw, ntiles, pp8, stride, lane, 32);
-      }
-    }
     if (pass < 2) {
       const int q = c == 0 ? 4 : (c <= 4 ? c - 1 : c);
       mx = imx + (q % 3 - 1) * 2;
@@ -1019,22 +1062,14 @@ __device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
       bmx = __shfl_sync(kFull, mx, p.lane);
       bmy = __shfl_sync(kFull, my, p.lane);
     }
-    if (fold && pass == 0) {
-      for (int o = 16; o > 0; o >>= 1) part8 += __shfl_xor_sync(kFull, part8, o);
-      const uint32_t cost8 = part8 + hevc_rate(lam, mx8, my8, p0x, p0y, p1x, p1y);
-      if (cost8 < bc) {
-        bc = cost8;
-        bsatd = part8;
-        bmx = mx8;
-        bmy = my8;
-      }
-    }
   }
   nsatd += 9;
   }
   write_result(out, bmx, bmy, r, bc, bsatd, imx, imy, int_cost, nsad, nsatd, lane);
   int cont = -1;
-  if (F.mode != RME_PRED_GIVEN && !amp_unit) {
+  if (ROW) {
+    if (lane == 0) st_relaxed64(F.mvf + t, mv_word(F.tag, bmx, bmy));
+  } else if (F.mode != RME_PRED_GIVEN && !amp_unit) {
     // The tasks reading this result: right and lower neighbours of this
     // level, the blocks of the next evaluated size inside this one, this
     // CU's AMP units; each lane releases one of them. Lane 0's result is
@@ -1274,7 +1309,7 @@ __device__ __forceinline__ void cta_satd(GroupSmem<S>& gs, int b, const DevPlane
 // search_full + refine_subpel of one STANDALONE square block of N in {32, 64}
 // by the whole CTA (all threads call). Returns a task it made ready to run
 // next (frame << 24 | task; another group task) or -1.
-template <class S, int N>
+template <class S, int N, bool ROW = false>
 __device__ int hevc_group_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, GroupSmem<S>& gs, int tid) {
   constexpr int SPW = 4 / sizeof(S), WR = N / SPW;
   const int lane = tid & 31;
@@ -1285,15 +1320,20 @@ __device__ int hevc_group_task(const LaunchDesc& L, const FrameDesc& F, int f, i
   const int x = lbx * N, y = lby * N;
   // The left, upper and parent results (threads 0..2), while all threads
   // stage the source block.
+  int didx = -1;
+  unsigned long long dw = 0ull;
   if (tid < 3) {
-    int didx = -1;
     if (tid == 0 && lbx > 0) didx = (F.base[l] + local - 1) * F.nref + r;
     if (tid == 1 && lby > 0) didx = (F.base[l] + local - nbx) * F.nref + r;
     if (tid == 2 && l > 0) {
       const int Np = F.size[l - 1], px = x / Np, py = y / Np;
       if (px < F.nbx[l - 1] && py < F.nby[l - 1]) didx = (F.base[l - 1] + py * F.nbx[l - 1] + px) * F.nref + r;
     }
-    gs.bc[tid] = didx >= 0 ? ldcg_u32(&F.out[didx].mv) : 0u;
+    if (ROW) {
+      if (didx >= 0) dw = ld_relaxed64(F.mvf + didx);
+    } else {
+      gs.bc[tid] = didx >= 0 ? ldcg_u32(&F.out[didx].mv) : 0u;
+    }
     gs.bc[3 + tid] = didx >= 0 ? 1u : 0u;
   }
   if (tid < 64) gs.cost[tid >> 5][tid & 31] = 0u;  // the first step's buffer (and the next)
@@ -1304,6 +1344,7 @@ __device__ int hevc_group_task(const LaunchDesc& L, const FrameDesc& F, int f, i
       gs.src[i] = ldw(so + (ptrdiff_t)row * F.src.stride + wd * SPW);
     }
   }
+  if (ROW && tid < 3) gs.bc[tid] = didx >= 0 ? (uint32_t)wait_word(L, F.mvf + didx, F.tag, dw) : 0u;
   __syncthreads();
   int p0x = 0, p0y = 0, p1x = 0, p1y = 0, na = 0;
   if (gs.bc[3]) {
@@ -1494,8 +1535,10 @@ __device__ int hevc_group_task(const LaunchDesc& L, const FrameDesc& F, int f, i
     gs.cnt[2] += nsatd;
     gs.cnt[3] += (unsigned long long)nsad * N * N;
     gs.cnt[4] += (unsigned long long)nsatd * N * N;
+    if (ROW) st_relaxed64(F.mvf + t, mv_word(F.tag, bmx, bmy));
   }
   __syncthreads();
+  if (ROW) return -1;
   // The tasks reading this result (warp 0 releases them, one per lane):
   // right and lower neighbours, the next size's blocks inside this one,
   // this CU's AMP units. A group task made ready is kept, if this CTA has
@@ -1531,6 +1574,48 @@ __device__ int hevc_group_task(const LaunchDesc& L, const FrameDesc& F, int f, i
   }
   __syncthreads();
   return (int)gs.bc[6];
+}
+
+// ---- the row form ------------------------------------------------------------
+
+// One row of an HEVC STANDALONE frame (a row_entry), its blocks left to right
+// by this warp (8x8 and 16x16) or this CTA (32x32 and 64x64). A block waits
+// only for the published vectors of its upper neighbour (the row above,
+// which its owner started earlier and runs ahead of this one) and of its
+// parent one size up; its left neighbour is this row's previous block. No
+// dependency counts, no queue traffic between the blocks of a row.
+__device__ __forceinline__ bool row_ok(const FrameDesc& F, uint32_t e, int& l, int& r, int& row) {
+  l = (int)((e >> 22) & 3u);
+  r = (int)((e >> 20) & 3u);
+  row = (int)(e & 0xfffffu);
+  return F.mvf != nullptr && F.codec == RME_CODEC_HEVC && F.mode == RME_PRED_STANDALONE && F.amp == 0 &&
+         l < F.nlevels && r < F.nref && row < F.nby[l];
+}
+
+template <class S, bool SPEC>
+__device__ void hevc_row(const LaunchDesc& L, const FrameDesc& F, int f, uint32_t e, WarpSmem<S>& sm, int lane) {
+  int l, r, row;
+  if (!row_ok(F, e, l, r, row) || F.size[l] > 16) {
+    if (lane == 0) atomicOr(L.status, kStatusBadTask);
+    return;
+  }
+  const int nbx = F.nbx[l], t0 = (F.base[l] + row * nbx) * F.nref + r;
+  for (int bx = 0; bx < nbx; ++bx) hevc_task<S, SPEC, true>(L, F, f, t0 + bx * F.nref, sm, lane);
+}
+
+template <class S>
+__device__ void hevc_group_row(const LaunchDesc& L, const FrameDesc& F, int f, uint32_t e, GroupSmem<S>& gs,
+                               int tid) {
+  int l, r, row;
+  if (!row_ok(F, e, l, r, row) || (F.size[l] != 32 && F.size[l] != 64)) {
+    if (tid == 0) atomicOr(L.status, kStatusBadTask);
+    return;
+  }
+  const int nbx = F.nbx[l], t0 = (F.base[l] + row * nbx) * F.nref + r;
+  if (F.size[l] == 64)
+    for (int bx = 0; bx < nbx; ++bx) hevc_group_task<S, 64, true>(L, F, f, t0 + bx * F.nref, gs, tid);
+  else
+    for (int bx = 0; bx < nbx; ++bx) hevc_group_task<S, 32, true>(L, F, f, t0 + bx * F.nref, gs, tid);
 }
 
 // ---- H.264 ------------------------------------------------------------------

@@ -219,11 +219,22 @@ void Server::start(Request& r) {
     st = &streams[r.stream];
   }
   const rme_frame f = frame_of(*st, r.frame);
-  r.status = rme_picture_upload(ctx, f.src_id, &st->d, r.luma, 1, upload);
+  // The picture's own search reads only its integer plane: it is handed to
+  // the engine before the interpolated planes, which only later frames
+  // read, are built behind it on the same stream.
+  r.status = rme::ctx_picture_upload(ctx, f.src_id, &st->d, r.luma, 1, false, upload);
   if (r.status == 0 && f.nref > 0) {
-    submit_search(r, *st);
+    const size_t ns = searching.size(), nb = submitting.size(), nc = copying.size();
+    submit_search(r, *st);  // the request goes into one of the three lists
+    const int rc = rme_picture_build_planes(ctx, f.src_id, upload);
+    Request* q = searching.size() > ns ? &searching.back()
+                 : submitting.size() > nb ? &submitting.back()
+                 : copying.size() > nc ? &copying.back()
+                                       : nullptr;
+    if (rc != 0 && q && q->status == 0) q->status = rc;
     return;
   }
+  if (r.status == 0) r.status = rme_picture_build_planes(ctx, f.src_id, upload);
   // Not searched (a stream's first frame) or failed: complete once the
   // upload has read the frame's buffer.
   r.slot = -1;

@@ -345,20 +345,44 @@ def test_the_gpu_reproduces_the_golden_fixtures(ms, name):
     assert_results_equal(got, z["results"].view(capi.RESULT_DTYPE), name)
 
 
-@pytest.mark.parametrize("bd", [8, 10])
-def test_every_launch_shape_gives_the_oracles_results(bd):
+@pytest.mark.parametrize("bd,amp", [(8, 0b1001), (10, 0b1001), (8, 0), (10, 0)])
+def test_every_launch_shape_gives_the_oracles_results(bd, amp):
     """A fresh context times each launch shape of a class on its first
     launches (occupancy variant, CTAs for the 32x32 and 64x64 blocks or
-    none, staged 8x8 patches or cache reads): the same frame searched once
-    per shape, and once more on the chosen one, equals the oracle every
-    time."""
+    none, staged 8x8 patches or cache reads, the row form where the frame
+    has no AMP units): the same frame searched once per shape, and once
+    more on the chosen one, equals the oracle every time."""
     import rivet_h26x_codecs_b200 as rme
     seq = synth.make_sequence(HEVC, 320, 192, bd, 3, 77 + bd, 64, 96, 2.0)
-    p = oracle.params(HEVC, 30, hevc_search_range=40, hevc_search_rings=1, hevc_amp=0b1001)
+    p = oracle.params(HEVC, 30, hevc_search_range=40, hevc_search_rings=1, hevc_amp=amp)
     want = oracle.frame_search(HEVC, bd, seq.frames[2], [seq.frames[1], seq.frames[0]], p)
     with rme.MotionSearch(0) as ms2:
         for i, f in enumerate(seq.frames):
             ms2.upload(i, f, HEVC, bd, as_ref=True)
-        for k in range(7):
+        for k in range(9):
             got = ms2.search(2, [1, 0], p)
             assert_results_equal(got, want, f"launch {k}")
+
+
+@pytest.mark.parametrize("bd", [8, 10])
+def test_row_form_batch_of_frames_of_two_sizes(bd):
+    """A latency launch of three frames (two sizes, one and two references,
+    the 16x16 level left out of one): in the row form the frames' rows are
+    interleaved in the queues; each frame equals the oracle."""
+    import rivet_h26x_codecs_b200 as rme
+    a = synth.make_sequence(HEVC, 256, 160, bd, 3, 31 + bd, 48, 64, 2.0).frames
+    b = synth.make_sequence(HEVC, 192, 128, bd, 2, 41 + bd, 48, 64, 2.0).frames
+    pa = oracle.params(HEVC, 32, hevc_search_range=32)
+    pb = oracle.params(HEVC, 28, hevc_search_range=24, hevc_pu_mask=0b1101)
+    wants = [oracle.frame_search(HEVC, bd, a[2], [a[1], a[0]], pa),
+             oracle.frame_search(HEVC, bd, a[1], [a[0]], pa),
+             oracle.frame_search(HEVC, bd, b[1], [b[0]], pb)]
+    with rme.MotionSearch(0) as ms2:
+        for i, f in enumerate(a):
+            ms2.upload(i, f, HEVC, bd, as_ref=True)
+        for i, f in enumerate(b):
+            ms2.upload(10 + i, f, HEVC, bd, as_ref=True)
+        for k in range(3):
+            got = ms2.search_batch([(2, [1, 0]), (1, [0]), (11, [10])], [pa, pa, pb])
+            for j, (g, w) in enumerate(zip(got, wants)):
+                assert_results_equal(g, w, f"launch {k} frame {j}")

@@ -15,11 +15,12 @@ from _common import assert_results_equal
 H264, HEVC = capi.RME_CODEC_H264, capi.RME_CODEC_HEVC
 pytestmark = pytest.mark.gpu
 
-STREAMS = [  # id, codec, bit depth, width, height, refs, qp
+STREAMS = [  # id, codec, bit depth, width, height, refs, qp (qp 31: HEVC with AMP units)
     (11, HEVC, 8, 192, 128, 2, 32),
     (12, HEVC, 10, 128, 96, 1, 30),
     (13, H264, 8, 96, 64, 1, 28),
     (14, HEVC, 8, 160, 96, 2, 34),
+    (15, HEVC, 8, 128, 96, 2, 31),
 ]
 NFRAMES = 4
 
@@ -29,9 +30,13 @@ def _frames(sid, codec, bd, w, h):
 
 
 def _params(codec, qp):
+    """HEVC frames without AMP run in the engine's row form; the qp-31
+    stream's AMP units keep the dataflow form."""
     p = capi.default_params(codec, qp)
     if codec == HEVC:
         p.hevc_search_range = 32
+        if qp == 31:
+            p.hevc_amp = 0b0101
     return p
 
 
