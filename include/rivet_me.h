@@ -453,7 +453,17 @@ typedef struct {
   uint64_t hbm_budget_bytes;  /* admission limit for resident pictures      */
   int32_t  max_frames_per_launch;
   int32_t  max_streams;
+  int32_t  mode;              /* RME_SERVE_LAUNCHES or RME_SERVE_RESIDENT     */
+  int32_t  reserved;          /* 0                                           */
 } rme_serve_opts;
+
+/* Serving modes. LAUNCHES (0): the frames that arrived since the last launch
+ * go into one search launch of their own as soon as one of three launch
+ * streams is free, so up to three launches overlap on the device (a launch
+ * of one or two frames runs the latency form). RESIDENT (1): one search
+ * kernel stays on the GPU and frames join its queue as they arrive. */
+#define RME_SERVE_LAUNCHES 0
+#define RME_SERVE_RESIDENT 1
 
 typedef struct {
   int64_t  request_id;

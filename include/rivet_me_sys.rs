@@ -42,7 +42,8 @@ use std::os::raw::{c_char, c_void};
     pub base: *const c_void, pub plane_elems: i64, pub stride: i32, pub pad: i32,
 }
 #[repr(C)] #[derive(Clone, Copy, Default)] pub struct rme_serve_opts {
-    pub hbm_budget_bytes: u64, pub max_frames_per_launch: i32, pub max_streams: i32,
+    pub hbm_budget_bytes: u64, pub max_frames_per_launch: i32, pub max_streams: i32, pub mode: i32,
+    pub reserved: i32,
 }
 #[repr(C)] #[derive(Clone, Copy, Default)] pub struct rme_completion {
     pub request_id: i64, pub stream_id: i32, pub status: i32, pub submit_s: f64, pub done_s: f64,

@@ -88,9 +88,12 @@ class Stats(C.Structure):
                 ("satd_samples", C.c_uint64), ("kernel_ms", C.c_float), ("planes_ms", C.c_float)]
 
 
+RME_SERVE_LAUNCHES, RME_SERVE_RESIDENT = 0, 1
+
+
 class ServeOpts(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_frames_per_launch", C.c_int32),
-                ("max_streams", C.c_int32)]
+                ("max_streams", C.c_int32), ("mode", C.c_int32), ("reserved", C.c_int32)]
 
 
 class Completion(C.Structure):

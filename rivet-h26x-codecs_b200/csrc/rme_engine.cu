@@ -108,13 +108,14 @@ __global__ void reset_heads_kernel(LaunchDesc L, uint32_t* stop) {
   *stop = 0u;
 }
 
-// Registers bounded as for three blocks per SM although the grid holds two:
-// the third block's share stays free for the kernels that run beside the
-// resident one (plane builds, frame preparation and publication). Bounded
-// for two, the engine would take every register of every SM, those kernels
-// could not start until it left, and it leaves only once no frame is in
-// flight: the frames queued behind them would never arrive.
-constexpr int kEngineMinBlocks = 3;
+// Registers: at most 112 a thread, so that the grid's two blocks per SM
+// (57,344 registers) leave 8,192 on every SM to the kernels that run beside
+// the resident one (plane builds in blocks of 128 threads, frame
+// preparation and publication, each within that share). With 128, the
+// engine would take every register of every SM, those kernels could not
+// start until it left, and it leaves only once no frame is in flight: the
+// frames queued behind them would never arrive.
+constexpr int kEngineMaxRegs = 112;
 
 // A CTA serving the ring of 32x32 and 64x64 HEVC blocks: all its threads
 // run each task together (hevc_group_task).
@@ -190,7 +191,7 @@ __device__ void engine_group_loop(const LaunchDesc& L, const EngineCtl& E, unsig
   if (tid < 5) atomicAdd(&L.counters[tid], g16.cnt[tid]);
 }
 
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, kEngineMinBlocks) engine_kernel(LaunchDesc L, EngineCtl E) {
+__global__ void __maxnreg__(kEngineMaxRegs) engine_kernel(LaunchDesc L, EngineCtl E) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ FrameDesc fdesc[kWarpsPerBlock];
   if ((int)blockIdx.x < L.group_ctas) {

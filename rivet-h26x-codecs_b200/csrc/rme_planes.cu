@@ -82,11 +82,14 @@ __constant__ int8_t c_qpel[4][8] = {{0, 0, 0, 0, 0, 0, 0, 0},
 
 // The fifteen phases of every padded position: the horizontal pass of each
 // fraction over TY + 7 rows kept in shared memory (int16, as the
-// reference's intermediate), the vertical passes from it.
+// reference's intermediate), the vertical passes from it. Blocks of 32 x 4
+// threads: one fits in the registers the resident engine leaves free on
+// every SM, so a picture's planes are built while the engine runs.
+constexpr int kPhaseTX = 32, kPhaseTY = 4;
 template <class S>
 __global__ void hevc_phase_kernel(const S* g, S* planes, int64_t plane_elems, int stride,
                                   int prow, int pcol, int bd) {
-  constexpr int TX = 32, TY = 8;
+  constexpr int TX = kPhaseTX, TY = kPhaseTY;
   __shared__ int tile[TY + 7][TX + 7];
   __shared__ int16_t hp[3][TY + 7][TX];
   int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
@@ -164,7 +167,7 @@ cudaError_t launch_h264_hpel(DevPlanes p, int bd, int cw, int ch, int pad, cudaS
 
 cudaError_t launch_hevc_phases(DevPlanes p, int bd, int w, int h, int pad, cudaStream_t s) {
   int prow = h + 2 * pad, pcol = w + 2 * pad;
-  dim3 blk(32, 8), grd((pcol + 31) / 32, (prow + 7) / 8);
+  dim3 blk(kPhaseTX, kPhaseTY), grd((pcol + kPhaseTX - 1) / kPhaseTX, (prow + kPhaseTY - 1) / kPhaseTY);
   prefer_max_shared(hevc_phase_kernel<uint8_t>);
   prefer_max_shared(hevc_phase_kernel<uint16_t>);
   if (bd == 8)

@@ -1,19 +1,27 @@
-// The serving loop: per-frame ME requests from many streams fed into the
-// resident engine (rme_engine.cu) as they arrive. A frame is uploaded into
-// its stream's ring of resident pictures on the upload stream, its planes are
-// built there, and it joins the engine's running search behind them: frames
-// that arrive while others are on the GPU are admitted as soon as a frame
-// slot and ring room are free, and their tasks share the SMs with the frames
-// already in flight (continuous batching at task granularity, not launch
-// granularity). Streams are admitted against an HBM budget of their
-// resident pictures.
+// The serving loop: per-frame ME requests from many streams, searched as
+// they arrive. A frame is uploaded into its stream's ring of resident
+// pictures on the upload stream; streams are admitted against an HBM budget
+// of their resident pictures. Two modes:
 //
-// One worker thread owns the context and the engine: it admits requests,
-// polls the engine's completion flags (host memory the device writes),
-// copies finished frames' results out on a copy stream and posts the
-// completions. Frames are searched STANDALONE against the stream's previous
-// `nref` source pictures (the reference's ME stage as a pre-pass, without
-// the reconstruction loop).
+//   RME_SERVE_LAUNCHES: the frames admitted since the last launch go into
+//   one search launch of their own as soon as one of kLaunchStreams launch
+//   streams is free, so launches overlap on the device (a frame that
+//   arrives while others are searched starts at once on another stream); a
+//   launch of one or two 1080p frames runs the latency form (the row form
+//   for HEVC), a larger one the throughput form.
+//
+//   RME_SERVE_RESIDENT: frames join the resident engine's running search
+//   (rme_engine.cu) behind their uploads, as soon as a frame slot and ring
+//   room are free; their work shares the SMs with the frames already in
+//   flight.
+//
+// One worker thread owns the context: it admits requests, launches or
+// submits them, polls for finished searches (launch events, or the
+// engine's completion flags in host memory the device writes), copies
+// finished frames' results out on a copy stream and posts the completions.
+// Frames are searched STANDALONE against the stream's previous `nref`
+// source pictures (the reference's ME stage as a pre-pass, without the
+// reconstruction loop).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -62,13 +70,25 @@ struct Request {
   double submit_s = 0.0;
   // in flight
   int64_t frame = -1;        // the stream's frame number
-  int slot = -1;             // the engine's frame slot (-1: not searched)
+  int slot = -1;             // the engine's frame slot, or the launch stream (-1: not searched)
   int nresults = 0;
   rme_result* staging = nullptr;
   size_t staging_n = 0;
   cudaEvent_t ev = nullptr;  // the upload (first frames) or the results copy
   int status = 0;
   double t_start = 0.0, t_flag = 0.0;  // host clock: handed to the engine, its flag seen
+  int64_t offset = 0;        // launch mode: the first result's index in the launch's buffer
+};
+
+// Launch mode: one of the launch streams, with the launch in flight on it.
+constexpr int kLaunchStreams = 3;
+struct LaunchStream {
+  cudaStream_t s = nullptr;
+  cudaEvent_t up = nullptr, done = nullptr, copied = nullptr;
+  rme_result* d_out = nullptr;  // the launch's results (device memory)
+  size_t cap = 0;
+  bool busy = false;
+  std::vector<Request> reqs;    // the frames it searches
 };
 
 struct Server {
@@ -91,7 +111,10 @@ struct Server {
   // it asynchronously, the worker returns it once its frame is complete.
   std::map<size_t, std::vector<void*>> pool;
   // worker-only state
+  bool resident_engine = false;  // RME_SERVE_RESIDENT
   rme::Engine* eng = nullptr;
+  LaunchStream ls[kLaunchStreams];
+  std::deque<Request> unlaunched;  // launch mode: admitted, waiting for a free launch stream
   cudaStream_t upload = nullptr, copy = nullptr;
   uint32_t* h_status = nullptr;  // pinned: the engine's status word, read back with each copy
   std::vector<Request> searching, copying, submitting;
@@ -138,6 +161,8 @@ struct Server {
   rme_frame frame_of(const Stream& st, int64_t j) const;
   void submit_search(Request& r, const Stream& st);
   void start(Request& r);
+  void launch_batch(LaunchStream& L, int k);
+  void poll_launches();
   void finish(Request& r, double t);
   void release_closed(bool engine_idle);
 };
@@ -243,6 +268,128 @@ void Server::start(Request& r) {
   copying.push_back(r);
 }
 
+// Launch mode: the oldest admitted frames (at most max_frames_per_launch)
+// go into one launch on launch stream k. Each is uploaded into its stream's
+// ring on the upload stream; its interpolated planes are built there before
+// the launch only when a later frame of the same launch reads it, else
+// behind the launch's wait (they run beside the search: only later frames
+// read them). The launch waits for the uploads and for the copies out of its
+// buffer from the stream's previous launch; its results stay in device
+// memory until poll_launches copies each frame's out.
+void Server::launch_batch(LaunchStream& L, int k) {
+  std::vector<Request> batch;
+  while (!unlaunched.empty() && (int)batch.size() < o.max_frames_per_launch) {
+    batch.push_back(std::move(unlaunched.front()));
+    unlaunched.pop_front();
+  }
+  std::map<int32_t, size_t> last;  // a stream's last frame in the batch
+  for (size_t i = 0; i < batch.size(); ++i) last[batch[i].stream] = i;
+  std::vector<rme_frame> frames;
+  std::vector<rme_params> params;
+  std::vector<int64_t> offs;
+  std::vector<size_t> searched;
+  std::vector<int32_t> planes_after;
+  int64_t total = 0;
+  for (size_t i = 0; i < batch.size(); ++i) {
+    Request& r = batch[i];
+    r.t_start = now();
+    const Stream* st;
+    {
+      std::lock_guard<std::mutex> lk(m);
+      st = &streams[r.stream];
+    }
+    const rme_frame f = frame_of(*st, r.frame);
+    const bool read_here = last[r.stream] != i;
+    r.status = rme::ctx_picture_upload(ctx, f.src_id, &st->d, r.luma, 1, read_here, upload);
+    if (r.status == 0 && !read_here) planes_after.push_back(f.src_id);
+    int32_t cnt = 0;
+    if (r.status == 0 && f.nref > 0) r.status = rme_frame_result_count(ctx, &f, &st->p, &cnt);
+    if (r.status != 0 || f.nref == 0) {
+      // Not searched (a stream's first frame) or failed: complete once the
+      // upload has read the frame's buffer.
+      r.slot = -1;
+      r.ev = take_event();
+      cudaEventRecord(r.ev, upload);
+      copying.push_back(r);
+      continue;
+    }
+    r.offset = total;
+    r.nresults = cnt;
+    total += cnt;
+    frames.push_back(f);
+    params.push_back(st->p);
+    offs.push_back(r.offset);
+    searched.push_back(i);
+  }
+  if (!frames.empty()) {
+    int rc = 0;
+    if (L.cap < (size_t)total) {
+      if (L.d_out) {
+        cudaEventSynchronize(L.copied);
+        cudaFree(L.d_out);
+      }
+      L.d_out = nullptr;
+      L.cap = 0;
+      if (cudaMalloc(&L.d_out, sizeof(rme_result) * total) == cudaSuccess) L.cap = (size_t)total;
+      else rc = RME_ENOMEM;
+    }
+    if (rc == 0 && (cudaEventRecord(L.up, upload) != cudaSuccess || cudaStreamWaitEvent(L.s, L.up, 0) != cudaSuccess ||
+                    cudaStreamWaitEvent(L.s, L.copied, 0) != cudaSuccess))
+      rc = RME_ECUDA;
+    if (rc == 0)
+      rc = rme_batch_search_async(ctx, frames.data(), params.data(), (int32_t)frames.size(), L.d_out, offs.data(), L.s);
+    if (rc == 0 && cudaEventRecord(L.done, L.s) != cudaSuccess) rc = RME_ECUDA;
+    for (size_t j : searched) {
+      Request& r = batch[j];
+      if (rc != 0) {
+        r.status = rc;
+        r.slot = -1;
+        r.ev = take_event();
+        cudaEventRecord(r.ev, upload);
+        copying.push_back(r);
+      } else {
+        r.slot = k;
+        L.reqs.push_back(r);
+      }
+    }
+    L.busy = !L.reqs.empty();
+  }
+  for (int32_t id : planes_after) rme_picture_build_planes(ctx, id, upload);
+}
+
+// Launch mode: finished launches (their event) are completed on the
+// context (status, launch slot), and each frame's results are copied out
+// on the copy stream into the caller's buffer (pinned) or a staging one.
+void Server::poll_launches() {
+  for (LaunchStream& L : ls) {
+    if (!L.busy || cudaEventQuery(L.done) != cudaSuccess) continue;
+    cudaGetLastError();
+    uint32_t dev_status = 0;
+    const int rc = rme_sync(ctx, L.s, &dev_status);
+    const double t = now();
+    for (Request& r : L.reqs) {
+      r.t_flag = t;
+      if (rc != 0) r.status = rc;
+      rme_result* dst = r.out;
+      if (!r.out_pinned) {
+        r.staging = take_staging((size_t)r.nresults);
+        r.staging_n = (size_t)r.nresults;
+        dst = r.staging;
+      }
+      if (r.status == 0 &&
+          (!dst || cudaMemcpyAsync(dst, L.d_out + r.offset, sizeof(rme_result) * r.nresults, cudaMemcpyDeviceToHost,
+                                   copy) != cudaSuccess))
+        r.status = RME_ECUDA;
+      r.ev = take_event();
+      cudaEventRecord(r.ev, copy);
+      copying.push_back(r);
+    }
+    cudaEventRecord(L.copied, copy);
+    L.reqs.clear();
+    L.busy = false;
+  }
+}
+
 void Server::finish(Request& r, double t) {  // lock held
   rme_completion c{};
   c.request_id = r.id;
@@ -284,7 +431,9 @@ void Server::run() {
   for (;;) {
     std::vector<Request> taken;
     bool any_close = false;
-    const bool busy = !searching.empty() || !copying.empty() || !submitting.empty();
+    bool launches_busy = !unlaunched.empty();
+    for (const LaunchStream& L : ls) launches_busy |= L.busy;
+    const bool busy = !searching.empty() || !copying.empty() || !submitting.empty() || launches_busy;
     {
       std::unique_lock<std::mutex> lk(m);
       if (busy)
@@ -297,7 +446,14 @@ void Server::run() {
       closes = 0;
       admit(taken);
     }
-    for (Request& r : taken) start(r);
+    if (resident_engine) {
+      for (Request& r : taken) start(r);
+    } else {
+      for (Request& r : taken) unlaunched.push_back(std::move(r));
+      poll_launches();
+      for (int k = 0; k < kLaunchStreams && !unlaunched.empty(); ++k)
+        if (!ls[k].busy) launch_batch(ls[k], k);
+    }
     // Frames the engine had no room for: again, oldest first.
     if (!submitting.empty()) {
       std::vector<Request> again;
@@ -338,7 +494,7 @@ void Server::run() {
       searching.pop_back();
     }
     // The engine leaves when idle: launch it again while frames are in flight.
-    if (!searching.empty()) rme::engine_keep_running(eng);
+    if (resident_engine && !searching.empty()) rme::engine_keep_running(eng);
     // Copies done: results to the caller, slots back to the engine.
     bool any = false;
     for (size_t i = 0; i < copying.size();) {
@@ -348,9 +504,9 @@ void Server::run() {
         continue;
       }
       if (r.slot >= 0) {
-        if (r.status == 0 && *(volatile uint32_t*)h_status != 0) r.status = RME_EDEVICE;
+        if (resident_engine && r.status == 0 && *(volatile uint32_t*)h_status != 0) r.status = RME_EDEVICE;
         if (r.status == 0 && r.staging) std::memcpy(r.out, r.staging, sizeof(rme_result) * r.nresults);
-        rme::engine_release(eng, r.slot);
+        if (resident_engine) rme::engine_release(eng, r.slot);
       }
       if (r.staging) staging_pool[r.staging_n].push_back(r.staging);
       events.push_back(r.ev);
@@ -370,6 +526,12 @@ void Server::run() {
     // Nothing in flight for a while: stop the engine kernel (the waiting
     // warps leave), so that it holds no SM while the server is idle; the
     // next frame launches it again.
+    if (!resident_engine) {
+      bool in_flight = !unlaunched.empty();
+      for (const LaunchStream& L : ls) in_flight |= L.busy;
+      if (!release_later.empty() || any || any_close) release_closed(!in_flight);
+      continue;
+    }
     if (searching.empty() && submitting.empty()) {
       if (any || !taken.empty()) idle_since = now();
       else if (now() - idle_since > 0.02) rme::engine_stop(eng);
@@ -387,15 +549,32 @@ extern "C" {
 int rme_serve_start(void* ctx, const rme_serve_opts* o, void** server) {
   if (!ctx || !o || !server || o->max_frames_per_launch < 1 || o->max_frames_per_launch > 255 || o->max_streams < 1)
     return RME_EINVAL;
+  if (o->mode != RME_SERVE_LAUNCHES && o->mode != RME_SERVE_RESIDENT) return RME_EINVAL;
   auto* s = new Server();
   s->ctx = ctx;
   s->o = *o;
+  s->resident_engine = o->mode == RME_SERVE_RESIDENT;
   cudaGetDevice(&s->device);
-  if (rme::engine_create(ctx, s->device, &s->eng) != 0 ||
+  bool ok = true;
+  if (!s->resident_engine)
+    for (LaunchStream& L : s->ls)
+      ok = ok && cudaStreamCreateWithFlags(&L.s, cudaStreamNonBlocking) == cudaSuccess &&
+           cudaEventCreateWithFlags(&L.up, cudaEventDisableTiming) == cudaSuccess &&
+           cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming) == cudaSuccess &&
+           cudaEventCreateWithFlags(&L.copied, cudaEventDisableTiming) == cudaSuccess;
+  if (!ok || (s->resident_engine && rme::engine_create(ctx, s->device, &s->eng) != 0) ||
       cudaStreamCreateWithFlags(&s->upload, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking) != cudaSuccess ||
       cudaMallocHost(&s->h_status, 64) != cudaSuccess) {
     if (s->eng) rme::engine_destroy(s->eng);
+    for (LaunchStream& L : s->ls) {
+      for (cudaEvent_t e : {L.up, L.done, L.copied})
+        if (e) cudaEventDestroy(e);
+      if (L.s) cudaStreamDestroy(L.s);
+    }
+    if (s->upload) cudaStreamDestroy(s->upload);
+    if (s->copy) cudaStreamDestroy(s->copy);
+    if (s->h_status) cudaFreeHost(s->h_status);
     delete s;
     return RME_ECUDA;
   }
@@ -502,6 +681,13 @@ int rme_serve_stop(void* server) {
   s->cv.notify_all();
   if (s->worker.joinable()) s->worker.join();
   rme::engine_destroy(s->eng);  // the kernel leaves (asked to), then its memory goes
+  for (LaunchStream& L : s->ls) {
+    if (L.s) cudaStreamSynchronize(L.s);
+    if (L.d_out) cudaFree(L.d_out);
+    for (cudaEvent_t e : {L.up, L.done, L.copied})
+      if (e) cudaEventDestroy(e);
+    if (L.s) cudaStreamDestroy(L.s);
+  }
   for (auto& kv : s->streams)
     for (int k = 0; k < kv.second.nref + kPerStream; ++k) rme_picture_release(s->ctx, kv.second.pic_base + k);
   for (auto& pr : s->release_later)

@@ -382,15 +382,18 @@ def distortion_batch(kind: str, a, a_stride: int, a_off, b, b_stride: int, b_off
 
 class Server:
     """The serving loop (rme_serve_*) on its own context: per-frame ME
-    requests of many streams, batched into persistent launches as they
-    arrive; each stream's reference pictures stay resident. The context is
-    the server's while it runs."""
+    requests of many streams; each stream's reference pictures stay
+    resident. `resident=False`: the frames that arrived since the last
+    launch go into a launch of their own, up to three launches overlapping
+    on the device; `resident=True`: one search kernel stays on the GPU and
+    frames join its queue. The context is the server's while it runs."""
 
     def __init__(self, ms: MotionSearch, hbm_budget_bytes: int, max_frames_per_launch: int = 32,
-                 max_streams: int = 256):
+                 max_streams: int = 256, resident: bool = False):
         self._lib = capi.lib()
         self.ms = ms
-        o = capi.ServeOpts(hbm_budget_bytes, max_frames_per_launch, max_streams)
+        o = capi.ServeOpts(hbm_budget_bytes, max_frames_per_launch, max_streams,
+                           capi.RME_SERVE_RESIDENT if resident else capi.RME_SERVE_LAUNCHES, 0)
         h = C.c_void_p()
         capi.check(self._lib.rme_serve_start(ms.ctx, C.byref(o), C.byref(h)))
         self.h = h

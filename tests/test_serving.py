@@ -1,7 +1,9 @@
-"""The serving loop: per-frame requests of several streams (two codecs, two
-bit depths, different sizes) give the same results when each stream is
-served alone and when all are in the mix, and the same as the plain
-per-frame path; admission refuses streams past the HBM budget."""
+"""The serving loop, in both modes (a launch per batch of arrivals with
+launches overlapping, and the resident engine): per-frame requests of
+several streams (two codecs, two bit depths, different sizes) give the same
+results when each stream is served alone and when all are in the mix, and
+the same as the plain per-frame path; admission refuses streams past the
+HBM budget."""
 import time
 
 import numpy as np
@@ -50,9 +52,9 @@ def _wait(server, n, timeout=60.0):
     return got
 
 
-def _serve(streams, interleave):
+def _serve(streams, interleave, resident):
     with host.MotionSearch(0) as ms:
-        srv = host.Server(ms, hbm_budget_bytes=8 << 30, max_frames_per_launch=8)
+        srv = host.Server(ms, hbm_budget_bytes=8 << 30, max_frames_per_launch=8, resident=resident)
         try:
             frames = {}
             for sid, codec, bd, w, h, nref, qp in streams:
@@ -80,12 +82,13 @@ def _serve(streams, interleave):
             srv.stop()
 
 
-def test_results_are_the_same_alone_and_in_the_mix():
+@pytest.mark.parametrize("resident", [False, True])
+def test_results_are_the_same_alone_and_in_the_mix(resident):
     alone = {}
     for s in STREAMS:
-        r, frames = _serve([s], interleave=False)
+        r, frames = _serve([s], interleave=False, resident=resident)
         alone.update(r)
-    mix, frames = _serve(STREAMS, interleave=True)
+    mix, frames = _serve(STREAMS, interleave=True, resident=resident)
     assert set(mix) == set(alone)
     for key in sorted(alone):
         assert_results_equal(mix[key], alone[key], f"stream {key[0]} frame {key[1]}")
@@ -121,12 +124,14 @@ def test_admission_is_bounded_by_the_budget():
             srv.stop()
 
 
-def test_many_frames_recycle_the_engine_slots_and_survive_idle_periods():
-    """300 frames of one stream and 60 of another through the resident
-    engine: more frames than it has frame slots (each slot reused with a new
-    generation), submitted in bursts with pauses long enough for the engine
-    kernel to leave and be launched again. Every checked frame equals the
-    plain per-frame path."""
+@pytest.mark.parametrize("resident", [False, True])
+def test_many_frames_recycle_the_engine_slots_and_survive_idle_periods(resident):
+    """300 frames of one stream and 60 of another, submitted in bursts with
+    pauses: through the resident engine, more frames than it has frame slots
+    (each slot reused with a new generation), and pauses long enough for the
+    engine kernel to leave and be launched again; through overlapping
+    launches, the launch streams' buffers reused. Every checked frame equals
+    the plain per-frame path."""
     streams = [(21, HEVC, 8, 128, 64, 2, 32), (22, H264, 8, 96, 64, 1, 28)]
     counts = {21: 300, 22: 60}
     seqs = {sid: synth.make_sequence(codec, w, h, bd, 8, 2000 + sid, 32, 32, 2.0).frames
@@ -134,7 +139,7 @@ def test_many_frames_recycle_the_engine_slots_and_survive_idle_periods():
     pics = {sid: [seqs[sid][t % 8] if (t // 8) % 2 == 0 else seqs[sid][7 - t % 8] for t in range(counts[sid])]
             for sid in counts}
     with host.MotionSearch(0) as ms:
-        srv = host.Server(ms, hbm_budget_bytes=8 << 30, max_frames_per_launch=8)
+        srv = host.Server(ms, hbm_budget_bytes=8 << 30, max_frames_per_launch=8, resident=resident)
         got = {}
         try:
             for sid, codec, bd, w, h, nref, qp in streams:
