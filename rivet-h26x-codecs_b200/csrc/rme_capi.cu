@@ -211,7 +211,7 @@ struct Shape {
   int variant, groups, patch, rows;
 };
 constexpr Shape kThroughputShapes[] = {{1, 0, 0, 0}, {0, 0, 0, 0}, {2, 0, 0, 0}};
-constexpr Shape kLatencyHevcShapes[] = {{0, 3, 1, 1}, {1, 3, 1, 1}, {0, 3, 0, 1}, {1, 2, 1, 0},
+constexpr Shape kLatencyHevcShapes[] = {{0, 3, 0, 1}, {0, 3, 1, 1}, {1, 3, 0, 1}, {1, 2, 1, 0},
                                         {1, 2, 0, 0}, {1, 1, 1, 0}, {1, 0, 0, 0}, {0, 2, 1, 0}};
 constexpr Shape kLatencyShapes[] = {{1, 0, 0, 0}, {0, 0, 0, 0}, {2, 0, 0, 0}};
 constexpr int kNumShapes[3] = {(int)(sizeof(kThroughputShapes) / sizeof(Shape)),

@@ -335,10 +335,12 @@ __device__ __forceinline__ void st_relaxed64(unsigned long long* p, unsigned lon
 }
 
 // The row form: the published word of a task another row owns, waited for
-// until it carries this search's tag (bounded: kSpinLimit polls with
-// backoff, then the status word's timeout bit and a zero vector, so that a
-// lost dependency ends the search with an error instead of hanging it). The
-// caller has loaded the word once already (`w`), while it staged its source.
+// until it carries this search's tag (bounded: kSpinLimit polls, then the
+// status word's timeout bit and a zero vector, so that a lost dependency
+// ends the search with an error instead of hanging it). The caller has
+// loaded the word once already (`w`), while it staged its source. The first
+// polls follow one another (the upper row is usually a block ahead, so the
+// word comes within a few round trips); later ones back off.
 __device__ __noinline__ unsigned long long wait_word(const LaunchDesc& L, const unsigned long long* p, uint32_t tag,
                                                      unsigned long long w) {
   uint32_t ns = 32;
@@ -347,8 +349,10 @@ __device__ __noinline__ unsigned long long wait_word(const LaunchDesc& L, const 
       atomicOr(L.status, kStatusWaitTimeout);
       return (unsigned long long)tag << 32;
     }
-    __nanosleep(ns);
-    if (ns < 256) ns <<= 1;
+    if (it >= 16) {
+      __nanosleep(ns);
+      if (ns < 256) ns <<= 1;
+    }
     w = ld_relaxed64(p);
   }
   return w;
@@ -719,19 +723,30 @@ __device__ __forceinline__ void refine8_patched(WarpSmem<S>& sm, const DevPlanes
   }
 }
 
+// The row form's place in its row: level, block, reference.
+struct RowPos {
+  int l, lbx, lby, r;
+};
+
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
 // Returns a task it made ready to run next (frame << 24 | task), or -1.
 // SPEC: the latency kernels' two-rounds-per-step 8x8 and 16x16 diamond.
 // ROW: the row form (the neighbours' vectors from their published words,
-// this task's published in turn; nothing released).
-template <class S, bool SPEC, bool ROW = false>
-__device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, WarpSmem<S>& sm, int lane) {
+// this task's published in turn; nothing released), at `rp` in its row,
+// blocks of NB samples (0: the level's size read at run time).
+template <class S, bool SPEC, bool ROW = false, int NB = 0>
+__device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, WarpSmem<S>& sm, int lane,
+                         RowPos* rp = nullptr) {
   int r, x, y, w, h, ns;
   int p0x, p0y, p1x, p1y;
   int sx = 0, sy = 0;  // this lane's seed (lane < ns)
   int l = 0, lbx = 0, lby = 0, local = 0;  // STANDALONE: level and block
   bool amp_unit = false;                   // STANDALONE: an AMP unit
   rme_result* out;
-  if (F.mode == RME_PRED_GIVEN) {
+  if (!ROW && F.mode == RME_PRED_GIVEN) {
     const rme_job* j = &F.jobs[t];
     if (!given_job_ok(F, j, RME_MAX_SEEDS)) {
       if (lane == 0) atomicOr(L.status, kStatusBadTask);
@@ -752,12 +767,14 @@ __device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
       sy = j->seeds[lane].y;
     }
     out = &F.out[t];
+  } else if (ROW) {
+    r = rp->r;
   } else {
     r = t % F.nref;
     const int blk = t / F.nref;
     amp_unit = blk >= F.base[F.nlevels];
   }
-  if (amp_unit) {
+  if (!ROW && amp_unit) {
     // An AMP unit (after every 2Nx2N block): its level, CU, mode and part.
     // It is searched from its CU's own 2Nx2N result: AMVP pair [own, 0],
     // seeds [own, mvp0, mvp1] (the parts search's own seed first).
@@ -795,14 +812,21 @@ __device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
     sx = lane == 0 || lane == 1 ? p0x : 0;
     sy = lane == 0 || lane == 1 ? p0y : 0;
     out = &F.out[t];
-  } else if (F.mode != RME_PRED_GIVEN) {
-    const int blk = t / F.nref;
-    while (l + 1 < F.nlevels && blk >= F.base[l + 1]) ++l;
-    local = blk - F.base[l];
+  } else if (ROW || F.mode != RME_PRED_GIVEN) {
+    if (ROW) {
+      l = rp->l;
+      lbx = rp->lbx;
+      lby = rp->lby;
+      local = lby * F.nbx[l] + lbx;
+    } else {
+      const int blk = t / F.nref;
+      while (l + 1 < F.nlevels && blk >= F.base[l + 1]) ++l;
+      local = blk - F.base[l];
+      lby = local / F.nbx[l];
+      lbx = local - lby * F.nbx[l];
+    }
     const int nbx = F.nbx[l];
-    lby = local / nbx;
-    lbx = local - lby * nbx;
-    const int N = F.size[l];
+    const int N = NB ? NB : F.size[l];
     x = lbx * N;
     y = lby * N;
     w = h = N;
@@ -827,6 +851,8 @@ __device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
     // The source block is staged while those loads are in flight.
     stage_src<S>(sm.src, plane_at<S>(F.src, 0, x, y), F.src.stride, w, h, lane);
     if (ROW && didx >= 0) dv = (uint32_t)wait_word(L, F.mvf + didx, F.tag, dw);
+    // The row form: the next block's source rows brought into L1 now.
+    if (ROW && lbx + 1 < nbx && lane < N) prefetch_l1(plane_at<S>(F.src, 0, x + N, y + lane));
     const uint32_t have = __ballot_sync(kFull, didx >= 0);
     const uint32_t va = __shfl_sync(kFull, dv, 0), vb = __shfl_sync(kFull, dv, 1), vp = __shfl_sync(kFull, dv, 2);
     int na = 0, ax = 0, ay = 0, cx = 0, cy = 0;
@@ -859,7 +885,7 @@ __device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
     out = &F.out[t];
   }
   const DevPlanes& R = F.ref[r];
-  if (F.mode == RME_PRED_GIVEN) {
+  if (!ROW && F.mode == RME_PRED_GIVEN) {
     if (F.bi_src)  // refine_bi: the target block stands in for the source
       stage_src<S>(sm.src, (const S*)F.bi_src + (int64_t)t * (kBiBlock * kBiBlock), kBiBlock, w, h, lane);
     else
@@ -1069,7 +1095,7 @@ __device__ int hevc_task(const LaunchDesc& L, const FrameDesc& F, int f, int t, 
   int cont = -1;
   if (ROW) {
     if (lane == 0) st_relaxed64(F.mvf + t, mv_word(F.tag, bmx, bmy));
-  } else if (F.mode != RME_PRED_GIVEN && !amp_unit) {
+  } else if (!ROW && F.mode != RME_PRED_GIVEN && !amp_unit) {
     // The tasks reading this result: right and lower neighbours of this
     // level, the blocks of the next evaluated size inside this one, this
     // CU's AMP units; each lane releases one of them. Lane 0's result is
@@ -1595,12 +1621,22 @@ __device__ __forceinline__ bool row_ok(const FrameDesc& F, uint32_t e, int& l, i
 template <class S, bool SPEC>
 __device__ void hevc_row(const LaunchDesc& L, const FrameDesc& F, int f, uint32_t e, WarpSmem<S>& sm, int lane) {
   int l, r, row;
-  if (!row_ok(F, e, l, r, row) || F.size[l] > 16) {
+  if (!row_ok(F, e, l, r, row) || (F.size[l] != 8 && F.size[l] != 16)) {
     if (lane == 0) atomicOr(L.status, kStatusBadTask);
     return;
   }
   const int nbx = F.nbx[l], t0 = (F.base[l] + row * nbx) * F.nref + r;
-  for (int bx = 0; bx < nbx; ++bx) hevc_task<S, SPEC, true>(L, F, f, t0 + bx * F.nref, sm, lane);
+  RowPos rp{l, 0, row, r};
+  if (F.size[l] == 8)
+    for (int bx = 0; bx < nbx; ++bx) {
+      rp.lbx = bx;
+      hevc_task<S, SPEC, true, 8>(L, F, f, t0 + bx * F.nref, sm, lane, &rp);
+    }
+  else
+    for (int bx = 0; bx < nbx; ++bx) {
+      rp.lbx = bx;
+      hevc_task<S, SPEC, true, 16>(L, F, f, t0 + bx * F.nref, sm, lane, &rp);
+    }
 }
 
 template <class S>
