@@ -307,10 +307,10 @@ def run_ours(args, world, rank, local):
     # Each frame's results go to a buffer the caller keeps (as an encoder
     # keeps its motion field) in pinned memory, which the results' copy
     # fills directly; touched before the timing.
-    # The tuner times its launch shapes (six for one HEVC frame) on the first
-    # launches of this size: one frame several times, so that they are
-    # compared on the same content.
-    for _ in range(8):
+    # The tuner times its launch shapes (eight for one HEVC frame, each
+    # twice) on the first launches of this size: one frame several times, so
+    # that they are compared on the same content.
+    for _ in range(18):
         ms.search(batch[0][0], batch[0][1], p, stream=sh)
     per_frame = ms.result_count(batch[0][0], batch[0][1], p)
     plain_bufs = []
@@ -327,10 +327,11 @@ def run_ours(args, world, rank, local):
     plain_fps = len(batch) / sum(lat)
 
     # ---- batched, device-resident -------------------------------------------
-    # Warm-up: the occupancy tuner times its variants on the first three
-    # launches of this size, and the winner's CUDA graph is captured the
-    # next time its shape comes; two more steps settle both before timing.
-    warm = max(args.warmup, 3) + 2
+    # Warm-up: the occupancy tuner times its three variants twice each on
+    # the first six launches of this size, and the winner's CUDA graph is
+    # captured the next time its shape comes; two more steps settle both
+    # before timing.
+    warm = max(args.warmup, 3) + 5
     for _ in range(warm):
         outs = step()
     outs = as_host(outs)
@@ -912,7 +913,7 @@ def run_configs(local: int = 0):
     def measure(name, frames, params, note):
         total = ms.batch_result_count(frames, params)
         dev = torch.empty(total * capi.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=f"cuda:{local}")
-        for _ in range(5):  # the tuner's three trials, the graph's capture, one more
+        for _ in range(8):  # the tuner's six trials, the graph's capture, one more
             outs = ms.search_batch(frames, params, 0, out=dev)
         torch.cuda.synchronize()
         ks = []
@@ -1014,7 +1015,7 @@ def other_configs(local: int = 0) -> dict:
         frames = [(100 + t, [100 + t - 1 - r for r in range(4)]) for t in range(4, 12)]
         total = ms.batch_result_count(frames, p2)
         dev = torch.empty(total * capi.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=f"cuda:{local}")
-        for _ in range(5):
+        for _ in range(8):  # the tuner's six trials, the graph's capture, one more
             outs = ms.search_batch(frames, p2, 0, out=dev)
         ks = []
         for _ in range(3):

@@ -214,6 +214,7 @@ constexpr Shape kThroughputShapes[] = {{1, 0, 0, 0}, {0, 0, 0, 0}, {2, 0, 0, 0}}
 constexpr Shape kLatencyHevcShapes[] = {{0, 3, 0, 1}, {0, 3, 1, 1}, {1, 3, 0, 1}, {1, 2, 1, 0},
                                         {1, 2, 0, 0}, {1, 1, 1, 0}, {1, 0, 0, 0}, {0, 2, 1, 0}};
 constexpr Shape kLatencyShapes[] = {{1, 0, 0, 0}, {0, 0, 0, 0}, {2, 0, 0, 0}};
+constexpr int kTuneRounds = 2;  // timings per shape before the tuner chooses (launch times vary)
 constexpr int kNumShapes[3] = {(int)(sizeof(kThroughputShapes) / sizeof(Shape)),
                                (int)(sizeof(kLatencyHevcShapes) / sizeof(Shape)),
                                (int)(sizeof(kLatencyShapes) / sizeof(Shape))};
@@ -261,7 +262,7 @@ struct Ctx {
   // kept. Results do not depend on the shape.
   struct Tune {
     int best = -1, tried = 0;
-    float ms[8] = {};
+    float ms[8] = {};  // per shape, its best time so far
   };
   std::map<std::pair<int, int>, Tune> tune;
   bool tune_on = true;
@@ -474,8 +475,10 @@ const Deps* get_deps(Ctx* c, const rme_picture_desc& d, const rme_params* p, int
     if (pend[t] == 0) dp.ready.push_back((uint32_t)t);
   dp.ntasks = pend.size();
   if (d.codec == RME_CODEC_HEVC && p->hevc_amp == 0) {
+    // Reference-major: a block's warps take consecutive rows of one
+    // reference, whose reference bands overlap in the SM's L1.
     struct Row {
-      int y, size;
+      int r, y, size;
       uint32_t entry;
     };
     std::vector<Row> all;
@@ -485,10 +488,11 @@ const Deps* get_deps(Ctx* c, const rme_picture_desc& d, const rme_params* p, int
       const int N = sizes[l];
       if (d.width / N == 0) continue;
       for (int row = 0; row < d.height / N; ++row)
-        for (int r = 0; r < nref; ++r) all.push_back({row * N, N, row_entry(l, r, row)});
+        for (int r = 0; r < nref; ++r) all.push_back({r, row * N, N, row_entry(l, r, row)});
     }
-    std::stable_sort(all.begin(), all.end(),
-                     [](const Row& a, const Row& b) { return a.y != b.y ? a.y < b.y : a.size > b.size; });
+    std::stable_sort(all.begin(), all.end(), [](const Row& a, const Row& b) {
+      return a.r != b.r ? a.r < b.r : a.y != b.y ? a.y < b.y : a.size > b.size;
+    });
     for (const Row& w : all) (w.size >= 32 ? dp.rows_big : dp.rows).push_back(w.entry);
   }
   cudaError_t e = cudaMalloc(&dp.pending, std::max<size_t>(pend.size(), 1) * sizeof(int32_t));
@@ -633,9 +637,12 @@ int finish_launch(Ctx* c, Slot& sl) {
   if (sl.tuning) {
     auto* T = (Ctx::Tune*)sl.tuning;
     sl.tuning = nullptr;
-    if (T->best < 0 && T->tried < sl.tune_shapes) {
-      T->ms[T->tried++] = ms;
-      if (T->tried == sl.tune_shapes) T->best = (int)(std::min_element(T->ms, T->ms + sl.tune_shapes) - T->ms);
+    if (T->best < 0 && T->tried < kTuneRounds * sl.tune_shapes) {
+      // Each shape is timed kTuneRounds times (in turn); its best time counts.
+      const int i = T->tried % sl.tune_shapes;
+      T->ms[i] = T->tried < sl.tune_shapes ? ms : std::min(T->ms[i], ms);
+      if (++T->tried == kTuneRounds * sl.tune_shapes)
+        T->best = (int)(std::min_element(T->ms, T->ms + sl.tune_shapes) - T->ms);
     }
   }
   c->last.planes_ms = 0.0f;
@@ -759,7 +766,7 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
       if (T.best >= 0) {
         shape[k] = shapes[T.best];
       } else if (nparts_used == 1 && !async) {
-        shape[k] = shapes[T.tried];
+        shape[k] = shapes[T.tried % nsh];
         tuning = &T;
         tune_shapes = nsh;
       }

@@ -82,26 +82,27 @@ __constant__ int8_t c_qpel[4][8] = {{0, 0, 0, 0, 0, 0, 0, 0},
 
 // The fifteen phases of every padded position: the horizontal pass of each
 // fraction over TY + 7 rows kept in shared memory (int16, as the
-// reference's intermediate), the vertical passes from it. Blocks of 32 x 4
-// threads: one fits in the registers the resident engine leaves free on
-// every SM, so a picture's planes are built while the engine runs.
-constexpr int kPhaseTX = 32, kPhaseTY = 4;
+// reference's intermediate), the vertical passes from it. A tile of 32 x 8
+// positions, blocks of 32 x 4 threads (two rows each): one block fits in
+// the registers the resident engine leaves free on every SM, so a
+// picture's planes are built while the engine runs.
+constexpr int kPhaseTX = 32, kPhaseTY = 8, kPhaseRows = 4;
 template <class S>
 __global__ void hevc_phase_kernel(const S* g, S* planes, int64_t plane_elems, int stride,
                                   int prow, int pcol, int bd) {
-  constexpr int TX = kPhaseTX, TY = kPhaseTY;
+  constexpr int TX = kPhaseTX, TY = kPhaseTY, NT = kPhaseTX * kPhaseRows;
   __shared__ int tile[TY + 7][TX + 7];
   __shared__ int16_t hp[3][TY + 7][TX];
   int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
   int tid = threadIdx.y * TX + threadIdx.x;
   int shift1 = min(bd, 12) - 8, shift3 = 14 - bd, maxv = (1 << bd) - 1, round3 = 1 << (shift3 - 1);
-  for (int i = tid; i < (TY + 7) * (TX + 7); i += TX * TY) {
+  for (int i = tid; i < (TY + 7) * (TX + 7); i += NT) {
     int ty = i / (TX + 7), tx = i % (TX + 7);
     int gx = min(max(x0 + tx - 3, 0), pcol - 1), gy = min(max(y0 + ty - 3, 0), prow - 1);
     tile[ty][tx] = g[(int64_t)gy * stride + gx];
   }
   __syncthreads();
-  for (int i = tid; i < 3 * (TY + 7) * TX; i += TX * TY) {
+  for (int i = tid; i < 3 * (TY + 7) * TX; i += NT) {
     int f = i / ((TY + 7) * TX), rem = i % ((TY + 7) * TX), ty = rem / TX, tx = rem % TX;
     int acc = 0;
 #pragma unroll
@@ -109,24 +110,27 @@ __global__ void hevc_phase_kernel(const S* g, S* planes, int64_t plane_elems, in
     hp[f][ty][tx] = (int16_t)(acc >> shift1);
   }
   __syncthreads();
-  int tx = threadIdx.x, ty = threadIdx.y, x = x0 + tx, y = y0 + ty;
-  if (x >= pcol || y >= prow) return;
-  int64_t o = (int64_t)y * stride + x;
-  auto put = [&](int phase, int v14) {
-    int v = min(max(((int)(int16_t)v14 + round3) >> shift3, 0), maxv);
-    planes[(int64_t)phase * plane_elems + o] = (S)v;
-  };
-  for (int fx = 1; fx < 4; ++fx) put(fx, hp[fx - 1][ty + 3][tx]);
-  for (int fy = 1; fy < 4; ++fy) {
-    int acc = 0;
+  const int tx = threadIdx.x, x = x0 + tx;
+  for (int ty = threadIdx.y; ty < TY; ty += kPhaseRows) {
+    const int y = y0 + ty;
+    if (x >= pcol || y >= prow) return;
+    const int64_t o = (int64_t)y * stride + x;
+    auto put = [&](int phase, int v14) {
+      int v = min(max(((int)(int16_t)v14 + round3) >> shift3, 0), maxv);
+      planes[(int64_t)phase * plane_elems + o] = (S)v;
+    };
+    for (int fx = 1; fx < 4; ++fx) put(fx, hp[fx - 1][ty + 3][tx]);
+    for (int fy = 1; fy < 4; ++fy) {
+      int acc = 0;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) acc += c_qpel[fy][k] * tile[ty + k][tx + 3];
-    put(fy * 4, acc >> shift1);
-    for (int fx = 1; fx < 4; ++fx) {
-      int a2 = 0;
+      for (int k = 0; k < 8; ++k) acc += c_qpel[fy][k] * tile[ty + k][tx + 3];
+      put(fy * 4, acc >> shift1);
+      for (int fx = 1; fx < 4; ++fx) {
+        int a2 = 0;
 #pragma unroll
-      for (int k = 0; k < 8; ++k) a2 += c_qpel[fy][k] * (int)hp[fx - 1][ty + k][tx];
-      put(fy * 4 + fx, a2 >> 6);
+        for (int k = 0; k < 8; ++k) a2 += c_qpel[fy][k] * (int)hp[fx - 1][ty + k][tx];
+        put(fy * 4 + fx, a2 >> 6);
+      }
     }
   }
 }
@@ -167,7 +171,7 @@ cudaError_t launch_h264_hpel(DevPlanes p, int bd, int cw, int ch, int pad, cudaS
 
 cudaError_t launch_hevc_phases(DevPlanes p, int bd, int w, int h, int pad, cudaStream_t s) {
   int prow = h + 2 * pad, pcol = w + 2 * pad;
-  dim3 blk(kPhaseTX, kPhaseTY), grd((pcol + kPhaseTX - 1) / kPhaseTX, (prow + kPhaseTY - 1) / kPhaseTY);
+  dim3 blk(kPhaseTX, kPhaseRows), grd((pcol + kPhaseTX - 1) / kPhaseTX, (prow + kPhaseTY - 1) / kPhaseTY);
   prefer_max_shared(hevc_phase_kernel<uint8_t>);
   prefer_max_shared(hevc_phase_kernel<uint16_t>);
   if (bd == 8)

@@ -350,7 +350,7 @@ def test_every_launch_shape_gives_the_oracles_results(bd, amp):
     """A fresh context times each launch shape of a class on its first
     launches (occupancy variant, CTAs for the 32x32 and 64x64 blocks or
     none, staged 8x8 patches or cache reads, the row form where the frame
-    has no AMP units): the same frame searched once per shape, and once
+    has no AMP units): the same frame searched twice per shape, and once
     more on the chosen one, equals the oracle every time."""
     import rivet_h26x_codecs_b200 as rme
     seq = synth.make_sequence(HEVC, 320, 192, bd, 3, 77 + bd, 64, 96, 2.0)
@@ -359,7 +359,7 @@ def test_every_launch_shape_gives_the_oracles_results(bd, amp):
     with rme.MotionSearch(0) as ms2:
         for i, f in enumerate(seq.frames):
             ms2.upload(i, f, HEVC, bd, as_ref=True)
-        for k in range(9):
+        for k in range(2 * 8 + 1):
             got = ms2.search(2, [1, 0], p)
             assert_results_equal(got, want, f"launch {k}")
 
