@@ -448,11 +448,12 @@ int engine_create(void* ctx, int device, Engine** out) {
   // At most two of the kernel's blocks per SM: room is left on every SM for
   // the uploads' plane builds, which run beside it.
   g->grid = nsm * std::min(2, engine_blocks_per_sm());
-  // Two thirds of them run the 32x32 and 64x64 HEVC blocks (a CTA per
-  // block, or per row of blocks in the row form), the rest's warps the
-  // smaller blocks: a 1080p frame of two references has 98 rows of large
-  // blocks and 404 of small ones, so two such frames run at once.
-  const int groups = std::max(1, g->grid * 2 / 3);
+  // Half of them run the 32x32 and 64x64 HEVC blocks (a CTA per block, or
+  // per row of blocks in the row form), the other half's warps the smaller
+  // blocks: a 1080p frame of two references has 98 rows of large blocks and
+  // 404 of small ones (a frame measured 5.6 ms this way, 6.2 ms with two
+  // thirds of the CTAs on large blocks).
+  const int groups = std::max(1, g->grid / 2);
   for (int k = kEngineFrames - 1; k >= 0; --k) g->free_slots.push_back(k);
   LaunchDesc& L = g->L;
   L.frames = g->d_frames;

@@ -45,6 +45,8 @@
 // for the queue itself (a slot not yet pushed: nothing is ready anywhere);
 // it is bounded (kSpinLimit polls with backoff), and a wait that runs out
 // sets a status bit the host turns into RME_EDEVICE instead of hanging.
+#include <algorithm>
+
 #include "rme_search_impl.cuh"
 
 namespace rme {
@@ -235,12 +237,35 @@ int blocks_per_sm() {
   return e == cudaSuccess && n > 0 ? n : 1;
 }
 
+// The shared-memory share of the SM's unified L1 that MINB blocks need
+// (percent, rounded up): the rest stays L1 data cache, which the
+// reference reads hit (a frame 3.9 -> 3.75 ms, an 8-frame launch 15.1 ->
+// 14.0 ms against the largest shared share).
+template <class S, int MINB>
+int carveout_pct() {
+  static int pct = -1;
+  if (pct < 0) {
+    int dev = 0, smem_sm = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+        smem_sm <= 0) {
+      cudaGetLastError();
+      return 100;
+    }
+    const long need = (long)MINB * ((long)smem_bytes<S>() + 1024);
+    pct = (int)std::min<long>(100, (need * 100 + smem_sm - 1) / smem_sm);
+  }
+  return pct;
+}
+
 template <class S, int CODEC, int MINB, bool SPEC>
 cudaError_t launch(const LaunchDesc& L, int grid, cudaStream_t s) {
   cudaError_t e = cudaFuncSetAttribute(search_kernel<S, CODEC, MINB, SPEC>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<S>());
   if (e != cudaSuccess) return e;
-  prefer_max_shared(search_kernel<S, CODEC, MINB, SPEC>);
+  e = cudaFuncSetAttribute(search_kernel<S, CODEC, MINB, SPEC>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           carveout_pct<S, MINB>());
+  if (e != cudaSuccess) return e;
   search_kernel<S, CODEC, MINB, SPEC><<<grid, kWarpsPerBlock * 32, smem_bytes<S>(), s>>>(L);
   return cudaGetLastError();
 }
