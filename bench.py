@@ -541,7 +541,7 @@ def run_ours(args, world, rank, local):
 P99_TARGET_MS = 8.0
 
 
-SERVED_LOADS = (0.04, 0.07, 0.1, 0.13, 0.16, 0.2, 0.3, 0.45)
+SERVED_LOADS = (0.04, 0.07, 0.1, 0.115, 0.13, 0.145, 0.16, 0.18, 0.2, 0.3, 0.45)
 
 
 def run_served(frames, capacity_fps: float, loads=SERVED_LOADS, min_requests: int = 1000,

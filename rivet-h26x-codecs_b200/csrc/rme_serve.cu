@@ -556,14 +556,20 @@ int rme_serve_start(void* ctx, const rme_serve_opts* o, void** server) {
   s->resident_engine = o->mode == RME_SERVE_RESIDENT;
   cudaGetDevice(&s->device);
   bool ok = true;
+  // Launch mode: the searches' streams at the greatest priority and the
+  // uploads' (whose plane builds run beside a search) at the least, so that
+  // a search's blocks are placed before pending plane-build blocks.
+  int prio_least = 0, prio_greatest = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest);
   if (!s->resident_engine)
     for (LaunchStream& L : s->ls)
-      ok = ok && cudaStreamCreateWithFlags(&L.s, cudaStreamNonBlocking) == cudaSuccess &&
+      ok = ok && cudaStreamCreateWithPriority(&L.s, cudaStreamNonBlocking, prio_greatest) == cudaSuccess &&
            cudaEventCreateWithFlags(&L.up, cudaEventDisableTiming) == cudaSuccess &&
            cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming) == cudaSuccess &&
            cudaEventCreateWithFlags(&L.copied, cudaEventDisableTiming) == cudaSuccess;
   if (!ok || (s->resident_engine && rme::engine_create(ctx, s->device, &s->eng) != 0) ||
-      cudaStreamCreateWithFlags(&s->upload, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&s->upload, cudaStreamNonBlocking, s->resident_engine ? 0 : prio_least) !=
+          cudaSuccess ||
       cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking) != cudaSuccess ||
       cudaMallocHost(&s->h_status, 64) != cudaSuccess) {
     if (s->eng) rme::engine_destroy(s->eng);
