@@ -465,7 +465,7 @@ def run_ours(args, world, rank, local):
     if not args.no_serve:
         served = run_served(frames, value / world, local=local)
         # The resident engine beside it (a shorter sweep: 500 requests a load).
-        served_resident = run_served(frames, value / world, loads=(0.04, 0.1, 0.2), min_requests=500, local=local,
+        served_resident = run_served(frames, value / world, rates=(60, 150, 300), min_requests=500, local=local,
                                      resident=True)
 
     # ---- CPU baseline (bounded sample) ---------------------------------------------
@@ -541,11 +541,14 @@ def run_ours(args, world, rank, local):
 P99_TARGET_MS = 8.0
 
 
-SERVED_LOADS = (0.04, 0.07, 0.1, 0.115, 0.13, 0.145, 0.16, 0.18, 0.2, 0.3, 0.45)
+# Offered rates of the served sweep (frames/s, 30 a stream), finest around
+# the p99 knee; each is reported with its fraction of the batched capacity.
+SERVED_RATES = (60, 90, 120, 150, 180, 210, 240, 270, 300, 360, 450, 630)
 
 
-def run_served(frames, capacity_fps: float, loads=SERVED_LOADS, min_requests: int = 1000,
-               warm_s: float = 0.5, local: int = 0, resident: bool = False, max_batch: int = 2) -> dict:
+def run_served(frames, capacity_fps: float, loads=None, min_requests: int = 1000,
+               warm_s: float = 0.5, local: int = 0, resident: bool = False, max_batch: int = 2,
+               rates=SERVED_RATES) -> dict:
     """The serving loop under Poisson load: streams of the 1080p workload at
     30 frames/s each, the total rate a fraction of the measured batched
     capacity; per-frame latency is submit -> results in the client's buffer
@@ -563,8 +566,8 @@ def run_served(frames, capacity_fps: float, loads=SERVED_LOADS, min_requests: in
     rng = np.random.default_rng(2024)
     per_stream = 4  # frames of a stream in flight at once (rme_serve_open_stream)
     count = 42900 * NREF
-    for load in loads:
-        rate = load * capacity_fps
+    points = [(l, l * capacity_fps) for l in loads] if loads is not None else [(r / capacity_fps, r) for r in rates]
+    for load, rate in points:
         nstreams = max(1, int(round(rate / 30.0)))
         seconds = max(2.0, min_requests / (nstreams * 30.0))
         with rme.MotionSearch(local) as ms:

@@ -850,13 +850,14 @@ int run_launch(Ctx* c, const rme_frame* frames, const rme_params* params, int n,
   for (int k = 0; k < kParts; ++k) {
     if (!rows[k]) continue;
     for (int big = 0; big < 2; ++big) {
+      auto list = [&](int i) -> const std::vector<uint32_t>& { return big ? fdeps[i]->rows_big : fdeps[i]->rows; };
       size_t most = 0;
       for (int i = 0; i < n; ++i)
-        if (part_of(sl.h_frames.p[i]) == k) most = std::max(most, (big ? fdeps[i]->rows_big : fdeps[i]->rows).size());
+        if (part_of(sl.h_frames.p[i]) == k) most = std::max(most, list(i).size());
       for (size_t j = 0; j < most; ++j)
         for (int i = 0; i < n; ++i) {
           if (part_of(sl.h_frames.p[i]) != k) continue;
-          const std::vector<uint32_t>& v = big ? fdeps[i]->rows_big : fdeps[i]->rows;
+          const std::vector<uint32_t>& v = list(i);
           if (j < v.size())
             (big ? init_big : init)[k].push_back(((unsigned long long)sl.epoch << 32) |
                                                  ((unsigned long long)i << 24) | v[j]);

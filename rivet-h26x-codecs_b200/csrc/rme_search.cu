@@ -137,7 +137,7 @@ __device__ void group_row_loop(const LaunchDesc& L, unsigned char* smem_raw) {
   if (tid < 5) atomicAdd(&L.counters[tid], gs.cnt[tid]);
 }
 
-template <class S>
+template <class S, bool SPEC>
 __device__ void row_loop(const LaunchDesc& L, WarpSmem<S>& sm, int lane) {
   const uint32_t epoch = __ldg(L.epoch);
   for (;;) {
@@ -155,7 +155,7 @@ __device__ void row_loop(const LaunchDesc& L, WarpSmem<S>& sm, int lane) {
       if (lane == 0) atomicOr(L.status, kStatusBadTask);
       continue;
     }
-    hevc_row<S, true>(L, F, f, e & 0xffffffu, sm, lane);
+    hevc_row<S, SPEC>(L, F, f, e & 0xffffffu, sm, lane);
   }
 }
 
@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, MINB) search_kernel(Launc
         WarpSmem<S>& sm = reinterpret_cast<WarpSmem<S>*>(smem_raw)[threadIdx.x >> 5];
         if (lane < 5) sm.cnt[lane] = 0;
         __syncwarp();
-        row_loop<S>(L, sm, lane);
+        row_loop<S, SPEC>(L, sm, lane);
         __syncwarp();
         if (lane < 5) atomicAdd(&L.counters[lane], sm.cnt[lane]);
       }

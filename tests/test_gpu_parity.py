@@ -189,6 +189,25 @@ def test_mixed_stream_batch_equals_the_per_frame_path(ms):
             ms.release(3000 + 10 * k + t)
 
 
+def test_throughput_launch_shapes_equal_the_per_frame_path():
+    """Four 1080p HEVC frames in one launch (343,200 tasks: the throughput
+    form), on every launch shape the tuner times (three occupancies, each
+    twice), then on the chosen one: every frame equals its per-frame search
+    (the latency form's row form) every time."""
+    import rivet_h26x_codecs_b200 as rme
+    seq = synth.make_sequence(HEVC, 1920, 1080, 8, 6, 91, 64, 160, 2.0)
+    p = oracle.params(HEVC, 32, hevc_search_range=64)
+    with rme.MotionSearch(0) as ms2:
+        for i, f in enumerate(seq.frames):
+            ms2.upload(i, f, HEVC, 8, as_ref=True)
+        frames = [(t, [t - 1, t - 2]) for t in range(2, 6)]
+        want = [ms2.search(t, refs, p) for t, refs in frames]
+        for k in range(2 * 3 + 1):
+            outs = ms2.search_batch(frames, p)
+            for j, (g, w) in enumerate(zip(outs, want)):
+                assert_results_equal(g, w, f"launch {k} frame {j}")
+
+
 def test_batch_equals_the_frames_and_the_oracle(ms):
     """Several frames of two formats in one persistent launch, three times
     (the second launch captures a graph, the third replays it)."""
