@@ -124,15 +124,12 @@ struct Server {
   bool trace = false;  // RME_SERVE_TRACE=1: one line per frame on stderr
   double idle_since = 0.0;  // nothing in flight since
 
-  void* take_buffer(size_t bytes) {  // lock held
+  void* take_buffer(size_t bytes) {  // lock held; null when the pool has none of this size
     auto& v = pool[bytes];
-    if (!v.empty()) {
-      void* b = v.back();
-      v.pop_back();
-      return b;
-    }
-    void* b = nullptr;
-    return cudaMallocHost(&b, bytes) == cudaSuccess ? b : nullptr;
+    if (v.empty()) return nullptr;
+    void* b = v.back();
+    v.pop_back();
+    return b;
   }
   cudaEvent_t take_event() {
     if (!events.empty()) {
@@ -604,9 +601,25 @@ int rme_serve_open_stream(void* server, int32_t stream_id, const rme_picture_des
   // The format and settings are checked the way a search would check them.
   if (rme_standalone_blocks(d, p, nullptr, &count) != 0) return RME_EINVAL;
   const uint64_t bytes = picture_bytes(*d) * (uint64_t)(nref + kPerStream);
+  // The stream's frame buffers (pinned host memory): as many as it can have
+  // open at once, and two more, pinned here rather than on its first
+  // submits, and before the lock (pinning is slow).
+  const size_t fb = (size_t)d->stride * d->height * (d->bit_depth == 8 ? 1 : 2);
+  std::vector<void*> bufs;
+  for (int k = 0; k < kPerStream + 2; ++k) {
+    void* b = nullptr;
+    if (cudaMallocHost(&b, fb) != cudaSuccess) break;
+    bufs.push_back(b);
+  }
   std::lock_guard<std::mutex> lk(s->m);
-  if (s->streams.count(stream_id)) return RME_EINVAL;
-  if ((int)s->streams.size() >= s->o.max_streams || s->resident + bytes > s->o.hbm_budget_bytes) return RME_EBUSY;
+  const int refuse = s->streams.count(stream_id) ? RME_EINVAL
+                     : ((int)s->streams.size() >= s->o.max_streams || s->resident + bytes > s->o.hbm_budget_bytes)
+                         ? RME_EBUSY
+                         : 0;
+  if (refuse) {
+    for (void* b : bufs) cudaFreeHost(b);
+    return refuse;
+  }
   Stream st;
   st.d = *d;
   st.p = *p;
@@ -616,6 +629,7 @@ int rme_serve_open_stream(void* server, int32_t stream_id, const rme_picture_des
   s->next_pic_base += RME_MAX_REFS + kPerStream;
   s->resident += bytes;
   s->streams[stream_id] = st;
+  for (void* b : bufs) s->pool[fb].push_back(b);
   return RME_OK;
 }
 
@@ -636,7 +650,18 @@ int rme_serve_submit(void* server, int32_t stream_id, const void* luma, rme_resu
   r.bytes = (size_t)d.stride * d.height * (d.bit_depth == 8 ? 1 : 2);
   if ((it->second.frames > 0 || it->second.pending > 0) && !out) return RME_EINVAL;  // this frame is searched
   r.luma = s->take_buffer(r.bytes);
-  if (!r.luma) return RME_ENOMEM;
+  if (!r.luma) {
+    // Pinning host memory is slow: it is done without the lock, so the
+    // worker and other submitters are not held up behind it.
+    lk.unlock();
+    if (cudaMallocHost(&r.luma, r.bytes) != cudaSuccess) return RME_ENOMEM;
+    lk.lock();
+    it = s->streams.find(stream_id);
+    if (it == s->streams.end() || it->second.closing) {
+      s->pool[r.bytes].push_back(r.luma);
+      return RME_ENOTFOUND;
+    }
+  }
   r.id = ++s->next_id;
   r.stream = stream_id;
   r.out = out;
