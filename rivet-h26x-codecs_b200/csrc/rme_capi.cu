@@ -621,7 +621,11 @@ int make_frame(Ctx* c, const rme_frame* f, const rme_params* p, FrameDesc* fd, r
 // Finish the launch in flight on slot `sl`: wait for it, check the device
 // status and the task count, keep its statistics (and feed the tuner), move
 // results bound for pageable memory. Returns 0 or an error code.
-int finish_launch(Ctx* c, Slot& sl) {
+// `wait_planes`: a synchronous call waits for the uploads since the previous
+// search to report their device time; an asynchronous launch's completion
+// (rme_sync, or its slot taken again) reports it only if they are done, so
+// that it never waits on uploads queued after the launch.
+int finish_launch(Ctx* c, Slot& sl, bool wait_planes = true) {
   if (!sl.busy) return 0;
   sl.busy = false;
   CK(cudaEventSynchronize(sl.done));
@@ -646,7 +650,7 @@ int finish_launch(Ctx* c, Slot& sl) {
     }
   }
   c->last.planes_ms = 0.0f;
-  if (c->planes_pending) {
+  if (c->planes_pending && (wait_planes || cudaEventQuery(c->evp1) == cudaSuccess)) {
     // Device time from the first upload since the previous search to the
     // end of the last one (the uploads' stream precedes this search's).
     cudaEventSynchronize(c->evp1);
@@ -654,6 +658,7 @@ int finish_launch(Ctx* c, Slot& sl) {
     cudaGetLastError();
     c->planes_pending = false;
   }
+  cudaGetLastError();
   if (status) return fail(c, RME_EDEVICE, "device status " + std::to_string(status));
   if (c->last.tasks != (unsigned long long)sl.total)
     return fail(c, RME_EDEVICE, "the launch ran " + std::to_string(c->last.tasks) + " of " + std::to_string(sl.total) +
@@ -673,7 +678,7 @@ Slot* take_slot(Ctx* c) {
   c->next_slot = (c->next_slot + 1) % kSlots;
   if (sl.busy) {
     const cudaStream_t st = sl.stream;
-    const int rc = finish_launch(c, sl);
+    const int rc = finish_launch(c, sl, false);
     if (rc) {
       auto& e = c->async_err[st];
       if (!e.first) e.first = rc;
@@ -1471,7 +1476,7 @@ int rme_sync(void* ctx, void* stream, uint32_t* device_status) {
   for (int k = 0; k < kSlots; ++k) {
     Slot& sl = c->slots[(c->next_slot + k) % kSlots];
     if (!sl.busy || sl.stream != s) continue;
-    const int r = finish_launch(c, sl);
+    const int r = finish_launch(c, sl, false);
     if (r == RME_EDEVICE) st |= (uint32_t)(sl.h_misc.p[kMiscStatus] & 0xffffffffu);
     if (r && !rc) rc = r;
   }
