@@ -439,11 +439,12 @@ int rme_satd_batch(const void* a, int64_t a_stride, const int64_t* a_off,
 
 /* ---- serving loop --------------------------------------------------------- */
 
-/* A continuous-batching request loop on one context (C++ host thread plus
- * the persistent search kernel). Streams are admitted against an HBM
- * budget; each stream keeps its reference pictures resident. Requests are
- * per-frame ME calls; they are admitted into free slots of the next launch
- * as they arrive, overlapping with work already on the device.
+/* A request loop on one context (a C++ host thread that owns it). Streams
+ * are admitted against an HBM budget; each stream keeps its reference
+ * pictures resident. Requests are per-frame ME calls; each starts on the
+ * device as it arrives, beside the work already there (`mode`: a launch of
+ * its own on one of three launch streams, or the resident search kernel's
+ * queue).
  * open_stream, submit, poll and close_stream may be called from any host
  * threads at once; stop once, after the others have returned. While a
  * server runs, its context takes no other calls. The first frame of a
